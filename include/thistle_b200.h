@@ -1,0 +1,113 @@
+/*
+ * thistle_b200 -- C-ABI of the B200 scattering-intensity path.
+ *
+ * Drop-in for THISTLE's Fortran calculation dispatcher and integrators:
+ * plain pointers and sizes, Fortran (column-major, 1-based index) layouts
+ * where the reference uses them, no torch types.  Every entry returns 0 on
+ * success or a negative THISTLE_ERR_* code and never exits the process;
+ * thistle_last_error_string() describes the last failure of the calling
+ * thread.  All computation runs on the current CUDA device; there is no CPU
+ * fallback.
+ */
+#ifndef THISTLE_B200_H
+#define THISTLE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define THISTLE_OK 0
+#define THISTLE_ERR_ARG -1        /* null pointer or bad size */
+#define THISTLE_ERR_SHAPE -2      /* inconsistent group / index layout */
+#define THISTLE_ERR_ANGMOM -3     /* l, m or n above 4 (g), or LLmax beyond the Bessel tables */
+#define THISTLE_ERR_NONFINITE -4  /* NaN or Inf in an input array */
+#define THISTLE_ERR_CUDA -5       /* CUDA runtime, cuBLAS or kernel failure */
+#define THISTLE_ERR_NOMEM -6      /* device allocation failed */
+#define THISTLE_ERR_TYPE -7       /* calculation type not provided */
+#define THISTLE_ERR_Q -8          /* q <= 0 (the reference divides by q; drivers use 1e-10 for 0) */
+#define THISTLE_ERR_TIMEOUT -10   /* a bounded device wait gave up */
+
+/* Calculation types, numbered as src/main_calculation.f90:99-497. */
+#define THISTLE_TOTAL_J0 1
+#define THISTLE_ELASTIC_J0 2
+#define THISTLE_TOTAL_ALIGNED 3
+#define THISTLE_TOTAL_J2 7
+
+const char *thistle_last_error_string(void);
+int thistle_version(void);
+
+/*
+ * Entry 1.  Replaces main_calculation_mod::total_scattering_calculation_2 with
+ * readrdm=.True. (src/main_calculation.f90:501-849; f2py call shape of
+ * total_scattering_calculation, :13-15, as driven by
+ * src/scattering_main_routine.py:240-247).  RDMs come in as arrays instead of
+ * files: mat/total/nmat are read_twordm's rows (src/one_rdm.f90:2112-2147),
+ * onerdm is read_onerdm's matrix (:2072-2108).
+ *
+ *   type          1 total j0, 2 elastic j0, 7 total j2 (3: see thistle_aligned)
+ *   Zn, geom      atomic numbers and (natoms,3) geometry; not used by these
+ *                 types (kept for the reference's argument list), may be NULL
+ *   maxl          maxval(l) as the reference passes it (checked, not trusted)
+ *   ga,l,m,n,xx,yy,zz  per primitive function, length ngto
+ *   mmod          (norbs, ngto) column-major MO coefficients of the primitives
+ *   q, nq         radial momentum transfer grid, q > 0
+ *   group         1-based shell index per function; shells contiguous
+ *   cutoffz, cutoffmd, cutoffcentre  the reference's three cutoffs
+ *   mat, total, nmat   (nmat,4) column-major 1-based MO indices and values
+ *                      (types 1 and 7)
+ *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (type 2)
+ *   q_abs_out     nq doubles, set to q (the reference returns |q| here)
+ *   result_out    nq doubles, I(q)
+ * All pointers are host pointers.
+ */
+int thistle_total_scattering(int32_t type, const double *Zn, const double *geom, int32_t natoms,
+                             int32_t maxl, int32_t ngto, int32_t ng, const double *ga,
+                             const int32_t *l, const int32_t *m, const int32_t *n,
+                             const double *xx, const double *yy, const double *zz,
+                             const double *mmod, int32_t norbs, const double *q, int32_t nq,
+                             const int32_t *group, double cutoffz, double cutoffmd,
+                             double cutoffcentre, const int32_t *mat, const double *total,
+                             int32_t nmat, const double *onerdm, int32_t nmo1,
+                             double *q_abs_out, double *result_out);
+
+/*
+ * Plan interface: one basis, density and q grid set up once (density
+ * transform on the device), then executed for any number of geometries.
+ * The routine-level split of variables_total / tot_integration
+ * (src/Variables.f90:948-1153, src/Integrals.f90:8-472).
+ */
+typedef struct thistle_plan thistle_plan;
+
+int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const double *ga,
+                        const int32_t *l, const int32_t *m, const int32_t *n, const double *xx,
+                        const double *yy, const double *zz, const int32_t *group,
+                        const double *mmod, int32_t norbs, const int32_t *mat,
+                        const double *total, int32_t nmat, const double *onerdm, int32_t nmo1,
+                        const double *q, int32_t nq, double cutoffz, double cutoffmd,
+                        double cutoffcentre);
+/* Move the Gaussian centres (host arrays of length ngto). */
+int thistle_plan_set_centres(thistle_plan *plan, const double *xx, const double *yy,
+                             const double *zz);
+/* Run the integrator for the current centres; result_host gets nq doubles. */
+int thistle_plan_execute(thistle_plan *plan, double *result_host);
+/* Same, leaving I(q) in device memory (nq doubles) on the plan's stream. */
+int thistle_plan_execute_device(thistle_plan *plan, double *result_dev);
+/* Evaluate only the listed group quartets (0-based gi,gj,gk,gr, 4 int32 each,
+ * each with its reference loop weight); result_host gets nq doubles. */
+int thistle_plan_execute_quartets(thistle_plan *plan, const int32_t *quartets, int64_t nquart,
+                                  double *result_host);
+/* Counts: [0] group quartets, [1] quartets on the P=Q branch in the last
+ * execution, [2] ng, [3] ngto, [4] nq. */
+int thistle_plan_info(const thistle_plan *plan, int64_t *info5);
+/* Device time in ms of the last execution's stages: [0] pair tables,
+ * [1] stage 1, [2] stage 2 (Bessel sum), [3] reduce; setup: [4] transform. */
+int thistle_plan_timings(const thistle_plan *plan, double *ms5);
+int thistle_plan_destroy(thistle_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* THISTLE_B200_H */

@@ -1,0 +1,171 @@
+"""ctypes wrapper of the C oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle_thistle.so`` (built from ``thistle_oracle.c`` by
+``oracle/build.py``).  Only tests, ``__graft_entry__.smoke()`` and bench.py's
+CPU-baseline and reference legs import this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle_thistle.so")
+        if not os.path.exists(path):
+            from . import build as _b  # type: ignore
+            _b.build()
+        _LIB = C.CDLL(path)
+        _LIB.orc_count_quartets.restype = C.c_long
+        _LIB.orc_enum_quartets.restype = C.c_long
+    return _LIB
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def count_quartets(ng: int) -> int:
+    return int(lib().orc_count_quartets(C.c_int(ng)))
+
+
+def enum_quartets(ng: int) -> np.ndarray:
+    n = count_quartets(ng)
+    out = np.zeros((n, 5), dtype=np.int32)
+    lib().orc_enum_quartets(C.c_int(ng), out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out
+
+
+def scattering(prob, type_: int = 1, *, bessel_mode: int = 0, nthreads: int = 0,
+               quartets=None, weights=None, q=None) -> np.ndarray:
+    """Reference restatement of total_scattering_calculation_2 (types 1, 2, 7)."""
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
+    nq = qv.size
+    out = np.zeros(nq)
+    mat_cm = np.asfortranarray(prob.mat.astype(np.int32)).ravel(order="F")
+    mmod_cm = np.asfortranarray(prob.mmod).ravel(order="F")
+    one_cm = np.asfortranarray(prob.onerdm).ravel(order="F")
+    if quartets is not None:
+        qt = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 5)
+        qptr, nqt = i(qt), qt.shape[0]
+    else:
+        qptr, nqt = None, 0
+    wptr = d(weights) if weights is not None else None
+    rc = lib().orc_scattering(
+        C.c_int(type_), C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n),
+        d(prob.xx), d(prob.yy), d(prob.zz), i(prob.group), d(mmod_cm), C.c_int(prob.nmo),
+        i(mat_cm), d(prob.total), C.c_int(prob.mat.shape[0]), d(one_cm), C.c_int(prob.onerdm.shape[0]),
+        d(qv), C.c_int(nq), C.c_double(prob.cutoffz), C.c_double(prob.cutoffmd),
+        C.c_double(prob.cutoffcentre), C.c_int(bessel_mode), C.c_int(nthreads),
+        qptr, C.c_long(nqt), wptr, out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_scattering failed with code {rc}")
+    return out
+
+
+def aligned(prob, qal: np.ndarray, *, nthreads: int = 0):
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qal = np.ascontiguousarray(qal, dtype=np.float64).reshape(-1, 3)
+    nq = qal.shape[0]
+    re, im = np.zeros(nq), np.zeros(nq)
+    mat_cm = np.asfortranarray(prob.mat.astype(np.int32)).ravel(order="F")
+    mmod_cm = np.asfortranarray(prob.mmod).ravel(order="F")
+    rc = lib().orc_aligned(
+        C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n), d(prob.xx), d(prob.yy),
+        d(prob.zz), i(prob.group), d(mmod_cm), C.c_int(prob.nmo), i(mat_cm), d(prob.total),
+        C.c_int(prob.mat.shape[0]), d(qal), C.c_int(nq), C.c_double(prob.cutoffz),
+        C.c_double(prob.cutoffmd), C.c_int(nthreads), re.ctypes.data_as(C.POINTER(C.c_double)),
+        im.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_aligned failed with code {rc}")
+    return re, im
+
+
+def qcoord3(k0: float = 10.583544175):
+    qx, qy, qz = np.zeros(3131), np.zeros(3131), np.zeros(3131)
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    lib().orc_qcoord3(C.c_double(k0), p(qx), p(qy), p(qz))
+    return np.stack([qx, qy, qz], axis=1)
+
+
+def kernel_quartet(kind, pzero, mu, l, m, n, group_start, group_count, hx, hy, hz, h,
+                   dx1, dy1, dz1, dx2, dy2, dz2, gi, gj, gk, gr, zcontr, zcontr2,
+                   cutoff1=1e-14, cutoff2=1e-14, bessel_mode=0):
+    """One per-quartet kernel with Fortran argument meaning and layouts."""
+    keep = []
+
+    def d(x):
+        a = np.asfortranarray(np.asarray(x, dtype=np.float64)).ravel(order="F")
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def i(x):
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.int32).ravel())
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_int))
+
+    mu = np.asarray(mu, dtype=np.float64)
+    dx1 = np.asarray(dx1, dtype=np.float64)
+    dt, dl = dx1.shape[0], dx1.shape[1]
+    f = np.zeros(mu.size)
+    rc = lib().orc_kernel_quartet(
+        C.c_int(kind), C.c_int(pzero), d(mu), C.c_int(mu.size), C.c_int(len(l)), i(l), i(m), i(n),
+        C.c_int(len(group_start)), i(group_start), i(group_count), C.c_double(hx), C.c_double(hy),
+        C.c_double(hz), C.c_double(h), d(dx1), d(dy1), d(dz1), d(dx2), d(dy2), d(dz2), C.c_int(dt),
+        C.c_int(dl), C.c_int(gi), C.c_int(gj), C.c_int(gk), C.c_int(gr), d(zcontr), d(zcontr2),
+        C.c_double(cutoff1), C.c_double(cutoff2), C.c_int(bessel_mode),
+        f.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle kernel failed with code {rc}")
+    return f
+
+
+def dphrec(x, lmax1: int, leps1: int = 100) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros((x.size, lmax1))
+    lib().orc_dphrec(x.ctypes.data_as(C.POINTER(C.c_double)), C.c_int(x.size), C.c_int(leps1),
+                     C.c_int(lmax1), out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def md_chain(l1, l2, PA, PB, a) -> np.ndarray:
+    out = np.zeros(l1 + l2 + 1)
+    lib().orc_md_chain(C.c_int(l1), C.c_int(l2), C.c_double(PA), C.c_double(PB), C.c_double(a),
+                       out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out

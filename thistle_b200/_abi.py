@@ -1,0 +1,109 @@
+"""ctypes binding of libthistle_b200.so (declared in include/thistle_b200.h).
+
+The library is built in-tree by ``thistle_b200.build``; importing this module
+without it raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libthistle_b200.so")
+
+ERRORS = {
+    -1: "THISTLE_ERR_ARG", -2: "THISTLE_ERR_SHAPE", -3: "THISTLE_ERR_ANGMOM", -4: "THISTLE_ERR_NONFINITE",
+    -5: "THISTLE_ERR_CUDA", -6: "THISTLE_ERR_NOMEM", -7: "THISTLE_ERR_TYPE", -8: "THISTLE_ERR_Q",
+    -10: "THISTLE_ERR_TIMEOUT",
+}
+
+# every symbol include/thistle_b200.h declares
+EXPORTS = [
+    "thistle_last_error_string", "thistle_version", "thistle_total_scattering",
+    "thistle_plan_create", "thistle_plan_set_centres", "thistle_plan_execute",
+    "thistle_plan_execute_device", "thistle_plan_execute_quartets", "thistle_plan_info",
+    "thistle_plan_timings", "thistle_plan_destroy",
+]
+
+
+class ThistleError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+D = C.POINTER(C.c_double)
+I32 = C.POINTER(C.c_int32)
+I64 = C.POINTER(C.c_int64)
+VP = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ThistleError(-5, f"CUDA extension not built: {LIB_PATH} is missing (run python -m thistle_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    L.thistle_last_error_string.restype = C.c_char_p
+    L.thistle_last_error_string.argtypes = []
+    L.thistle_version.restype = C.c_int
+    L.thistle_total_scattering.restype = C.c_int
+    L.thistle_total_scattering.argtypes = [
+        C.c_int32, D, D, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D, I32, I32, I32, D, D, D, D, C.c_int32,
+        D, C.c_int32, I32, C.c_double, C.c_double, C.c_double, I32, D, C.c_int32, D, C.c_int32, D, D]
+    L.thistle_plan_create.restype = C.c_int
+    L.thistle_plan_create.argtypes = [
+        C.POINTER(VP), C.c_int32, C.c_int32, D, I32, I32, I32, D, D, D, I32, D, C.c_int32, I32, D, C.c_int32,
+        D, C.c_int32, D, C.c_int32, C.c_double, C.c_double, C.c_double]
+    L.thistle_plan_set_centres.restype = C.c_int
+    L.thistle_plan_set_centres.argtypes = [VP, D, D, D]
+    L.thistle_plan_execute.restype = C.c_int
+    L.thistle_plan_execute.argtypes = [VP, D]
+    L.thistle_plan_execute_device.restype = C.c_int
+    L.thistle_plan_execute_device.argtypes = [VP, VP]
+    L.thistle_plan_execute_quartets.restype = C.c_int
+    L.thistle_plan_execute_quartets.argtypes = [VP, I32, C.c_int64, D]
+    L.thistle_plan_info.restype = C.c_int
+    L.thistle_plan_info.argtypes = [VP, I64]
+    L.thistle_plan_timings.restype = C.c_int
+    L.thistle_plan_timings.argtypes = [VP, D]
+    L.thistle_plan_destroy.restype = C.c_int
+    L.thistle_plan_destroy.argtypes = [VP]
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = lib().thistle_last_error_string()
+        raise ThistleError(rc, msg.decode() if msg else "")
+
+
+def dptr(a):
+    return None if a is None else a.ctypes.data_as(D)
+
+
+def iptr(a):
+    return None if a is None else a.ctypes.data_as(I32)
+
+
+def as_f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def as_i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def colmajor_f64(a):
+    """Fortran-order flat copy of a 2-D array."""
+    return None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.float64).T)
+
+
+def colmajor_i32(a):
+    return None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.int32).T)

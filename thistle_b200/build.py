@@ -1,0 +1,75 @@
+"""Build recipe for libthistle_b200.so (sm_100a), in-tree.
+
+``python -m thistle_b200.build`` compiles every CUDA source under
+``thistle_b200/csrc`` with nvcc for ``compute_100a/sm_100a`` into
+``thistle_b200/libthistle_b200.so``.  nvcc cross-compiles without a GPU.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libthistle_b200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def deps():
+    return sources() + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + \
+        sorted(glob.glob(os.path.join(HERE, "csrc", "*.h"))) + [os.path.join(ROOT, "include", "thistle_b200.h")]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(d) <= t for d in deps())
+
+
+def build(verbose: bool = False, force: bool = False, extra=None) -> str:
+    if up_to_date() and not force:
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "csrc"),
+              "--expt-relaxed-constexpr", "-Xptxas", "-v" if verbose else "-O3"]
+    if extra:
+        common += list(extra)
+    headers = [d for d in deps() if not d.endswith(".cu")]
+    newest_header = max(os.path.getmtime(h) for h in headers)
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
+                and os.path.getmtime(obj) >= newest_header):
+            continue
+        cmd = common + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lcublas"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    import sys
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,555 @@
+// CUDA kernels of the scattering-intensity path (sm_100a, FP64 throughout).
+//
+//  tb_pair_tables   Gaussian-product tables per unordered group pair
+//                   (src/Variables.f90:1113-1148 and fill_md_table :8-946)
+//  tb_stage1<L,K>   per group quartet: Hermite density and Bessel / P0
+//                   coefficients (tot_integral_k_ijkr :5068-5226, the pzero
+//                   kernels :4751-5067, their j2 and elastic variants)
+//  tb_stage2        the quartet x q Bessel sum (bessels0rr :6662-6739 with an
+//                   accurate generator), warp per quartet, lanes over q,
+//                   accumulated per warp in shared memory
+//  tb_reduce        fixed-order sum of the per-block partial I(q)
+//  tb_ghat_scatter / tb_pack_pairs / tb_sym_small: the density transform's
+//                   gathers (variables_total z11/z22 :1045-1065 re-expressed
+//                   as a 4-index transform)
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_kernels.h"
+#include "tb_math.cuh"
+
+namespace tb {
+
+// ---------------------------------------------------------------------------
+// pair tables
+// ---------------------------------------------------------------------------
+__global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gstart,
+                                   const int *__restrict__ flmn, const double *__restrict__ ga,
+                                   const double *__restrict__ xyz, double *__restrict__ tab) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs(ng)) return;
+  int i = 0, rem = p;
+  while (rem >= ng - i) { rem -= ng - i; ++i; }
+  int j = i + rem;
+  int fi = gstart[i], fj = gstart[j];
+  double ai = ga[fi], aj = ga[fj];
+  double gaP = ai + aj;
+  double *t = tab + (size_t)p * PAIR_STRIDE;
+  double d2 = 0.0;
+  for (int ax = 0; ax < 3; ++ax) {
+    double xi = xyz[3 * fi + ax], xj = xyz[3 * fj + ax];
+    double P = (ai * xi + aj * xj) / gaP;
+    t[ax] = P;
+    double d = xi - xj;
+    d2 = d2 + d * d;
+    double PA = P - xi, PB = P - xj, a = 0.5 / gaP;
+    double E[2 * MAXA + 2];
+    double *dst = t + 8 + ax * ESZ;
+    for (int la = 0; la <= maxa; ++la)
+      for (int lb = 0; lb <= maxa; ++lb) {
+        // larger exponent first, with its own centre (src/Variables.f90:36-48)
+        if (la >= lb) md_chain(la, lb, PA, PB, a, E);
+        else md_chain(lb, la, PB, PA, a, E);
+        for (int tt = 0; tt <= la + lb; ++tt) dst[(la * (MAXA + 1) + lb) * E_T + tt] = E[tt];
+      }
+  }
+  t[3] = gaP;
+  t[4] = pow(TB_PI_SP / gaP, 1.5) * exp(-ai * aj / gaP * d2);
+  t[5] = 0.25 / gaP;
+  t[6] = 0.0;
+  t[7] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// stage 1: Hermite density and expansion coefficients, one thread per quartet
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void unpack_quartet(uint64_t pk, int &gi, int &gj, int &gk, int &gr) {
+  gi = (int)(pk & 0xffff);
+  gj = (int)((pk >> 16) & 0xffff);
+  gk = (int)((pk >> 32) & 0xffff);
+  gr = (int)((pk >> 48) & 0xffff);
+}
+
+// The five loops of tot_integration give these weights (src/Integrals.f90:158,243,325,402,462).
+__device__ __forceinline__ int quartet_loop(int gi, int gj, int gk, int gr) {
+  if (gi == gj) return gk == gr ? (gi == gk ? 5 : 4) : 3;
+  return gk == gi ? 2 : 1;
+}
+__device__ __forceinline__ double loop_weight(int loop) {
+  return loop == 1 ? 8.0 : (loop <= 3 ? 4.0 : (loop == 4 ? 2.0 : 1.0));
+}
+
+template <int L, int KIND>
+__global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
+  int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= A.qend) return;
+  int gi, gj, gk, gr;
+  unpack_quartet(A.quartets[qi], gi, gj, gk, gr);
+  const double *tb = A.pairtab + (size_t)pair_index(gi, gj, A.ng) * PAIR_STRIDE;
+  const double *tk = A.pairtab + (size_t)pair_index(gk, gr, A.ng) * PAIR_STRIDE;
+  // hx = px(k,r) - px(i,j)  (src/Integrals.f90:83-86)
+  double Hx = tk[0] - tb[0], Hy = tk[1] - tb[1], Hz = tk[2] - tb[2];
+  double h = sqrt(Hx * Hx + Hy * Hy + Hz * Hz);
+  int loop = quartet_loop(gi, gj, gk, gr);
+  bool p0 = loop == 5 || h < A.cutoffcentre;
+  // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp)
+  int skip = p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
+
+  constexpr int NT = ntuv(L);
+  double D[NT];
+#pragma unroll
+  for (int i = 0; i < NT; ++i) D[i] = 0.0;
+
+  const int si = A.gstart[gi], ni = A.gcount[gi];
+  const int sj = A.gstart[gj], nj = A.gcount[gj];
+  const int sk = A.gstart[gk], nk = A.gcount[gk];
+  const int sr = A.gstart[gr], nr = A.gcount[gr];
+  const double *Eb = tb + 8, *Ek = tk + 8;
+  for (int a = 0; a < ni; ++a) {
+    const int fa = si + a, la = A.flmn[fa];
+    for (int b = 0; b < nj; ++b) {
+      const int fb = sj + b, lb = A.flmn[fb];
+      const int64_t rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      const double zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      const double *ex1 = Eb + 0 * ESZ + ((la & 0xff) * (MAXA + 1) + (lb & 0xff)) * E_T;
+      const double *ey1 = Eb + 1 * ESZ + (((la >> 8) & 0xff) * (MAXA + 1) + ((lb >> 8) & 0xff)) * E_T;
+      const double *ez1 = Eb + 2 * ESZ + (((la >> 16) & 0xff) * (MAXA + 1) + ((lb >> 16) & 0xff)) * E_T;
+      const int nx1 = (la & 0xff) + (lb & 0xff), ny1 = ((la >> 8) & 0xff) + ((lb >> 8) & 0xff);
+      const int nz1 = ((la >> 16) & 0xff) + ((lb >> 16) & 0xff);
+      for (int c = 0; c < nk; ++c) {
+        const int fc = sk + c, lc = A.flmn[fc];
+        for (int d = 0; d < nr; ++d) {
+          const int fd = sr + d, ld = A.flmn[fd];
+          double ztot;
+          if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
+          else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+          if (fabs(ztot) < A.cutoffz) continue;
+          const double *ex2 = Ek + 0 * ESZ + ((lc & 0xff) * (MAXA + 1) + (ld & 0xff)) * E_T;
+          const double *ey2 = Ek + 1 * ESZ + (((lc >> 8) & 0xff) * (MAXA + 1) + ((ld >> 8) & 0xff)) * E_T;
+          const double *ez2 = Ek + 2 * ESZ + (((lc >> 16) & 0xff) * (MAXA + 1) + ((ld >> 16) & 0xff)) * E_T;
+          const int nx2 = (lc & 0xff) + (ld & 0xff), ny2 = ((lc >> 8) & 0xff) + ((ld >> 8) & 0xff);
+          const int nz2 = ((lc >> 16) & 0xff) + ((ld >> 16) & 0xff);
+          for (int t = 0; t <= nx1; ++t) {
+            double e1 = ex1[t];
+            if ((skip & 1) && fabs(e1) < TB_SKIP30) continue;
+            double p1 = e1 * ztot;
+            for (int u = 0; u <= ny1; ++u) {
+              double e2 = ey1[u];
+              if ((skip & 2) && fabs(e2) < TB_SKIP30) continue;
+              double p2 = e2 * p1;
+              for (int v = 0; v <= nz1; ++v) {
+                double e3 = ez1[v];
+                if ((skip & 4) && fabs(e3) < TB_SKIP30) continue;
+                double p3 = (((t + u + v) & 1) ? -e3 : e3) * p2;
+                for (int t2 = 0; t2 <= nx2; ++t2) {
+                  double e4 = ex2[t2];
+                  if ((skip & 8) && fabs(e4) < TB_SKIP30) continue;
+                  double p4 = e4 * p3;
+                  for (int u2 = 0; u2 <= ny2; ++u2) {
+                    double e5 = ey2[u2];
+                    if ((skip & 16) && fabs(e5) < TB_SKIP30) continue;
+                    double p5 = e5 * p4;
+                    for (int v2 = 0; v2 <= nz2; ++v2) {
+                      double p6 = ez2[v2] * p5;
+                      if (fabs(p6) > A.cutoffmd) D[tuv_index(t + t2, u + u2, v + v2)] += p6;
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  const double pre = loop_weight(loop) * tb[4] * tk[4];
+  double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
+  r[1] = tb[5] + tk[5];
+  if (p0) {
+    // F(q) = sum_s c_s q^{2s} with c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
+    constexpr int NS = L / 2 + 1;
+    r[0] = 0.0;
+    r[2] = (double)REC_P0;
+    r[3] = (double)(NS - 1);
+    const double fj2 = sqrt(5.0 / TB_PI);
+    for (int s = 0; s < NS; ++s) {
+      double acc = 0.0;
+      for (int T = 0; T <= 2 * s; T += 2)
+        for (int U = 0; U <= 2 * s - T; U += 2) {
+          int V = 2 * s - T - U;
+          double f = p0_factor(T, U, V, KIND == KIND_J2);
+          if (KIND == KIND_J2) f = (T + U - 2 * V) / 4.0 * f;
+          acc += D[tuv_index(T, U, V)] * f;
+        }
+      if (KIND == KIND_J2) acc *= fj2;
+      r[4 + s] = pre * ((s & 1) ? -acc : acc);
+    }
+    return;
+  }
+
+  // Bessel expansion: h[b] = sum_TUV D[TUV] sum_{p} a(T,px) b(U,py) c(V,pz),
+  // b = (T+px)/2 + (U+py)/2 + (V+pz)/2 (BesselDeriv); for j2 the four-term
+  // BesselDeriv2j form with two extra orders (src/Integrals.f90:6370-6434).
+  constexpr int LB = KIND == KIND_J2 ? L + 2 : L;
+  constexpr int TP = tp_size(L);
+  double ax[TP], ay[TP], az[TP];
+  hermite_table(L, Hx, ax);
+  hermite_table(L, Hy, ay);
+  hermite_table(L, Hz, az);
+  double hh[LB + 1];
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
+  const double eta = 3.0 * (Hz * Hz) - h * h;
+  for (int T = 0; T <= L; ++T)
+    for (int U = 0; U <= L - T; ++U)
+      for (int V = 0; V <= L - T - U; ++V) {
+        double d = D[tuv_index(T, U, V)];
+        if (d == 0.0) continue;
+        for (int k1 = 0; 2 * k1 <= T; ++k1) {
+          double cx = ax[tp_off(T) + k1];
+          double cx1 = (double)(2 * (T - k1)) * cx;
+          for (int k2 = 0; 2 * k2 <= U; ++k2) {
+            double cy = ay[tp_off(U) + k2];
+            double cy1 = (double)(2 * (U - k2)) * cy;
+            for (int k3 = 0; 2 * k3 <= V; ++k3) {
+              double cz = az[tp_off(V) + k3];
+              int s3 = (T - k1) + (U - k2) + (V - k3);
+              if (KIND != KIND_J2) {
+                hh[s3] += d * (cx * cy * cz);
+              } else {
+                double cz1 = (double)(2 * (V - k3)) * cz;
+                hh[s3 + 2] += d * (cx * cy * cz * eta);
+                hh[s3 + 1] += d * (cx1 * cy * cz + cx * cy1 * cz - 2.0 * (cx * cy * cz1));
+              }
+            }
+          }
+        }
+      }
+  if (KIND == KIND_J2) {
+    const double f = 0.25 * sqrt(5.0 / TB_PI);
+#pragma unroll
+    for (int b = 0; b <= LB; ++b) hh[b] *= f;
+  }
+  if (KIND == KIND_ELASTIC) {
+    // integral_k_ijkr returns F = 0 when sum(h_saved) == 0 (src/Integrals.f90:5883-5886)
+    double sum = 0.0;
+#pragma unroll
+    for (int b = 0; b <= LB; ++b) sum += hh[b];
+    if (sum == 0.0) {
+#pragma unroll
+      for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
+    }
+  }
+  r[0] = h;
+  r[2] = (double)(KIND == KIND_J2 ? REC_BESSEL_J2 : REC_BESSEL);
+  r[3] = (double)LB;
+  // hhat_b = h_b / H^{2b}: F = sum_b hhat_b j_b(x) x^b, x = qH
+  const double invH2 = 1.0 / (h * h);
+  double f = pre;
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) {
+    r[4 + b] = hh[b] * f;
+    f *= invH2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage 2: the Bessel sum, warp per quartet, lanes over q
+// ---------------------------------------------------------------------------
+
+// u_n(y) = sum_k c_{n,k} y^k, Horner in y
+template <int N, int K>
+__device__ __forceinline__ double series_u(double y) {
+  double p = series_coef(N, K);
+#pragma unroll
+  for (int k = K - 1; k >= 0; --k) p = fma(p, y, series_coef(N, k));
+  return p;
+}
+
+// F = sum_{b<=LB} hh[b] j_b(x) x^b for x = q H (hh already divided by H^{2b}).
+template <int LB>
+__device__ __forceinline__ double bessel_sum(const double *hh, double x) {
+  if (LB == 0) return hh[0] * (sin(x) / x);
+  const double y = x * x;
+  if (x >= bessel_crossover(LB)) {
+    // upward: g0 = sin x / x, g1 = g0 - cos x, g_{b+1} = (2b+1) g_b - x^2 g_{b-1}
+    double sn, cs;
+    sincos(x, &sn, &cs);
+    double g0 = sn / x;
+    double g1 = g0 - cs;
+    double F = fma(hh[1], g1, hh[0] * g0);
+#pragma unroll
+    for (int b = 1; b < LB; ++b) {
+      double g2 = fma((double)(2 * b + 1), g1, -y * g0);
+      F = fma(hh[b + 1], g2, F);
+      g0 = g1;
+      g1 = g2;
+    }
+    return F;
+  }
+  // small x: series for u_LB, u_{LB+1}; downward u_{b-1} = u_b - y u_{b+1}/((2b+1)(2b+3));
+  // Horner in y/(2b+1) for the x^{2b}/(2b+1)!! weights.
+  constexpr int K = series_terms(LB);
+  double uhi = series_u<LB + 1, K>(y);
+  double umid = series_u<LB, K>(y);
+  double acc = hh[LB] * umid;
+#pragma unroll
+  for (int b = LB; b >= 1; --b) {
+    double ulo = umid - (y * (1.0 / ((2.0 * b + 1.0) * (2.0 * b + 3.0)))) * uhi;
+    acc = fma(acc, y * (1.0 / (2.0 * b + 1.0)), hh[b - 1] * ulo);
+    uhi = umid;
+    umid = ulo;
+  }
+  return acc;
+}
+
+template <int LB>
+__device__ __noinline__ void stage2_bessel(const double *__restrict__ c, double H, double s, bool j2,
+                                           const double *q_s, const double *q2_s, const double *iq2_s,
+                                           double *acc, int nq, int lane) {
+  double hh[LB + 1];
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) hh[b] = c[b];
+  for (int iq = lane; iq < nq; iq += 32) {
+    double q = q_s[iq];
+    double q2 = q2_s[iq];
+    double F = bessel_sum<LB>(hh, q * H);
+    F *= exp(-q2 * s);
+    if (j2) F *= iq2_s[iq];
+    acc[iq] += F;
+  }
+}
+
+__device__ __noinline__ void stage2_p0(const double *__restrict__ c, int ns, double s, const double *q2_s,
+                                       double *acc, int nq, int lane) {
+  for (int iq = lane; iq < nq; iq += 32) {
+    double q2 = q2_s[iq];
+    double F = c[ns - 1];
+    for (int k = ns - 2; k >= 0; --k) F = fma(F, q2, c[k]);
+    acc[iq] += F * exp(-q2 * s);
+  }
+}
+
+typedef void (*bessel_fn)(const double *, double, double, bool, const double *, const double *,
+                          const double *, double *, int, int);
+
+__device__ __forceinline__ void stage2_dispatch(int LB, const double *c, double H, double s, bool j2,
+                                                const double *q_s, const double *q2_s, const double *iq2_s,
+                                                double *acc, int nq, int lane) {
+  switch (LB) {
+#define TB_CASE(n) case n: stage2_bessel<n>(c, H, s, j2, q_s, q2_s, iq2_s, acc, nq, lane); break;
+    TB_CASE(0) TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
+    TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE(12) TB_CASE(13) TB_CASE(14)
+    TB_CASE(15) TB_CASE(16) TB_CASE(17) TB_CASE(18)
+#undef TB_CASE
+    default: break;
+  }
+}
+
+__global__ void __launch_bounds__(256) stage2_kernel(Stage2Args A) {
+  extern __shared__ double sm[];
+  const int nqp = A.nqp;
+  double *q_s = sm, *q2_s = sm + nqp, *iq2_s = sm + 2 * nqp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double *acc = sm + (3 + warp) * nqp;
+  for (int i = threadIdx.x; i < A.nq; i += blockDim.x) {
+    double q = A.q[i];
+    q_s[i] = q;
+    q2_s[i] = q * q;
+    iq2_s[i] = 1.0 / pow(q, 2.0);
+  }
+  for (int i = threadIdx.x; i < nw * nqp; i += blockDim.x) sm[3 * nqp + i] = 0.0;
+  __syncthreads();
+  const int64_t gw = (int64_t)blockIdx.x * nw + warp, W = (int64_t)gridDim.x * nw;
+  const int64_t nchunks = (A.nquart + A.chunk - 1) / A.chunk;
+  for (int64_t ch = gw; ch < nchunks; ch += W) {
+    int64_t q0 = ch * A.chunk, q1 = min(A.nquart, q0 + A.chunk);
+    for (int64_t qi = q0; qi < q1; ++qi) {
+      int c = 0;
+      while (c < A.ncls - 1 && qi >= A.cls_end[c]) ++c;
+      const double *r = A.rec + A.cls_recoff[c] + (qi - A.cls_begin[c]) * (int64_t)A.cls_rs[c];
+      double H = r[0], s = r[1];
+      int kind = (int)r[2], LB = (int)r[3];
+      if (kind == REC_P0) stage2_p0(r + 4, LB + 1, s, q2_s, acc, A.nq, lane);
+      else stage2_dispatch(LB, r + 4, H, s, kind == REC_BESSEL_J2, q_s, q2_s, iq2_s, acc, A.nq, lane);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < A.nq; i += blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sm[(3 + w) * nqp + i];
+    A.partial[(size_t)blockIdx.x * A.pstride + i] = t;
+  }
+}
+
+__global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  double t = 0.0;
+  for (int b = 0; b < nblocks; ++b) t += partial[(size_t)b * nq + i];
+  out[i] = t;
+}
+
+// ---------------------------------------------------------------------------
+// density transform helpers
+// ---------------------------------------------------------------------------
+
+// Ghat[x][y][z][w] += Gamma_t/8 over the eight index placements of a row
+// (both orders inside each pair, both pair orders); see tb_plan.cu.
+__global__ void ghat_scatter_kernel(const int *__restrict__ mat, const double *__restrict__ total, int nmat,
+                                    int n, double *__restrict__ G) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nmat) return;
+  int a = mat[t] - 1, b = mat[t + nmat] - 1, c = mat[t + 2 * nmat] - 1, d = mat[t + 3 * nmat] - 1;
+  double v = total[t] * 0.125;
+  int P[8][4] = {{a, b, c, d}, {b, a, c, d}, {a, b, d, c}, {b, a, d, c},
+                 {c, d, a, b}, {d, c, a, b}, {c, d, b, a}, {d, c, b, a}};
+  for (int k = 0; k < 8; ++k) {
+    size_t idx = (((size_t)P[k][0] * n + P[k][1]) * n + P[k][2]) * n + P[k][3];
+    atomicAdd(&G[idx], v);
+  }
+}
+
+// out[b][fpair(c,d)] = in[b][c][d] for c <= d
+__global__ void pack_pairs_kernel(const double *__restrict__ in, int64_t nb, int ngto, double *__restrict__ out) {
+  int64_t np = (int64_t)ngto * (ngto + 1) / 2;
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb * np) return;
+  int64_t b = i / np, p = i % np;
+  // invert fpair: d = largest with d(d+1)/2 <= p
+  int d = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+  while ((int64_t)(d + 1) * (d + 2) / 2 <= p) ++d;
+  while ((int64_t)d * (d + 1) / 2 > p) --d;
+  int c = (int)(p - (int64_t)d * (d + 1) / 2);
+  out[i] = in[((size_t)b * ngto + c) * ngto + d];
+}
+
+// out = 0.5 (in + in^T) for a small n x n matrix
+__global__ void sym_small_kernel(const double *__restrict__ in, int n, double *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * n) return;
+  int r = i / n, c = i % n;
+  out[i] = 0.5 * (in[r * n + c] + in[c * n + r]);
+}
+
+// ---------------------------------------------------------------------------
+// quartet enumeration
+// ---------------------------------------------------------------------------
+// The five loops of tot_integration visit, for bra pair (i,j):
+//   i <  j : kets (k,r) with k < r and k >= i          (loops 1 and 2)
+//   i == j : every ket (k,r) with k < r                 (loop 3)
+//            and (k,k) with k >= i                      (loops 4 and 5)
+// bra_off[b] is the first quartet of bra pair b (pair_index order).
+__global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off, int nbra, int64_t nquart,
+                                    const int *__restrict__ gL, uint64_t *__restrict__ quart,
+                                    uint32_t *__restrict__ keys) {
+  int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= nquart) return;
+  int lo = 0, hi = nbra - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (bra_off[mid] <= qi) lo = mid; else hi = mid - 1;
+  }
+  int b = lo;
+  int i = 0, rem = b;
+  while (rem >= ng - i) { rem -= ng - i; ++i; }
+  int j = i + rem;
+  int64_t m = qi - bra_off[b];
+  int k, r;
+  int64_t noff_all = (int64_t)ng * (ng - 1) / 2;
+  if (i < j || m < noff_all) {
+    // m-th off-diagonal pair (k < r) starting at k = (i < j ? i : 0)
+    k = i < j ? i : 0;
+    while (m >= ng - 1 - k) { m -= ng - 1 - k; ++k; }
+    r = k + 1 + (int)m;
+  } else {
+    k = i + (int)(m - noff_all);
+    r = k;
+  }
+  quart[qi] = (uint64_t)i | ((uint64_t)j << 16) | ((uint64_t)k << 32) | ((uint64_t)r << 48);
+  int Li = gL[i], Lj = gL[j], Lk = gL[k], Lr = gL[r];
+  keys[qi] = (uint32_t)(((((Li + Lj + Lk + Lr) * 5 + Li) * 5 + Lj) * 5 + Lk) * 5 + Lr);
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
+                               const double *xyz, double *tab, cudaStream_t st) {
+  int n = npairs(ng);
+  pair_tables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab);
+  return cudaGetLastError();
+}
+
+template <int K>
+static cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st) {
+  int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+  unsigned grid = (unsigned)((n + 127) / 128);
+  switch (L) {
+#define TB_S1(l) case l: stage1_kernel<l, K><<<grid, 128, 0, st>>>(a); break;
+    TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
+    TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
+#undef TB_S1
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, st);
+  return launch_stage1_k<KIND_J2>(L, a, st);
+}
+
+size_t stage2_smem_bytes(int nqp, int nwarps) { return sizeof(double) * (size_t)nqp * (3 + nwarps); }
+
+cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st) {
+  size_t smem = stage2_smem_bytes(a.nqp, nwarps);
+  cudaError_t e = cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage2_kernel<<<grid, nwarps * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st) {
+  reduce_kernel<<<(nq + 127) / 128, 128, 0, st>>>(partial, nblocks, nq, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ghat_scatter(const int *mat, const double *total, int nmat, int n, double *G, cudaStream_t st) {
+  if (nmat <= 0) return cudaSuccess;
+  ghat_scatter_kernel<<<(nmat + 255) / 256, 256, 0, st>>>(mat, total, nmat, n, G);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st) {
+  int64_t tot = nb * ((int64_t)ngto * (ngto + 1) / 2);
+  if (tot <= 0) return cudaSuccess;
+  pack_pairs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, nb, ngto, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,
+                                uint64_t *quart, uint32_t *keys, cudaStream_t st) {
+  if (nquart <= 0) return cudaSuccess;
+  quartet_fill_kernel<<<(unsigned)((nquart + 255) / 256), 256, 0, st>>>(ng, bra_off, npairs(ng), nquart, gL,
+                                                                        quart, keys);
+  return cudaGetLastError();
+}
+
+int stage2_blocks_per_sm(int nqp, int nwarps) {
+  int nb = 0;
+  size_t smem = stage2_smem_bytes(nqp, nwarps);
+  cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage2_kernel, nwarps * 32, smem) != cudaSuccess) return 1;
+  return nb > 0 ? nb : 1;
+}
+
+cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st) {
+  sym_small_kernel<<<(n * n + 127) / 128, 128, 0, st>>>(in, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace tb

@@ -1,0 +1,55 @@
+// Internal launch interface between the plan code and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tb {
+
+struct Stage1Args {
+  const uint64_t *quartets;   // packed gi | gj<<16 | gk<<32 | gr<<48, sorted by class
+  int64_t qbegin, qend;       // this launch's quartet range (one LLmax class)
+  const double *pairtab;      // PAIR_STRIDE doubles per unordered group pair
+  int ng;
+  const int *gstart, *gcount; // 0-based first function and size of each group
+  const int *flmn;            // l | m<<8 | n<<16 per function
+  const double *rho;          // pair density (np x np), total / j2
+  int64_t np;
+  const double *zao;          // AO density (ngto x ngto), elastic
+  int ngto;
+  double cutoffz, cutoffmd, cutoffcentre;
+  double *rec;                // records: [H, 1/4p+1/4p', kind, order, coefs...]
+  int64_t recbase;
+  int rs;
+};
+
+constexpr int MAXCLS = 20;
+
+struct Stage2Args {
+  const double *rec;
+  int ncls;
+  int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
+  int cls_rs[MAXCLS];
+  int64_t nquart;
+  int chunk;
+  const double *q;
+  int nq, nqp;
+  double *partial;            // this q tile's column of a (gridDim.x x pstride) array
+  int64_t pstride;
+};
+
+cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
+                               const double *xyz, double *tab, cudaStream_t st);
+cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st);
+size_t stage2_smem_bytes(int nqp, int nwarps);
+cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
+cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);
+cudaError_t launch_ghat_scatter(const int *mat, const double *total, int nmat, int n, double *G,
+                                cudaStream_t st);
+cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
+cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st);
+int stage2_blocks_per_sm(int nqp, int nwarps);
+cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,
+                                uint64_t *quart, uint32_t *keys, cudaStream_t st);
+
+}  // namespace tb

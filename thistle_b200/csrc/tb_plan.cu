@@ -1,0 +1,700 @@
+// Host side of the C-ABI: validation, device set-up and the execution order
+// of the scattering-intensity path.
+//
+// Reference map:
+//   group_start/group_count       src/main_calculation.f90:85-93
+//   z11/z22 and the per-quartet dgemm pair (zcontrred, zcontrred2)
+//                                 src/Variables.f90:1045-1065, src/Integrals.f90:109-127
+//       -> one 4-index transform rho(ab,cd) = sum Ghat C C C C on the device
+//   pair centres, E12, MD tables  src/Variables.f90:1113-1148
+//   the five quartet loops        src/Integrals.f90:79-468 (bra pair i<=j, ket pair k<=r)
+//   per-quartet kernels           src/Integrals.f90:4955-5226 and variants
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tb_kernels.h"
+#include "tb_math.cuh"
+#include "thistle_b200.h"
+
+using namespace tb;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define TB_CK(x)                                                                            \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) return fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define TB_CB(x)                                                                            \
+  do {                                                                                      \
+    cublasStatus_t s_ = (x);                                                                \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                                        \
+      return fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); \
+  } while (0)
+
+template <class T>
+static int dalloc(T **p, size_t n, const char *what) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? THISTLE_ERR_NOMEM : THISTLE_ERR_CUDA,
+                std::string("cudaMalloc of ") + what + " (" + std::to_string(n * sizeof(T)) + " bytes): " +
+                    cudaGetErrorString(e));
+  }
+  return THISTLE_OK;
+}
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+struct thistle_plan {
+  int type = 0, kind = 0;
+  int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nq = 0, maxa = 0, nmat = 0;
+  double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
+  std::vector<int> gstart, gcount, gL, flmn;
+  int64_t nquart = 0, np = 0;
+  int ncls = 0;
+  int cls_L[MAXCLS];
+  int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
+  int cls_rs[MAXCLS];
+  int64_t rec_total = 0;
+  int *d_gstart = nullptr, *d_gcount = nullptr, *d_flmn = nullptr;
+  double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr;
+  double *d_rho = nullptr, *d_zao = nullptr, *d_rec = nullptr, *d_partial = nullptr, *d_result = nullptr;
+  uint64_t *d_quart = nullptr;
+  int s2_grid = 0, s2_warps = 8, s2_chunk = 4, s2_qtile = 0;
+  cudaStream_t st = nullptr;
+  cublasHandle_t cb = nullptr;
+  cudaEvent_t ev[8];
+  bool have_ev = false;
+  float ms[5] = {0, 0, 0, 0, 0};
+};
+
+// ---------------------------------------------------------------------------
+// validation
+// ---------------------------------------------------------------------------
+static bool finite_all(const double *a, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+static int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const int32_t *l, const int32_t *m,
+                       const int32_t *n, const double *xx, const double *yy, const double *zz,
+                       const int32_t *group) {
+  if (ngto <= 0) return fail(THISTLE_ERR_ARG, "ngto must be positive");
+  if (!ga || !l || !m || !n || !xx || !yy || !zz || !group) return fail(THISTLE_ERR_ARG, "null basis array");
+  if (!finite_all(ga, ngto) || !finite_all(xx, ngto) || !finite_all(yy, ngto) || !finite_all(zz, ngto))
+    return fail(THISTLE_ERR_NONFINITE, "non-finite exponent or centre");
+  int ng = 0, maxa = 0;
+  for (int i = 0; i < ngto; ++i) {
+    if (!(ga[i] > 0.0)) return fail(THISTLE_ERR_ARG, "exponent must be positive (function " + std::to_string(i + 1) + ")");
+    if (l[i] < 0 || m[i] < 0 || n[i] < 0) return fail(THISTLE_ERR_ARG, "negative angular exponent");
+    if (l[i] > MAXA || m[i] > MAXA || n[i] > MAXA || l[i] + m[i] + n[i] > MAXA)
+      return fail(THISTLE_ERR_ANGMOM,
+                  "McMurchie-Davidson coefficients are only implemented up to g functions (function " +
+                      std::to_string(i + 1) + ")");
+    maxa = std::max(maxa, std::max(l[i], std::max(m[i], n[i])));
+    if (group[i] < 1) return fail(THISTLE_ERR_SHAPE, "group ids are 1-based");
+    ng = std::max(ng, (int)group[i]);
+  }
+  if (ng > 65535) return fail(THISTLE_ERR_SHAPE, "more than 65535 groups");
+  P->ngto = ngto;
+  P->ng = ng;
+  P->maxa = maxa;
+  P->gstart.assign(ng, -1);
+  P->gcount.assign(ng, 0);
+  P->gL.assign(ng, 0);
+  P->flmn.resize(ngto);
+  for (int i = 0; i < ngto; ++i) {
+    int g = group[i] - 1;
+    if (P->gstart[g] < 0) P->gstart[g] = i;
+    else if (group[i - 1] != group[i])
+      return fail(THISTLE_ERR_SHAPE, "functions of group " + std::to_string(g + 1) + " are not contiguous");
+    P->gcount[g] += 1;
+    P->flmn[i] = l[i] | (m[i] << 8) | (n[i] << 16);
+  }
+  for (int g = 0; g < ng; ++g) {
+    if (P->gstart[g] < 0) return fail(THISTLE_ERR_SHAPE, "group " + std::to_string(g + 1) + " has no function");
+    int h = P->gstart[g];
+    P->gL[g] = l[h] + m[h] + n[h];
+    for (int i = h; i < h + P->gcount[g]; ++i) {
+      if (ga[i] != ga[h] || xx[i] != xx[h] || yy[i] != yy[h] || zz[i] != zz[h] ||
+          l[i] + m[i] + n[i] != P->gL[g])
+        return fail(THISTLE_ERR_SHAPE, "group " + std::to_string(g + 1) +
+                                           " mixes exponents, centres or shells (one shell per group)");
+    }
+  }
+  return THISTLE_OK;
+}
+
+static int check_q(const double *q, int32_t nq) {
+  if (!q || nq <= 0) return fail(THISTLE_ERR_ARG, "empty q grid");
+  for (int i = 0; i < nq; ++i) {
+    if (!std::isfinite(q[i])) return fail(THISTLE_ERR_NONFINITE, "non-finite q");
+    if (!(q[i] > 0.0))
+      return fail(THISTLE_ERR_Q, "q must be > 0 (the reference divides by q; its drivers put 1e-10 for 0)");
+  }
+  return THISTLE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// quartet classes
+// ---------------------------------------------------------------------------
+static int64_t bra_count(int i, int j, int ng) {
+  if (i < j) return (int64_t)(ng - i) * (ng - i - 1) / 2;
+  return (int64_t)ng * (ng - 1) / 2 + (ng - i);
+}
+
+static inline int class_key(int Li, int Lj, int Lk, int Lr) {
+  return ((((Li + Lj + Lk + Lr) * 5 + Li) * 5 + Lj) * 5 + Lk) * 5 + Lr;
+}
+
+// Quartet counts per class key, without enumerating quartets.
+static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt) {
+  int ng = (int)gL.size();
+  cnt.assign(17 * 625, 0);
+  // off[k][a][b]: #{(k',r): k <= k' < r, gL[k']=a, gL[r]=b}; diag[k][a]: #{k' >= k: gL[k'] = a}
+  std::vector<int64_t> off((size_t)(ng + 1) * 25, 0), after(5, 0), diag((size_t)(ng + 1) * 5, 0);
+  for (int k = ng - 1; k >= 0; --k) {
+    for (int t = 0; t < 25; ++t) off[(size_t)k * 25 + t] = off[(size_t)(k + 1) * 25 + t];
+    for (int b = 0; b < 5; ++b) off[(size_t)k * 25 + gL[k] * 5 + b] += after[b];
+    after[gL[k]] += 1;
+    for (int a = 0; a < 5; ++a) diag[(size_t)k * 5 + a] = diag[(size_t)(k + 1) * 5 + a];
+    diag[(size_t)k * 5 + gL[k]] += 1;
+  }
+  for (int i = 0; i < ng; ++i)
+    for (int j = i; j < ng; ++j) {
+      int Li = gL[i], Lj = gL[j];
+      const int64_t *o = &off[(size_t)(i < j ? i : 0) * 25];
+      for (int a = 0; a < 5; ++a)
+        for (int b = 0; b < 5; ++b)
+          if (o[a * 5 + b]) cnt[class_key(Li, Lj, a, b)] += o[a * 5 + b];
+      if (i == j)
+        for (int a = 0; a < 5; ++a)
+          if (diag[(size_t)i * 5 + a]) cnt[class_key(Li, Lj, a, a)] += diag[(size_t)i * 5 + a];
+    }
+}
+
+// Sorted-by-key layout -> contiguous LLmax classes and record offsets.
+static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
+  int64_t pos = 0, recoff = 0;
+  P->ncls = 0;
+  for (int LL = 0; LL <= LMAXQ; ++LL) {
+    int64_t c = 0;
+    for (int t = 0; t < 625; ++t) c += cnt[LL * 625 + t];
+    if (c == 0) continue;
+    if (P->ncls >= MAXCLS) return fail(THISTLE_ERR_ARG, "too many quartet classes");
+    int k = P->ncls++;
+    P->cls_L[k] = LL;
+    P->cls_begin[k] = pos;
+    P->cls_end[k] = pos + c;
+    int rs = LL + 7;  // [H, s, kind, order] + up to LL+3 coefficients
+    rs += rs & 1;
+    (void)kind;
+    P->cls_rs[k] = rs;
+    P->cls_recoff[k] = recoff;
+    recoff += c * rs;
+    pos += c;
+  }
+  P->nquart = pos;
+  P->rec_total = recoff;
+  return THISTLE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// density transform on the device
+// ---------------------------------------------------------------------------
+// rho(ab,cd) = 1/8 sum_t G_t [S12_t(ab) S34_t(cd) + S34_t(ab) S12_t(cd)],
+// S12_t(ab) = C_{m1 a} C_{m2 b} + C_{m1 b} C_{m2 a}: the ztot of
+// src/Integrals.f90:5163 for every primitive pair pair.  With
+// Ghat[x][y][z][w] = G_t/8 summed over the eight placements of each row this is
+// the 4-index transform rho = sum Ghat C_x,a C_y,b C_z,c C_w,d, run as four
+// DGEMM passes: m4 -> d, m3 -> c (pack c<=d), m2 -> b, m1 -> a (pack a<=b).
+static int density_total(thistle_plan *P, const double *mmod, int32_t norbs, const int32_t *mat,
+                         const double *total, int32_t nmat) {
+  const int n = norbs, ngto = P->ngto;
+  const int64_t np = (int64_t)ngto * (ngto + 1) / 2;
+  P->np = np;
+  double *dC = nullptr, *dG = nullptr, *dT1 = nullptr, *dT2 = nullptr, *dV = nullptr, *dT3 = nullptr;
+  int *dmat = nullptr;
+  double *dtot = nullptr;
+  int rc = THISTLE_OK;
+  const double one = 1.0, zero = 0.0;
+  const int64_t n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
+#define TB_TRY(x)             \
+  do {                        \
+    rc = (x);                 \
+    if (rc != THISTLE_OK) goto done; \
+  } while (0)
+#define TB_TRYC(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) { rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); goto done; } \
+  } while (0)
+#define TB_TRYB(x)                                                                          \
+  do {                                                                                      \
+    cublasStatus_t s_ = (x);                                                                \
+    if (s_ != CUBLAS_STATUS_SUCCESS) { rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); goto done; } \
+  } while (0)
+  TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
+  TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
+  if (nmat == 0) goto done;
+  TB_TRY(dalloc(&dC, (size_t)n * ngto, "MO coefficients"));
+  TB_TRY(dalloc(&dG, (size_t)n4, "Ghat"));
+  TB_TRY(dalloc(&dmat, (size_t)nmat * 4, "2-RDM indices"));
+  TB_TRY(dalloc(&dtot, (size_t)nmat, "2-RDM values"));
+  TB_TRYC(cudaMemcpyAsync(dC, mmod, sizeof(double) * (size_t)n * ngto, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(dmat, mat, sizeof(int) * (size_t)nmat * 4, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(dtot, total, sizeof(double) * (size_t)nmat, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemsetAsync(dG, 0, sizeof(double) * (size_t)n4, P->st));
+  TB_TRYC(launch_ghat_scatter(dmat, dtot, nmat, n, dG, P->st));
+  // T1'(ngto x n^3) = C^T Ghat'   (C is (n, ngto) column-major, the mmod layout)
+  TB_TRY(dalloc(&dT1, (size_t)(n3 * ngto), "transform T1"));
+  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, (int)n3, n, &one, dC, n, dG, n, &zero, dT1, ngto));
+  dfree(dG);
+  // T2[X] (ngto x ngto) = T1[X]' C, X over n^2
+  TB_TRY(dalloc(&dT2, (size_t)(n2 * ngto * ngto), "transform T2"));
+  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, ngto, ngto, n, &one, dT1, ngto,
+                                    (long long)n * ngto, dC, n, 0, &zero, dT2, ngto, (long long)ngto * ngto,
+                                    (int)n2));
+  dfree(dT1);
+  TB_TRY(dalloc(&dV, (size_t)(n2 * np), "transform V"));
+  TB_TRYC(launch_pack_pairs(dT2, n2, ngto, dV, P->st));
+  dfree(dT2);
+  // T3[m1] (np x ngto) = V[m1]' C
+  TB_TRY(dalloc(&dT3, (size_t)((int64_t)n * ngto * np), "transform T3"));
+  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, ngto, n, &one, dV, (int)np,
+                                    (long long)n * np, dC, n, 0, &zero, dT3, (int)np, (long long)ngto * np, n));
+  dfree(dV);
+  // rho rows (a<=b, b fixed): (np x b+1) = T3[:,b,:]' C[:,0..b]
+  for (int b = 0; b < ngto; ++b) {
+    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, b + 1, n, &one, dT3 + (size_t)b * np,
+                        (int)((int64_t)ngto * np), dC, n, &zero, P->d_rho + (size_t)fpair(0, b) * np, (int)np));
+  }
+done:
+  dfree(dC); dfree(dG); dfree(dT1); dfree(dT2); dfree(dV); dfree(dT3); dfree(dmat); dfree(dtot);
+  return rc;
+}
+
+// Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217)
+static int density_elastic(thistle_plan *P, const double *mmod, int32_t norbs, const double *onerdm, int32_t nmo1) {
+  const int ngto = P->ngto;
+  double *dC = nullptr, *dD = nullptr, *dDs = nullptr, *dY = nullptr;
+  int rc = THISTLE_OK;
+  const double one = 1.0, zero = 0.0;
+  TB_TRY(dalloc(&P->d_zao, (size_t)ngto * ngto, "AO density"));
+  TB_TRY(dalloc(&dC, (size_t)norbs * ngto, "MO coefficients"));
+  TB_TRY(dalloc(&dD, (size_t)nmo1 * nmo1, "1-RDM"));
+  TB_TRY(dalloc(&dDs, (size_t)nmo1 * nmo1, "1-RDM"));
+  TB_TRY(dalloc(&dY, (size_t)nmo1 * ngto, "1-RDM x C"));
+  TB_TRYC(cudaMemcpyAsync(dC, mmod, sizeof(double) * (size_t)norbs * ngto, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(dD, onerdm, sizeof(double) * (size_t)nmo1 * nmo1, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(launch_sym_small(dD, nmo1, dDs, P->st));
+  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, nmo1, ngto, nmo1, &one, dDs, nmo1, dC, norbs, &zero, dY, nmo1));
+  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, ngto, nmo1, &one, dC, norbs, dY, nmo1, &zero,
+                      P->d_zao, ngto));
+done:
+  dfree(dC); dfree(dD); dfree(dDs); dfree(dY);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// quartets on the device: enumerate in bra-pair order, then a stable radix
+// sort on the class key so that each LLmax class is contiguous and each warp
+// of stage 1 sees quartets with identical loop bounds.
+// ---------------------------------------------------------------------------
+static int build_quartets(thistle_plan *P) {
+  const int ng = P->ng, nb = npairs(ng);
+  std::vector<int64_t> off(nb + 1);
+  int64_t acc = 0;
+  for (int i = 0, b = 0; i < ng; ++i)
+    for (int j = i; j < ng; ++j, ++b) {
+      off[b] = acc;
+      acc += bra_count(i, j, ng);
+    }
+  off[nb] = acc;
+  if (acc != P->nquart) return fail(THISTLE_ERR_ARG, "internal: quartet count mismatch");
+  if (acc >= ((int64_t)1 << 31)) return fail(THISTLE_ERR_ARG, "more than 2^31 group quartets");
+  int rc = THISTLE_OK;
+  int64_t *doff = nullptr;
+  int *dgL = nullptr;
+  uint32_t *k0 = nullptr, *k1 = nullptr;
+  uint64_t *v0 = nullptr;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0;
+  TB_TRY(dalloc(&doff, (size_t)nb + 1, "bra offsets"));
+  TB_TRY(dalloc(&dgL, (size_t)ng, "group L"));
+  TB_TRY(dalloc(&k0, (size_t)acc, "quartet keys"));
+  TB_TRY(dalloc(&k1, (size_t)acc, "quartet keys"));
+  TB_TRY(dalloc(&v0, (size_t)acc, "quartets"));
+  TB_TRY(dalloc(&P->d_quart, (size_t)acc, "quartets"));
+  TB_TRYC(cudaMemcpyAsync(doff, off.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(dgL, P->gL.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(launch_quartet_fill(ng, doff, acc, dgL, v0, k0, P->st));
+  TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, P->d_quart, (int)acc, 0, 14, P->st));
+  TB_TRY(dalloc((char **)&tmp, tmp_bytes, "sort scratch"));
+  TB_TRYC(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, P->d_quart, (int)acc, 0, 14, P->st));
+done:
+  dfree(doff); dfree(dgL); dfree(k0); dfree(k1); dfree(v0);
+  if (tmp) cudaFree(tmp);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// plan lifecycle
+// ---------------------------------------------------------------------------
+static void plan_free(thistle_plan *P) {
+  if (!P) return;
+  dfree(P->d_gstart); dfree(P->d_gcount); dfree(P->d_flmn); dfree(P->d_ga); dfree(P->d_xyz);
+  dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
+  dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
+  if (P->cb) cublasDestroy(P->cb);
+  if (P->have_ev)
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(P->ev[i]);
+  if (P->st) cudaStreamDestroy(P->st);
+  delete P;
+}
+
+static int upload_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
+  std::vector<double> xyz((size_t)P->ngto * 3);
+  for (int i = 0; i < P->ngto; ++i) {
+    xyz[3 * i] = xx[i];
+    xyz[3 * i + 1] = yy[i];
+    xyz[3 * i + 2] = zz[i];
+  }
+  TB_CK(cudaMemcpyAsync(P->d_xyz, xyz.data(), sizeof(double) * xyz.size(), cudaMemcpyHostToDevice, P->st));
+  TB_CK(cudaStreamSynchronize(P->st));
+  return THISTLE_OK;
+}
+
+static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga, const int32_t *l,
+                       const int32_t *m, const int32_t *n, const double *xx, const double *yy, const double *zz,
+                       const int32_t *group, const double *mmod, int32_t norbs, const int32_t *mat,
+                       const double *total, int32_t nmat, const double *onerdm, int32_t nmo1, const double *q,
+                       int32_t nq, double cutoffz, double cutoffmd, double cutoffcentre) {
+  if (!out) return fail(THISTLE_ERR_ARG, "null plan pointer");
+  *out = nullptr;
+  if (type != THISTLE_TOTAL_J0 && type != THISTLE_ELASTIC_J0 && type != THISTLE_TOTAL_J2)
+    return fail(THISTLE_ERR_TYPE, "calculation type " + std::to_string(type) + " is not provided by this entry");
+  thistle_plan *P = new thistle_plan();
+  int rc = THISTLE_OK;
+  std::vector<int64_t> cnt;
+  TB_TRY(check_basis(P, ngto, ga, l, m, n, xx, yy, zz, group));
+  TB_TRY(check_q(q, nq));
+  if (!std::isfinite(cutoffz) || !std::isfinite(cutoffmd) || !std::isfinite(cutoffcentre) || cutoffz < 0 ||
+      cutoffmd < 0 || cutoffcentre < 0) {
+    rc = fail(THISTLE_ERR_ARG, "cutoffs must be finite and non-negative");
+    goto done;
+  }
+  if (!mmod || norbs <= 0) { rc = fail(THISTLE_ERR_ARG, "missing MO coefficients"); goto done; }
+  if (!finite_all(mmod, (int64_t)norbs * ngto)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite MO coefficient"); goto done; }
+  P->type = type;
+  P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL : (type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC : KIND_J2);
+  P->nq = nq;
+  P->nmo = norbs;
+  P->cutoffz = cutoffz;
+  P->cutoffmd = cutoffmd;
+  P->cutoffcentre = cutoffcentre;
+  if (P->kind == KIND_ELASTIC) {
+    if (!onerdm || nmo1 <= 0 || nmo1 > norbs) { rc = fail(THISTLE_ERR_ARG, "1-RDM must be (nmo1,nmo1) with nmo1 <= norbs"); goto done; }
+    if (!finite_all(onerdm, (int64_t)nmo1 * nmo1)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 1-RDM"); goto done; }
+    P->nmo1 = nmo1;
+  } else {
+    if (nmat < 0 || (nmat > 0 && (!mat || !total))) { rc = fail(THISTLE_ERR_ARG, "missing 2-RDM rows"); goto done; }
+    for (int64_t i = 0; i < (int64_t)nmat * 4; ++i)
+      if (mat[i] < 1 || mat[i] > norbs) {
+        rc = fail(THISTLE_ERR_SHAPE, "2-RDM index out of range 1..norbs at row " + std::to_string(i % nmat + 1));
+        goto done;
+      }
+    if (nmat > 0 && !finite_all(total, nmat)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 2-RDM value"); goto done; }
+    P->nmat = nmat;
+  }
+  class_counts(P->gL, cnt);
+  TB_TRY(setup_classes(P, cnt, P->kind));
+  TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
+  for (int i = 0; i < 8; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
+  P->have_ev = true;
+  TB_TRYB(cublasCreate(&P->cb));
+  TB_TRYB(cublasSetStream(P->cb, P->st));
+  TB_TRYB(cublasSetMathMode(P->cb, CUBLAS_PEDANTIC_MATH));
+  TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
+  TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
+  TB_TRY(dalloc(&P->d_flmn, (size_t)ngto, "functions"));
+  TB_TRY(dalloc(&P->d_ga, (size_t)ngto, "exponents"));
+  TB_TRY(dalloc(&P->d_xyz, (size_t)ngto * 3, "centres"));
+  TB_TRY(dalloc(&P->d_q, (size_t)nq, "q"));
+  TB_TRY(dalloc(&P->d_result, (size_t)nq, "result"));
+  TB_TRY(dalloc(&P->d_pairtab, (size_t)npairs(P->ng) * PAIR_STRIDE, "pair tables"));
+  TB_TRYC(cudaMemcpyAsync(P->d_gstart, P->gstart.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_gcount, P->gcount.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_flmn, P->flmn.data(), sizeof(int) * ngto, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_ga, ga, sizeof(double) * ngto, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
+  TB_TRY(upload_centres(P, xx, yy, zz));
+  TB_TRYC(cudaEventRecord(P->ev[6], P->st));
+  if (P->kind == KIND_ELASTIC) TB_TRY(density_elastic(P, mmod, norbs, onerdm, nmo1));
+  else TB_TRY(density_total(P, mmod, norbs, mat, total, nmat));
+  TB_TRYC(cudaEventRecord(P->ev[7], P->st));
+  TB_TRY(build_quartets(P));
+  TB_TRY(dalloc(&P->d_rec, (size_t)P->rec_total, "quartet records"));
+  {
+    int dev = 0, nsm = 0;
+    TB_TRYC(cudaGetDevice(&dev));
+    TB_TRYC(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    int maxsm = 0;
+    TB_TRYC(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // q tile held in shared memory: (3 + warps) doubles per q point
+    P->s2_warps = 8;
+    int qt = std::min(nq, 2048);
+    while ((size_t)(3 + P->s2_warps) * qt * sizeof(double) > (size_t)maxsm && qt > 32) qt /= 2;
+    P->s2_qtile = qt;
+    int bps = stage2_blocks_per_sm(qt, P->s2_warps);
+    P->s2_grid = nsm * bps;
+    TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_grid * nq, "partial sums"));
+  }
+  TB_TRYC(cudaStreamSynchronize(P->st));
+  {
+    float t = 0;
+    cudaEventElapsedTime(&t, P->ev[6], P->ev[7]);
+    P->ms[4] = t;
+  }
+done:
+  if (rc != THISTLE_OK) {
+    plan_free(P);
+    return rc;
+  }
+  *out = P;
+  return THISTLE_OK;
+}
+
+static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
+                      const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
+                      double *d_out) {
+  TB_CK(cudaEventRecord(P->ev[0], P->st));
+  TB_CK(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->st));
+  TB_CK(cudaEventRecord(P->ev[1], P->st));
+  for (int c = 0; c < ncls; ++c) {
+    Stage1Args a;
+    a.quartets = d_quart;
+    a.qbegin = cb[c];
+    a.qend = ce[c];
+    a.pairtab = P->d_pairtab;
+    a.ng = P->ng;
+    a.gstart = P->d_gstart;
+    a.gcount = P->d_gcount;
+    a.flmn = P->d_flmn;
+    a.rho = P->d_rho;
+    a.np = P->np;
+    a.zao = P->d_zao;
+    a.ngto = P->ngto;
+    a.cutoffz = P->cutoffz;
+    a.cutoffmd = P->cutoffmd;
+    a.cutoffcentre = P->cutoffcentre;
+    a.rec = d_rec;
+    a.recbase = recoff[c];
+    a.rs = rs[c];
+    TB_CK(launch_stage1(P->kind, cL[c], a, P->st));
+  }
+  TB_CK(cudaEventRecord(P->ev[2], P->st));
+  int64_t nq_all = 0;
+  for (int c = 0; c < ncls; ++c) nq_all = std::max(nq_all, ce[c]);
+  for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
+    Stage2Args s;
+    s.rec = d_rec;
+    s.ncls = ncls;
+    for (int c = 0; c < ncls; ++c) {
+      s.cls_begin[c] = cb[c];
+      s.cls_end[c] = ce[c];
+      s.cls_recoff[c] = recoff[c];
+      s.cls_rs[c] = rs[c];
+    }
+    s.nquart = nq_all;
+    s.chunk = P->s2_chunk;
+    s.q = P->d_q + q0;
+    s.nq = std::min(P->s2_qtile, P->nq - q0);
+    s.nqp = P->s2_qtile;
+    s.partial = P->d_partial + q0;
+    s.pstride = P->nq;
+    TB_CK(launch_stage2(s, P->s2_grid, P->s2_warps, P->st));
+  }
+  TB_CK(cudaEventRecord(P->ev[3], P->st));
+  TB_CK(launch_reduce(P->d_partial, P->s2_grid, P->nq, d_out, P->st));
+  TB_CK(cudaEventRecord(P->ev[4], P->st));
+  return THISTLE_OK;
+}
+
+static int plan_exec(thistle_plan *P, double *d_out) {
+  return run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
+                    P->cls_rs, d_out);
+}
+
+static void read_timings(thistle_plan *P) {
+  for (int i = 0; i < 4; ++i) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, P->ev[i], P->ev[i + 1]) == cudaSuccess) P->ms[i] = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *thistle_last_error_string(void) { return g_err.c_str(); }
+
+int thistle_version(void) { return 100; }
+
+int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const double *ga, const int32_t *l,
+                        const int32_t *m, const int32_t *n, const double *xx, const double *yy, const double *zz,
+                        const int32_t *group, const double *mmod, int32_t norbs, const int32_t *mat,
+                        const double *total, int32_t nmat, const double *onerdm, int32_t nmo1, const double *q,
+                        int32_t nq, double cutoffz, double cutoffmd, double cutoffcentre) {
+  return plan_create(plan, type, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, mat, total, nmat, onerdm, nmo1,
+                     q, nq, cutoffz, cutoffmd, cutoffcentre);
+}
+
+int thistle_plan_set_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
+  if (!P || !xx || !yy || !zz) return fail(THISTLE_ERR_ARG, "null argument");
+  if (!finite_all(xx, P->ngto) || !finite_all(yy, P->ngto) || !finite_all(zz, P->ngto))
+    return fail(THISTLE_ERR_NONFINITE, "non-finite centre");
+  for (int g = 0; g < P->ng; ++g) {
+    int h = P->gstart[g];
+    for (int i = h; i < h + P->gcount[g]; ++i)
+      if (xx[i] != xx[h] || yy[i] != yy[h] || zz[i] != zz[h])
+        return fail(THISTLE_ERR_SHAPE, "functions of one group must share a centre");
+  }
+  return upload_centres(P, xx, yy, zz);
+}
+
+int thistle_plan_execute_device(thistle_plan *P, double *result_dev) {
+  if (!P || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  return plan_exec(P, result_dev);
+}
+
+int thistle_plan_execute(thistle_plan *P, double *result_host) {
+  if (!P || !result_host) return fail(THISTLE_ERR_ARG, "null argument");
+  int rc = plan_exec(P, P->d_result);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
+  TB_CK(cudaStreamSynchronize(P->st));
+  read_timings(P);
+  return THISTLE_OK;
+}
+
+int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int64_t nquart, double *result_host) {
+  if (!P || !result_host || (nquart > 0 && !quartets) || nquart < 0) return fail(THISTLE_ERR_ARG, "null argument");
+  // host-side class sort of the (small) list
+  std::vector<std::pair<int, uint64_t>> items((size_t)nquart);
+  for (int64_t t = 0; t < nquart; ++t) {
+    int gi = quartets[4 * t], gj = quartets[4 * t + 1], gk = quartets[4 * t + 2], gr = quartets[4 * t + 3];
+    if (gi < 0 || gj < 0 || gk < 0 || gr < 0 || gi >= P->ng || gj >= P->ng || gk >= P->ng || gr >= P->ng ||
+        gi > gj || gk > gr)
+      return fail(THISTLE_ERR_SHAPE, "quartet " + std::to_string(t) + " needs 0 <= gi <= gj < ng, 0 <= gk <= gr < ng");
+    int key = class_key(P->gL[gi], P->gL[gj], P->gL[gk], P->gL[gr]);
+    items[t] = {key, (uint64_t)gi | ((uint64_t)gj << 16) | ((uint64_t)gk << 32) | ((uint64_t)gr << 48)};
+  }
+  std::stable_sort(items.begin(), items.end(),
+                   [](const std::pair<int, uint64_t> &a, const std::pair<int, uint64_t> &b) { return a.first < b.first; });
+  int64_t cb[MAXCLS], ce[MAXCLS], ro[MAXCLS];
+  int cL[MAXCLS], rs[MAXCLS], ncls = 0;
+  int64_t roff = 0;
+  for (int64_t t = 0; t < nquart;) {
+    int LL = items[t].first / 625;
+    int64_t u = t;
+    while (u < nquart && items[u].first / 625 == LL) ++u;
+    cb[ncls] = t; ce[ncls] = u; cL[ncls] = LL;
+    rs[ncls] = (LL + 7) + ((LL + 7) & 1);
+    ro[ncls] = roff;
+    roff += (u - t) * rs[ncls];
+    ++ncls;
+    t = u;
+  }
+  std::vector<uint64_t> packed((size_t)nquart);
+  for (int64_t t = 0; t < nquart; ++t) packed[t] = items[t].second;
+  uint64_t *dq = nullptr;
+  double *drec = nullptr;
+  int rc = THISTLE_OK;
+  TB_TRY(dalloc(&dq, (size_t)nquart, "quartet list"));
+  TB_TRY(dalloc(&drec, (size_t)roff, "quartet records"));
+  TB_TRYC(cudaMemcpyAsync(dq, packed.data(), sizeof(uint64_t) * nquart, cudaMemcpyHostToDevice, P->st));
+  if (nquart == 0) {
+    TB_TRYC(cudaMemsetAsync(P->d_result, 0, sizeof(double) * P->nq, P->st));
+  } else {
+    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result));
+  }
+  TB_TRYC(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
+  TB_TRYC(cudaStreamSynchronize(P->st));
+done:
+  dfree(dq);
+  dfree(drec);
+  return rc;
+}
+
+int thistle_plan_info(const thistle_plan *P, int64_t *info) {
+  if (!P || !info) return fail(THISTLE_ERR_ARG, "null argument");
+  info[0] = P->nquart;
+  info[1] = 0;
+  info[2] = P->ng;
+  info[3] = P->ngto;
+  info[4] = P->nq;
+  return THISTLE_OK;
+}
+
+int thistle_plan_timings(const thistle_plan *P, double *ms) {
+  if (!P || !ms) return fail(THISTLE_ERR_ARG, "null argument");
+  for (int i = 0; i < 5; ++i) ms[i] = P->ms[i];
+  return THISTLE_OK;
+}
+
+int thistle_plan_destroy(thistle_plan *P) {
+  if (P) {
+    if (P->st) cudaStreamSynchronize(P->st);
+    plan_free(P);
+  }
+  return THISTLE_OK;
+}
+
+int thistle_total_scattering(int32_t type, const double *Zn, const double *geom, int32_t natoms, int32_t maxl,
+                             int32_t ngto, int32_t ng, const double *ga, const int32_t *l, const int32_t *m,
+                             const int32_t *n, const double *xx, const double *yy, const double *zz,
+                             const double *mmod, int32_t norbs, const double *q, int32_t nq, const int32_t *group,
+                             double cutoffz, double cutoffmd, double cutoffcentre, const int32_t *mat,
+                             const double *total, int32_t nmat, const double *onerdm, int32_t nmo1,
+                             double *q_abs_out, double *result_out) {
+  (void)Zn; (void)geom; (void)natoms;
+  if (!result_out) return fail(THISTLE_ERR_ARG, "null result");
+  if (maxl < 0) return fail(THISTLE_ERR_ARG, "maxl must be >= 0");
+  thistle_plan *P = nullptr;
+  int rc = plan_create(&P, type, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, mat, total, nmat, onerdm, nmo1,
+                       q, nq, cutoffz, cutoffmd, cutoffcentre);
+  if (rc != THISTLE_OK) return rc;
+  if (ng != P->ng) {
+    plan_free(P);
+    return fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
+  }
+  rc = thistle_plan_execute(P, result_out);
+  if (rc == THISTLE_OK && q_abs_out)
+    for (int i = 0; i < nq; ++i) q_abs_out[i] = q[i];
+  thistle_plan_destroy(P);
+  return rc;
+}
+
+}  // extern "C"

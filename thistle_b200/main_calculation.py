@@ -1,0 +1,190 @@
+"""Host-side mirror of THISTLE's calculation dispatcher, on the B200 path.
+
+``total_scattering_calculation`` keeps the argument meaning and order of the
+f2py call the reference's Python driver makes
+(``main_calculation.total_scattering_calculation``, src/main_calculation.f90:13-15,
+called at src/scattering_main_routine.py:240-247) and returns ``(q_abs, result)``
+like it.  The CI vectors of that call (``confs, civecs``) are replaced by the
+RDMs they produce, which is the ``readrdm`` form of
+``total_scattering_calculation_2`` (src/main_calculation.f90:501-849);
+``total_scattering_calculation_2`` itself reads the same RDM files as the
+reference (read_twordm / read_onerdm, src/one_rdm.f90:2072-2147).
+
+Every call runs on the current CUDA device through libthistle_b200.so; errors
+come back as :class:`ThistleError` with the library's status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import ThistleError, check, colmajor_f64, colmajor_i32, dptr, iptr
+
+TOTAL_J0 = 1
+ELASTIC_J0 = 2
+TOTAL_ALIGNED = 3
+TOTAL_J2 = 7
+
+
+def read_twordm(filename):
+    """Rows ``p q r s value`` of a 2-RDM file (src/one_rdm.f90:2112-2147)."""
+    rows = np.loadtxt(filename, ndmin=2)
+    mat = rows[:, :4].astype(np.int32)
+    total = rows[:, 4].astype(np.float64)
+    return mat, total
+
+
+def read_onerdm(filename):
+    """Rows ``i j value``; the matrix size is the last row's i (src/one_rdm.f90:2072-2108)."""
+    rows = np.loadtxt(filename, ndmin=2)
+    maxnmo = int(rows[-1, 0])
+    D = np.zeros((maxnmo, maxnmo))
+    for i, j, v in rows:
+        D[int(i) - 1, int(j) - 1] = v
+    return D
+
+
+def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
+                                 mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=None, total=None,
+                                 onerdm=None):
+    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 7 total j2).
+
+    ``mmod`` is (norbs, ngto) as the reference passes it; ``mat``/``total``
+    are the 2-RDM rows (types 1 and 7), ``onerdm`` the 1-RDM (type 2).
+    ``state1``/``state2`` select CI states in the reference and are unused
+    here, where the RDMs are inputs.  Returns ``(q_abs, result)``.
+    """
+    del state1, state2
+    ga = _abi.as_f64(ga)
+    l, m, n, group = (_abi.as_i32(a) for a in (l, m, n, group))
+    xx, yy, zz, q = (_abi.as_f64(a) for a in (xx, yy, zz, q))
+    mmod = np.asarray(mmod, dtype=np.float64)
+    norbs = mmod.shape[0]
+    mcm = colmajor_f64(mmod)
+    matcm = colmajor_i32(mat) if mat is not None else None
+    tot = _abi.as_f64(total) if total is not None else None
+    nmat = 0 if mat is None else int(np.asarray(mat).shape[0])
+    one = colmajor_f64(onerdm) if onerdm is not None else None
+    nmo1 = 0 if onerdm is None else int(np.asarray(onerdm).shape[0])
+    Zn = _abi.as_f64(Zn) if Zn is not None else None
+    geom = colmajor_f64(geom) if geom is not None else None
+    natoms = 0 if geom is None else int(np.asarray(geom).shape[0]) if np.asarray(geom).ndim == 2 else 0
+    q_abs = np.zeros(int(nq))
+    result = np.zeros(int(nq))
+    rc = _abi.lib().thistle_total_scattering(
+        int(type), dptr(Zn), dptr(geom), natoms, int(maxl), int(ngto), int(ng), dptr(ga), iptr(l), iptr(m),
+        iptr(n), dptr(xx), dptr(yy), dptr(zz), dptr(mcm), norbs, dptr(q), int(nq), iptr(group),
+        float(cutoffz), float(cutoffmd), float(cutoffcentre), iptr(matcm), dptr(tot), nmat, dptr(one), nmo1,
+        dptr(q_abs), dptr(result))
+    check(rc)
+    return q_abs, result
+
+
+def total_scattering_calculation_2(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
+                                   mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, fileJ, fileJ_2,
+                                   readrdm=True):
+    """The ``readrdm`` branch of total_scattering_calculation_2: type 1 and 7
+    read the 2-RDM from ``fileJ_2``, type 2 the 1-RDM from ``fileJ``."""
+    if not readrdm:
+        raise ThistleError(-7, "only the readrdm path is provided; CI-vector RDM construction is upstream")
+    mat = total = onerdm = None
+    if type in (TOTAL_J0, TOTAL_J2):
+        mat, total = read_twordm(fileJ_2)
+    elif type == ELASTIC_J0:
+        onerdm = read_onerdm(fileJ)
+    return total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy,
+                                        zz, mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=mat,
+                                        total=total, onerdm=onerdm)
+
+
+class ScatteringPlan:
+    """One basis + density + q grid on the device, executed per geometry."""
+
+    def __init__(self, type, ga, l, m, n, xx, yy, zz, group, mmod, q, cutoffz, cutoffmd, cutoffcentre,
+                 mat=None, total=None, onerdm=None):
+        self._p = C.c_void_p()
+        self.type = int(type)
+        self._keep = [_abi.as_f64(ga), _abi.as_i32(l), _abi.as_i32(m), _abi.as_i32(n), _abi.as_f64(xx),
+                      _abi.as_f64(yy), _abi.as_f64(zz), _abi.as_i32(group)]
+        ga, l, m, n, xx, yy, zz, group = self._keep
+        mmod = np.asarray(mmod, dtype=np.float64)
+        self.ngto = int(ga.size)
+        self.q = _abi.as_f64(q)
+        self.nq = int(self.q.size)
+        mcm = colmajor_f64(mmod)
+        matcm = colmajor_i32(mat) if mat is not None else None
+        tot = _abi.as_f64(total) if total is not None else None
+        one = colmajor_f64(onerdm) if onerdm is not None else None
+        rc = _abi.lib().thistle_plan_create(
+            C.byref(self._p), self.type, self.ngto, dptr(ga), iptr(l), iptr(m), iptr(n), dptr(xx), dptr(yy),
+            dptr(zz), iptr(group), dptr(mcm), int(mmod.shape[0]), iptr(matcm), dptr(tot),
+            0 if mat is None else int(np.asarray(mat).shape[0]), dptr(one),
+            0 if onerdm is None else int(np.asarray(onerdm).shape[0]), dptr(self.q), self.nq, float(cutoffz),
+            float(cutoffmd), float(cutoffcentre))
+        check(rc)
+
+    @classmethod
+    def from_problem(cls, prob, type=TOTAL_J0, q=None):
+        return cls(type, prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.group, prob.mmod,
+                   prob.q if q is None else q, prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
+                   mat=prob.mat if type != ELASTIC_J0 else None, total=prob.total if type != ELASTIC_J0 else None,
+                   onerdm=prob.onerdm if type == ELASTIC_J0 else None)
+
+    def set_centres(self, xx, yy, zz):
+        xx, yy, zz = (_abi.as_f64(a) for a in (xx, yy, zz))
+        check(_abi.lib().thistle_plan_set_centres(self._p, dptr(xx), dptr(yy), dptr(zz)))
+
+    def execute(self, out=None):
+        out = np.zeros(self.nq) if out is None else out
+        check(_abi.lib().thistle_plan_execute(self._p, dptr(out)))
+        return out
+
+    def execute_device(self, ptr: int):
+        check(_abi.lib().thistle_plan_execute_device(self._p, C.c_void_p(ptr)))
+
+    def execute_quartets(self, quartets):
+        qt = np.ascontiguousarray(np.asarray(quartets, dtype=np.int32).reshape(-1, 4))
+        out = np.zeros(self.nq)
+        check(_abi.lib().thistle_plan_execute_quartets(self._p, iptr(qt), qt.shape[0], dptr(out)))
+        return out
+
+    def info(self):
+        a = np.zeros(5, dtype=np.int64)
+        check(_abi.lib().thistle_plan_info(self._p, a.ctypes.data_as(_abi.I64)))
+        return dict(nquart=int(a[0]), ng=int(a[2]), ngto=int(a[3]), nq=int(a[4]))
+
+    def timings(self):
+        a = np.zeros(5)
+        check(_abi.lib().thistle_plan_timings(self._p, dptr(a)))
+        return dict(pair_tables=a[0], stage1=a[1], stage2=a[2], reduce=a[3], transform=a[4])
+
+    def close(self):
+        if self._p:
+            _abi.lib().thistle_plan_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def scattering(prob, type=TOTAL_J0, q=None):
+    """I(q) of an :class:`thistle_b200.inputs.Problem` through Entry 1."""
+    qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
+    _, res = total_scattering_calculation(
+        type, None, prob.atoms, 0, 0, int(max(prob.l.max(), prob.m.max(), prob.n.max())), prob.ngto, prob.ng,
+        prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.mmod, qv, qv.size, prob.group,
+        prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
+        mat=prob.mat if type != ELASTIC_J0 else None, total=prob.total if type != ELASTIC_J0 else None,
+        onerdm=prob.onerdm if type == ELASTIC_J0 else None)
+    return res
