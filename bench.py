@@ -1,0 +1,348 @@
+"""Benchmark of the B200 scattering-intensity path.
+
+Workload (one step): the total j0 intensity of the AB6 octahedral molecule of
+the benchmark configurations -- 7 atoms, 203 primitives in 98 shells, 40 MOs,
+a 5 % sparse PSD 2-RDM (134 401 rows), 500 q points on 0..15 bohr^-1 --
+computed from inputs already resident in HBM: density transform, quartet
+enumeration, pair tables, stage 1 (Hermite densities and expansion
+coefficients) and stage 2 (the quartet x q Bessel sum), i.e. everything the
+reference's tot_integration does for the 11 920 622 group quartets of its five
+loops.  The metric is reference-defined quartet.q evaluations per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl thistle|reference]
+
+N > 1 (under torchrun) runs N independent replicas, one per GPU ("replicas
+only": the path needs no collective); value = all ranks' quartet.q / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 quartet.q evals/s (total j0, AB6 octahedral, 500 q)"
+UNIT = "quartet.q/s"
+
+
+def fb_flops(L: int) -> int:
+    """Algorithmic FLOPs of one Bessel-branch quartet.q: per order 2 (j_b by
+    recurrence) + 1 ((q/H)^b update) + 2 (FMA into the sum); fixed 10: qH, 1/x,
+    sincos (2), Gaussian exponent (2), exp (1), x K K' w (2), accumulate (1)."""
+    return 5 * (L + 1) + 10
+
+
+def p0_flops(L: int) -> int:
+    """P = Q branch: Horner over L/2+1 even powers (2 each) + exp, scale, add."""
+    return 2 * (L // 2 + 1) + 3
+
+
+WORKLOAD = "ab6"
+
+
+def workload():
+    from thistle_b200 import inputs as I
+    if WORKLOAD == "ab6_4atom":
+        return I.config3_ab6(natoms=4)
+    return I.config3_ab6()
+
+
+def workload_config(p, nquart):
+    return {
+        "workload": f"ab6_total_j0: {len(p.atoms)} atoms, {p.ngto} primitives ({p.ng} shells), {p.nmo} MOs, "
+                    f"{p.mat.shape[0]}-row 5% sparse 2-RDM, {p.nq} q on 0..15 bohr^-1",
+        "quartets_per_step": int(nquart),
+        "quartet_q_per_step": int(nquart) * p.nq,
+        "l2": "inputs larger than L2 (pair density %.1f GB, quartet records > 0.5 GB); no flush"
+              % (8 * (p.ngto * (p.ngto + 1) / 2) ** 2 / 1e9),
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smmax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smmax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smmax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(p, target_s: float = 12.0, seed: int = 11):
+    """The oracle (C restatement of the reference's loops and per-quartet dgemm)
+    on a random sample of the workload's quartets, all host threads."""
+    from oracle import oracle as O
+    ncores = os.cpu_count() or 1
+    qs = O.enum_quartets(p.ng)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(qs))
+    n = 8
+    t_per = None
+    while True:
+        sample = qs[np.sort(order[:n])]
+        t0 = time.perf_counter()
+        O.scattering(p, 1, quartets=sample, nthreads=ncores)
+        dt = time.perf_counter() - t0
+        t_per = dt / n
+        if dt >= target_s or n >= len(qs):
+            break
+        n = int(min(len(qs), max(2 * n, target_s / max(t_per, 1e-6) * 1.05)))
+    value = n * p.nq / dt
+    return {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
+            "sample": f"{n} of {len(qs)} group quartets drawn uniformly at random (seed {seed}), all {p.nq} q; "
+                      f"{dt:.1f} s on {ncores} host threads; oracle/thistle_oracle.c restating "
+                      f"tot_integration with its per-quartet dgemm"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    p = workload()
+    ncores = os.cpu_count() or 1
+    qs = O.enum_quartets(p.ng)
+    rng = np.random.default_rng(17)
+    per_step = 24
+    times = []
+    for s in range(args.warmup + args.steps):
+        idx = np.sort(rng.choice(len(qs), size=per_step, replace=False))
+        t0 = time.perf_counter()
+        O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = per_step * p.nq * len(times) / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; BASELINE configuration 3 shapes)",
+        "config": {"workload": workload_config(p, len(qs))["workload"],
+                   "sample_per_step": f"{per_step} random group quartets x {p.nq} q"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
+                         "sample": f"{per_step} random group quartets per step, {ncores} host threads; the C "
+                                   f"restatement of tot_integration (no Fortran compiler on this image)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def h2d_bytes(p):
+    ng = p.ng
+    npair = ng * (ng + 1) // 2
+    return int(8 * p.ngto + 24 * p.ngto + 4 * p.ngto + 8 * ng + 8 * p.nq + 8 * p.nmo * p.ngto
+               + 16 * p.mat.shape[0] + 8 * p.mat.shape[0] + 8 * (npair + 1) + 4 * ng)
+
+
+def e2e_entry1(p, steps, warmup):
+    """Entry 1 (thistle_total_scattering) from pinned host buffers: set-up,
+    H2D, transform, enumeration, integrator, D2H -- per step."""
+    import torch
+    from thistle_b200 import main_calculation as MC
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.int32: torch.int32}[a.dtype.type],
+                        pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    args = dict(ga=pinned(p.ga), l=pinned(p.l), m=pinned(p.m), n=pinned(p.n), xx=pinned(p.xx), yy=pinned(p.yy),
+                zz=pinned(p.zz), group=pinned(p.group), mmod=pinned(np.ascontiguousarray(p.mmod)),
+                q=pinned(p.q), mat=pinned(np.ascontiguousarray(p.mat)), total=pinned(p.total))
+
+    def call():
+        return MC.total_scattering_calculation(
+            1, None, None, 0, 0, 2, p.ngto, p.ng, args["ga"], args["l"], args["m"], args["n"], args["xx"],
+            args["yy"], args["zz"], args["mmod"], args["q"], p.nq, args["group"], p.cutoffz, p.cutoffmd,
+            p.cutoffcentre, mat=args["mat"], total=args["total"])[1]
+
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        res = call()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    return dt, res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="thistle", choices=["thistle", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--workload", default="ab6", choices=["ab6", "ab6_4atom"],
+                    help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis")
+    args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = args.workload
+    args.warmup = max(args.warmup, 3) if args.impl == "thistle" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from thistle_b200 import _abi
+    from thistle_b200 import main_calculation as MC
+    import ctypes as C
+
+    p = workload()
+    stream = torch.cuda.current_stream()
+    plan = MC.ScatteringPlan.from_problem(p, MC.TOTAL_J0)
+    plan.set_stream(stream.cuda_stream)
+    nquart = plan.info()["nquart"]
+    out = torch.empty(p.nq, dtype=torch.float64, device="cuda")
+
+    peak = C.c_double(0.0)
+    _abi.check(_abi.lib().thistle_probe_fp64_peak(5, C.byref(peak)))
+    peak_tf = peak.value
+
+    for _ in range(args.warmup):
+        plan.recompute_device(out.data_ptr())
+    torch.cuda.synchronize()
+    plan.stage_totals()  # reset
+    launches_per_step = plan.info()["launches"]
+    counts = plan.class_counts()
+
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ
+                           else local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.recompute_device(out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    st = plan.stage_totals()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    result = out.cpu().numpy()
+
+    qq_step = nquart * p.nq
+    value = world * qq_step * args.steps / (ms * 1e-3)
+    # roofline of the dominant kernel (stage 2, the Bessel sum), averaged over the timed launches
+    n2 = max(st["executions"], 1)
+    s2_ms = st["stage2"] / n2
+    flops = 0
+    for L, (n, n0) in counts.items():
+        flops += ((n - n0) * fb_flops(L) + n0 * p0_flops(L)) * p.nq
+    achieved = flops / (s2_ms * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stage2_ab6_dram.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                "frac": achieved / peak_tf if peak_tf > 0 else None, "traffic": traffic,
+                "kernel": "stage2_kernel (quartet x q Bessel sum)", "kernel_ms": s2_ms,
+                "flops_per_launch": flops,
+                "peak_source": "measured FP64 FMA rate of this GPU (thistle_probe_fp64_peak, in this run)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; BASELINE configuration 3 shapes)",
+        "config": dict(workload_config(p, nquart), parallelism=("replicas x%d" % world) if world > 1 else "1 GPU"),
+        "roofline": roofline,
+        "stage_ms_per_step": {k: v / n2 for k, v in st.items() if k != "executions"},
+        "p0_quartets_per_step": int(sum(n0 for _, (_, n0) in counts.items())),
+        "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clocks,
+        "sum_rule_check": float(result[0] / (p.nelec * (p.nelec - 1) * (float(np.float32(np.pi)) / np.pi) ** 3)),
+    }
+    if rank == 0:
+        if args.e2e_steps > 0:
+            dt_e2e, res_e2e = e2e_entry1(p, args.e2e_steps, 1)
+            line["e2e"] = {"value": qq_step / dt_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes(p),
+                           "d2h_bytes_per_step": 8 * p.nq, "ms_per_step": dt_e2e * 1e3,
+                           "path": "thistle_total_scattering (Entry 1), pinned host inputs, plan set-up included"}
+            line["e2e_matches_device"] = bool(np.max(np.abs(res_e2e - result)) <= 1e-12 * np.max(np.abs(result)))
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(p)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -29,6 +29,10 @@ extern "C" {
 #define THISTLE_ERR_Q -8          /* q <= 0 (the reference divides by q; drivers use 1e-10 for 0) */
 #define THISTLE_ERR_TIMEOUT -10   /* a bounded device wait gave up */
 
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (a
+ * register-resident chain kernel, best of `reps`); the roofline denominator. */
+int thistle_probe_fp64_peak(int32_t reps, double *tflops);
+
 /* Calculation types, numbered as src/main_calculation.f90:99-497. */
 #define THISTLE_TOTAL_J0 1
 #define THISTLE_ELASTIC_J0 2
@@ -46,7 +50,7 @@ int thistle_version(void);
  * files: mat/total/nmat are read_twordm's rows (src/one_rdm.f90:2112-2147),
  * onerdm is read_onerdm's matrix (:2072-2108).
  *
- *   type          1 total j0, 2 elastic j0, 7 total j2 (3: see thistle_aligned)
+ *   type          1 total j0, 2 elastic j0, 7 total j2
  *   Zn, geom      atomic numbers and (natoms,3) geometry; not used by these
  *                 types (kept for the reference's argument list), may be NULL
  *   maxl          maxval(l) as the reference passes it (checked, not trusted)
@@ -87,6 +91,9 @@ int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const d
                         const double *total, int32_t nmat, const double *onerdm, int32_t nmo1,
                         const double *q, int32_t nq, double cutoffz, double cutoffmd,
                         double cutoffcentre);
+/* Run the plan on a caller-owned cudaStream_t (passed as void*); the plan
+ * stops using its own stream.  The caller keeps the stream alive. */
+int thistle_plan_set_stream(thistle_plan *plan, void *stream);
 /* Move the Gaussian centres (host arrays of length ngto). */
 int thistle_plan_set_centres(thistle_plan *plan, const double *xx, const double *yy,
                              const double *zz);
@@ -94,16 +101,27 @@ int thistle_plan_set_centres(thistle_plan *plan, const double *xx, const double 
 int thistle_plan_execute(thistle_plan *plan, double *result_host);
 /* Same, leaving I(q) in device memory (nq doubles) on the plan's stream. */
 int thistle_plan_execute_device(thistle_plan *plan, double *result_dev);
+/* Redo the whole device pipeline from the device-resident inputs (density
+ * transform, quartet enumeration, then the integrator); I(q) to device memory. */
+int thistle_plan_recompute_device(thistle_plan *plan, double *result_dev);
 /* Evaluate only the listed group quartets (0-based gi,gj,gk,gr, 4 int32 each,
  * each with its reference loop weight); result_host gets nq doubles. */
 int thistle_plan_execute_quartets(thistle_plan *plan, const int32_t *quartets, int64_t nquart,
                                   double *result_host);
-/* Counts: [0] group quartets, [1] quartets on the P=Q branch in the last
- * execution, [2] ng, [3] ngto, [4] nq. */
-int thistle_plan_info(const thistle_plan *plan, int64_t *info5);
-/* Device time in ms of the last execution's stages: [0] pair tables,
- * [1] stage 1, [2] stage 2 (Bessel sum), [3] reduce; setup: [4] transform. */
-int thistle_plan_timings(const thistle_plan *plan, double *ms5);
+/* Counts: [0] group quartets, [1] LLmax classes, [2] ng, [3] ngto, [4] nq,
+ * [5] kernels of this library launched by the last call. */
+int thistle_plan_info(const thistle_plan *plan, int64_t *info6);
+/* Per LLmax = 0..16: (LLmax, quartets, quartets on the P=Q branch in the
+ * last execution) -- 51 int64 values. */
+int thistle_plan_class_counts(const thistle_plan *plan, int64_t *out51);
+/* Device time in ms: [0] pair tables, [1] stage 1, [2] stage 2 (Bessel sum),
+ * [3] reduce of the last execution; [4] density transform and [5] quartet
+ * enumeration of the set-up. */
+int thistle_plan_timings(const thistle_plan *plan, double *ms6);
+/* Waits for the plan's stream, then sums the device time of each stage
+ * ([0] pair tables, [1] stage 1, [2] stage 2, [3] reduce) over the executions
+ * since the previous call (at most the last 64); *nexec gets their number. */
+int thistle_plan_stage_totals(thistle_plan *plan, double *ms4, int64_t *nexec);
 int thistle_plan_destroy(thistle_plan *plan);
 
 #ifdef __cplusplus

@@ -1,0 +1,32 @@
+"""Generate the committed golden I(q) vectors from the C oracle.
+
+    python tests/golden/make_golden.py
+
+Inputs are regenerated from the seeded generators in thistle_b200.inputs;
+outputs are the oracle's restatement of the reference integrators
+(bessel_mode 0: the reference's own 100-term dphrec start).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+from thistle_b200 import inputs as I  # noqa: E402
+
+
+def main():
+    for cfg in (1, 2):
+        p = I.CONFIGS[cfg]()
+        out = {"q": p.q}
+        for t in (1, 2, 7):
+            out[f"type{t}"] = O.scattering(p, t, nthreads=8)
+        np.savez(os.path.join(HERE, f"golden_cfg{cfg}.npz"), **out)
+        print(cfg, {k: v[:2] for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+"""Parity of the CUDA path with the oracle (GPU tests, run on the B200).
+
+Tolerance: 1e-10 relative per q point, with a floor of 1e-12 of the largest
+|I(q)| for points where I(q) itself crosses zero (j2 near q = 0).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from thistle_b200 import inputs as I
+from thistle_b200 import main_calculation as MC
+from thistle_b200._abi import ThistleError
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+HERE = os.path.dirname(os.path.abspath(__file__))
+SP = (float(np.float32(np.pi)) / np.pi) ** 3
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+@pytest.mark.parametrize("type_", [1, 2, 7])
+def test_golden(cfg, type_):
+    g = np.load(os.path.join(HERE, "golden", f"golden_cfg{cfg}.npz"))
+    p = I.CONFIGS[cfg]()
+    np.testing.assert_array_equal(p.q, g["q"])
+    got = MC.scattering(p, type_)
+    assert np.max(rel_err(got, g[f"type{type_}"])) < TOL
+
+
+@pytest.mark.parametrize("type_", [1, 2, 7])
+def test_h2_against_live_oracle(oracle, type_):
+    p = I.config1_h2()
+    assert np.max(rel_err(MC.scattering(p, type_), oracle.scattering(p, type_))) < TOL
+
+
+def _cfg3_sample(oracle, p, n, seed):
+    qs = oracle.enum_quartets(p.ng)
+    gl = np.array([p.l[s] + p.m[s] + p.n[s] for s in np.searchsorted(p.group, np.arange(1, p.ng + 1))])
+    L = gl[qs[:, 0]] + gl[qs[:, 1]] + gl[qs[:, 2]] + gl[qs[:, 3]]
+    rng = np.random.default_rng(seed)
+    pick = []
+    for LL in np.unique(L):
+        idx = np.flatnonzero(L == LL)
+        pick.extend(rng.choice(idx, size=min(len(idx), max(2, n // 9)), replace=False))
+    return qs[np.sort(np.array(pick))]
+
+
+@pytest.fixture(scope="module")
+def cfg3():
+    return I.config3_ab6()
+
+
+@pytest.fixture(scope="module")
+def plan3(cfg3):
+    with MC.ScatteringPlan.from_problem(cfg3, MC.TOTAL_J0) as pl:
+        yield pl
+
+
+def test_cfg3_sampled_quartets_vs_oracle(oracle, cfg3, plan3):
+    """Every angular-momentum class of the 11.9M-quartet AB6 case, sampled."""
+    qs = _cfg3_sample(oracle, cfg3, 270, 7)
+    got = plan3.execute_quartets(qs[:, :4])
+    accurate = oracle.scattering(cfg3, 1, quartets=qs, bessel_mode=1, nthreads=8)
+    assert np.max(rel_err(got, accurate)) < TOL
+    # against the reference's own Bessel start where it has converged (qH <= 70)
+    ref = oracle.scattering(cfg3, 1, quartets=qs, bessel_mode=0, nthreads=8)
+    hmax = 2 * 2.95
+    ok = cfg3.q * hmax <= 70.0
+    assert np.max(rel_err(got[ok], ref[ok])) < TOL
+
+
+def test_cfg3_full_sum_rule(cfg3, plan3):
+    r = plan3.execute()
+    n = cfg3.nelec
+    assert abs(r[0] / (n * (n - 1) * SP) - 1) < 1e-10
+    assert np.all(np.isfinite(r))
+
+
+def test_cfg3_elastic_sum_rule(cfg3):
+    with MC.ScatteringPlan.from_problem(cfg3, MC.ELASTIC_J0) as pl:
+        r = pl.execute()
+    n = cfg3.nelec
+    assert abs(r[0] / (n * n * SP) - 1) < 1e-10
+
+
+def test_plan_set_centres_matches_fresh_plan():
+    p = I.config2_diatomic()
+    shifted = p.with_geometry(p.atoms + np.array([0.3, -0.2, 0.1]) + np.array([[0, 0, 0], [0.05, 0.0, -0.1]]))
+    with MC.ScatteringPlan.from_problem(p) as pl:
+        a0 = pl.execute()
+        pl.set_centres(shifted.xx, shifted.yy, shifted.zz)
+        a1 = pl.execute()
+    b1 = MC.scattering(shifted, 1)
+    assert np.max(rel_err(a1, b1)) < 1e-13
+    assert np.max(np.abs(a1 - a0)) > 1e-6
+
+
+def test_translation_invariance():
+    p = I.config2_diatomic()
+    t = p.with_geometry(p.atoms + np.array([1.7, -0.4, 2.2]))
+    assert np.max(rel_err(MC.scattering(t, 1), MC.scattering(p, 1))) < 1e-10
+
+
+def test_rotation_invariance_s_basis():
+    rng = np.random.default_rng(3)
+    atoms = rng.uniform(-2, 2, size=(3, 3))
+    shells = [[(0, e) for e in (0.3, 1.2, 6.0)] for _ in range(3)]
+    ga, L, M, N, X, Y, Z, grp, aof = I.build_basis(atoms, shells)
+    C = I.lowdin_mos(rng, 4, ga, L, M, N, X, Y, Z)
+    G4 = I.rdm2_dense(rng, 4, 4)
+    mat, tot = I.rdm_rows(G4)
+    q = I.q_grid(9.0, 64)
+    p = I.Problem("s3", atoms, ga, L, M, N, X, Y, Z, grp, aof, C, mat, tot, I.onerdm_from_2rdm(G4, 4), q, 4)
+    a, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    r = p.with_geometry(atoms @ a.T)
+    assert np.max(rel_err(MC.scattering(r, 1), MC.scattering(p, 1))) < 1e-10
+
+
+def test_empty_rdm_gives_zero():
+    p = I.config1_h2()
+    _, res = MC.total_scattering_calculation(1, None, None, 0, 0, 1, p.ngto, p.ng, p.ga, p.l, p.m, p.n, p.xx,
+                                             p.yy, p.zz, p.mmod, p.q, p.nq, p.group, p.cutoffz, p.cutoffmd,
+                                             p.cutoffcentre, mat=np.zeros((0, 4), np.int32),
+                                             total=np.zeros(0))
+    assert np.all(res == 0.0)
+
+
+def test_j2_vanishes_for_one_s_atom():
+    rng = np.random.default_rng(5)
+    atoms = np.zeros((1, 3))
+    ga, L, M, N, X, Y, Z, grp, aof = I.build_basis(atoms, [[(0, e) for e in (0.2, 1.0, 5.0, 25.0)]])
+    C = I.lowdin_mos(rng, 3, ga, L, M, N, X, Y, Z)
+    G4 = I.rdm2_dense(rng, 3, 4)
+    mat, tot = I.rdm_rows(G4)
+    p = I.Problem("s1", atoms, ga, L, M, N, X, Y, Z, grp, aof, C, mat, tot, I.onerdm_from_2rdm(G4, 4),
+                  I.q_grid(8.0, 40), 4)
+    assert np.max(np.abs(MC.scattering(p, 7))) == 0.0
+
+
+def test_ng_mismatch_is_reported():
+    p = I.config1_h2()
+    with pytest.raises(ThistleError) as e:
+        MC.total_scattering_calculation(1, None, None, 0, 0, 1, p.ngto, p.ng + 1, p.ga, p.l, p.m, p.n, p.xx,
+                                        p.yy, p.zz, p.mmod, p.q, p.nq, p.group, p.cutoffz, p.cutoffmd,
+                                        p.cutoffcentre, mat=p.mat, total=p.total)
+    assert e.value.code == -2
+
+
+def test_large_q_tiles():
+    """More q points than one shared-memory tile: the q-tiled launch path."""
+    p = I.config1_h2()
+    q = I.q_grid(10.0, 5000)
+    with MC.ScatteringPlan.from_problem(p, 1, q=q) as pl:
+        got = pl.execute()
+    ref = MC.scattering(p, 1, q=q[::7])
+    assert np.max(rel_err(got[::7], ref)) < 1e-13

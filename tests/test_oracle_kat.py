@@ -184,3 +184,16 @@ def test_qcoord3_grid(oracle):
     q = oracle.qcoord3()
     assert q.shape == (3131, 3)
     assert np.all(np.isfinite(q))
+
+
+def test_cutoffmd_is_numerically_inert(oracle):
+    """The reference's per-term |prod6| > cutoffmd test (1e-20) changes I(q) by
+    rounding only; the CUDA path accumulates Hermite densities in factorised
+    form without it (the |ztot| < cutoffz and |E| < 1e-30 tests are kept)."""
+    from dataclasses import replace
+    p = I.config2_diatomic()
+    for t in (1, 2, 7):
+        a = oracle.scattering(p, t, nthreads=8)
+        b = oracle.scattering(replace(p, cutoffmd=0.0), t, nthreads=8)
+        s = np.max(np.abs(a))
+        assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-12 * s)) < 1e-14

@@ -20,12 +20,13 @@ ERRORS = {
 }
 
 # every symbol include/thistle_b200.h declares
-EXPORTS = [
-    "thistle_last_error_string", "thistle_version", "thistle_total_scattering",
-    "thistle_plan_create", "thistle_plan_set_centres", "thistle_plan_execute",
-    "thistle_plan_execute_device", "thistle_plan_execute_quartets", "thistle_plan_info",
-    "thistle_plan_timings", "thistle_plan_destroy",
-]
+EXPORTS = sorted([
+    "thistle_last_error_string", "thistle_version", "thistle_total_scattering", "thistle_probe_fp64_peak",
+    "thistle_plan_create", "thistle_plan_set_stream", "thistle_plan_set_centres", "thistle_plan_execute",
+    "thistle_plan_execute_device", "thistle_plan_recompute_device", "thistle_plan_execute_quartets",
+    "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
+    "thistle_plan_destroy",
+])
 
 
 class ThistleError(RuntimeError):
@@ -60,6 +61,16 @@ def lib():
     L.thistle_plan_create.argtypes = [
         C.POINTER(VP), C.c_int32, C.c_int32, D, I32, I32, I32, D, D, D, I32, D, C.c_int32, I32, D, C.c_int32,
         D, C.c_int32, D, C.c_int32, C.c_double, C.c_double, C.c_double]
+    L.thistle_probe_fp64_peak.restype = C.c_int
+    L.thistle_probe_fp64_peak.argtypes = [C.c_int32, D]
+    L.thistle_plan_set_stream.restype = C.c_int
+    L.thistle_plan_set_stream.argtypes = [VP, VP]
+    L.thistle_plan_recompute_device.restype = C.c_int
+    L.thistle_plan_recompute_device.argtypes = [VP, VP]
+    L.thistle_plan_class_counts.restype = C.c_int
+    L.thistle_plan_class_counts.argtypes = [VP, I64]
+    L.thistle_plan_stage_totals.restype = C.c_int
+    L.thistle_plan_stage_totals.argtypes = [VP, D, I64]
     L.thistle_plan_set_centres.restype = C.c_int
     L.thistle_plan_set_centres.argtypes = [VP, D, D, D]
     L.thistle_plan_execute.restype = C.c_int

@@ -79,10 +79,41 @@ __device__ __forceinline__ double loop_weight(int loop) {
   return loop == 1 ? 8.0 : (loop <= 3 ? 4.0 : (loop == 4 ? 2.0 : 1.0));
 }
 
+// Simplex layout of D[T][U][V], T+U+V <= L, with V contiguous:
+// idx = ntuv(L) - ntuv(L-T) + U (L-T+1) - U (U-1)/2 + V.
+template <int L>
+__device__ __forceinline__ int dindex(int T, int U, int V) {
+  return ntuv(L) - ntuv(L - T) + U * (L - T + 1) - (U * (U - 1)) / 2 + V;
+}
+
+// Threads that share one quartet: the heavy angular-momentum classes have
+// few quartets and up to ~1e5 Hermite terms each, so their primitive loop is
+// split over S threads whose partial densities are summed in a fixed order.
+TB_HD constexpr int stage1_split(int L) { return L <= 4 ? 1 : (L <= 6 ? 8 : (L <= 15 ? 32 : 16)); }
+
+// Sum over the S lanes of one quartet's thread group (result in its first lane).
+template <int S>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int off = S / 2; off > 0; off >>= 1) v += __shfl_down_sync(mask, v, off, S);
+  return v;
+}
+
 template <int L, int KIND>
-__global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
-  int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void stage1_kernel(Stage1Args A) {
+  // Each thread owns a column of the block's shared array; element k of its
+  // (partial) Hermite density sits at sD[k * blockDim.x + threadIdx.x].
+  constexpr int S = stage1_split(L);
+  extern __shared__ double sD[];
+  const int nthr = blockDim.x;
+  const int sub = threadIdx.x % S;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
+  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
+  // whole groups of S threads leave together (S divides 32); the group's
+  // shuffles and warp syncs use its own lane mask only
   if (qi >= A.qend) return;
+  double *D = sD + threadIdx.x;
   int gi, gj, gk, gr;
   unpack_quartet(A.quartets[qi], gi, gj, gk, gr);
   const double *tb = A.pairtab + (size_t)pair_index(gi, gj, A.ng) * PAIR_STRIDE;
@@ -92,98 +123,147 @@ __global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
   double h = sqrt(Hx * Hx + Hy * Hy + Hz * Hz);
   int loop = quartet_loop(gi, gj, gk, gr);
   bool p0 = loop == 5 || h < A.cutoffcentre;
-  // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp)
-  int skip = p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
+  // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
+  // a skipped factor removes every term it multiplies, i.e. it is a zero.
+  const int skip = p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
 
   constexpr int NT = ntuv(L);
-  double D[NT];
-#pragma unroll
-  for (int i = 0; i < NT; ++i) D[i] = 0.0;
+  for (int k = 0; k < NT; ++k) D[k * nthr] = 0.0;
 
   const int si = A.gstart[gi], ni = A.gcount[gi];
   const int sj = A.gstart[gj], nj = A.gcount[gj];
   const int sk = A.gstart[gk], nk = A.gcount[gk];
   const int sr = A.gstart[gr], nr = A.gcount[gr];
   const double *Eb = tb + 8, *Ek = tk + 8;
-  for (int a = 0; a < ni; ++a) {
-    const int fa = si + a, la = A.flmn[fa];
-    for (int b = 0; b < nj; ++b) {
-      const int fb = sj + b, lb = A.flmn[fb];
-      const int64_t rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-      const double zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
-      const double *ex1 = Eb + 0 * ESZ + ((la & 0xff) * (MAXA + 1) + (lb & 0xff)) * E_T;
-      const double *ey1 = Eb + 1 * ESZ + (((la >> 8) & 0xff) * (MAXA + 1) + ((lb >> 8) & 0xff)) * E_T;
-      const double *ez1 = Eb + 2 * ESZ + (((la >> 16) & 0xff) * (MAXA + 1) + ((lb >> 16) & 0xff)) * E_T;
-      const int nx1 = (la & 0xff) + (lb & 0xff), ny1 = ((la >> 8) & 0xff) + ((lb >> 8) & 0xff);
-      const int nz1 = ((la >> 16) & 0xff) + ((lb >> 16) & 0xff);
-      for (int c = 0; c < nk; ++c) {
-        const int fc = sk + c, lc = A.flmn[fc];
-        for (int d = 0; d < nr; ++d) {
-          const int fd = sr + d, ld = A.flmn[fd];
-          double ztot;
-          if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
-          else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
-          if (fabs(ztot) < A.cutoffz) continue;
-          const double *ex2 = Ek + 0 * ESZ + ((lc & 0xff) * (MAXA + 1) + (ld & 0xff)) * E_T;
-          const double *ey2 = Ek + 1 * ESZ + (((lc >> 8) & 0xff) * (MAXA + 1) + ((ld >> 8) & 0xff)) * E_T;
-          const double *ez2 = Ek + 2 * ESZ + (((lc >> 16) & 0xff) * (MAXA + 1) + ((ld >> 16) & 0xff)) * E_T;
-          const int nx2 = (lc & 0xff) + (ld & 0xff), ny2 = ((lc >> 8) & 0xff) + ((ld >> 8) & 0xff);
-          const int nz2 = ((lc >> 16) & 0xff) + ((ld >> 16) & 0xff);
-          for (int t = 0; t <= nx1; ++t) {
-            double e1 = ex1[t];
-            if ((skip & 1) && fabs(e1) < TB_SKIP30) continue;
-            double p1 = e1 * ztot;
-            for (int u = 0; u <= ny1; ++u) {
-              double e2 = ey1[u];
-              if ((skip & 2) && fabs(e2) < TB_SKIP30) continue;
-              double p2 = e2 * p1;
-              for (int v = 0; v <= nz1; ++v) {
-                double e3 = ez1[v];
-                if ((skip & 4) && fabs(e3) < TB_SKIP30) continue;
-                double p3 = (((t + u + v) & 1) ? -e3 : e3) * p2;
-                for (int t2 = 0; t2 <= nx2; ++t2) {
-                  double e4 = ex2[t2];
-                  if ((skip & 8) && fabs(e4) < TB_SKIP30) continue;
-                  double p4 = e4 * p3;
-                  for (int u2 = 0; u2 <= ny2; ++u2) {
-                    double e5 = ey2[u2];
-                    if ((skip & 16) && fabs(e5) < TB_SKIP30) continue;
-                    double p5 = e5 * p4;
-                    for (int v2 = 0; v2 <= nz2; ++v2) {
-                      double p6 = ez2[v2] * p5;
-                      if (fabs(p6) > A.cutoffmd) D[tuv_index(t + t2, u + u2, v + v2)] += p6;
-                    }
-                  }
-                }
-              }
-            }
-          }
-        }
+  // sum over primitive quartets of ztot * (Cx (x) Cy (x) Cz), C_axis = the
+  // convolution of the bra coefficients (with the (-1)^t sign of
+  // src/Integrals.f90:5181) and the ket coefficients: the six-deep loop of
+  // :5170-5210 with the per-axis sums done first.
+  const int nket = nk * nr, nprim = ni * nj * nket;
+  int cur_ab = -1;
+  double bx[L + 1], by[L + 1], bz[L + 1];
+  int nx1 = 0, ny1 = 0, nz1 = 0;
+  int64_t rowp = 0;
+  double zab = 0.0;
+  for (int pidx = sub; pidx < nprim; pidx += S) {
+    const int ab = pidx / nket, cd = pidx - ab * nket;
+    if (ab != cur_ab) {
+      cur_ab = ab;
+      const int fa = si + ab / nj, fb = sj + ab % nj;
+      const int la = A.flmn[fa], lb = A.flmn[fb];
+      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      const int lx1 = la & 0xff, ly1 = (la >> 8) & 0xff, lz1 = (la >> 16) & 0xff;
+      const int lx2 = lb & 0xff, ly2 = (lb >> 8) & 0xff, lz2 = (lb >> 16) & 0xff;
+      nx1 = lx1 + lx2;
+      ny1 = ly1 + ly2;
+      nz1 = lz1 + lz2;
+      const double *ex = Eb + 0 * ESZ + (lx1 * (MAXA + 1) + lx2) * E_T;
+      const double *ey = Eb + 1 * ESZ + (ly1 * (MAXA + 1) + ly2) * E_T;
+      const double *ez = Eb + 2 * ESZ + (lz1 * (MAXA + 1) + lz2) * E_T;
+#pragma unroll
+      for (int t = 0; t <= L; ++t) {
+        double vx = t <= nx1 ? ex[t] : 0.0, vy = t <= ny1 ? ey[t] : 0.0, vz = t <= nz1 ? ez[t] : 0.0;
+        if ((skip & 1) && fabs(vx) < TB_SKIP30) vx = 0.0;
+        if ((skip & 2) && fabs(vy) < TB_SKIP30) vy = 0.0;
+        if ((skip & 4) && fabs(vz) < TB_SKIP30) vz = 0.0;
+        bx[t] = (t & 1) ? -vx : vx;
+        by[t] = (t & 1) ? -vy : vy;
+        bz[t] = (t & 1) ? -vz : vz;
       }
     }
+    const int fc = sk + cd / nr, fd = sr + cd % nr;
+    double ztot;
+    if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
+    else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+    if (fabs(ztot) < A.cutoffz) continue;
+    const int lc = A.flmn[fc], ld = A.flmn[fd];
+    const int lx3 = lc & 0xff, ly3 = (lc >> 8) & 0xff, lz3 = (lc >> 16) & 0xff;
+    const int lx4 = ld & 0xff, ly4 = (ld >> 8) & 0xff, lz4 = (ld >> 16) & 0xff;
+    const int nx2 = lx3 + lx4, ny2 = ly3 + ly4, nz2 = lz3 + lz4;
+    const double *ex = Ek + 0 * ESZ + (lx3 * (MAXA + 1) + lx4) * E_T;
+    const double *ey = Ek + 1 * ESZ + (ly3 * (MAXA + 1) + ly4) * E_T;
+    const double *ez = Ek + 2 * ESZ + (lz3 * (MAXA + 1) + lz4) * E_T;
+    double cx[L + 1], cy[L + 1], cz[L + 1];
+    const int nx = nx1 + nx2, ny = ny1 + ny2, nz = nz1 + nz2;
+    for (int T = 0; T <= nx; ++T) {
+      double acc = 0.0;
+      for (int t = max(0, T - nx2); t <= min(T, nx1); ++t) {
+        double e = ex[T - t];
+        if ((skip & 8) && fabs(e) < TB_SKIP30) e = 0.0;
+        acc = fma(bx[t], e, acc);
+      }
+      cx[T] = acc * ztot;
+    }
+    for (int U = 0; U <= ny; ++U) {
+      double acc = 0.0;
+      for (int u = max(0, U - ny2); u <= min(U, ny1); ++u) {
+        double e = ey[U - u];
+        if ((skip & 16) && fabs(e) < TB_SKIP30) e = 0.0;
+        acc = fma(by[u], e, acc);
+      }
+      cy[U] = acc;
+    }
+    for (int V = 0; V <= nz; ++V) {
+      double acc = 0.0;
+      for (int v = max(0, V - nz2); v <= min(V, nz1); ++v) acc = fma(bz[v], ez[V - v], acc);
+      cz[V] = acc;
+    }
+    for (int T = 0; T <= nx; ++T) {
+      const int baseT = ntuv(L) - ntuv(L - T);
+      for (int U = 0; U <= ny; ++U) {
+        const double w = cx[T] * cy[U];
+        double *row = D + (baseT + U * (L - T + 1) - (U * (U - 1)) / 2) * nthr;
+        for (int V = 0; V <= nz; ++V) row[V * nthr] = fma(w, cz[V], row[V * nthr]);
+      }
+    }
+  }
+  if (S > 1) {
+    // fixed-order sum of the S partial densities into the group's first column
+    __syncwarp(gmask);
+    const int base = threadIdx.x - sub;
+    for (int k = sub; k < NT; k += S) {
+      double t = 0.0;
+      for (int j = 0; j < S; ++j) t += sD[k * nthr + base + j];
+      sD[k * nthr + base] = t;
+    }
+    __syncwarp(gmask);
+    D = sD + base;
   }
 
   const double pre = loop_weight(loop) * tb[4] * tk[4];
   double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
-  r[1] = tb[5] + tk[5];
+  const bool leader = sub == 0;
   if (p0) {
-    // F(q) = sum_s c_s q^{2s} with c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
+    // F(q) = sum_s c_s q^{2s}, c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
     constexpr int NS = L / 2 + 1;
-    r[0] = 0.0;
-    r[2] = (double)REC_P0;
-    r[3] = (double)(NS - 1);
-    const double fj2 = sqrt(5.0 / TB_PI);
-    for (int s = 0; s < NS; ++s) {
-      double acc = 0.0;
-      for (int T = 0; T <= 2 * s; T += 2)
-        for (int U = 0; U <= 2 * s - T; U += 2) {
-          int V = 2 * s - T - U;
+    double cs[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) cs[k] = 0.0;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k)
+      for (int T = 0; T <= 2 * k; T += 2)
+        for (int U = 0; U <= 2 * k - T; U += 2) {
+          if ((cnt++ % S) != sub) continue;
+          int V = 2 * k - T - U;
           double f = p0_factor(T, U, V, KIND == KIND_J2);
           if (KIND == KIND_J2) f = (T + U - 2 * V) / 4.0 * f;
-          acc += D[tuv_index(T, U, V)] * f;
+          cs[k] += D[dindex<L>(T, U, V) * nthr] * f;
         }
-      if (KIND == KIND_J2) acc *= fj2;
-      r[4 + s] = pre * ((s & 1) ? -acc : acc);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) cs[k] = group_sum<S>(cs[k], gmask);
+    if (!leader) return;
+    atomicAdd(A.p0count, 1ull);
+    const double fj2 = sqrt(5.0 / TB_PI);
+    r[0] = 0.0;
+    r[1] = tb[5] + tk[5];
+    r[2] = (double)REC_P0;
+    r[3] = (double)(NS - 1);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      double acc = KIND == KIND_J2 ? cs[k] * fj2 : cs[k];
+      r[4 + k] = pre * ((k & 1) ? -acc : acc);
     }
     return;
   }
@@ -201,10 +281,12 @@ __global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
 #pragma unroll
   for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
   const double eta = 3.0 * (Hz * Hz) - h * h;
+  int cnt = 0;
   for (int T = 0; T <= L; ++T)
     for (int U = 0; U <= L - T; ++U)
       for (int V = 0; V <= L - T - U; ++V) {
-        double d = D[tuv_index(T, U, V)];
+        if ((cnt++ % S) != sub) continue;
+        double d = D[dindex<L>(T, U, V) * nthr];
         if (d == 0.0) continue;
         for (int k1 = 0; 2 * k1 <= T; ++k1) {
           double cx = ax[tp_off(T) + k1];
@@ -226,6 +308,9 @@ __global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
           }
         }
       }
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) hh[b] = group_sum<S>(hh[b], gmask);
+  if (!leader) return;
   if (KIND == KIND_J2) {
     const double f = 0.25 * sqrt(5.0 / TB_PI);
 #pragma unroll
@@ -242,6 +327,7 @@ __global__ void __launch_bounds__(128) stage1_kernel(Stage1Args A) {
     }
   }
   r[0] = h;
+  r[1] = tb[5] + tk[5];
   r[2] = (double)(KIND == KIND_J2 ? REC_BESSEL_J2 : REC_BESSEL);
   r[3] = (double)LB;
   // hhat_b = h_b / H^{2b}: F = sum_b hhat_b j_b(x) x^b, x = qH
@@ -268,15 +354,15 @@ __device__ __forceinline__ double series_u(double y) {
 }
 
 // F = sum_{b<=LB} hh[b] j_b(x) x^b for x = q H (hh already divided by H^{2b}).
+// F = sum_{b<=LB} hh[b] j_b(x) x^b for x = q H (hh already divided by H^{2b}),
+// given sin x, cos x and 1/x.
 template <int LB>
-__device__ __forceinline__ double bessel_sum(const double *hh, double x) {
-  if (LB == 0) return hh[0] * (sin(x) / x);
+__device__ __forceinline__ double bessel_sum(const double *hh, double x, double sn, double cs, double invx) {
+  if (LB == 0) return hh[0] * (sn * invx);
   const double y = x * x;
   if (x >= bessel_crossover(LB)) {
     // upward: g0 = sin x / x, g1 = g0 - cos x, g_{b+1} = (2b+1) g_b - x^2 g_{b-1}
-    double sn, cs;
-    sincos(x, &sn, &cs);
-    double g0 = sn / x;
+    double g0 = sn * invx;
     double g1 = g0 - cs;
     double F = fma(hh[1], g1, hh[0] * g0);
 #pragma unroll
@@ -304,21 +390,75 @@ __device__ __forceinline__ double bessel_sum(const double *hh, double x) {
   return acc;
 }
 
+// Generic q grids: sincos and exp at every point.
+template <int LB>
+__device__ __forceinline__ void bessel_points_direct(const double *hh, double H, double invH, double s, bool j2,
+                                                     const double *q_s, const double *q2_s, const double *iq_s,
+                                                     double *acc, int i0, int nq) {
+  for (int iq = i0; iq < nq; iq += 32) {
+    double q = q_s[iq], q2 = q2_s[iq];
+    double x = q * H, sn, cs;
+    sincos(x, &sn, &cs);
+    double F = bessel_sum<LB>(hh, x, sn, cs, iq_s[iq] * invH);
+    F *= exp(-q2 * s);
+    if (j2) F *= iq_s[iq] * iq_s[iq];
+    acc[iq] += F;
+  }
+}
+
+// Uniform q grids (q_i = q_first + (i - first) dq): the lane's points are
+// 32 dq apart, so sin/cos advance by a rotation through 32 dq H and the
+// Gaussian exp(-q^2 s) by g *= r, r *= k with r = exp(-(2 q D + D^2) s),
+// k = exp(-2 D^2 s), D = 32 dq; both restart from direct values every 16 steps.
+template <int LB>
+__device__ __forceinline__ void bessel_points_uniform(const double *hh, double H, double invH, double s, bool j2,
+                                                      const double *q_s, const double *iq_s, double dq,
+                                                      double *acc, int i0, int nq) {
+  const double Dq = 32.0 * dq;
+  double sd, cd;
+  sincos(Dq * H, &sd, &cd);
+  const double kk = exp(-2.0 * Dq * Dq * s);
+  int m = 0;
+  double sn = 0, cs = 0, g = 0, r = 0;
+  for (int iq = i0; iq < nq; iq += 32, ++m) {
+    double q = q_s[iq];
+    double x = q * H;
+    if ((m & 15) == 0) {
+      sincos(x, &sn, &cs);
+      g = exp(-(q * q) * s);
+      r = exp(-(2.0 * q * Dq + Dq * Dq) * s);
+    }
+    double F = bessel_sum<LB>(hh, x, sn, cs, iq_s[iq] * invH);
+    F *= g;
+    if (j2) F *= iq_s[iq] * iq_s[iq];
+    acc[iq] += F;
+    double sn2 = fma(sn, cd, cs * sd);
+    cs = fma(cs, cd, -sn * sd);
+    sn = sn2;
+    g *= r;
+    r *= kk;
+  }
+}
+
 template <int LB>
 __device__ __noinline__ void stage2_bessel(const double *__restrict__ c, double H, double s, bool j2,
-                                           const double *q_s, const double *q2_s, const double *iq2_s,
-                                           double *acc, int nq, int lane) {
+                                           const double *q_s, const double *q2_s, const double *iq_s,
+                                           double *acc, int nq, int lane, int uniform, int first_on_grid,
+                                           double dq) {
   double hh[LB + 1];
 #pragma unroll
   for (int b = 0; b <= LB; ++b) hh[b] = c[b];
-  for (int iq = lane; iq < nq; iq += 32) {
-    double q = q_s[iq];
-    double q2 = q2_s[iq];
-    double F = bessel_sum<LB>(hh, q * H);
-    F *= exp(-q2 * s);
-    if (j2) F *= iq2_s[iq];
-    acc[iq] += F;
+  const double invH = 1.0 / H;
+  if (!uniform) {
+    bessel_points_direct<LB>(hh, H, invH, s, j2, q_s, q2_s, iq_s, acc, lane, nq);
+    return;
   }
+  int i0 = lane;
+  if (!first_on_grid && lane == 0) {
+    bessel_points_direct<LB>(hh, H, invH, s, j2, q_s, q2_s, iq_s, acc, 0, 1);
+    i0 = 32;
+  }
+  bessel_points_uniform<LB>(hh, H, invH, s, j2, q_s, iq_s, dq, acc, i0, nq);
 }
 
 __device__ __noinline__ void stage2_p0(const double *__restrict__ c, int ns, double s, const double *q2_s,
@@ -331,14 +471,13 @@ __device__ __noinline__ void stage2_p0(const double *__restrict__ c, int ns, dou
   }
 }
 
-typedef void (*bessel_fn)(const double *, double, double, bool, const double *, const double *,
-                          const double *, double *, int, int);
-
 __device__ __forceinline__ void stage2_dispatch(int LB, const double *c, double H, double s, bool j2,
-                                                const double *q_s, const double *q2_s, const double *iq2_s,
-                                                double *acc, int nq, int lane) {
+                                                const double *q_s, const double *q2_s, const double *iq_s,
+                                                double *acc, int nq, int lane, int uniform, int first_on_grid,
+                                                double dq) {
   switch (LB) {
-#define TB_CASE(n) case n: stage2_bessel<n>(c, H, s, j2, q_s, q2_s, iq2_s, acc, nq, lane); break;
+#define TB_CASE(n) \
+  case n: stage2_bessel<n>(c, H, s, j2, q_s, q2_s, iq_s, acc, nq, lane, uniform, first_on_grid, dq); break;
     TB_CASE(0) TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
     TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE(12) TB_CASE(13) TB_CASE(14)
     TB_CASE(15) TB_CASE(16) TB_CASE(17) TB_CASE(18)
@@ -350,14 +489,14 @@ __device__ __forceinline__ void stage2_dispatch(int LB, const double *c, double 
 __global__ void __launch_bounds__(256) stage2_kernel(Stage2Args A) {
   extern __shared__ double sm[];
   const int nqp = A.nqp;
-  double *q_s = sm, *q2_s = sm + nqp, *iq2_s = sm + 2 * nqp;
+  double *q_s = sm, *q2_s = sm + nqp, *iq_s = sm + 2 * nqp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double *acc = sm + (3 + warp) * nqp;
   for (int i = threadIdx.x; i < A.nq; i += blockDim.x) {
     double q = A.q[i];
     q_s[i] = q;
     q2_s[i] = q * q;
-    iq2_s[i] = 1.0 / pow(q, 2.0);
+    iq_s[i] = 1.0 / q;
   }
   for (int i = threadIdx.x; i < nw * nqp; i += blockDim.x) sm[3 * nqp + i] = 0.0;
   __syncthreads();
@@ -372,7 +511,9 @@ __global__ void __launch_bounds__(256) stage2_kernel(Stage2Args A) {
       double H = r[0], s = r[1];
       int kind = (int)r[2], LB = (int)r[3];
       if (kind == REC_P0) stage2_p0(r + 4, LB + 1, s, q2_s, acc, A.nq, lane);
-      else stage2_dispatch(LB, r + 4, H, s, kind == REC_BESSEL_J2, q_s, q2_s, iq2_s, acc, A.nq, lane);
+      else
+        stage2_dispatch(LB, r + 4, H, s, kind == REC_BESSEL_J2, q_s, q2_s, iq_s, acc, A.nq, lane, A.uniform,
+                        A.first_on_grid, A.dq);
     }
   }
   __syncthreads();
@@ -482,13 +623,32 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
   return cudaGetLastError();
 }
 
+// threads per block so that the Hermite densities of the block fit in 96 KB
+// of shared memory (2 blocks per SM for the large classes)
+static int stage1_threads(int L) {
+  int t = 128;
+  while (t > stage1_split(L) && (size_t)ntuv(L) * sizeof(double) * t > 96 * 1024) t /= 2;
+  return t;
+}
+
+template <int L, int K>
+static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t st) {
+  int thr = stage1_threads(L);
+  size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
+  cudaError_t e = cudaFuncSetAttribute(stage1_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  constexpr int S = stage1_split(L);
+  int64_t threads = n * S;
+  stage1_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <int K>
 static cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st) {
   int64_t n = a.qend - a.qbegin;
   if (n <= 0) return cudaSuccess;
-  unsigned grid = (unsigned)((n + 127) / 128);
   switch (L) {
-#define TB_S1(l) case l: stage1_kernel<l, K><<<grid, 128, 0, st>>>(a); break;
+#define TB_S1(l) case l: return launch_stage1_l<l, K>(a, n, st);
     TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
     TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
 #undef TB_S1

@@ -21,6 +21,7 @@ struct Stage1Args {
   double *rec;                // records: [H, 1/4p+1/4p', kind, order, coefs...]
   int64_t recbase;
   int rs;
+  unsigned long long *p0count; // P=Q quartets counted for this launch's class
 };
 
 constexpr int MAXCLS = 20;
@@ -34,6 +35,9 @@ struct Stage2Args {
   int chunk;
   const double *q;
   int nq, nqp;
+  int uniform;                // q (this tile) is uniform from index 1 with step dq
+  int first_on_grid;          // q[0] lies on that grid too
+  double dq;
   double *partial;            // this q tile's column of a (gridDim.x x pstride) array
   int64_t pstride;
 };

@@ -69,6 +69,7 @@ struct thistle_plan {
   int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nq = 0, maxa = 0, nmat = 0;
   double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
   std::vector<int> gstart, gcount, gL, flmn;
+  std::vector<double> hq;            // host copy of the q grid
   int64_t nquart = 0, np = 0;
   int ncls = 0;
   int cls_L[MAXCLS];
@@ -79,12 +80,30 @@ struct thistle_plan {
   double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr;
   double *d_rho = nullptr, *d_zao = nullptr, *d_rec = nullptr, *d_partial = nullptr, *d_result = nullptr;
   uint64_t *d_quart = nullptr;
+  // device-resident density inputs and transform workspaces
+  int *d_mat = nullptr;
+  double *d_C = nullptr, *d_tot = nullptr, *d_D = nullptr, *d_Ds = nullptr, *d_Y = nullptr;
+  double *d_G = nullptr, *d_T1 = nullptr, *d_T2 = nullptr, *d_V = nullptr, *d_T3 = nullptr;
+  // quartet enumeration workspaces
+  int64_t *d_braoff = nullptr;
+  int *d_gL = nullptr;
+  uint32_t *d_k0 = nullptr, *d_k1 = nullptr;
+  uint64_t *d_v0 = nullptr;
+  void *d_sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+  int64_t *d_p0count = nullptr;      // P=Q quartets per class in the last execution
   int s2_grid = 0, s2_warps = 8, s2_chunk = 4, s2_qtile = 0;
   cudaStream_t st = nullptr;
+  bool own_stream = true;
   cublasHandle_t cb = nullptr;
-  cudaEvent_t ev[8];
+  cudaEvent_t ev[10];
+  // per-execution stage events: slot = execution index mod NRING
+  static const int NRING = 64;
+  cudaEvent_t rev[64][5];
+  int64_t ring_next = 0, ring_base = 0;
   bool have_ev = false;
-  float ms[5] = {0, 0, 0, 0, 0};
+  float ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t launches = 0;              // own kernels launched by the last call
 };
 
 // ---------------------------------------------------------------------------
@@ -224,95 +243,109 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
 // ---------------------------------------------------------------------------
 // rho(ab,cd) = 1/8 sum_t G_t [S12_t(ab) S34_t(cd) + S34_t(ab) S12_t(cd)],
 // S12_t(ab) = C_{m1 a} C_{m2 b} + C_{m1 b} C_{m2 a}: the ztot of
-// src/Integrals.f90:5163 for every primitive pair pair.  With
-// Ghat[x][y][z][w] = G_t/8 summed over the eight placements of each row this is
-// the 4-index transform rho = sum Ghat C_x,a C_y,b C_z,c C_w,d, run as four
-// DGEMM passes: m4 -> d, m3 -> c (pack c<=d), m2 -> b, m1 -> a (pack a<=b).
-static int density_total(thistle_plan *P, const double *mmod, int32_t norbs, const int32_t *mat,
-                         const double *total, int32_t nmat) {
-  const int n = norbs, ngto = P->ngto;
-  const int64_t np = (int64_t)ngto * (ngto + 1) / 2;
-  P->np = np;
-  double *dC = nullptr, *dG = nullptr, *dT1 = nullptr, *dT2 = nullptr, *dV = nullptr, *dT3 = nullptr;
-  int *dmat = nullptr;
-  double *dtot = nullptr;
-  int rc = THISTLE_OK;
-  const double one = 1.0, zero = 0.0;
-  const int64_t n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
-#define TB_TRY(x)             \
-  do {                        \
-    rc = (x);                 \
+// src/Integrals.f90:5163 for every pair of primitive pairs.  With
+// Ghat[x][y][z][w] = G_t/8 summed over the eight placements of each row this
+// is the 4-index transform rho = sum Ghat C_x,a C_y,b C_z,c C_w,d, run as
+// four DGEMM passes: m4 -> d, m3 -> c (pack c<=d), m2 -> b, m1 -> a (a<=b).
+
+#define TB_TRY(x)                    \
+  do {                               \
+    rc = (x);                        \
     if (rc != THISTLE_OK) goto done; \
   } while (0)
-#define TB_TRYC(x)                                                                          \
-  do {                                                                                      \
-    cudaError_t e_ = (x);                                                                   \
-    if (e_ != cudaSuccess) { rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); goto done; } \
+#define TB_TRYC(x)                                                                                        \
+  do {                                                                                                    \
+    cudaError_t e_ = (x);                                                                                 \
+    if (e_ != cudaSuccess) {                                                                              \
+      rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                       \
+      goto done;                                                                                          \
+    }                                                                                                     \
   } while (0)
-#define TB_TRYB(x)                                                                          \
-  do {                                                                                      \
-    cublasStatus_t s_ = (x);                                                                \
-    if (s_ != CUBLAS_STATUS_SUCCESS) { rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); goto done; } \
+#define TB_TRYB(x)                                                                                        \
+  do {                                                                                                    \
+    cublasStatus_t s_ = (x);                                                                              \
+    if (s_ != CUBLAS_STATUS_SUCCESS) {                                                                    \
+      rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_));        \
+      goto done;                                                                                          \
+    }                                                                                                     \
   } while (0)
-  TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
-  TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
-  if (nmat == 0) goto done;
-  TB_TRY(dalloc(&dC, (size_t)n * ngto, "MO coefficients"));
-  TB_TRY(dalloc(&dG, (size_t)n4, "Ghat"));
-  TB_TRY(dalloc(&dmat, (size_t)nmat * 4, "2-RDM indices"));
-  TB_TRY(dalloc(&dtot, (size_t)nmat, "2-RDM values"));
-  TB_TRYC(cudaMemcpyAsync(dC, mmod, sizeof(double) * (size_t)n * ngto, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemcpyAsync(dmat, mat, sizeof(int) * (size_t)nmat * 4, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemcpyAsync(dtot, total, sizeof(double) * (size_t)nmat, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemsetAsync(dG, 0, sizeof(double) * (size_t)n4, P->st));
-  TB_TRYC(launch_ghat_scatter(dmat, dtot, nmat, n, dG, P->st));
-  // T1'(ngto x n^3) = C^T Ghat'   (C is (n, ngto) column-major, the mmod layout)
-  TB_TRY(dalloc(&dT1, (size_t)(n3 * ngto), "transform T1"));
-  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, (int)n3, n, &one, dC, n, dG, n, &zero, dT1, ngto));
-  dfree(dG);
-  // T2[X] (ngto x ngto) = T1[X]' C, X over n^2
-  TB_TRY(dalloc(&dT2, (size_t)(n2 * ngto * ngto), "transform T2"));
-  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, ngto, ngto, n, &one, dT1, ngto,
-                                    (long long)n * ngto, dC, n, 0, &zero, dT2, ngto, (long long)ngto * ngto,
-                                    (int)n2));
-  dfree(dT1);
-  TB_TRY(dalloc(&dV, (size_t)(n2 * np), "transform V"));
-  TB_TRYC(launch_pack_pairs(dT2, n2, ngto, dV, P->st));
-  dfree(dT2);
-  // T3[m1] (np x ngto) = V[m1]' C
-  TB_TRY(dalloc(&dT3, (size_t)((int64_t)n * ngto * np), "transform T3"));
-  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, ngto, n, &one, dV, (int)np,
-                                    (long long)n * np, dC, n, 0, &zero, dT3, (int)np, (long long)ngto * np, n));
-  dfree(dV);
-  // rho rows (a<=b, b fixed): (np x b+1) = T3[:,b,:]' C[:,0..b]
-  for (int b = 0; b < ngto; ++b) {
-    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, b + 1, n, &one, dT3 + (size_t)b * np,
-                        (int)((int64_t)ngto * np), dC, n, &zero, P->d_rho + (size_t)fpair(0, b) * np, (int)np));
+
+static int density_alloc(thistle_plan *P) {
+  int rc = THISTLE_OK;
+  const int n = P->nmo, ngto = P->ngto;
+  const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
+  TB_TRY(dalloc(&P->d_C, (size_t)n * ngto, "MO coefficients"));
+  if (P->kind == KIND_ELASTIC) {
+    TB_TRY(dalloc(&P->d_zao, (size_t)ngto * ngto, "AO density"));
+    TB_TRY(dalloc(&P->d_D, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
+    TB_TRY(dalloc(&P->d_Ds, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
+    TB_TRY(dalloc(&P->d_Y, (size_t)P->nmo1 * ngto, "1-RDM x C"));
+  } else {
+    TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
+    TB_TRY(dalloc(&P->d_mat, (size_t)P->nmat * 4, "2-RDM indices"));
+    TB_TRY(dalloc(&P->d_tot, (size_t)P->nmat, "2-RDM values"));
+    TB_TRY(dalloc(&P->d_G, (size_t)n4, "Ghat"));
+    TB_TRY(dalloc(&P->d_T1, (size_t)(n3 * ngto), "transform T1"));
+    TB_TRY(dalloc(&P->d_T2, (size_t)(n2 * ngto * ngto), "transform T2"));
+    TB_TRY(dalloc(&P->d_V, (size_t)(n2 * np), "transform V"));
+    TB_TRY(dalloc(&P->d_T3, (size_t)((int64_t)n * ngto * np), "transform T3"));
   }
 done:
-  dfree(dC); dfree(dG); dfree(dT1); dfree(dT2); dfree(dV); dfree(dT3); dfree(dmat); dfree(dtot);
   return rc;
 }
 
-// Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217)
-static int density_elastic(thistle_plan *P, const double *mmod, int32_t norbs, const double *onerdm, int32_t nmo1) {
-  const int ngto = P->ngto;
-  double *dC = nullptr, *dD = nullptr, *dDs = nullptr, *dY = nullptr;
+static int density_upload(thistle_plan *P, const double *mmod, const int32_t *mat, const double *total,
+                          const double *onerdm) {
+  TB_CK(cudaMemcpyAsync(P->d_C, mmod, sizeof(double) * (size_t)P->nmo * P->ngto, cudaMemcpyHostToDevice, P->st));
+  if (P->kind == KIND_ELASTIC) {
+    TB_CK(cudaMemcpyAsync(P->d_D, onerdm, sizeof(double) * (size_t)P->nmo1 * P->nmo1, cudaMemcpyHostToDevice,
+                          P->st));
+  } else if (P->nmat > 0) {
+    TB_CK(cudaMemcpyAsync(P->d_mat, mat, sizeof(int) * (size_t)P->nmat * 4, cudaMemcpyHostToDevice, P->st));
+    TB_CK(cudaMemcpyAsync(P->d_tot, total, sizeof(double) * (size_t)P->nmat, cudaMemcpyHostToDevice, P->st));
+  }
+  return THISTLE_OK;
+}
+
+// Pair density (total, j2) or AO density (elastic) from the device-resident inputs.
+static int density_run(thistle_plan *P) {
   int rc = THISTLE_OK;
+  const int n = P->nmo, ngto = P->ngto;
+  const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
   const double one = 1.0, zero = 0.0;
-  TB_TRY(dalloc(&P->d_zao, (size_t)ngto * ngto, "AO density"));
-  TB_TRY(dalloc(&dC, (size_t)norbs * ngto, "MO coefficients"));
-  TB_TRY(dalloc(&dD, (size_t)nmo1 * nmo1, "1-RDM"));
-  TB_TRY(dalloc(&dDs, (size_t)nmo1 * nmo1, "1-RDM"));
-  TB_TRY(dalloc(&dY, (size_t)nmo1 * ngto, "1-RDM x C"));
-  TB_TRYC(cudaMemcpyAsync(dC, mmod, sizeof(double) * (size_t)norbs * ngto, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemcpyAsync(dD, onerdm, sizeof(double) * (size_t)nmo1 * nmo1, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(launch_sym_small(dD, nmo1, dDs, P->st));
-  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, nmo1, ngto, nmo1, &one, dDs, nmo1, dC, norbs, &zero, dY, nmo1));
-  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, ngto, nmo1, &one, dC, norbs, dY, nmo1, &zero,
-                      P->d_zao, ngto));
+  if (P->kind == KIND_ELASTIC) {
+    // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217)
+    const int k = P->nmo1;
+    TB_TRYC(launch_sym_small(P->d_D, k, P->d_Ds, P->st));
+    P->launches += 1;
+    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, k, ngto, k, &one, P->d_Ds, k, P->d_C, n, &zero, P->d_Y, k));
+    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, ngto, k, &one, P->d_C, n, P->d_Y, k, &zero, P->d_zao,
+                        ngto));
+    goto done;
+  }
+  TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
+  if (P->nmat == 0) goto done;
+  TB_TRYC(cudaMemsetAsync(P->d_G, 0, sizeof(double) * (size_t)n4, P->st));
+  TB_TRYC(launch_ghat_scatter(P->d_mat, P->d_tot, P->nmat, n, P->d_G, P->st));
+  P->launches += 1;
+  // T1'(ngto x n^3) = C^T Ghat'   (C is (n, ngto) column-major, the mmod layout)
+  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, (int)n3, n, &one, P->d_C, n, P->d_G, n, &zero, P->d_T1,
+                      ngto));
+  // T2[X] (ngto x ngto) = T1[X]' C, X over n^2
+  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, ngto, ngto, n, &one, P->d_T1, ngto,
+                                    (long long)n * ngto, P->d_C, n, 0, &zero, P->d_T2, ngto, (long long)ngto * ngto,
+                                    (int)n2));
+  TB_TRYC(launch_pack_pairs(P->d_T2, n2, ngto, P->d_V, P->st));
+  P->launches += 1;
+  // T3[m1] (np x ngto) = V[m1]' C
+  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, ngto, n, &one, P->d_V, (int)np,
+                                    (long long)n * np, P->d_C, n, 0, &zero, P->d_T3, (int)np, (long long)ngto * np,
+                                    n));
+  // rho rows (a<=b, b fixed): (np x b+1) = T3[:,b,:]' C[:,0..b]
+  for (int b = 0; b < ngto; ++b)
+    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, b + 1, n, &one, P->d_T3 + (size_t)b * np,
+                        (int)((int64_t)ngto * np), P->d_C, n, &zero, P->d_rho + (size_t)fpair(0, b) * np, (int)np));
 done:
-  dfree(dC); dfree(dD); dfree(dDs); dfree(dY);
   return rc;
 }
 
@@ -321,7 +354,7 @@ done:
 // sort on the class key so that each LLmax class is contiguous and each warp
 // of stage 1 sees quartets with identical loop bounds.
 // ---------------------------------------------------------------------------
-static int build_quartets(thistle_plan *P) {
+static int quartets_alloc(thistle_plan *P) {
   const int ng = P->ng, nb = npairs(ng);
   std::vector<int64_t> off(nb + 1);
   int64_t acc = 0;
@@ -334,27 +367,28 @@ static int build_quartets(thistle_plan *P) {
   if (acc != P->nquart) return fail(THISTLE_ERR_ARG, "internal: quartet count mismatch");
   if (acc >= ((int64_t)1 << 31)) return fail(THISTLE_ERR_ARG, "more than 2^31 group quartets");
   int rc = THISTLE_OK;
-  int64_t *doff = nullptr;
-  int *dgL = nullptr;
-  uint32_t *k0 = nullptr, *k1 = nullptr;
-  uint64_t *v0 = nullptr;
-  void *tmp = nullptr;
-  size_t tmp_bytes = 0;
-  TB_TRY(dalloc(&doff, (size_t)nb + 1, "bra offsets"));
-  TB_TRY(dalloc(&dgL, (size_t)ng, "group L"));
-  TB_TRY(dalloc(&k0, (size_t)acc, "quartet keys"));
-  TB_TRY(dalloc(&k1, (size_t)acc, "quartet keys"));
-  TB_TRY(dalloc(&v0, (size_t)acc, "quartets"));
+  TB_TRY(dalloc(&P->d_braoff, (size_t)nb + 1, "bra offsets"));
+  TB_TRY(dalloc(&P->d_gL, (size_t)ng, "group L"));
+  TB_TRY(dalloc(&P->d_k0, (size_t)acc, "quartet keys"));
+  TB_TRY(dalloc(&P->d_k1, (size_t)acc, "quartet keys"));
+  TB_TRY(dalloc(&P->d_v0, (size_t)acc, "quartets"));
   TB_TRY(dalloc(&P->d_quart, (size_t)acc, "quartets"));
-  TB_TRYC(cudaMemcpyAsync(doff, off.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemcpyAsync(dgL, P->gL.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(launch_quartet_fill(ng, doff, acc, dgL, v0, k0, P->st));
-  TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, P->d_quart, (int)acc, 0, 14, P->st));
-  TB_TRY(dalloc((char **)&tmp, tmp_bytes, "sort scratch"));
-  TB_TRYC(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, P->d_quart, (int)acc, 0, 14, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_braoff, off.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cudaMemcpyAsync(P->d_gL, P->gL.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->sort_tmp_bytes, P->d_k0, P->d_k1, P->d_v0, P->d_quart,
+                                          (int)acc, 0, 14, P->st));
+  TB_TRY(dalloc((char **)&P->d_sort_tmp, P->sort_tmp_bytes, "sort scratch"));
 done:
-  dfree(doff); dfree(dgL); dfree(k0); dfree(k1); dfree(v0);
-  if (tmp) cudaFree(tmp);
+  return rc;
+}
+
+static int quartets_run(thistle_plan *P) {
+  int rc = THISTLE_OK;
+  TB_TRYC(launch_quartet_fill(P->ng, P->d_braoff, P->nquart, P->d_gL, P->d_v0, P->d_k0, P->st));
+  P->launches += 1;
+  TB_TRYC(cub::DeviceRadixSort::SortPairs(P->d_sort_tmp, P->sort_tmp_bytes, P->d_k0, P->d_k1, P->d_v0, P->d_quart,
+                                          (int)P->nquart, 0, 14, P->st));
+done:
   return rc;
 }
 
@@ -366,10 +400,17 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_gstart); dfree(P->d_gcount); dfree(P->d_flmn); dfree(P->d_ga); dfree(P->d_xyz);
   dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
   dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
+  dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
+  dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3);
+  dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
+  if (P->d_sort_tmp) cudaFree(P->d_sort_tmp);
   if (P->cb) cublasDestroy(P->cb);
-  if (P->have_ev)
-    for (int i = 0; i < 8; ++i) cudaEventDestroy(P->ev[i]);
-  if (P->st) cudaStreamDestroy(P->st);
+  if (P->have_ev) {
+    for (int i = 0; i < 10; ++i) cudaEventDestroy(P->ev[i]);
+    for (int r = 0; r < thistle_plan::NRING; ++r)
+      for (int i = 0; i < 5; ++i) cudaEventDestroy(P->rev[r][i]);
+  }
+  if (P->st && P->own_stream) cudaStreamDestroy(P->st);
   delete P;
 }
 
@@ -409,10 +450,12 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   P->type = type;
   P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL : (type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC : KIND_J2);
   P->nq = nq;
+  P->hq.assign(q, q + nq);
   P->nmo = norbs;
   P->cutoffz = cutoffz;
   P->cutoffmd = cutoffmd;
   P->cutoffcentre = cutoffcentre;
+  P->np = (int64_t)ngto * (ngto + 1) / 2;
   if (P->kind == KIND_ELASTIC) {
     if (!onerdm || nmo1 <= 0 || nmo1 > norbs) { rc = fail(THISTLE_ERR_ARG, "1-RDM must be (nmo1,nmo1) with nmo1 <= norbs"); goto done; }
     if (!finite_all(onerdm, (int64_t)nmo1 * nmo1)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 1-RDM"); goto done; }
@@ -430,7 +473,9 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   class_counts(P->gL, cnt);
   TB_TRY(setup_classes(P, cnt, P->kind));
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
-  for (int i = 0; i < 8; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
+  for (int i = 0; i < 10; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
+  for (int r = 0; r < thistle_plan::NRING; ++r)
+    for (int i = 0; i < 5; ++i) TB_TRYC(cudaEventCreate(&P->rev[r][i]));
   P->have_ev = true;
   TB_TRYB(cublasCreate(&P->cb));
   TB_TRYB(cublasSetStream(P->cb, P->st));
@@ -443,23 +488,21 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(dalloc(&P->d_q, (size_t)nq, "q"));
   TB_TRY(dalloc(&P->d_result, (size_t)nq, "result"));
   TB_TRY(dalloc(&P->d_pairtab, (size_t)npairs(P->ng) * PAIR_STRIDE, "pair tables"));
+  TB_TRY(dalloc(&P->d_p0count, (size_t)MAXCLS, "P0 counters"));
   TB_TRYC(cudaMemcpyAsync(P->d_gstart, P->gstart.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_gcount, P->gcount.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_flmn, P->flmn.data(), sizeof(int) * ngto, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_ga, ga, sizeof(double) * ngto, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
   TB_TRY(upload_centres(P, xx, yy, zz));
-  TB_TRYC(cudaEventRecord(P->ev[6], P->st));
-  if (P->kind == KIND_ELASTIC) TB_TRY(density_elastic(P, mmod, norbs, onerdm, nmo1));
-  else TB_TRY(density_total(P, mmod, norbs, mat, total, nmat));
-  TB_TRYC(cudaEventRecord(P->ev[7], P->st));
-  TB_TRY(build_quartets(P));
+  TB_TRY(density_alloc(P));
+  TB_TRY(density_upload(P, mmod, mat, total, onerdm));
+  TB_TRY(quartets_alloc(P));
   TB_TRY(dalloc(&P->d_rec, (size_t)P->rec_total, "quartet records"));
   {
-    int dev = 0, nsm = 0;
+    int dev = 0, nsm = 0, maxsm = 0;
     TB_TRYC(cudaGetDevice(&dev));
     TB_TRYC(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int maxsm = 0;
     TB_TRYC(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     // q tile held in shared memory: (3 + warps) doubles per q point
     P->s2_warps = 8;
@@ -470,11 +513,17 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     P->s2_grid = nsm * bps;
     TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_grid * nq, "partial sums"));
   }
+  P->launches = 0;
+  TB_TRYC(cudaEventRecord(P->ev[6], P->st));
+  TB_TRY(density_run(P));
+  TB_TRYC(cudaEventRecord(P->ev[7], P->st));
+  TB_TRY(quartets_run(P));
+  TB_TRYC(cudaEventRecord(P->ev[8], P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));
   {
     float t = 0;
-    cudaEventElapsedTime(&t, P->ev[6], P->ev[7]);
-    P->ms[4] = t;
+    if (cudaEventElapsedTime(&t, P->ev[6], P->ev[7]) == cudaSuccess) P->ms[4] = t;
+    if (cudaEventElapsedTime(&t, P->ev[7], P->ev[8]) == cudaSuccess) P->ms[5] = t;
   }
 done:
   if (rc != THISTLE_OK) {
@@ -485,12 +534,33 @@ done:
   return THISTLE_OK;
 }
 
+// A tile q[0..n) is "uniform" when q[1..n) is an arithmetic progression to
+// within 2e-14 of its largest value; q[0] may sit off it (the drivers put
+// 1e-10 where the grid starts at 0).
+static void grid_info(const double *q, int n, int &uniform, int &first_on_grid, double &dq) {
+  uniform = 0;
+  first_on_grid = 0;
+  dq = 0.0;
+  if (n < 4) return;
+  dq = (q[n - 1] - q[1]) / (double)(n - 2);
+  if (!(dq > 0.0)) return;
+  double tol = 2e-14 * std::max(std::fabs(q[n - 1]), std::fabs(q[1]));
+  for (int i = 1; i < n; ++i)
+    if (std::fabs(q[i] - (q[1] + (double)(i - 1) * dq)) > tol) return;
+  uniform = 1;
+  first_on_grid = std::fabs(q[0] - (q[1] - dq)) <= tol ? 1 : 0;
+}
+
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
                       double *d_out) {
-  TB_CK(cudaEventRecord(P->ev[0], P->st));
+  cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
+  P->ring_next += 1;
+  TB_CK(cudaEventRecord(E[0], P->st));
   TB_CK(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->st));
-  TB_CK(cudaEventRecord(P->ev[1], P->st));
+  P->launches += 1;
+  TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS, P->st));
+  TB_CK(cudaEventRecord(E[1], P->st));
   for (int c = 0; c < ncls; ++c) {
     Stage1Args a;
     a.quartets = d_quart;
@@ -511,9 +581,11 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.rec = d_rec;
     a.recbase = recoff[c];
     a.rs = rs[c];
+    a.p0count = (unsigned long long *)(P->d_p0count + c);
     TB_CK(launch_stage1(P->kind, cL[c], a, P->st));
+    P->launches += 1;
   }
-  TB_CK(cudaEventRecord(P->ev[2], P->st));
+  TB_CK(cudaEventRecord(E[2], P->st));
   int64_t nq_all = 0;
   for (int c = 0; c < ncls; ++c) nq_all = std::max(nq_all, ce[c]);
   for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
@@ -533,11 +605,14 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     s.nqp = P->s2_qtile;
     s.partial = P->d_partial + q0;
     s.pstride = P->nq;
+    grid_info(P->hq.data() + q0, s.nq, s.uniform, s.first_on_grid, s.dq);
     TB_CK(launch_stage2(s, P->s2_grid, P->s2_warps, P->st));
+    P->launches += 1;
   }
-  TB_CK(cudaEventRecord(P->ev[3], P->st));
+  TB_CK(cudaEventRecord(E[3], P->st));
   TB_CK(launch_reduce(P->d_partial, P->s2_grid, P->nq, d_out, P->st));
-  TB_CK(cudaEventRecord(P->ev[4], P->st));
+  P->launches += 1;
+  TB_CK(cudaEventRecord(E[4], P->st));
   return THISTLE_OK;
 }
 
@@ -547,9 +622,11 @@ static int plan_exec(thistle_plan *P, double *d_out) {
 }
 
 static void read_timings(thistle_plan *P) {
+  if (P->ring_next == 0) return;
+  cudaEvent_t *E = P->rev[(P->ring_next - 1) % thistle_plan::NRING];
   for (int i = 0; i < 4; ++i) {
     float t = 0;
-    if (cudaEventElapsedTime(&t, P->ev[i], P->ev[i + 1]) == cudaSuccess) P->ms[i] = t;
+    if (cudaEventElapsedTime(&t, E[i], E[i + 1]) == cudaSuccess) P->ms[i] = t;
   }
 }
 
@@ -571,6 +648,16 @@ int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const d
                      q, nq, cutoffz, cutoffmd, cutoffcentre);
 }
 
+int thistle_plan_set_stream(thistle_plan *P, void *stream) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  TB_CK(cudaStreamSynchronize(P->st));
+  if (P->own_stream) cudaStreamDestroy(P->st);
+  P->st = (cudaStream_t)stream;
+  P->own_stream = false;
+  TB_CB(cublasSetStream(P->cb, P->st));
+  return THISTLE_OK;
+}
+
 int thistle_plan_set_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
   if (!P || !xx || !yy || !zz) return fail(THISTLE_ERR_ARG, "null argument");
   if (!finite_all(xx, P->ngto) || !finite_all(yy, P->ngto) || !finite_all(zz, P->ngto))
@@ -586,11 +673,26 @@ int thistle_plan_set_centres(thistle_plan *P, const double *xx, const double *yy
 
 int thistle_plan_execute_device(thistle_plan *P, double *result_dev) {
   if (!P || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  return plan_exec(P, result_dev);
+}
+
+int thistle_plan_recompute_device(thistle_plan *P, double *result_dev) {
+  if (!P || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  TB_CK(cudaEventRecord(P->ev[6], P->st));
+  int rc = density_run(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaEventRecord(P->ev[7], P->st));
+  rc = quartets_run(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaEventRecord(P->ev[8], P->st));
   return plan_exec(P, result_dev);
 }
 
 int thistle_plan_execute(thistle_plan *P, double *result_host) {
   if (!P || !result_host) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
   int rc = plan_exec(P, P->d_result);
   if (rc != THISTLE_OK) return rc;
   TB_CK(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
@@ -632,6 +734,7 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
   uint64_t *dq = nullptr;
   double *drec = nullptr;
   int rc = THISTLE_OK;
+  P->launches = 0;
   TB_TRY(dalloc(&dq, (size_t)nquart, "quartet list"));
   TB_TRY(dalloc(&drec, (size_t)roff, "quartet records"));
   TB_TRYC(cudaMemcpyAsync(dq, packed.data(), sizeof(uint64_t) * nquart, cudaMemcpyHostToDevice, P->st));
@@ -651,16 +754,48 @@ done:
 int thistle_plan_info(const thistle_plan *P, int64_t *info) {
   if (!P || !info) return fail(THISTLE_ERR_ARG, "null argument");
   info[0] = P->nquart;
-  info[1] = 0;
+  info[1] = P->ncls;
   info[2] = P->ng;
   info[3] = P->ngto;
   info[4] = P->nq;
+  info[5] = P->launches;
+  return THISTLE_OK;
+}
+
+int thistle_plan_class_counts(const thistle_plan *P, int64_t *out) {
+  if (!P || !out) return fail(THISTLE_ERR_ARG, "null argument");
+  int64_t p0[MAXCLS] = {0};
+  TB_CK(cudaMemcpy(p0, P->d_p0count, sizeof(int64_t) * MAXCLS, cudaMemcpyDeviceToHost));
+  for (int i = 0; i <= LMAXQ; ++i) { out[3 * i] = i; out[3 * i + 1] = 0; out[3 * i + 2] = 0; }
+  for (int c = 0; c < P->ncls; ++c) {
+    out[3 * P->cls_L[c] + 1] = P->cls_end[c] - P->cls_begin[c];
+    out[3 * P->cls_L[c] + 2] = p0[c];
+  }
+  return THISTLE_OK;
+}
+
+int thistle_plan_stage_totals(thistle_plan *P, double *ms4, int64_t *nexec) {
+  if (!P || !ms4 || !nexec) return fail(THISTLE_ERR_ARG, "null argument");
+  TB_CK(cudaStreamSynchronize(P->st));
+  for (int i = 0; i < 4; ++i) ms4[i] = 0.0;
+  int64_t first = std::max(P->ring_base, P->ring_next - thistle_plan::NRING);
+  for (int64_t k = first; k < P->ring_next; ++k) {
+    cudaEvent_t *E = P->rev[k % thistle_plan::NRING];
+    for (int i = 0; i < 4; ++i) {
+      float t = 0;
+      TB_CK(cudaEventElapsedTime(&t, E[i], E[i + 1]));
+      ms4[i] += t;
+    }
+  }
+  *nexec = P->ring_next - first;
+  P->ring_base = P->ring_next;
+  read_timings(P);
   return THISTLE_OK;
 }
 
 int thistle_plan_timings(const thistle_plan *P, double *ms) {
   if (!P || !ms) return fail(THISTLE_ERR_ARG, "null argument");
-  for (int i = 0; i < 5; ++i) ms[i] = P->ms[i];
+  for (int i = 0; i < 6; ++i) ms[i] = P->ms[i];
   return THISTLE_OK;
 }
 

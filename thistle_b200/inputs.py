@@ -297,16 +297,18 @@ def _ab6_shells():
             + [(2, 0.6)])
 
 
-def config3_ab6(nq: int = 500) -> Problem:
+def config3_ab6(nq: int = 500, natoms: int = 7) -> Problem:
     """Octahedral AB6 (S-F 2.95 bohr); per atom s(8, 0.1-1e5), p(5, 0.15-200),
     d(1, 0.6); 40 MOs; 5 % nonzero sparse PSD 2-RDM, trace N(N-1), N = 70;
-    q = 0..15 (500 points)."""
+    q = 0..15 (500 points).  ``natoms < 7`` keeps the first atoms only (a
+    smaller case of the same basis, for profiling)."""
     rng = np.random.default_rng(SEED0 + 3)
     r = 2.95
     atoms = np.array([[0, 0, 0], [r, 0, 0], [-r, 0, 0], [0, r, 0], [0, -r, 0], [0, 0, r], [0, 0, -r]],
-                     dtype=float)
-    shells = [_ab6_shells() for _ in range(7)]
-    return _problem("ab6", atoms, shells, 40, 70, q_grid(15.0, nq), rng, density=0.05)
+                     dtype=float)[:natoms]
+    shells = [_ab6_shells() for _ in range(natoms)]
+    name = "ab6" if natoms == 7 else f"ab6_{natoms}atom"
+    return _problem(name, atoms, shells, 40, 70, q_grid(15.0, nq), rng, density=0.05)
 
 
 def hexagon(radius: float = 2.64) -> np.ndarray:

@@ -142,7 +142,23 @@ class ScatteringPlan:
         return out
 
     def execute_device(self, ptr: int):
+        """Integrator only, I(q) to the device address ``ptr`` (stream-ordered)."""
         check(_abi.lib().thistle_plan_execute_device(self._p, C.c_void_p(ptr)))
+
+    def recompute_device(self, ptr: int):
+        """Density transform + quartet enumeration + integrator from the
+        device-resident inputs, I(q) to the device address ``ptr``."""
+        check(_abi.lib().thistle_plan_recompute_device(self._p, C.c_void_p(ptr)))
+
+    def set_stream(self, stream_handle: int):
+        """Use a caller-owned CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        check(_abi.lib().thistle_plan_set_stream(self._p, C.c_void_p(stream_handle)))
+
+    def class_counts(self):
+        a = np.zeros(51, dtype=np.int64)
+        check(_abi.lib().thistle_plan_class_counts(self._p, a.ctypes.data_as(_abi.I64)))
+        a = a.reshape(17, 3)
+        return {int(L): (int(n), int(p0)) for L, n, p0 in a if n}
 
     def execute_quartets(self, quartets):
         qt = np.ascontiguousarray(np.asarray(quartets, dtype=np.int32).reshape(-1, 4))
@@ -151,14 +167,22 @@ class ScatteringPlan:
         return out
 
     def info(self):
-        a = np.zeros(5, dtype=np.int64)
+        a = np.zeros(6, dtype=np.int64)
         check(_abi.lib().thistle_plan_info(self._p, a.ctypes.data_as(_abi.I64)))
-        return dict(nquart=int(a[0]), ng=int(a[2]), ngto=int(a[3]), nq=int(a[4]))
+        return dict(nquart=int(a[0]), nclasses=int(a[1]), ng=int(a[2]), ngto=int(a[3]), nq=int(a[4]),
+                    launches=int(a[5]))
 
     def timings(self):
-        a = np.zeros(5)
+        a = np.zeros(6)
         check(_abi.lib().thistle_plan_timings(self._p, dptr(a)))
-        return dict(pair_tables=a[0], stage1=a[1], stage2=a[2], reduce=a[3], transform=a[4])
+        return dict(pair_tables=a[0], stage1=a[1], stage2=a[2], reduce=a[3], transform=a[4], quartets=a[5])
+
+    def stage_totals(self):
+        """Summed device ms per stage over the executions since the last call."""
+        a = np.zeros(4)
+        n = np.zeros(1, dtype=np.int64)
+        check(_abi.lib().thistle_plan_stage_totals(self._p, dptr(a), n.ctypes.data_as(_abi.I64)))
+        return dict(pair_tables=a[0], stage1=a[1], stage2=a[2], reduce=a[3], executions=int(n[0]))
 
     def close(self):
         if self._p:
