@@ -122,6 +122,15 @@ int thistle_plan_timings(const thistle_plan *plan, double *ms6);
  * ([0] pair tables, [1] stage 1, [2] stage 2, [3] reduce) over the executions
  * since the previous call (at most the last 64); *nexec gets their number. */
 int thistle_plan_stage_totals(thistle_plan *plan, double *ms4, int64_t *nexec);
+/* The stage-1 records of the last execution and the q grid, in device memory
+ * owned by the plan (valid until its next execution or destroy).  Per LLmax
+ * class c < *ncls (at most 20 classes; the arrays need that room): quartets
+ * [cls_begin[c], cls_end[c]) in class order, their records at cls_recoff[c]
+ * doubles with stride cls_rs[c].  A record is [H, 1/4p+1/4p', kind (0 Bessel
+ * j0, 1 Bessel j2, 2 P=Q polynomial in q^2), order, coefficients...]. */
+int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32_t *ncls,
+                         int64_t *cls_begin, int64_t *cls_end, int64_t *cls_recoff,
+                         int32_t *cls_rs, const double **q_dev);
 int thistle_plan_destroy(thistle_plan *plan);
 
 #ifdef __cplusplus

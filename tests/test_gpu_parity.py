@@ -158,3 +158,14 @@ def test_large_q_tiles():
         got = pl.execute()
     ref = MC.scattering(p, 1, q=q[::7])
     assert np.max(rel_err(got[::7], ref)) < 1e-13
+
+
+def test_plan_records_describe_the_quartets():
+    p = I.config1_h2()
+    with MC.ScatteringPlan.from_problem(p) as pl:
+        pl.execute()
+        r = pl.records()
+        assert r["rec"] and r["q"]
+        assert r["begin"][0] == 0 and r["end"][-1] == pl.info()["nquart"]
+        assert np.all(r["begin"][1:] == r["end"][:-1])
+        assert np.all(r["rs"] % 2 == 0)

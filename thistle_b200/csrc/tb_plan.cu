@@ -751,6 +751,22 @@ done:
   return rc;
 }
 
+int thistle_plan_records(const thistle_plan *P, const double **rec_dev, int32_t *ncls, int64_t *cls_begin,
+                         int64_t *cls_end, int64_t *cls_recoff, int32_t *cls_rs, const double **q_dev) {
+  if (!P || !rec_dev || !ncls || !cls_begin || !cls_end || !cls_recoff || !cls_rs || !q_dev)
+    return fail(THISTLE_ERR_ARG, "null argument");
+  *rec_dev = P->d_rec;
+  *q_dev = P->d_q;
+  *ncls = P->ncls;
+  for (int c = 0; c < P->ncls; ++c) {
+    cls_begin[c] = P->cls_begin[c];
+    cls_end[c] = P->cls_end[c];
+    cls_recoff[c] = P->cls_recoff[c];
+    cls_rs[c] = P->cls_rs[c];
+  }
+  return THISTLE_OK;
+}
+
 int thistle_plan_info(const thistle_plan *P, int64_t *info) {
   if (!P || !info) return fail(THISTLE_ERR_ARG, "null argument");
   info[0] = P->nquart;

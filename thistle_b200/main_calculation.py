@@ -177,6 +177,21 @@ class ScatteringPlan:
         check(_abi.lib().thistle_plan_timings(self._p, dptr(a)))
         return dict(pair_tables=a[0], stage1=a[1], stage2=a[2], reduce=a[3], transform=a[4], quartets=a[5])
 
+    def records(self):
+        """Device address of the last execution's stage-1 records, the class
+        table (begin, end, record offset, stride per LLmax class) and the
+        device address of the q grid."""
+        rec, qd = C.c_void_p(), C.c_void_p()
+        n = np.zeros(1, dtype=np.int32)
+        b, e, o = (np.zeros(20, dtype=np.int64) for _ in range(3))
+        rs = np.zeros(20, dtype=np.int32)
+        check(_abi.lib().thistle_plan_records(self._p, C.byref(rec), iptr(n), b.ctypes.data_as(_abi.I64),
+                                              e.ctypes.data_as(_abi.I64), o.ctypes.data_as(_abi.I64),
+                                              iptr(rs), C.byref(qd)))
+        k = int(n[0])
+        return dict(rec=rec.value, q=qd.value, ncls=k, begin=b[:k].copy(), end=e[:k].copy(),
+                    recoff=o[:k].copy(), rs=rs[:k].copy())
+
     def stage_totals(self):
         """Summed device ms per stage over the executions since the last call."""
         a = np.zeros(4)
