@@ -133,6 +133,27 @@ int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32
                          int32_t *cls_rs, const double **q_dev);
 int thistle_plan_destroy(thistle_plan *plan);
 
+/*
+ * Stage 2 without any device allocation.  No counterpart in the reference
+ * (whose integrators allocate freely on the host).  For callers that cannot
+ * call cudaMalloc when they evaluate -- a host application that hands this
+ * library device buffers and forbids allocations, or one that has already
+ * given all device memory to its own pool -- this evaluates the Bessel sum of
+ * stage-1 records the caller already holds (thistle_plan_records layout) on
+ * the caller's q grid and writes nq doubles of I(q) to result_dev, on `stream`.
+ * Its scratch is a fixed 2.4 MB array inside the library (296 blocks x 1024 q
+ * points), so nq is limited to 1024 per call; larger nq is rejected with
+ * THISTLE_ERR_ARG.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture.  All calls on a device share the array and it
+ * keeps the last call's contents: calls that overlap on the GPU (different
+ * streams, or threads) race and must be serialised by the caller.
+ */
+int thistle_bessel_sum_static(const double *rec_dev, int32_t ncls, const int64_t *cls_begin,
+                              const int64_t *cls_end, const int64_t *cls_recoff,
+                              const int32_t *cls_rs, const double *q_dev, int32_t nq,
+                              double *result_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,7 @@ EXPORTS = sorted([
     "thistle_plan_create", "thistle_plan_set_stream", "thistle_plan_set_centres", "thistle_plan_execute",
     "thistle_plan_execute_device", "thistle_plan_recompute_device", "thistle_plan_execute_quartets",
     "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
-    "thistle_plan_destroy", "thistle_plan_records",
+    "thistle_plan_destroy", "thistle_plan_records", "thistle_bessel_sum_static",
 ])
 
 
@@ -73,6 +73,8 @@ def lib():
     L.thistle_plan_stage_totals.argtypes = [VP, D, I64]
     L.thistle_plan_records.restype = C.c_int
     L.thistle_plan_records.argtypes = [VP, C.POINTER(VP), I32, I64, I64, I64, I32, C.POINTER(VP)]
+    L.thistle_bessel_sum_static.restype = C.c_int
+    L.thistle_bessel_sum_static.argtypes = [VP, C.c_int32, I64, I64, I64, I32, VP, C.c_int32, VP, VP]
     L.thistle_plan_set_centres.restype = C.c_int
     L.thistle_plan_set_centres.argtypes = [VP, D, D, D]
     L.thistle_plan_execute.restype = C.c_int

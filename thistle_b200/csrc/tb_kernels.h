@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 namespace tb {
 
 struct Stage1Args {
@@ -41,6 +43,9 @@ struct Stage2Args {
   double *partial;            // this q tile's column of a (gridDim.x x pstride) array
   int64_t pstride;
 };
+
+// Sets the calling thread's error string (thistle_last_error_string) and returns code.
+int set_error(int code, const std::string &msg);
 
 cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
                                const double *xyz, double *tab, cudaStream_t st);

@@ -32,6 +32,10 @@ static int fail(int code, const std::string &msg) {
   return code;
 }
 
+namespace tb {
+int set_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace tb
+
 #define TB_CK(x)                                                                            \
   do {                                                                                      \
     cudaError_t e_ = (x);                                                                   \
