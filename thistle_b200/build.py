@@ -53,16 +53,24 @@ def build(verbose: bool = False, force: bool = False, extra=None) -> str:
         common += list(extra)
     headers = [d for d in deps() if not d.endswith(".cu")]
     newest_header = max(os.path.getmtime(h) for h in headers)
+    todo = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= newest_header):
             continue
-        cmd = common + ["-c", src, "-o", obj]
+        todo.append(common + ["-c", src, "-o", obj])
+    # one nvcc per translation unit, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        procs = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), todo))
+    for cmd, pr in zip(todo, procs):
         if verbose:
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
+            print(pr.stdout + pr.stderr)
+        if pr.returncode != 0:
+            raise RuntimeError("nvcc failed: " + " ".join(cmd) + "\n" + pr.stdout + pr.stderr)
     cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lcublas"]
     if verbose:
         print(" ".join(cmd))

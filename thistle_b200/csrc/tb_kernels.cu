@@ -2,9 +2,7 @@
 //
 //  tb_pair_tables   Gaussian-product tables per unordered group pair
 //                   (src/Variables.f90:1113-1148 and fill_md_table :8-946)
-//  tb_stage1<L,K>   per group quartet: Hermite density and Bessel / P0
-//                   coefficients (tot_integral_k_ijkr :5068-5226, the pzero
-//                   kernels :4751-5067, their j2 and elastic variants)
+//  (stage 1, per group quartet: tb_stage1.cuh, one translation unit per kind)
 //  tb_stage2        the quartet x q Bessel sum (bessels0rr :6662-6739 with an
 //                   accurate generator), warp per quartet, lanes over q,
 //                   accumulated per warp in shared memory
@@ -23,11 +21,22 @@ namespace tb {
 // ---------------------------------------------------------------------------
 // pair tables
 // ---------------------------------------------------------------------------
+int64_t esoa_doubles(int ng, int maxa) {
+  return 2 * (int64_t)3 * (maxa + 1) * (maxa + 1) * E_T * npairs(ng);
+}
+
+// One thread per unordered group pair.  Besides the pair record it writes the
+// transposed E table: element t of (axis, la, lb) at
+// esoa[((axis (maxa+1) + la) (maxa+1) + lb) E_T + t][pair], zero for
+// t > la + lb, and a second copy with |E| < 1e-30 set to zero (the MD skips).
 __global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gstart,
                                    const int *__restrict__ flmn, const double *__restrict__ ga,
-                                   const double *__restrict__ xyz, double *__restrict__ tab) {
+                                   const double *__restrict__ xyz, double *__restrict__ tab,
+                                   double *__restrict__ esoa) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npairs(ng)) return;
+  const int64_t npair = npairs(ng);
+  if (p >= npair) return;
+  const int64_t skipoff = (int64_t)3 * (maxa + 1) * (maxa + 1) * E_T * npair;
   int i = 0, rem = p;
   while (rem >= ng - i) { rem -= ng - i; ++i; }
   int j = i + rem;
@@ -51,6 +60,12 @@ __global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gst
         if (la >= lb) md_chain(la, lb, PA, PB, a, E);
         else md_chain(lb, la, PB, PA, a, E);
         for (int tt = 0; tt <= la + lb; ++tt) dst[(la * (MAXA + 1) + lb) * E_T + tt] = E[tt];
+        const int64_t slot = ((int64_t)(ax * (maxa + 1) + la) * (maxa + 1) + lb) * E_T;
+        for (int tt = 0; tt < E_T; ++tt) {
+          double v = tt <= la + lb ? E[tt] : 0.0;
+          esoa[(slot + tt) * npair + p] = v;
+          esoa[skipoff + (slot + tt) * npair + p] = fabs(v) < TB_SKIP30 ? 0.0 : v;
+        }
       }
   }
   t[3] = gaP;
@@ -58,286 +73,6 @@ __global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gst
   t[5] = 0.25 / gaP;
   t[6] = 0.0;
   t[7] = 0.0;
-}
-
-// ---------------------------------------------------------------------------
-// stage 1: Hermite density and expansion coefficients, one thread per quartet
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void unpack_quartet(uint64_t pk, int &gi, int &gj, int &gk, int &gr) {
-  gi = (int)(pk & 0xffff);
-  gj = (int)((pk >> 16) & 0xffff);
-  gk = (int)((pk >> 32) & 0xffff);
-  gr = (int)((pk >> 48) & 0xffff);
-}
-
-// The five loops of tot_integration give these weights (src/Integrals.f90:158,243,325,402,462).
-__device__ __forceinline__ int quartet_loop(int gi, int gj, int gk, int gr) {
-  if (gi == gj) return gk == gr ? (gi == gk ? 5 : 4) : 3;
-  return gk == gi ? 2 : 1;
-}
-__device__ __forceinline__ double loop_weight(int loop) {
-  return loop == 1 ? 8.0 : (loop <= 3 ? 4.0 : (loop == 4 ? 2.0 : 1.0));
-}
-
-// Simplex layout of D[T][U][V], T+U+V <= L, with V contiguous:
-// idx = ntuv(L) - ntuv(L-T) + U (L-T+1) - U (U-1)/2 + V.
-template <int L>
-__device__ __forceinline__ int dindex(int T, int U, int V) {
-  return ntuv(L) - ntuv(L - T) + U * (L - T + 1) - (U * (U - 1)) / 2 + V;
-}
-
-// Threads that share one quartet: the heavy angular-momentum classes have
-// few quartets and up to ~1e5 Hermite terms each, so their primitive loop is
-// split over S threads whose partial densities are summed in a fixed order.
-TB_HD constexpr int stage1_split(int L) { return L <= 4 ? 1 : (L <= 6 ? 8 : (L <= 15 ? 32 : 16)); }
-
-// Sum over the S lanes of one quartet's thread group (result in its first lane).
-template <int S>
-__device__ __forceinline__ double group_sum(double v, unsigned mask) {
-#pragma unroll
-  for (int off = S / 2; off > 0; off >>= 1) v += __shfl_down_sync(mask, v, off, S);
-  return v;
-}
-
-template <int L, int KIND>
-__global__ void stage1_kernel(Stage1Args A) {
-  // Each thread owns a column of the block's shared array; element k of its
-  // (partial) Hermite density sits at sD[k * blockDim.x + threadIdx.x].
-  constexpr int S = stage1_split(L);
-  extern __shared__ double sD[];
-  const int nthr = blockDim.x;
-  const int sub = threadIdx.x % S;
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
-  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
-  // whole groups of S threads leave together (S divides 32); the group's
-  // shuffles and warp syncs use its own lane mask only
-  if (qi >= A.qend) return;
-  double *D = sD + threadIdx.x;
-  int gi, gj, gk, gr;
-  unpack_quartet(A.quartets[qi], gi, gj, gk, gr);
-  const double *tb = A.pairtab + (size_t)pair_index(gi, gj, A.ng) * PAIR_STRIDE;
-  const double *tk = A.pairtab + (size_t)pair_index(gk, gr, A.ng) * PAIR_STRIDE;
-  // hx = px(k,r) - px(i,j)  (src/Integrals.f90:83-86)
-  double Hx = tk[0] - tb[0], Hy = tk[1] - tb[1], Hz = tk[2] - tb[2];
-  double h = sqrt(Hx * Hx + Hy * Hy + Hz * Hz);
-  int loop = quartet_loop(gi, gj, gk, gr);
-  bool p0 = loop == 5 || h < A.cutoffcentre;
-  // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
-  // a skipped factor removes every term it multiplies, i.e. it is a zero.
-  const int skip = p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
-
-  constexpr int NT = ntuv(L);
-  for (int k = 0; k < NT; ++k) D[k * nthr] = 0.0;
-
-  const int si = A.gstart[gi], ni = A.gcount[gi];
-  const int sj = A.gstart[gj], nj = A.gcount[gj];
-  const int sk = A.gstart[gk], nk = A.gcount[gk];
-  const int sr = A.gstart[gr], nr = A.gcount[gr];
-  const double *Eb = tb + 8, *Ek = tk + 8;
-  // sum over primitive quartets of ztot * (Cx (x) Cy (x) Cz), C_axis = the
-  // convolution of the bra coefficients (with the (-1)^t sign of
-  // src/Integrals.f90:5181) and the ket coefficients: the six-deep loop of
-  // :5170-5210 with the per-axis sums done first.
-  const int nket = nk * nr, nprim = ni * nj * nket;
-  int cur_ab = -1;
-  double bx[L + 1], by[L + 1], bz[L + 1];
-  int nx1 = 0, ny1 = 0, nz1 = 0;
-  int64_t rowp = 0;
-  double zab = 0.0;
-  for (int pidx = sub; pidx < nprim; pidx += S) {
-    const int ab = pidx / nket, cd = pidx - ab * nket;
-    if (ab != cur_ab) {
-      cur_ab = ab;
-      const int fa = si + ab / nj, fb = sj + ab % nj;
-      const int la = A.flmn[fa], lb = A.flmn[fb];
-      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-      zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
-      const int lx1 = la & 0xff, ly1 = (la >> 8) & 0xff, lz1 = (la >> 16) & 0xff;
-      const int lx2 = lb & 0xff, ly2 = (lb >> 8) & 0xff, lz2 = (lb >> 16) & 0xff;
-      nx1 = lx1 + lx2;
-      ny1 = ly1 + ly2;
-      nz1 = lz1 + lz2;
-      const double *ex = Eb + 0 * ESZ + (lx1 * (MAXA + 1) + lx2) * E_T;
-      const double *ey = Eb + 1 * ESZ + (ly1 * (MAXA + 1) + ly2) * E_T;
-      const double *ez = Eb + 2 * ESZ + (lz1 * (MAXA + 1) + lz2) * E_T;
-#pragma unroll
-      for (int t = 0; t <= L; ++t) {
-        double vx = t <= nx1 ? ex[t] : 0.0, vy = t <= ny1 ? ey[t] : 0.0, vz = t <= nz1 ? ez[t] : 0.0;
-        if ((skip & 1) && fabs(vx) < TB_SKIP30) vx = 0.0;
-        if ((skip & 2) && fabs(vy) < TB_SKIP30) vy = 0.0;
-        if ((skip & 4) && fabs(vz) < TB_SKIP30) vz = 0.0;
-        bx[t] = (t & 1) ? -vx : vx;
-        by[t] = (t & 1) ? -vy : vy;
-        bz[t] = (t & 1) ? -vz : vz;
-      }
-    }
-    const int fc = sk + cd / nr, fd = sr + cd % nr;
-    double ztot;
-    if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
-    else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
-    if (fabs(ztot) < A.cutoffz) continue;
-    const int lc = A.flmn[fc], ld = A.flmn[fd];
-    const int lx3 = lc & 0xff, ly3 = (lc >> 8) & 0xff, lz3 = (lc >> 16) & 0xff;
-    const int lx4 = ld & 0xff, ly4 = (ld >> 8) & 0xff, lz4 = (ld >> 16) & 0xff;
-    const int nx2 = lx3 + lx4, ny2 = ly3 + ly4, nz2 = lz3 + lz4;
-    const double *ex = Ek + 0 * ESZ + (lx3 * (MAXA + 1) + lx4) * E_T;
-    const double *ey = Ek + 1 * ESZ + (ly3 * (MAXA + 1) + ly4) * E_T;
-    const double *ez = Ek + 2 * ESZ + (lz3 * (MAXA + 1) + lz4) * E_T;
-    double cx[L + 1], cy[L + 1], cz[L + 1];
-    const int nx = nx1 + nx2, ny = ny1 + ny2, nz = nz1 + nz2;
-    for (int T = 0; T <= nx; ++T) {
-      double acc = 0.0;
-      for (int t = max(0, T - nx2); t <= min(T, nx1); ++t) {
-        double e = ex[T - t];
-        if ((skip & 8) && fabs(e) < TB_SKIP30) e = 0.0;
-        acc = fma(bx[t], e, acc);
-      }
-      cx[T] = acc * ztot;
-    }
-    for (int U = 0; U <= ny; ++U) {
-      double acc = 0.0;
-      for (int u = max(0, U - ny2); u <= min(U, ny1); ++u) {
-        double e = ey[U - u];
-        if ((skip & 16) && fabs(e) < TB_SKIP30) e = 0.0;
-        acc = fma(by[u], e, acc);
-      }
-      cy[U] = acc;
-    }
-    for (int V = 0; V <= nz; ++V) {
-      double acc = 0.0;
-      for (int v = max(0, V - nz2); v <= min(V, nz1); ++v) acc = fma(bz[v], ez[V - v], acc);
-      cz[V] = acc;
-    }
-    for (int T = 0; T <= nx; ++T) {
-      const int baseT = ntuv(L) - ntuv(L - T);
-      for (int U = 0; U <= ny; ++U) {
-        const double w = cx[T] * cy[U];
-        double *row = D + (baseT + U * (L - T + 1) - (U * (U - 1)) / 2) * nthr;
-        for (int V = 0; V <= nz; ++V) row[V * nthr] = fma(w, cz[V], row[V * nthr]);
-      }
-    }
-  }
-  if (S > 1) {
-    // fixed-order sum of the S partial densities into the group's first column
-    __syncwarp(gmask);
-    const int base = threadIdx.x - sub;
-    for (int k = sub; k < NT; k += S) {
-      double t = 0.0;
-      for (int j = 0; j < S; ++j) t += sD[k * nthr + base + j];
-      sD[k * nthr + base] = t;
-    }
-    __syncwarp(gmask);
-    D = sD + base;
-  }
-
-  const double pre = loop_weight(loop) * tb[4] * tk[4];
-  double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
-  const bool leader = sub == 0;
-  if (p0) {
-    // F(q) = sum_s c_s q^{2s}, c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
-    constexpr int NS = L / 2 + 1;
-    double cs[NS];
-#pragma unroll
-    for (int k = 0; k < NS; ++k) cs[k] = 0.0;
-    int cnt = 0;
-#pragma unroll
-    for (int k = 0; k < NS; ++k)
-      for (int T = 0; T <= 2 * k; T += 2)
-        for (int U = 0; U <= 2 * k - T; U += 2) {
-          if ((cnt++ % S) != sub) continue;
-          int V = 2 * k - T - U;
-          double f = p0_factor(T, U, V, KIND == KIND_J2);
-          if (KIND == KIND_J2) f = (T + U - 2 * V) / 4.0 * f;
-          cs[k] += D[dindex<L>(T, U, V) * nthr] * f;
-        }
-#pragma unroll
-    for (int k = 0; k < NS; ++k) cs[k] = group_sum<S>(cs[k], gmask);
-    if (!leader) return;
-    atomicAdd(A.p0count, 1ull);
-    const double fj2 = sqrt(5.0 / TB_PI);
-    r[0] = 0.0;
-    r[1] = tb[5] + tk[5];
-    r[2] = (double)REC_P0;
-    r[3] = (double)(NS - 1);
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      double acc = KIND == KIND_J2 ? cs[k] * fj2 : cs[k];
-      r[4 + k] = pre * ((k & 1) ? -acc : acc);
-    }
-    return;
-  }
-
-  // Bessel expansion: h[b] = sum_TUV D[TUV] sum_{p} a(T,px) b(U,py) c(V,pz),
-  // b = (T+px)/2 + (U+py)/2 + (V+pz)/2 (BesselDeriv); for j2 the four-term
-  // BesselDeriv2j form with two extra orders (src/Integrals.f90:6370-6434).
-  constexpr int LB = KIND == KIND_J2 ? L + 2 : L;
-  constexpr int TP = tp_size(L);
-  double ax[TP], ay[TP], az[TP];
-  hermite_table(L, Hx, ax);
-  hermite_table(L, Hy, ay);
-  hermite_table(L, Hz, az);
-  double hh[LB + 1];
-#pragma unroll
-  for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
-  const double eta = 3.0 * (Hz * Hz) - h * h;
-  int cnt = 0;
-  for (int T = 0; T <= L; ++T)
-    for (int U = 0; U <= L - T; ++U)
-      for (int V = 0; V <= L - T - U; ++V) {
-        if ((cnt++ % S) != sub) continue;
-        double d = D[dindex<L>(T, U, V) * nthr];
-        if (d == 0.0) continue;
-        for (int k1 = 0; 2 * k1 <= T; ++k1) {
-          double cx = ax[tp_off(T) + k1];
-          double cx1 = (double)(2 * (T - k1)) * cx;
-          for (int k2 = 0; 2 * k2 <= U; ++k2) {
-            double cy = ay[tp_off(U) + k2];
-            double cy1 = (double)(2 * (U - k2)) * cy;
-            for (int k3 = 0; 2 * k3 <= V; ++k3) {
-              double cz = az[tp_off(V) + k3];
-              int s3 = (T - k1) + (U - k2) + (V - k3);
-              if (KIND != KIND_J2) {
-                hh[s3] += d * (cx * cy * cz);
-              } else {
-                double cz1 = (double)(2 * (V - k3)) * cz;
-                hh[s3 + 2] += d * (cx * cy * cz * eta);
-                hh[s3 + 1] += d * (cx1 * cy * cz + cx * cy1 * cz - 2.0 * (cx * cy * cz1));
-              }
-            }
-          }
-        }
-      }
-#pragma unroll
-  for (int b = 0; b <= LB; ++b) hh[b] = group_sum<S>(hh[b], gmask);
-  if (!leader) return;
-  if (KIND == KIND_J2) {
-    const double f = 0.25 * sqrt(5.0 / TB_PI);
-#pragma unroll
-    for (int b = 0; b <= LB; ++b) hh[b] *= f;
-  }
-  if (KIND == KIND_ELASTIC) {
-    // integral_k_ijkr returns F = 0 when sum(h_saved) == 0 (src/Integrals.f90:5883-5886)
-    double sum = 0.0;
-#pragma unroll
-    for (int b = 0; b <= LB; ++b) sum += hh[b];
-    if (sum == 0.0) {
-#pragma unroll
-      for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
-    }
-  }
-  r[0] = h;
-  r[1] = tb[5] + tk[5];
-  r[2] = (double)(KIND == KIND_J2 ? REC_BESSEL_J2 : REC_BESSEL);
-  r[3] = (double)LB;
-  // hhat_b = h_b / H^{2b}: F = sum_b hhat_b j_b(x) x^b, x = qH
-  const double invH2 = 1.0 / (h * h);
-  double f = pre;
-#pragma unroll
-  for (int b = 0; b <= LB; ++b) {
-    r[4 + b] = hh[b] * f;
-    f *= invH2;
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -617,47 +352,14 @@ __global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off,
 // host-side launchers
 // ---------------------------------------------------------------------------
 cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
-                               const double *xyz, double *tab, cudaStream_t st) {
+                               const double *xyz, double *tab, double *esoa, cudaStream_t st) {
   int n = npairs(ng);
-  pair_tables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab);
-  return cudaGetLastError();
-}
-
-// threads per block so that the Hermite densities of the block fit in 96 KB
-// of shared memory (2 blocks per SM for the large classes)
-static int stage1_threads(int L) {
-  int t = 128;
-  while (t > stage1_split(L) && (size_t)ntuv(L) * sizeof(double) * t > 96 * 1024) t /= 2;
-  return t;
-}
-
-template <int L, int K>
-static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t st) {
-  int thr = stage1_threads(L);
-  size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
-  cudaError_t e = cudaFuncSetAttribute(stage1_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  constexpr int S = stage1_split(L);
-  int64_t threads = n * S;
-  stage1_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
-  return cudaGetLastError();
-}
-
-template <int K>
-static cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st) {
-  int64_t n = a.qend - a.qbegin;
-  if (n <= 0) return cudaSuccess;
-  switch (L) {
-#define TB_S1(l) case l: return launch_stage1_l<l, K>(a, n, st);
-    TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
-    TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
-#undef TB_S1
-    default: return cudaErrorInvalidValue;
-  }
+  pair_tables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab, esoa);
   return cudaGetLastError();
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st) {
+  // instantiated in tb_stage1_total.cu, tb_stage1_elastic.cu, tb_stage1_j2.cu
   if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, st);
   if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, st);
   return launch_stage1_k<KIND_J2>(L, a, st);

@@ -20,6 +20,10 @@ struct Stage1Args {
   const double *zao;          // AO density (ngto x ngto), elastic
   int ngto;
   double cutoffz, cutoffmd, cutoffcentre;
+  const double *esoa;         // E^{la,lb}_t transposed: [variant][axis][la][lb][t][pair]
+  int64_t eskip;              // offset of the variant with |E| < 1e-30 set to zero
+  int emaxa;                  // la, lb range of the transposed table (0..emaxa)
+  int64_t npair;              // group pairs (the table's innermost extent)
   double *rec;                // records: [H, 1/4p+1/4p', kind, order, coefs...]
   int64_t recbase;
   int rs;
@@ -47,8 +51,12 @@ struct Stage2Args {
 // Sets the calling thread's error string (thistle_last_error_string) and returns code.
 int set_error(int code, const std::string &msg);
 
+// Doubles of the transposed E table (both variants) for ng groups.
+int64_t esoa_doubles(int ng, int maxa);
 cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
-                               const double *xyz, double *tab, cudaStream_t st);
+                               const double *xyz, double *tab, double *esoa, cudaStream_t st);
+template <int K>
+cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st);
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);

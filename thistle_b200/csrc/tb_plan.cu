@@ -81,7 +81,7 @@ struct thistle_plan {
   int cls_rs[MAXCLS];
   int64_t rec_total = 0;
   int *d_gstart = nullptr, *d_gcount = nullptr, *d_flmn = nullptr;
-  double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr;
+  double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr, *d_esoa = nullptr;
   double *d_rho = nullptr, *d_zao = nullptr, *d_rec = nullptr, *d_partial = nullptr, *d_result = nullptr;
   uint64_t *d_quart = nullptr;
   // device-resident density inputs and transform workspaces
@@ -402,7 +402,7 @@ done:
 static void plan_free(thistle_plan *P) {
   if (!P) return;
   dfree(P->d_gstart); dfree(P->d_gcount); dfree(P->d_flmn); dfree(P->d_ga); dfree(P->d_xyz);
-  dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
+  dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
   dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
   dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3);
@@ -492,6 +492,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(dalloc(&P->d_q, (size_t)nq, "q"));
   TB_TRY(dalloc(&P->d_result, (size_t)nq, "result"));
   TB_TRY(dalloc(&P->d_pairtab, (size_t)npairs(P->ng) * PAIR_STRIDE, "pair tables"));
+  TB_TRY(dalloc(&P->d_esoa, (size_t)esoa_doubles(P->ng, P->maxa), "transposed E tables"));
   TB_TRY(dalloc(&P->d_p0count, (size_t)MAXCLS, "P0 counters"));
   TB_TRYC(cudaMemcpyAsync(P->d_gstart, P->gstart.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_gcount, P->gcount.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
@@ -561,7 +562,8 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
   cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
   P->ring_next += 1;
   TB_CK(cudaEventRecord(E[0], P->st));
-  TB_CK(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->st));
+  TB_CK(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa,
+                           P->st));
   P->launches += 1;
   TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS, P->st));
   TB_CK(cudaEventRecord(E[1], P->st));
@@ -582,6 +584,10 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.cutoffz = P->cutoffz;
     a.cutoffmd = P->cutoffmd;
     a.cutoffcentre = P->cutoffcentre;
+    a.esoa = P->d_esoa;
+    a.eskip = esoa_doubles(P->ng, P->maxa) / 2;
+    a.emaxa = P->maxa;
+    a.npair = npairs(P->ng);
     a.rec = d_rec;
     a.recbase = recoff[c];
     a.rs = rs[c];

@@ -1,0 +1,524 @@
+// Stage 1 of the quartet evaluation: per group quartet, the Hermite-space
+// density D[T][U][V] summed over its primitive (function) quartets with the
+// reference's cutoffs (tot_integral_k_ijkr, src/Integrals.f90:5155-5219, and
+// the pzero / elastic / j2 variants), then either the Bessel expansion
+// coefficients h_b (BesselDeriv :4708-4746, BesselDeriv2j :6370-6434) or the
+// P = Q polynomial (P_LMN :3102-3135, P_LMN_j2 :3137-3170).
+//
+// Two kernels produce D:
+//   stage1_reg_kernel<L, K>   LLmax <= 8: D lives in registers with a
+//       compile-time shape.  S = stage1_reg_split(L) threads share a quartet;
+//       thread s of the group owns the entries with V = s (mod S), all S walk
+//       the same function quartets (no divergence inside a warp whose
+//       quartets have equal shell types, the order the class sort produces).
+//       Per function quartet the six-deep loop of the reference becomes three
+//       full-length 1-D convolutions and one outer product, all unrolled.
+//   stage1_smem_kernel<L, K>  LLmax 9..16 (f and g shells): each thread keeps
+//       a partial density in its own shared-memory column; S threads split the
+//       function-quartet loop and are summed in a fixed order.
+// Both hand D to the same epilogue through a shared-memory column.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_kernels.h"
+#include "tb_math.cuh"
+
+namespace tb {
+
+__device__ __forceinline__ void unpack_quartet(uint64_t pk, int &gi, int &gj, int &gk, int &gr) {
+  gi = (int)(pk & 0xffff);
+  gj = (int)((pk >> 16) & 0xffff);
+  gk = (int)((pk >> 32) & 0xffff);
+  gr = (int)((pk >> 48) & 0xffff);
+}
+
+// The five loops of tot_integration give these weights (src/Integrals.f90:158,243,325,402,462).
+__device__ __forceinline__ int quartet_loop(int gi, int gj, int gk, int gr) {
+  if (gi == gj) return gk == gr ? (gi == gk ? 5 : 4) : 3;
+  return gk == gi ? 2 : 1;
+}
+__device__ __forceinline__ double loop_weight(int loop) {
+  return loop == 1 ? 8.0 : (loop <= 3 ? 4.0 : (loop == 4 ? 2.0 : 1.0));
+}
+
+// Simplex layout of D[T][U][V], T+U+V <= L, with V contiguous:
+// idx = ntuv(L) - ntuv(L-T) + U (L-T+1) - U (U-1)/2 + V.
+template <int L>
+__device__ __forceinline__ int dindex(int T, int U, int V) {
+  return ntuv(L) - ntuv(L - T) + U * (L - T + 1) - (U * (U - 1)) / 2 + V;
+}
+
+// Sum over the S lanes of one quartet's thread group (result in its first lane).
+template <int S>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int off = S / 2; off > 0; off >>= 1) v += __shfl_down_sync(mask, v, off, S);
+  return v;
+}
+
+// Largest LLmax handled by the register kernel, and its threads per quartet.
+constexpr int STAGE1_REG_MAXL = 8;
+TB_HD constexpr int stage1_reg_split(int L) { return L <= 4 ? 1 : (L == 5 ? 2 : (L == 6 ? 4 : 8)); }
+// Threads per quartet of the shared-memory kernel.
+TB_HD constexpr int stage1_smem_split(int L) { return L <= 15 ? 32 : 16; }
+TB_HD constexpr int stage1_split(int L) {
+  return L <= STAGE1_REG_MAXL ? stage1_reg_split(L) : stage1_smem_split(L);
+}
+// Resident blocks asked of the register allocator: the largest count whose
+// register cap (65536 / (128 x blocks)) still holds the kernel without spills.
+TB_HD constexpr int stage1_reg_minblocks(int L) { return L <= 2 ? 4 : (L == 3 ? 3 : 2); }
+// Register entries of one thread: (T, U, j) with V = S j + s <= L - T - U for some s.
+TB_HD constexpr int reg_entries(int L, int S) {
+  int n = 0;
+  for (int T = 0; T <= L; ++T)
+    for (int U = 0; U <= L - T; ++U) n += (L - T - U) / S + 1;
+  return n;
+}
+
+struct QuartetHead {
+  int gi, gj, gk, gr, loop;
+  bool p0;
+  int skip;
+  double Hx, Hy, Hz, h;
+  const double *tb, *tk;
+};
+
+template <int KIND>
+__device__ __forceinline__ QuartetHead quartet_head(const Stage1Args &A, int64_t qi) {
+  QuartetHead Q;
+  unpack_quartet(A.quartets[qi], Q.gi, Q.gj, Q.gk, Q.gr);
+  Q.tb = A.pairtab + (size_t)pair_index(Q.gi, Q.gj, A.ng) * PAIR_STRIDE;
+  Q.tk = A.pairtab + (size_t)pair_index(Q.gk, Q.gr, A.ng) * PAIR_STRIDE;
+  // hx = px(k,r) - px(i,j)  (src/Integrals.f90:83-86)
+  Q.Hx = Q.tk[0] - Q.tb[0];
+  Q.Hy = Q.tk[1] - Q.tb[1];
+  Q.Hz = Q.tk[2] - Q.tb[2];
+  Q.h = sqrt(Q.Hx * Q.Hx + Q.Hy * Q.Hy + Q.Hz * Q.Hz);
+  Q.loop = quartet_loop(Q.gi, Q.gj, Q.gk, Q.gr);
+  Q.p0 = Q.loop == 5 || Q.h < A.cutoffcentre;
+  // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
+  // a skipped factor removes every term it multiplies, i.e. it is a zero.
+  Q.skip = Q.p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
+  return Q;
+}
+
+// From the quartet's Hermite density (entry k at D[k * dstride], the whole
+// density visible to every thread of the group) to its record
+// [H, 1/4p+1/4p', kind, order, coefficients...].  Thread `sub` of the S-group
+// handles every S-th term; the group leader writes the record.
+template <int L, int KIND, int S>
+__device__ __forceinline__ void stage1_finish(const Stage1Args &A, const QuartetHead &Q, const double *D, int dstride,
+                                              int64_t qi, int sub, unsigned gmask) {
+  const double pre = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
+  double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
+  const bool leader = sub == 0;
+  if (Q.p0) {
+    // F(q) = sum_s c_s q^{2s}, c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
+    constexpr int NS = L / 2 + 1;
+    double cs[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) cs[k] = 0.0;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k)
+      for (int T = 0; T <= 2 * k; T += 2)
+        for (int U = 0; U <= 2 * k - T; U += 2) {
+          if ((cnt++ % S) != sub) continue;
+          int V = 2 * k - T - U;
+          double f = p0_factor(T, U, V, KIND == KIND_J2);
+          if (KIND == KIND_J2) f = (T + U - 2 * V) / 4.0 * f;
+          cs[k] += D[dindex<L>(T, U, V) * dstride] * f;
+        }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) cs[k] = group_sum<S>(cs[k], gmask);
+    if (!leader) return;
+    atomicAdd(A.p0count, 1ull);
+    const double fj2 = sqrt(5.0 / TB_PI);
+    r[0] = 0.0;
+    r[1] = Q.tb[5] + Q.tk[5];
+    r[2] = (double)REC_P0;
+    r[3] = (double)(NS - 1);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      double acc = KIND == KIND_J2 ? cs[k] * fj2 : cs[k];
+      r[4 + k] = pre * ((k & 1) ? -acc : acc);
+    }
+    return;
+  }
+
+  // Bessel expansion: h[b] = sum_TUV D[TUV] sum_{p} a(T,px) b(U,py) c(V,pz),
+  // b = (T+px)/2 + (U+py)/2 + (V+pz)/2 (BesselDeriv); for j2 the four-term
+  // BesselDeriv2j form with two extra orders (src/Integrals.f90:6370-6434).
+  constexpr int LB = KIND == KIND_J2 ? L + 2 : L;
+  constexpr int TP = tp_size(L);
+  double ax[TP], ay[TP], az[TP];
+  hermite_table(L, Q.Hx, ax);
+  hermite_table(L, Q.Hy, ay);
+  hermite_table(L, Q.Hz, az);
+  double hh[LB + 1];
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
+  const double eta = 3.0 * (Q.Hz * Q.Hz) - Q.h * Q.h;
+  int cnt = 0;
+  for (int T = 0; T <= L; ++T)
+    for (int U = 0; U <= L - T; ++U)
+      for (int V = 0; V <= L - T - U; ++V) {
+        if ((cnt++ % S) != sub) continue;
+        double d = D[dindex<L>(T, U, V) * dstride];
+        if (d == 0.0) continue;
+        for (int k1 = 0; 2 * k1 <= T; ++k1) {
+          double cx = ax[tp_off(T) + k1];
+          double cx1 = (double)(2 * (T - k1)) * cx;
+          for (int k2 = 0; 2 * k2 <= U; ++k2) {
+            double cy = ay[tp_off(U) + k2];
+            double cy1 = (double)(2 * (U - k2)) * cy;
+            for (int k3 = 0; 2 * k3 <= V; ++k3) {
+              double cz = az[tp_off(V) + k3];
+              int s3 = (T - k1) + (U - k2) + (V - k3);
+              if (KIND != KIND_J2) {
+                hh[s3] += d * (cx * cy * cz);
+              } else {
+                double cz1 = (double)(2 * (V - k3)) * cz;
+                hh[s3 + 2] += d * (cx * cy * cz * eta);
+                hh[s3 + 1] += d * (cx1 * cy * cz + cx * cy1 * cz - 2.0 * (cx * cy * cz1));
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) hh[b] = group_sum<S>(hh[b], gmask);
+  if (!leader) return;
+  if (KIND == KIND_J2) {
+    const double f = 0.25 * sqrt(5.0 / TB_PI);
+#pragma unroll
+    for (int b = 0; b <= LB; ++b) hh[b] *= f;
+  }
+  if (KIND == KIND_ELASTIC) {
+    // integral_k_ijkr returns F = 0 when sum(h_saved) == 0 (src/Integrals.f90:5883-5886)
+    double sum = 0.0;
+#pragma unroll
+    for (int b = 0; b <= LB; ++b) sum += hh[b];
+    if (sum == 0.0) {
+#pragma unroll
+      for (int b = 0; b <= LB; ++b) hh[b] = 0.0;
+    }
+  }
+  r[0] = Q.h;
+  r[1] = Q.tb[5] + Q.tk[5];
+  r[2] = (double)(KIND == KIND_J2 ? REC_BESSEL_J2 : REC_BESSEL);
+  r[3] = (double)LB;
+  // hhat_b = h_b / H^{2b}: F = sum_b hhat_b j_b(x) x^b, x = qH
+  const double invH2 = 1.0 / (Q.h * Q.h);
+  double f = pre;
+#pragma unroll
+  for (int b = 0; b <= LB; ++b) {
+    r[4 + b] = hh[b] * f;
+    f *= invH2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// register kernel (LLmax <= 8)
+// ---------------------------------------------------------------------------
+// E^{la,lb}_t of one axis of one group pair in the transposed table: element t
+// of slot (axis, la, lb) at e[(slot * E_T + t) * npairs], zero for t > la + lb.
+__device__ __forceinline__ const double *esoa_slot(const Stage1Args &A, bool skipped, int axis, int la, int lb,
+                                                   int pair) {
+  const int m1 = A.emaxa + 1;
+  const int slot = (axis * m1 + la) * m1 + lb;
+  return A.esoa + (skipped ? A.eskip : 0) + (int64_t)slot * E_T * A.npair + pair;
+}
+
+template <int L, int KIND>
+__global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kernel(Stage1Args A) {
+  constexpr int S = stage1_reg_split(L);
+  constexpr int NE = reg_entries(L, S);
+  constexpr int NG = 128 / S;            // quartet groups per block
+  constexpr int TMAX = L < 2 * MAXA ? L : 2 * MAXA;  // last E index an axis can reach
+  extern __shared__ double sD[];         // ntuv(L) x NG: one density column per group
+  const int sub = threadIdx.x % S, grp = threadIdx.x / S;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
+  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
+  // whole groups leave together (S divides 32)
+  if (qi >= A.qend) return;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const int pb = pair_index(Q.gi, Q.gj, A.ng), pk = pair_index(Q.gk, Q.gr, A.ng);
+  const int64_t np = A.npair;
+
+  double D[NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) D[e] = 0.0;
+
+  const int si = A.gstart[Q.gi], ni = A.gcount[Q.gi];
+  const int sj = A.gstart[Q.gj], nj = A.gcount[Q.gj];
+  const int sk = A.gstart[Q.gk], nk = A.gcount[Q.gk];
+  const int sr = A.gstart[Q.gr], nr = A.gcount[Q.gr];
+  for (int ia = 0; ia < ni; ++ia) {
+    for (int ib = 0; ib < nj; ++ib) {
+      const int fa = si + ia, fb = sj + ib;
+      const int la = A.flmn[fa], lb = A.flmn[fb];
+      const int64_t rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      const double zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      // bra coefficients with the (-1)^t sign of src/Integrals.f90:5181
+      double bx[L + 1], by[L + 1], bz[L + 1];
+      {
+        const double *ex = esoa_slot(A, Q.skip & 1, 0, la & 0xff, lb & 0xff, pb);
+        const double *ey = esoa_slot(A, Q.skip & 2, 1, (la >> 8) & 0xff, (lb >> 8) & 0xff, pb);
+        const double *ez = esoa_slot(A, Q.skip & 4, 2, (la >> 16) & 0xff, (lb >> 16) & 0xff, pb);
+#pragma unroll
+        for (int t = 0; t <= L; ++t) {
+          double vx = t <= TMAX ? ex[t * np] : 0.0;
+          double vy = t <= TMAX ? ey[t * np] : 0.0;
+          double vz = t <= TMAX ? ez[t * np] : 0.0;
+          bx[t] = (t & 1) ? -vx : vx;
+          by[t] = (t & 1) ? -vy : vy;
+          bz[t] = (t & 1) ? -vz : vz;
+        }
+      }
+      for (int ic = 0; ic < nk; ++ic) {
+        for (int id = 0; id < nr; ++id) {
+          const int fc = sk + ic, fd = sr + id;
+          double z;
+          if (KIND == KIND_ELASTIC) z = A.zao[(size_t)fc * A.ngto + fd] * zab;
+          else z = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+          // the reference skips primitive quartets with |ztot| < cutoffz
+          z = fabs(z) < A.cutoffz ? 0.0 : z;
+          const int lc = A.flmn[fc], ld = A.flmn[fd];
+          const double *ex = esoa_slot(A, Q.skip & 8, 0, lc & 0xff, ld & 0xff, pk);
+          const double *ey = esoa_slot(A, Q.skip & 16, 1, (lc >> 8) & 0xff, (ld >> 8) & 0xff, pk);
+          const double *ez = esoa_slot(A, false, 2, (lc >> 16) & 0xff, (ld >> 16) & 0xff, pk);
+          double kx[TMAX + 1], ky[TMAX + 1], kz[TMAX + 1];
+#pragma unroll
+          for (int t = 0; t <= TMAX; ++t) {
+            kx[t] = ex[t * np];
+            ky[t] = ey[t * np];
+            kz[t] = ez[t * np];
+          }
+          // C_axis[T] = sum_t b[t] k[T - t] over the full (zero-padded) range
+          double Cx[L + 1], Cy[L + 1], Cz[L + 1];
+#pragma unroll
+          for (int T = 0; T <= L; ++T) {
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+            for (int t = 0; t <= T; ++t) {
+              if (T - t > TMAX) continue;
+              sx = fma(bx[t], kx[T - t], sx);
+              sy = fma(by[t], ky[T - t], sy);
+              sz = fma(bz[t], kz[T - t], sz);
+            }
+            Cx[T] = sx * z;
+            Cy[T] = sy;
+            Cz[T] = sz;
+          }
+          // this thread's z values: V = S j + sub
+          double Czs[L / S + 1];
+#pragma unroll
+          for (int j = 0; j <= L / S; ++j) {
+            double v = Cz[S * j];
+#pragma unroll
+            for (int u = 1; u < S; ++u)
+              if (S * j + u <= L) v = sub == u ? Cz[S * j + u] : v;
+            Czs[j] = v;
+          }
+          int e = 0;
+#pragma unroll
+          for (int T = 0; T <= L; ++T)
+#pragma unroll
+            for (int U = 0; U <= L - T; ++U) {
+              const double w = Cx[T] * Cy[U];
+#pragma unroll
+              for (int j = 0; j <= (L - T - U) / S; ++j, ++e) D[e] = fma(w, Czs[j], D[e]);
+            }
+        }
+      }
+    }
+  }
+  // hand the density to the epilogue through the group's shared column
+  double *col = sD + grp;
+  {
+    int e = 0;
+#pragma unroll
+    for (int T = 0; T <= L; ++T)
+#pragma unroll
+      for (int U = 0; U <= L - T; ++U)
+#pragma unroll
+        for (int j = 0; j <= (L - T - U) / S; ++j, ++e) {
+          const int V = S * j + sub;
+          if (S == 1 || V <= L - T - U) col[dindex<L>(T, U, V) * NG] = D[e];
+        }
+  }
+  if (S > 1) __syncwarp(gmask);
+  stage1_finish<L, KIND, S>(A, Q, col, NG, qi, sub, gmask);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory kernel (LLmax 9..16)
+// ---------------------------------------------------------------------------
+template <int L, int KIND>
+__global__ void stage1_smem_kernel(Stage1Args A) {
+  // Each thread owns a column of the block's shared array; element k of its
+  // (partial) Hermite density sits at sD[k * blockDim.x + threadIdx.x].
+  constexpr int S = stage1_smem_split(L);
+  extern __shared__ double sD[];
+  const int nthr = blockDim.x;
+  const int sub = threadIdx.x % S;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
+  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
+  if (qi >= A.qend) return;
+  double *D = sD + threadIdx.x;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const int skip = Q.skip;
+
+  constexpr int NT = ntuv(L);
+  for (int k = 0; k < NT; ++k) D[k * nthr] = 0.0;
+
+  const int si = A.gstart[Q.gi], ni = A.gcount[Q.gi];
+  const int sj = A.gstart[Q.gj], nj = A.gcount[Q.gj];
+  const int sk = A.gstart[Q.gk], nk = A.gcount[Q.gk];
+  const int sr = A.gstart[Q.gr], nr = A.gcount[Q.gr];
+  const double *Eb = Q.tb + 8, *Ek = Q.tk + 8;
+  const int nket = nk * nr, nprim = ni * nj * nket;
+  int cur_ab = -1;
+  double bx[L + 1], by[L + 1], bz[L + 1];
+  int nx1 = 0, ny1 = 0, nz1 = 0;
+  int64_t rowp = 0;
+  double zab = 0.0;
+  for (int pidx = sub; pidx < nprim; pidx += S) {
+    const int ab = pidx / nket, cd = pidx - ab * nket;
+    if (ab != cur_ab) {
+      cur_ab = ab;
+      const int fa = si + ab / nj, fb = sj + ab % nj;
+      const int la = A.flmn[fa], lb = A.flmn[fb];
+      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      const int lx1 = la & 0xff, ly1 = (la >> 8) & 0xff, lz1 = (la >> 16) & 0xff;
+      const int lx2 = lb & 0xff, ly2 = (lb >> 8) & 0xff, lz2 = (lb >> 16) & 0xff;
+      nx1 = lx1 + lx2;
+      ny1 = ly1 + ly2;
+      nz1 = lz1 + lz2;
+      const double *ex = Eb + 0 * ESZ + (lx1 * (MAXA + 1) + lx2) * E_T;
+      const double *ey = Eb + 1 * ESZ + (ly1 * (MAXA + 1) + ly2) * E_T;
+      const double *ez = Eb + 2 * ESZ + (lz1 * (MAXA + 1) + lz2) * E_T;
+#pragma unroll
+      for (int t = 0; t <= L; ++t) {
+        double vx = t <= nx1 ? ex[t] : 0.0, vy = t <= ny1 ? ey[t] : 0.0, vz = t <= nz1 ? ez[t] : 0.0;
+        if ((skip & 1) && fabs(vx) < TB_SKIP30) vx = 0.0;
+        if ((skip & 2) && fabs(vy) < TB_SKIP30) vy = 0.0;
+        if ((skip & 4) && fabs(vz) < TB_SKIP30) vz = 0.0;
+        bx[t] = (t & 1) ? -vx : vx;
+        by[t] = (t & 1) ? -vy : vy;
+        bz[t] = (t & 1) ? -vz : vz;
+      }
+    }
+    const int fc = sk + cd / nr, fd = sr + cd % nr;
+    double ztot;
+    if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
+    else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+    if (fabs(ztot) < A.cutoffz) continue;
+    const int lc = A.flmn[fc], ld = A.flmn[fd];
+    const int lx3 = lc & 0xff, ly3 = (lc >> 8) & 0xff, lz3 = (lc >> 16) & 0xff;
+    const int lx4 = ld & 0xff, ly4 = (ld >> 8) & 0xff, lz4 = (ld >> 16) & 0xff;
+    const int nx2 = lx3 + lx4, ny2 = ly3 + ly4, nz2 = lz3 + lz4;
+    const double *ex = Ek + 0 * ESZ + (lx3 * (MAXA + 1) + lx4) * E_T;
+    const double *ey = Ek + 1 * ESZ + (ly3 * (MAXA + 1) + ly4) * E_T;
+    const double *ez = Ek + 2 * ESZ + (lz3 * (MAXA + 1) + lz4) * E_T;
+    double cx[L + 1], cy[L + 1], cz[L + 1];
+    const int nx = nx1 + nx2, ny = ny1 + ny2, nz = nz1 + nz2;
+    for (int T = 0; T <= nx; ++T) {
+      double acc = 0.0;
+      for (int t = max(0, T - nx2); t <= min(T, nx1); ++t) {
+        double e = ex[T - t];
+        if ((skip & 8) && fabs(e) < TB_SKIP30) e = 0.0;
+        acc = fma(bx[t], e, acc);
+      }
+      cx[T] = acc * ztot;
+    }
+    for (int U = 0; U <= ny; ++U) {
+      double acc = 0.0;
+      for (int u = max(0, U - ny2); u <= min(U, ny1); ++u) {
+        double e = ey[U - u];
+        if ((skip & 16) && fabs(e) < TB_SKIP30) e = 0.0;
+        acc = fma(by[u], e, acc);
+      }
+      cy[U] = acc;
+    }
+    for (int V = 0; V <= nz; ++V) {
+      double acc = 0.0;
+      for (int v = max(0, V - nz2); v <= min(V, nz1); ++v) acc = fma(bz[v], ez[V - v], acc);
+      cz[V] = acc;
+    }
+    for (int T = 0; T <= nx; ++T) {
+      const int baseT = ntuv(L) - ntuv(L - T);
+      for (int U = 0; U <= ny; ++U) {
+        const double w = cx[T] * cy[U];
+        double *row = D + (baseT + U * (L - T + 1) - (U * (U - 1)) / 2) * nthr;
+        for (int V = 0; V <= nz; ++V) row[V * nthr] = fma(w, cz[V], row[V * nthr]);
+      }
+    }
+  }
+  // fixed-order sum of the S partial densities into the group's first column
+  __syncwarp(gmask);
+  const int base = threadIdx.x - sub;
+  for (int k = sub; k < NT; k += S) {
+    double t = 0.0;
+    for (int j = 0; j < S; ++j) t += sD[k * nthr + base + j];
+    sD[k * nthr + base] = t;
+  }
+  __syncwarp(gmask);
+  stage1_finish<L, KIND, S>(A, Q, sD + base, nthr, qi, sub, gmask);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+// threads per block of the shared-memory kernel so that the Hermite densities
+// of the block fit in 96 KB (2 blocks per SM)
+static inline int stage1_smem_threads(int L) {
+  int t = 128;
+  while (t > stage1_smem_split(L) && (size_t)ntuv(L) * sizeof(double) * t > 96 * 1024) t /= 2;
+  return t;
+}
+
+template <int L, int K>
+static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t st) {
+  if constexpr (L <= STAGE1_REG_MAXL) {
+    constexpr int S = stage1_reg_split(L);
+    const int thr = 128;
+    size_t smem = (size_t)ntuv(L) * sizeof(double) * (thr / S);
+    cudaError_t e =
+        cudaFuncSetAttribute(stage1_reg_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int64_t threads = n * S;
+    stage1_reg_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
+  } else {
+    constexpr int S = stage1_smem_split(L);
+    int thr = stage1_smem_threads(L);
+    size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
+    cudaError_t e =
+        cudaFuncSetAttribute(stage1_smem_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int64_t threads = n * S;
+    stage1_smem_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st) {
+  int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+  switch (L) {
+#define TB_S1(l) case l: return launch_stage1_l<l, K>(a, n, st);
+    TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
+    TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
+#undef TB_S1
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace tb
