@@ -157,7 +157,10 @@ def test_large_q_tiles():
     with MC.ScatteringPlan.from_problem(p, 1, q=q) as pl:
         got = pl.execute()
     ref = MC.scattering(p, 1, q=q[::7])
-    assert np.max(rel_err(got[::7], ref)) < 1e-13
+    # both runs use the uniform-grid recurrences, with steps dq and 7 dq: they
+    # differ by the recurrences' rounding (~1e-13 after 64 steps), far below
+    # the 1e-10 parity bar
+    assert np.max(rel_err(got[::7], ref)) < 1e-11
 
 
 def test_plan_records_describe_the_quartets():

@@ -11,7 +11,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libthistle_b200.so")
+# THISTLE_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("THISTLE_B200_LIB") or os.path.join(_HERE, "libthistle_b200.so")
 
 ERRORS = {
     -1: "THISTLE_ERR_ARG", -2: "THISTLE_ERR_SHAPE", -3: "THISTLE_ERR_ANGMOM", -4: "THISTLE_ERR_NONFINITE",

@@ -40,10 +40,14 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
-def build(verbose: bool = False, force: bool = False, extra=None) -> str:
-    if up_to_date() and not force:
+def build(verbose: bool = False, force: bool = False, extra=None, out: str | None = None,
+          objdir: str | None = None) -> str:
+    """Compile into ``out`` (default: the in-tree library); ``extra`` nvcc flags
+    and a separate ``objdir`` give a differently configured build."""
+    if out is None and up_to_date() and not force:
         return LIB
-    objdir = os.path.join(HERE, "_build")
+    LIBOUT = out or LIB
+    objdir = objdir or os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -71,11 +75,11 @@ def build(verbose: bool = False, force: bool = False, extra=None) -> str:
             print(pr.stdout + pr.stderr)
         if pr.returncode != 0:
             raise RuntimeError("nvcc failed: " + " ".join(cmd) + "\n" + pr.stdout + pr.stderr)
-    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lcublas"]
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIBOUT, *objs, "-lcublas"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
-    return LIB
+    return LIBOUT
 
 
 if __name__ == "__main__":

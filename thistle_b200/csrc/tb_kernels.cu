@@ -409,6 +409,17 @@ int stage2_blocks_per_sm(int nqp, int nwarps) {
   return nb > 0 ? nb : 1;
 }
 
+__global__ void iota_kernel(uint32_t *v, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (uint32_t)i;
+}
+
+cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  iota_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st) {
   sym_small_kernel<<<(n * n + 127) / 128, 128, 0, st>>>(in, n, out);
   return cudaGetLastError();

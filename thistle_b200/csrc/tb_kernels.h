@@ -28,6 +28,8 @@ struct Stage1Args {
   int64_t recbase;
   int rs;
   unsigned long long *p0count; // P=Q quartets counted for this launch's class
+  uint32_t *s2key;            // optional: stage-2 order key per quartet, (cls << 6) | h bucket
+  int cls;                    // this launch's class index (for s2key)
 };
 
 constexpr int MAXCLS = 20;
@@ -48,6 +50,28 @@ struct Stage2Args {
   int64_t pstride;
 };
 
+// Stage 2 of one LLmax class: lanes over quartets, K quartets per lane.
+struct Stage2ClassArgs {
+  const double *rec;          // the class's first record
+  int rs;                     // record stride (doubles)
+  int64_t nquart;             // quartets in the class
+  const uint32_t *perm;       // optional: slot -> quartet index (class-relative after subtracting pbase)
+  int64_t pbase;
+  const double *q;            // this q tile
+  int nq;
+  int uniform, first_on_grid; // q[1..nq) uniform with step dq; q[0] on that grid too
+  double dq;
+  int j2;                     // Bessel records are j2 (F / q^2)
+  double *partial;            // gridDim.x rows of pstride doubles, accumulated (+=)
+  int64_t pstride;
+};
+constexpr int STAGE2_WARPS = 8;
+// q points a stage-2 block holds in shared memory at once
+constexpr int STAGE2_QTILE = 1024;
+int stage2_quartets_per_warp(int LB);
+int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st);
+
 // Sets the calling thread's error string (thistle_last_error_string) and returns code.
 int set_error(int code, const std::string &msg);
 
@@ -64,6 +88,7 @@ cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *ou
 cudaError_t launch_ghat_scatter(const int *mat, const double *total, int nmat, int n, double *G,
                                 cudaStream_t st);
 cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
+cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
 cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st);
 int stage2_blocks_per_sm(int nqp, int nwarps);
 cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,

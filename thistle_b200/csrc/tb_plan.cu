@@ -96,7 +96,12 @@ struct thistle_plan {
   void *d_sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
   int64_t *d_p0count = nullptr;      // P=Q quartets per class in the last execution
-  int s2_grid = 0, s2_warps = 8, s2_chunk = 4, s2_qtile = 0;
+  // stage-2 visiting order: keys written by stage 1, sorted with the quartet index
+  uint32_t *d_s2key = nullptr, *d_s2key_sorted = nullptr, *d_iota = nullptr, *d_perm = nullptr;
+  void *d_s2sort_tmp = nullptr;
+  size_t s2sort_bytes = 0;
+  int nsm = 0, s2_rows = 0, s2_qtile = 0;
+  int s2_bps[LMAXB + 1];             // resident stage-2 blocks per SM, per Bessel order
   cudaStream_t st = nullptr;
   bool own_stream = true;
   cublasHandle_t cb = nullptr;
@@ -407,6 +412,8 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
   dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
+  dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
+  if (P->d_s2sort_tmp) cudaFree(P->d_s2sort_tmp);
   if (P->d_sort_tmp) cudaFree(P->d_sort_tmp);
   if (P->cb) cublasDestroy(P->cb);
   if (P->have_ev) {
@@ -505,18 +512,28 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(quartets_alloc(P));
   TB_TRY(dalloc(&P->d_rec, (size_t)P->rec_total, "quartet records"));
   {
-    int dev = 0, nsm = 0, maxsm = 0;
+    int dev = 0;
     TB_TRYC(cudaGetDevice(&dev));
-    TB_TRYC(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    TB_TRYC(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    // q tile held in shared memory: (3 + warps) doubles per q point
-    P->s2_warps = 8;
-    int qt = std::min(nq, 2048);
-    while ((size_t)(3 + P->s2_warps) * qt * sizeof(double) > (size_t)maxsm && qt > 32) qt /= 2;
-    P->s2_qtile = qt;
-    int bps = stage2_blocks_per_sm(qt, P->s2_warps);
-    P->s2_grid = nsm * bps;
-    TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_grid * nq, "partial sums"));
+    TB_TRYC(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
+    P->s2_qtile = std::min(nq, STAGE2_QTILE);
+    int maxbps = 1;
+    for (int b = 0; b <= LMAXB; ++b) P->s2_bps[b] = 0;
+    for (int c = 0; c < P->ncls; ++c) {
+      int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
+      P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, P->kind == KIND_J2, P->s2_qtile);
+      maxbps = std::max(maxbps, P->s2_bps[LB]);
+    }
+    P->s2_rows = P->nsm * maxbps;
+    TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_rows * nq, "partial sums"));
+    const int64_t n = std::max<int64_t>(P->nquart, 1);
+    TB_TRY(dalloc(&P->d_s2key, (size_t)n, "stage-2 keys"));
+    TB_TRY(dalloc(&P->d_s2key_sorted, (size_t)n, "stage-2 keys"));
+    TB_TRY(dalloc(&P->d_iota, (size_t)n, "quartet indices"));
+    TB_TRY(dalloc(&P->d_perm, (size_t)n, "stage-2 order"));
+    TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->s2sort_bytes, P->d_s2key, P->d_s2key_sorted, P->d_iota,
+                                            P->d_perm, (int)n, 0, 11, P->st));
+    TB_TRY(dalloc((char **)&P->d_s2sort_tmp, P->s2sort_bytes, "stage-2 sort scratch"));
+    TB_TRYC(launch_iota(P->d_iota, P->nquart, P->st));
   }
   P->launches = 0;
   TB_TRYC(cudaEventRecord(P->ev[6], P->st));
@@ -556,9 +573,11 @@ static void grid_info(const double *q, int n, int &uniform, int &first_on_grid, 
   first_on_grid = std::fabs(q[0] - (q[1] - dq)) <= tol ? 1 : 0;
 }
 
+// Pair tables, stage 1 per class, the stage-2 visiting order (when `order`),
+// stage 2 per class and q tile, and the fixed-order reduction into d_out.
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
-                      double *d_out) {
+                      double *d_out, bool order) {
   cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
   P->ring_next += 1;
   TB_CK(cudaEventRecord(E[0], P->st));
@@ -592,35 +611,51 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.recbase = recoff[c];
     a.rs = rs[c];
     a.p0count = (unsigned long long *)(P->d_p0count + c);
+    a.s2key = order ? P->d_s2key : nullptr;
+    a.cls = c;
     TB_CK(launch_stage1(P->kind, cL[c], a, P->st));
     P->launches += 1;
   }
   TB_CK(cudaEventRecord(E[2], P->st));
-  int64_t nq_all = 0;
-  for (int c = 0; c < ncls; ++c) nq_all = std::max(nq_all, ce[c]);
-  for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
-    Stage2Args s;
-    s.rec = d_rec;
-    s.ncls = ncls;
-    for (int c = 0; c < ncls; ++c) {
-      s.cls_begin[c] = cb[c];
-      s.cls_end[c] = ce[c];
-      s.cls_recoff[c] = recoff[c];
-      s.cls_rs[c] = rs[c];
-    }
-    s.nquart = nq_all;
-    s.chunk = P->s2_chunk;
-    s.q = P->d_q + q0;
-    s.nq = std::min(P->s2_qtile, P->nq - q0);
-    s.nqp = P->s2_qtile;
-    s.partial = P->d_partial + q0;
-    s.pstride = P->nq;
-    grid_info(P->hq.data() + q0, s.nq, s.uniform, s.first_on_grid, s.dq);
-    TB_CK(launch_stage2(s, P->s2_grid, P->s2_warps, P->st));
+  int64_t nall = ncls > 0 ? ce[ncls - 1] : 0;
+  if (order && nall > 0) {
+    size_t bytes = P->s2sort_bytes;
+    TB_CK(cub::DeviceRadixSort::SortPairs(P->d_s2sort_tmp, bytes, P->d_s2key, P->d_s2key_sorted, P->d_iota,
+                                          P->d_perm, (int)nall, 0, 11, P->st));
     P->launches += 1;
   }
+  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
+  for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
+    const int tn = std::min(P->s2_qtile, P->nq - q0);
+    int uniform = 0, first_on_grid = 0;
+    double dq = 0.0;
+    grid_info(P->hq.data() + q0, tn, uniform, first_on_grid, dq);
+    for (int c = 0; c < ncls; ++c) {
+      const int LB = cL[c] + (P->kind == KIND_J2 ? 2 : 0);
+      Stage2ClassArgs s;
+      s.rec = d_rec + recoff[c];
+      s.rs = rs[c];
+      s.nquart = ce[c] - cb[c];
+      s.perm = order ? P->d_perm : nullptr;
+      s.pbase = cb[c];
+      s.q = P->d_q + q0;
+      s.nq = tn;
+      s.uniform = uniform;
+      s.first_on_grid = first_on_grid;
+      s.dq = dq;
+      s.j2 = P->kind == KIND_J2;
+      s.partial = P->d_partial + q0;
+      s.pstride = P->nq;
+      const int64_t per_warp = stage2_quartets_per_warp(LB);
+      const int64_t nblk = (s.nquart + per_warp * STAGE2_WARPS - 1) / (per_warp * STAGE2_WARPS);
+      const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
+      const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
+      TB_CK(launch_stage2_class(LB, s, grid, P->st));
+      P->launches += 1;
+    }
+  }
   TB_CK(cudaEventRecord(E[3], P->st));
-  TB_CK(launch_reduce(P->d_partial, P->s2_grid, P->nq, d_out, P->st));
+  TB_CK(launch_reduce(P->d_partial, P->s2_rows, P->nq, d_out, P->st));
   P->launches += 1;
   TB_CK(cudaEventRecord(E[4], P->st));
   return THISTLE_OK;
@@ -628,7 +663,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
 
 static int plan_exec(thistle_plan *P, double *d_out) {
   return run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                    P->cls_rs, d_out);
+                    P->cls_rs, d_out, true);
 }
 
 static void read_timings(thistle_plan *P) {
@@ -751,7 +786,7 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
   if (nquart == 0) {
     TB_TRYC(cudaMemsetAsync(P->d_result, 0, sizeof(double) * P->nq, P->st));
   } else {
-    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result));
+    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result, false));
   }
   TB_TRYC(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));

@@ -108,9 +108,16 @@ __device__ __forceinline__ QuartetHead quartet_head(const Stage1Args &A, int64_t
 // density visible to every thread of the group) to its record
 // [H, 1/4p+1/4p', kind, order, coefficients...].  Thread `sub` of the S-group
 // handles every S-th term; the group leader writes the record.
+// Stage-2 order key: P = Q quartets first (bucket 0), then quarter octaves of H.
+__device__ __forceinline__ uint32_t h_bucket(double h) {
+  int b = (int)floor(4.0 * log2(h)) + 32;
+  return (uint32_t)min(max(b, 1), 63);
+}
+
 template <int L, int KIND, int S>
 __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const QuartetHead &Q, const double *D, int dstride,
                                               int64_t qi, int sub, unsigned gmask) {
+  if (A.s2key && sub == 0) A.s2key[qi] = ((uint32_t)A.cls << 6) | (Q.p0 ? 0u : h_bucket(Q.h));
   const double pre = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
   double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
   const bool leader = sub == 0;

@@ -1,0 +1,301 @@
+// Stage 2 of the quartet evaluation, one launch per LLmax class: the sum over
+// the class's group quartets of F(q) exp(-q^2 (1/4p + 1/4p')) at every q point
+// (bessels0rr, src/Integrals.f90:6662-6739, with an accurate generator; the
+// P = Q polynomial of set_P0/P_LMN, :3001-3031, :3102-3135).
+//
+// Layout of the work: lanes over quartets, K quartets per lane, every lane of
+// a warp at the same q point.  A warp takes 32 K quartets at a time and walks
+// the q tile; per point each lane evaluates its K quartets (the Bessel order
+// LB is a compile-time constant of the launch), the warp sums them with a
+// butterfly and one lane adds the total into the warp's row of I(q) in shared
+// memory.  Quartets are visited in the order of `perm` when given (sorted by
+// quarter-octave of H, so that the lanes of a warp take the same branch of
+// the Bessel generator at the same q).
+//
+// Generator, for F = sum_b hhat_b g_b(x), g_b = j_b(x) x^b, x = qH (hhat_b =
+// h_b / H^{2b} is prepared by stage 1):
+//   x >= x_c(LB): upward recurrence g_{b+1} = (2b+1) g_b - x^2 g_{b-1} from
+//                 g_0 = sin x / x, g_1 = g_0 - cos x;
+//   x <  x_c(LB): power series of u_n = j_n (2n+1)!! / x^n for the top two
+//                 orders, then the stable downward recurrence, accumulated by
+//                 Horner in x^2 / (2b+1).
+// On uniform q grids sin/cos(qH) advance by a rotation through dq H and
+// exp(-q^2 s) by g <- g r, r <- r k (r = exp(-(2 q dq + dq^2) s),
+// k = exp(-2 dq^2 s)), both restarted from direct values every 64 points.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_kernels.h"
+#include "tb_math.cuh"
+
+namespace tb {
+
+namespace {
+
+constexpr int RESEED = 64;
+
+// Coefficients that lanes without a quartet point at: a zero record body,
+// with room for the [H, s, kind, order] head in front of it.
+__device__ const double kZeroRecord[4 + LMAXB + 4] = {0};
+
+template <int N, int NK>
+__device__ __forceinline__ double series_u(double y) {
+  double p = series_coef(N, NK);
+#pragma unroll
+  for (int k = NK - 1; k >= 0; --k) p = fma(p, y, series_coef(N, k));
+  return p;
+}
+
+// x below the crossover: coefficients read from the record (h[0..LB]).
+template <int LB>
+__device__ __noinline__ double bessel_small(const double *__restrict__ h, double y) {
+  constexpr int NK = series_terms(LB);
+  double uhi = series_u<LB + 1, NK>(y);
+  double umid = series_u<LB, NK>(y);
+  double acc = h[LB] * umid;
+#pragma unroll
+  for (int b = LB; b >= 1; --b) {
+    double ulo = umid - (y * (1.0 / ((2.0 * b + 1.0) * (2.0 * b + 3.0)))) * uhi;
+    acc = fma(acc, y * (1.0 / (2.0 * b + 1.0)), h[b - 1] * ulo);
+    uhi = umid;
+    umid = ulo;
+  }
+  return acc;
+}
+
+template <int LB>
+__device__ __forceinline__ double bessel_up(const double *h, double x, double sn, double cs, double invx) {
+  double g0 = sn * invx;
+  if (LB == 0) return h[0] * g0;
+  double g1 = g0 - cs;
+  double F = fma(h[1], g1, h[0] * g0);
+  const double y = x * x;
+#pragma unroll
+  for (int b = 1; b < LB; ++b) {
+    double g2 = fma((double)(2 * b + 1), g1, -y * g0);
+    F = fma(h[b + 1], g2, F);
+    g0 = g1;
+    g1 = g2;
+  }
+  return F;
+}
+
+// sum_{j <= n} c_j q2^j (the P = Q polynomial)
+__device__ __noinline__ double p0_poly(const double *__restrict__ c, int n, double q2) {
+  double F = c[n];
+  for (int j = n - 1; j >= 0; --j) F = fma(F, q2, c[j]);
+  return F;
+}
+
+struct Seed {
+  double sn, cs, g, r;
+};
+
+__device__ __noinline__ Seed seed_point(double q, double H, double s, double dq) {
+  Seed z;
+  sincos(q * H, &z.sn, &z.cs);
+  z.g = exp(-(q * q) * s);
+  z.r = exp(-(2.0 * q * dq + dq * dq) * s);
+  return z;
+}
+
+// quartets per lane, and the resident blocks per SM the register allocation aims at
+#ifndef TB_S2_K_LO
+#define TB_S2_K_LO 2
+#endif
+#ifndef TB_S2_K_MID
+#define TB_S2_K_MID 2
+#endif
+#ifndef TB_S2_MINB
+#define TB_S2_MINB 2
+#endif
+TB_HD constexpr int stage2_k(int LB) { return LB <= 2 ? TB_S2_K_LO : (LB <= 8 ? TB_S2_K_MID : 1); }
+
+template <int LB, int K, bool J2>
+__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
+  extern __shared__ double sm[];
+  const int nq = A.nq;
+  double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = STAGE2_WARPS;
+  double *acc = sm + 2 * nq + warp * nq;
+  for (int i = threadIdx.x; i < nq; i += blockDim.x) {
+    const double q = A.q[i];
+    qs[i] = make_double2(q, 1.0 / q);
+  }
+  for (int i = threadIdx.x; i < NW * nq; i += blockDim.x) sm[2 * nq + i] = 0.0;
+  __syncthreads();
+
+  constexpr double XC = bessel_crossover(LB);
+  const int64_t per = 32 * K;
+  const int64_t nb = (A.nquart + per - 1) / per;
+  const double dq = A.dq;
+  for (int64_t bt = (int64_t)blockIdx.x * NW + warp; bt < nb; bt += (int64_t)gridDim.x * NW) {
+    double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K], hh[K][LB + 1];
+    const double *hm[K];
+    int p0n[K];  // P = Q polynomial order, or -1 for a Bessel quartet
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t slot = bt * per + k * 32 + lane;
+      const double *rec = kZeroRecord;
+      double h = 1.0;
+      p0n[k] = -1;
+      if (slot < A.nquart) {
+        const int64_t idx = A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot;
+        rec = A.rec + idx * A.rs;
+        if ((int)rec[2] == REC_P0) p0n[k] = (int)rec[3];
+        else h = rec[0];
+      }
+      hm[k] = rec + 4;
+      H[k] = h;
+      invH[k] = 1.0 / h;
+#pragma unroll
+      for (int b = 0; b <= LB; ++b) hh[k][b] = p0n[k] < 0 ? hm[k][b] : 0.0;
+      const double s = rec[1];
+      sincos(dq * h, &sd[k], &cd[k]);
+      kk[k] = exp(-2.0 * dq * dq * s);
+      sn[k] = cs[k] = g[k] = r[k] = 0.0;
+    }
+    int next_seed = 0;
+    for (int m = 0; m < nq; ++m) {
+      const double2 qq = qs[m];
+      const double q = qq.x, iq = qq.y;
+      if (m == next_seed) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const Seed z = seed_point(q, H[k], hm[k][-3], dq);
+          sn[k] = z.sn;
+          cs[k] = z.cs;
+          g[k] = z.g;
+          r[k] = z.r;
+        }
+        next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + RESEED);
+      }
+      // the upward recurrence for all K quartets as straight-line code, then
+      // the rare lanes below the crossover or with P = Q patched in
+      double F[K];
+      bool special = false;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double x = q * H[k];
+        F[k] = bessel_up<LB>(hh[k], x, sn[k], cs[k], iq * invH[k]);
+        if (J2) F[k] *= iq * iq;
+        special |= (x < XC) | (p0n[k] >= 0);
+      }
+      if (special) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const double x = q * H[k];
+          if (p0n[k] >= 0) {
+            F[k] = p0_poly(hm[k], p0n[k], q * q);
+          } else if (x < XC) {
+            F[k] = bessel_small<LB>(hm[k], x * x);
+            if (J2) F[k] *= iq * iq;
+          }
+        }
+      }
+      double Fs = 0.0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        Fs = fma(F[k], g[k], Fs);
+        const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
+        cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
+        sn[k] = s2;
+        g[k] *= r[k];
+        r[k] *= kk[k];
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) Fs += __shfl_xor_sync(0xffffffffu, Fs, off);
+      if (lane == 0) acc[m] += Fs;
+    }
+  }
+  __syncthreads();
+  // fixed-order sum of the warp rows, added to this block's partial row
+  for (int i = threadIdx.x; i < nq; i += blockDim.x) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) t += sm[2 * nq + w * nq + i];
+    A.partial[(size_t)blockIdx.x * A.pstride + i] += t;
+  }
+}
+
+size_t class_smem(int nq) { return sizeof(double) * (size_t)nq * (2 + STAGE2_WARPS); }
+
+template <int LB, bool J2>
+cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, cudaStream_t st) {
+  constexpr int K = stage2_k(LB);
+  size_t smem = class_smem(a.nq);
+  cudaError_t e =
+      cudaFuncSetAttribute(stage2_class_kernel<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage2_class_kernel<LB, K, J2><<<grid, STAGE2_WARPS * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int LB, bool J2>
+int blocks_per_sm_l(int nq) {
+  constexpr int K = stage2_k(LB);
+  size_t smem = class_smem(nq);
+  if (cudaFuncSetAttribute(stage2_class_kernel<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 1;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage2_class_kernel<LB, K, J2>, STAGE2_WARPS * 32, smem) !=
+      cudaSuccess)
+    return 1;
+  return nb > 0 ? nb : 1;
+}
+
+}  // namespace
+
+int stage2_quartets_per_warp(int LB) {
+  switch (LB) {
+#define TB_K(n) case n: return 32 * stage2_k(n);
+    TB_K(0) TB_K(1) TB_K(2) TB_K(3) TB_K(4) TB_K(5) TB_K(6) TB_K(7) TB_K(8) TB_K(9)
+    TB_K(10) TB_K(11) TB_K(12) TB_K(13) TB_K(14) TB_K(15) TB_K(16) TB_K(17) TB_K(18)
+#undef TB_K
+    default: return 32;
+  }
+}
+
+// total / elastic classes have LB = LLmax (0..16), j2 classes LLmax + 2 (2..18)
+int stage2_class_blocks_per_sm(int LB, bool j2, int nq) {
+  if (j2) {
+    switch (LB) {
+#define TB_B(n) case n: return blocks_per_sm_l<n, true>(nq);
+      TB_B(2) TB_B(3) TB_B(4) TB_B(5) TB_B(6) TB_B(7) TB_B(8) TB_B(9) TB_B(10)
+      TB_B(11) TB_B(12) TB_B(13) TB_B(14) TB_B(15) TB_B(16) TB_B(17) TB_B(18)
+#undef TB_B
+      default: return 1;
+    }
+  }
+  switch (LB) {
+#define TB_B(n) case n: return blocks_per_sm_l<n, false>(nq);
+    TB_B(0) TB_B(1) TB_B(2) TB_B(3) TB_B(4) TB_B(5) TB_B(6) TB_B(7) TB_B(8)
+    TB_B(9) TB_B(10) TB_B(11) TB_B(12) TB_B(13) TB_B(14) TB_B(15) TB_B(16)
+#undef TB_B
+    default: return 1;
+  }
+}
+
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st) {
+  if (a.nquart <= 0 || grid <= 0) return cudaSuccess;
+  if (a.j2) {
+    switch (LB) {
+#define TB_L(n) case n: return launch_class_l<n, true>(a, grid, st);
+      TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8) TB_L(9) TB_L(10)
+      TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16) TB_L(17) TB_L(18)
+#undef TB_L
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (LB) {
+#define TB_L(n) case n: return launch_class_l<n, false>(a, grid, st);
+    TB_L(0) TB_L(1) TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8)
+    TB_L(9) TB_L(10) TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16)
+#undef TB_L
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace tb
