@@ -61,6 +61,7 @@ struct Stage2ClassArgs {
   int nq;
   int uniform, first_on_grid; // q[1..nq) uniform with step dq; q[0] on that grid too
   double dq;
+  int chunk;                  // q points per work item (multiple of 64), 0 = the whole tile
   int j2;                     // Bessel records are j2 (F / q^2)
   double *partial;            // gridDim.x rows of pstride doubles, accumulated (+=)
   int64_t pstride;

@@ -646,9 +646,18 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       s.j2 = P->kind == KIND_J2;
       s.partial = P->d_partial + q0;
       s.pstride = P->nq;
+      // a class too small to fill the GPU several times over is also split
+      // over q, in chunks of 64 points (the reseed interval)
       const int64_t per_warp = stage2_quartets_per_warp(LB);
-      const int64_t nblk = (s.nquart + per_warp * STAGE2_WARPS - 1) / (per_warp * STAGE2_WARPS);
       const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
+      const int64_t resident = (int64_t)P->nsm * bps * STAGE2_WARPS;
+      const int64_t nbatch = (s.nquart + per_warp - 1) / per_warp;
+      const int nseg = (tn + 63) / 64;
+      int nch = (int)std::min<int64_t>(nseg, std::max<int64_t>(1, (8 * resident + nbatch - 1) / nbatch));
+      s.chunk = nch <= 1 ? 0 : 64 * ((nseg + nch - 1) / nch);
+      if (s.chunk > 0) nch = (tn + s.chunk - 1) / s.chunk;
+      const int64_t items = nbatch * nch;
+      const int64_t nblk = (items + STAGE2_WARPS - 1) / STAGE2_WARPS;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
       TB_CK(launch_stage2_class(LB, s, grid, P->st));
       P->launches += 1;

@@ -111,26 +111,43 @@ __device__ __noinline__ Seed seed_point(double q, double H, double s, double dq)
 #endif
 TB_HD constexpr int stage2_k(int LB) { return LB <= 2 ? TB_S2_K_LO : (LB <= 8 ? TB_S2_K_MID : 1); }
 
+// q points per reduction block: the warp sums QB points at once with a
+// reduce-scatter (3 halving rounds over lane bits 4..2, then 2 butterfly
+// rounds), so the shuffle latency is paid once per QB points.
+#ifndef TB_S2_QB
+#define TB_S2_QB 8
+#endif
+constexpr int QB = TB_S2_QB;
+TB_HD constexpr int padded_nq(int nq) { return (nq + QB - 1) / QB * QB; }
+
 template <int LB, int K, bool J2>
 __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
   extern __shared__ double sm[];
-  const int nq = A.nq;
-  double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q)
+  const int nq = A.nq, nqb = padded_nq(nq);
+  double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q), padded with the last point
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = STAGE2_WARPS;
-  double *acc = sm + 2 * nq + warp * nq;
-  for (int i = threadIdx.x; i < nq; i += blockDim.x) {
-    const double q = A.q[i];
+  double *acc = sm + 2 * nqb + warp * nqb;
+  for (int i = threadIdx.x; i < nqb; i += blockDim.x) {
+    const double q = A.q[i < nq ? i : nq - 1];
     qs[i] = make_double2(q, 1.0 / q);
   }
-  for (int i = threadIdx.x; i < NW * nq; i += blockDim.x) sm[2 * nq + i] = 0.0;
+  for (int i = threadIdx.x; i < NW * nqb; i += blockDim.x) sm[2 * nqb + i] = 0.0;
   __syncthreads();
 
   constexpr double XC = bessel_crossover(LB);
   const int64_t per = 32 * K;
   const int64_t nb = (A.nquart + per - 1) / per;
+  // work item = (batch of 32 K quartets, chunk of the q tile); chunks start
+  // on reseed points, so splitting a small class over q costs no accuracy
+  const int chunk = A.chunk > 0 ? A.chunk : nqb;
+  const int nch = (nqb + chunk - 1) / chunk;
+  const int64_t nitems = nb * nch;
   const double dq = A.dq;
-  for (int64_t bt = (int64_t)blockIdx.x * NW + warp; bt < nb; bt += (int64_t)gridDim.x * NW) {
+  const int jsel = (lane / (32 / QB)) & (QB - 1);
+  for (int64_t it = (int64_t)blockIdx.x * NW + warp; it < nitems; it += (int64_t)gridDim.x * NW) {
+    const int64_t bt = it / nch;
+    const int m0 = (int)(it - bt * nch) * chunk, m1 = min(nqb, m0 + chunk);
     double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K], hh[K][LB + 1];
     const double *hm[K];
     int p0n[K];  // P = Q polynomial order, or -1 for a Bessel quartet
@@ -156,57 +173,76 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
       kk[k] = exp(-2.0 * dq * dq * s);
       sn[k] = cs[k] = g[k] = r[k] = 0.0;
     }
-    int next_seed = 0;
-    for (int m = 0; m < nq; ++m) {
-      const double2 qq = qs[m];
-      const double q = qq.x, iq = qq.y;
-      if (m == next_seed) {
+    int next_seed = m0;
+    for (int mb = m0; mb < m1; mb += QB) {
+      double Fv[QB];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const Seed z = seed_point(q, H[k], hm[k][-3], dq);
-          sn[k] = z.sn;
-          cs[k] = z.cs;
-          g[k] = z.g;
-          r[k] = z.r;
+      for (int j = 0; j < QB; ++j) {
+        const int m = mb + j;
+        const double2 qq = qs[m];
+        const double q = qq.x, iq = qq.y;
+        if (m == next_seed) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const Seed z = seed_point(q, H[k], hm[k][-3], dq);
+            sn[k] = z.sn;
+            cs[k] = z.cs;
+            g[k] = z.g;
+            r[k] = z.r;
+          }
+          next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + RESEED);
         }
-        next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + RESEED);
-      }
-      // the upward recurrence for all K quartets as straight-line code, then
-      // the rare lanes below the crossover or with P = Q patched in
-      double F[K];
-      bool special = false;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const double x = q * H[k];
-        F[k] = bessel_up<LB>(hh[k], x, sn[k], cs[k], iq * invH[k]);
-        if (J2) F[k] *= iq * iq;
-        special |= (x < XC) | (p0n[k] >= 0);
-      }
-      if (special) {
+        // the upward recurrence for all K quartets as straight-line code,
+        // then the rare lanes below the crossover or with P = Q patched in
+        double F[K];
+        bool special = false;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const double x = q * H[k];
-          if (p0n[k] >= 0) {
-            F[k] = p0_poly(hm[k], p0n[k], q * q);
-          } else if (x < XC) {
-            F[k] = bessel_small<LB>(hm[k], x * x);
-            if (J2) F[k] *= iq * iq;
+          F[k] = bessel_up<LB>(hh[k], x, sn[k], cs[k], iq * invH[k]);
+          if (J2) F[k] *= iq * iq;
+          special |= (x < XC) | (p0n[k] >= 0);
+        }
+        if (special) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const double x = q * H[k];
+            if (p0n[k] >= 0) {
+              F[k] = p0_poly(hm[k], p0n[k], q * q);
+            } else if (x < XC) {
+              F[k] = bessel_small<LB>(hm[k], x * x);
+              if (J2) F[k] *= iq * iq;
+            }
           }
         }
-      }
-      double Fs = 0.0;
+        double Fs = 0.0;
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        Fs = fma(F[k], g[k], Fs);
-        const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
-        cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
-        sn[k] = s2;
-        g[k] *= r[k];
-        r[k] *= kk[k];
+        for (int k = 0; k < K; ++k) {
+          Fs = fma(F[k], g[k], Fs);
+          const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
+          cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
+          sn[k] = s2;
+          g[k] *= r[k];
+          r[k] *= kk[k];
+        }
+        Fv[j] = Fs;
       }
+      // reduce-scatter: after the halving rounds over lane bits 4, 3, 2 the
+      // lane holds point jsel summed over 8 lanes; two butterfly rounds finish
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) Fs += __shfl_xor_sync(0xffffffffu, Fs, off);
-      if (lane == 0) acc[m] += Fs;
+      for (int half = QB / 2, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool up = lane & bit;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+          const double send = up ? Fv[i] : Fv[i + half];
+          const double keep = up ? Fv[i + half] : Fv[i];
+          Fv[i] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
+        }
+      }
+      double t = Fv[0];
+#pragma unroll
+      for (int bit = 32 / QB / 2; bit >= 1; bit >>= 1) t += __shfl_xor_sync(0xffffffffu, t, bit);
+      if ((lane & (32 / QB - 1)) == 0) acc[mb + jsel] += t;
     }
   }
   __syncthreads();
@@ -214,12 +250,12 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
   for (int i = threadIdx.x; i < nq; i += blockDim.x) {
     double t = 0.0;
 #pragma unroll
-    for (int w = 0; w < NW; ++w) t += sm[2 * nq + w * nq + i];
+    for (int w = 0; w < NW; ++w) t += sm[2 * nqb + w * nqb + i];
     A.partial[(size_t)blockIdx.x * A.pstride + i] += t;
   }
 }
 
-size_t class_smem(int nq) { return sizeof(double) * (size_t)nq * (2 + STAGE2_WARPS); }
+size_t class_smem(int nq) { return sizeof(double) * (size_t)padded_nq(nq) * (2 + STAGE2_WARPS); }
 
 template <int LB, bool J2>
 cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, cudaStream_t st) {
