@@ -134,6 +134,19 @@ int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32
 int thistle_plan_destroy(thistle_plan *plan);
 
 /*
+ * Device buffers released by plans stay cached in the library (per device) and
+ * are reused by later plans of a similar size, so that repeated plans and
+ * thistle_total_scattering calls do not pay cudaMalloc/cudaFree each time; a
+ * failed allocation returns the cache to the driver and retries.  No
+ * counterpart in the reference (whose arrays are Fortran allocatables).
+ * thistle_release_device_cache frees the cached buffers and idle cuBLAS
+ * handles of the current device; thistle_device_cache_bytes reports the bytes
+ * cached and the bytes held by live plans on the current device.
+ */
+int thistle_release_device_cache(void);
+int thistle_device_cache_bytes(int64_t *cached, int64_t *in_use);
+
+/*
  * Stage 2 without any device allocation.  No counterpart in the reference
  * (whose integrators allocate freely on the host).  For callers that cannot
  * call cudaMalloc when they evaluate -- a host application that hands this

@@ -172,3 +172,21 @@ def test_plan_records_describe_the_quartets():
         assert r["begin"][0] == 0 and r["end"][-1] == pl.info()["nquart"]
         assert np.all(r["begin"][1:] == r["end"][:-1])
         assert np.all(r["rs"] % 2 == 0)
+
+
+@pytest.mark.gpu
+def test_device_cache_reuses_buffers():
+    """A second plan of the same shape reuses the cached buffers; release empties the cache."""
+    from thistle_b200 import _abi
+    p = I.config2_diatomic()
+    with MC.ScatteringPlan.from_problem(p, 1) as pl:
+        a = pl.execute()
+    cached, in_use = _abi.device_cache_bytes()
+    assert cached > 0
+    with MC.ScatteringPlan.from_problem(p, 1) as pl:
+        c2, u2 = _abi.device_cache_bytes()
+        b = pl.execute()
+    assert c2 < cached and u2 > 0
+    assert np.array_equal(a, b)
+    _abi.release_device_cache()
+    assert _abi.device_cache_bytes()[0] == 0

@@ -27,6 +27,7 @@ EXPORTS = sorted([
     "thistle_plan_execute_device", "thistle_plan_recompute_device", "thistle_plan_execute_quartets",
     "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
     "thistle_plan_destroy", "thistle_plan_records", "thistle_bessel_sum_static",
+    "thistle_release_device_cache", "thistle_device_cache_bytes",
 ])
 
 
@@ -90,8 +91,24 @@ def lib():
     L.thistle_plan_timings.argtypes = [VP, D]
     L.thistle_plan_destroy.restype = C.c_int
     L.thistle_plan_destroy.argtypes = [VP]
+    L.thistle_release_device_cache.restype = C.c_int
+    L.thistle_release_device_cache.argtypes = []
+    L.thistle_device_cache_bytes.restype = C.c_int
+    L.thistle_device_cache_bytes.argtypes = [I64, I64]
     _lib = L
     return L
+
+
+def device_cache_bytes():
+    """(cached, in_use) bytes of the library's device-buffer cache on the current device."""
+    c, u = C.c_int64(0), C.c_int64(0)
+    check(lib().thistle_device_cache_bytes(C.byref(c), C.byref(u)))
+    return c.value, u.value
+
+
+def release_device_cache():
+    """Return the cached device buffers and idle cuBLAS handles of the current device to the driver."""
+    check(lib().thistle_release_device_cache())
 
 
 def check(rc: int):

@@ -7,7 +7,7 @@
 //                   accurate generator), warp per quartet, lanes over q,
 //                   accumulated per warp in shared memory
 //  tb_reduce        fixed-order sum of the per-block partial I(q)
-//  tb_ghat_scatter / tb_pack_pairs / tb_sym_small: the density transform's
+//  ghat_emit / ghat_runs / pack_pairs / sym_small: the density transform's
 //                   gathers (variables_total z11/z22 :1045-1065 re-expressed
 //                   as a 4-index transform)
 #include <cuda_runtime.h>
@@ -271,10 +271,13 @@ __global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, i
 // density transform helpers
 // ---------------------------------------------------------------------------
 
-// Ghat[x][y][z][w] += Gamma_t/8 over the eight index placements of a row
-// (both orders inside each pair, both pair orders); see tb_plan.cu.
-__global__ void ghat_scatter_kernel(const int *__restrict__ mat, const double *__restrict__ total, int nmat,
-                                    int n, double *__restrict__ G) {
+// Ghat[x][y][z][w] = sum of Gamma_t/8 over the eight index placements of
+// every row (both orders inside each pair, both pair orders); see tb_plan.cu.
+// Deterministic in two steps: every (row, placement) emits (flat index,
+// value); after a stable sort by index each run of equal indices is summed
+// in its sorted (row, placement) order by the run's first element.
+__global__ void ghat_emit_kernel(const int *__restrict__ mat, const double *__restrict__ total, int nmat, int n,
+                                 int *__restrict__ keys, double *__restrict__ vals) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nmat) return;
   int a = mat[t] - 1, b = mat[t + nmat] - 1, c = mat[t + 2 * nmat] - 1, d = mat[t + 3 * nmat] - 1;
@@ -282,9 +285,18 @@ __global__ void ghat_scatter_kernel(const int *__restrict__ mat, const double *_
   int P[8][4] = {{a, b, c, d}, {b, a, c, d}, {a, b, d, c}, {b, a, d, c},
                  {c, d, a, b}, {d, c, a, b}, {c, d, b, a}, {d, c, b, a}};
   for (int k = 0; k < 8; ++k) {
-    size_t idx = (((size_t)P[k][0] * n + P[k][1]) * n + P[k][2]) * n + P[k][3];
-    atomicAdd(&G[idx], v);
+    keys[8 * t + k] = ((P[k][0] * n + P[k][1]) * n + P[k][2]) * n + P[k][3];
+    vals[8 * t + k] = v;
   }
+}
+
+__global__ void ghat_runs_kernel(const int *__restrict__ keys, const double *__restrict__ vals, int64_t m,
+                                 double *__restrict__ G) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m || (i > 0 && keys[i - 1] == keys[i])) return;
+  double s = vals[i];
+  for (int64_t j = i + 1; j < m && keys[j] == keys[i]; ++j) s += vals[j];
+  G[keys[i]] = s;
 }
 
 // out[b][fpair(c,d)] = in[b][c][d] for c <= d
@@ -380,9 +392,16 @@ cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *ou
   return cudaGetLastError();
 }
 
-cudaError_t launch_ghat_scatter(const int *mat, const double *total, int nmat, int n, double *G, cudaStream_t st) {
+cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int n, int *keys, double *vals,
+                             cudaStream_t st) {
   if (nmat <= 0) return cudaSuccess;
-  ghat_scatter_kernel<<<(nmat + 255) / 256, 256, 0, st>>>(mat, total, nmat, n, G);
+  ghat_emit_kernel<<<(nmat + 255) / 256, 256, 0, st>>>(mat, total, nmat, n, keys, vals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  ghat_runs_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(keys, vals, m, G);
   return cudaGetLastError();
 }
 

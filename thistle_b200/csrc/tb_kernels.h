@@ -1,6 +1,7 @@
 // Internal launch interface between the plan code and the kernels.
 #pragma once
 
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -73,6 +74,12 @@ int stage2_quartets_per_warp(int LB);
 int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
 cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st);
 
+// Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
+cudaError_t pool_malloc(void **p, size_t bytes);
+void pool_free(void *p);
+cublasHandle_t pool_cublas();
+void pool_cublas_release(cublasHandle_t h);
+
 // Sets the calling thread's error string (thistle_last_error_string) and returns code.
 int set_error(int code, const std::string &msg);
 
@@ -86,8 +93,9 @@ cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st)
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);
-cudaError_t launch_ghat_scatter(const int *mat, const double *total, int nmat, int n, double *G,
-                                cudaStream_t st);
+cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int n, int *keys, double *vals,
+                             cudaStream_t st);
+cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st);
 cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
 cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st);

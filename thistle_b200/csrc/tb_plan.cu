@@ -14,7 +14,10 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -26,6 +29,19 @@
 using namespace tb;
 
 static thread_local std::string g_err;
+
+// THISTLE_B200_TRACE=1 prints the host-side duration of the set-up phases to stderr.
+struct PhaseTrace {
+  bool on = std::getenv("THISTLE_B200_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  void mark(const char *what) {
+    if (!on) return;
+    auto t1 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[thistle_b200] %-28s %9.3f ms\n", what,
+                 std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
 
 static int fail(int code, const std::string &msg) {
   g_err = msg;
@@ -48,23 +64,25 @@ int set_error(int code, const std::string &msg) { return fail(code, msg); }
       return fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); \
   } while (0)
 
+// Device buffers come from the process-wide cache (tb_pool.cu).
 template <class T>
 static int dalloc(T **p, size_t n, const char *what) {
   *p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  void *v = nullptr;
+  cudaError_t e = pool_malloc(&v, n * sizeof(T));
   if (e != cudaSuccess) {
-    *p = nullptr;
     cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? THISTLE_ERR_NOMEM : THISTLE_ERR_CUDA,
                 std::string("cudaMalloc of ") + what + " (" + std::to_string(n * sizeof(T)) + " bytes): " +
                     cudaGetErrorString(e));
   }
+  *p = (T *)v;
   return THISTLE_OK;
 }
 template <class T>
 static void dfree(T *&p) {
-  if (p) cudaFree(p);
+  if (p) pool_free((void *)p);
   p = nullptr;
 }
 
@@ -88,6 +106,12 @@ struct thistle_plan {
   int *d_mat = nullptr;
   double *d_C = nullptr, *d_tot = nullptr, *d_D = nullptr, *d_Ds = nullptr, *d_Y = nullptr;
   double *d_G = nullptr, *d_T1 = nullptr, *d_T2 = nullptr, *d_V = nullptr, *d_T3 = nullptr;
+  // Ghat build: (index, value) per row placement, sorted by index
+  int *d_gk0 = nullptr, *d_gk1 = nullptr;
+  double *d_gv0 = nullptr, *d_gv1 = nullptr;
+  void *d_gsort_tmp = nullptr;
+  size_t gsort_bytes = 0;
+  int gbits = 0;
   // quartet enumeration workspaces
   int64_t *d_braoff = nullptr;
   int *d_gL = nullptr;
@@ -298,6 +322,16 @@ static int density_alloc(thistle_plan *P) {
     TB_TRY(dalloc(&P->d_T2, (size_t)(n2 * ngto * ngto), "transform T2"));
     TB_TRY(dalloc(&P->d_V, (size_t)(n2 * np), "transform V"));
     TB_TRY(dalloc(&P->d_T3, (size_t)((int64_t)n * ngto * np), "transform T3"));
+    const int64_t m = std::max<int64_t>(8 * (int64_t)P->nmat, 1);
+    TB_TRY(dalloc(&P->d_gk0, (size_t)m, "Ghat keys"));
+    TB_TRY(dalloc(&P->d_gk1, (size_t)m, "Ghat keys"));
+    TB_TRY(dalloc(&P->d_gv0, (size_t)m, "Ghat values"));
+    TB_TRY(dalloc(&P->d_gv1, (size_t)m, "Ghat values"));
+    P->gbits = 1;
+    while (P->gbits < 31 && ((int64_t)1 << P->gbits) < n4) ++P->gbits;
+    TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->gsort_bytes, P->d_gk0, P->d_gk1, P->d_gv0, P->d_gv1,
+                                            (int)m, 0, P->gbits, P->st));
+    TB_TRY(dalloc((char **)&P->d_gsort_tmp, P->gsort_bytes, "Ghat sort scratch"));
   }
 done:
   return rc;
@@ -335,8 +369,15 @@ static int density_run(thistle_plan *P) {
   TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
   if (P->nmat == 0) goto done;
   TB_TRYC(cudaMemsetAsync(P->d_G, 0, sizeof(double) * (size_t)n4, P->st));
-  TB_TRYC(launch_ghat_scatter(P->d_mat, P->d_tot, P->nmat, n, P->d_G, P->st));
-  P->launches += 1;
+  {
+    const int64_t m = 8 * (int64_t)P->nmat;
+    size_t bytes = P->gsort_bytes;
+    TB_TRYC(launch_ghat_emit(P->d_mat, P->d_tot, P->nmat, n, P->d_gk0, P->d_gv0, P->st));
+    TB_TRYC(cub::DeviceRadixSort::SortPairs(P->d_gsort_tmp, bytes, P->d_gk0, P->d_gk1, P->d_gv0, P->d_gv1, (int)m,
+                                            0, P->gbits, P->st));
+    TB_TRYC(launch_ghat_runs(P->d_gk1, P->d_gv1, m, P->d_G, P->st));
+    P->launches += 3;
+  }
   // T1'(ngto x n^3) = C^T Ghat'   (C is (n, ngto) column-major, the mmod layout)
   TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, (int)n3, n, &one, P->d_C, n, P->d_G, n, &zero, P->d_T1,
                       ngto));
@@ -411,11 +452,12 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
   dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3);
+  dfree(P->d_gk0); dfree(P->d_gk1); dfree(P->d_gv0); dfree(P->d_gv1); dfree(P->d_gsort_tmp);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
   dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
-  if (P->d_s2sort_tmp) cudaFree(P->d_s2sort_tmp);
-  if (P->d_sort_tmp) cudaFree(P->d_sort_tmp);
-  if (P->cb) cublasDestroy(P->cb);
+  dfree(P->d_s2sort_tmp);
+  dfree(P->d_sort_tmp);
+  if (P->cb) pool_cublas_release(P->cb);
   if (P->have_ev) {
     for (int i = 0; i < 10; ++i) cudaEventDestroy(P->ev[i]);
     for (int r = 0; r < thistle_plan::NRING; ++r)
@@ -449,6 +491,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   thistle_plan *P = new thistle_plan();
   int rc = THISTLE_OK;
   std::vector<int64_t> cnt;
+  PhaseTrace tr;
   TB_TRY(check_basis(P, ngto, ga, l, m, n, xx, yy, zz, group));
   TB_TRY(check_q(q, nq));
   if (!std::isfinite(cutoffz) || !std::isfinite(cutoffmd) || !std::isfinite(cutoffcentre) || cutoffz < 0 ||
@@ -473,6 +516,10 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     P->nmo1 = nmo1;
   } else {
     if (nmat < 0 || (nmat > 0 && (!mat || !total))) { rc = fail(THISTLE_ERR_ARG, "missing 2-RDM rows"); goto done; }
+    if (norbs > 215) {
+      rc = fail(THISTLE_ERR_ARG, "at most 215 MOs for the 2-RDM transform (norbs^4 must index in 32 bits)");
+      goto done;
+    }
     for (int64_t i = 0; i < (int64_t)nmat * 4; ++i)
       if (mat[i] < 1 || mat[i] > norbs) {
         rc = fail(THISTLE_ERR_SHAPE, "2-RDM index out of range 1..norbs at row " + std::to_string(i % nmat + 1));
@@ -483,14 +530,20 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   }
   class_counts(P->gL, cnt);
   TB_TRY(setup_classes(P, cnt, P->kind));
+  tr.mark("validation, classes");
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
   for (int i = 0; i < 10; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
   for (int r = 0; r < thistle_plan::NRING; ++r)
     for (int i = 0; i < 5; ++i) TB_TRYC(cudaEventCreate(&P->rev[r][i]));
   P->have_ev = true;
-  TB_TRYB(cublasCreate(&P->cb));
+  P->cb = pool_cublas();
+  if (!P->cb) {
+    rc = fail(THISTLE_ERR_CUDA, "cublasCreate failed");
+    goto done;
+  }
   TB_TRYB(cublasSetStream(P->cb, P->st));
   TB_TRYB(cublasSetMathMode(P->cb, CUBLAS_PEDANTIC_MATH));
+  tr.mark("stream, events, cuBLAS");
   TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_flmn, (size_t)ngto, "functions"));
@@ -507,10 +560,13 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRYC(cudaMemcpyAsync(P->d_ga, ga, sizeof(double) * ngto, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
   TB_TRY(upload_centres(P, xx, yy, zz));
+  tr.mark("small buffers, uploads");
   TB_TRY(density_alloc(P));
   TB_TRY(density_upload(P, mmod, mat, total, onerdm));
+  tr.mark("density buffers");
   TB_TRY(quartets_alloc(P));
   TB_TRY(dalloc(&P->d_rec, (size_t)P->rec_total, "quartet records"));
+  tr.mark("quartet buffers");
   {
     int dev = 0;
     TB_TRYC(cudaGetDevice(&dev));
@@ -535,6 +591,8 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     TB_TRY(dalloc((char **)&P->d_s2sort_tmp, P->s2sort_bytes, "stage-2 sort scratch"));
     TB_TRYC(launch_iota(P->d_iota, P->nquart, P->st));
   }
+  TB_TRYC(cudaStreamSynchronize(P->st));
+  tr.mark("stage-2 buffers");
   P->launches = 0;
   TB_TRYC(cudaEventRecord(P->ev[6], P->st));
   TB_TRY(density_run(P));
@@ -542,6 +600,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(quartets_run(P));
   TB_TRYC(cudaEventRecord(P->ev[8], P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));
+  tr.mark("density transform, quartets");
   {
     float t = 0;
     if (cudaEventElapsedTime(&t, P->ev[6], P->ev[7]) == cudaSuccess) P->ms[4] = t;
@@ -871,8 +930,10 @@ int thistle_plan_timings(const thistle_plan *P, double *ms) {
 
 int thistle_plan_destroy(thistle_plan *P) {
   if (P) {
+    PhaseTrace tr;
     if (P->st) cudaStreamSynchronize(P->st);
     plan_free(P);
+    tr.mark("plan destroy");
   }
   return THISTLE_OK;
 }
@@ -895,7 +956,9 @@ int thistle_total_scattering(int32_t type, const double *Zn, const double *geom,
     plan_free(P);
     return fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
   }
+  PhaseTrace tr;
   rc = thistle_plan_execute(P, result_out);
+  tr.mark("execute");
   if (rc == THISTLE_OK && q_abs_out)
     for (int i = 0; i < nq; ++i) q_abs_out[i] = q[i];
   thistle_plan_destroy(P);

@@ -61,10 +61,14 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
 // Largest LLmax handled by the register kernel, and its threads per quartet.
 constexpr int STAGE1_REG_MAXL = 8;
 TB_HD constexpr int stage1_reg_split(int L) { return L <= 4 ? 1 : (L == 5 ? 2 : (L == 6 ? 4 : 8)); }
+// The heaviest classes have few quartets with many function quartets each:
+// P groups of S threads split the bra function pairs of a quartet, and the P
+// partial densities are summed in a fixed order.
+TB_HD constexpr int stage1_reg_parts(int L) { return L >= 7 ? 4 : 1; }
 // Threads per quartet of the shared-memory kernel.
 TB_HD constexpr int stage1_smem_split(int L) { return L <= 15 ? 32 : 16; }
 TB_HD constexpr int stage1_split(int L) {
-  return L <= STAGE1_REG_MAXL ? stage1_reg_split(L) : stage1_smem_split(L);
+  return L <= STAGE1_REG_MAXL ? stage1_reg_split(L) * stage1_reg_parts(L) : stage1_smem_split(L);
 }
 // Resident blocks asked of the register allocator: the largest count whose
 // register cap (65536 / (128 x blocks)) still holds the kernel without spills.
@@ -242,14 +246,17 @@ __device__ __forceinline__ const double *esoa_slot(const Stage1Args &A, bool ski
 template <int L, int KIND>
 __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kernel(Stage1Args A) {
   constexpr int S = stage1_reg_split(L);
+  constexpr int PP = stage1_reg_parts(L);
+  constexpr int G = S * PP;              // threads per quartet
   constexpr int NE = reg_entries(L, S);
-  constexpr int NG = 128 / S;            // quartet groups per block
+  constexpr int NG = 128 / S;            // density columns per block: one per S threads
   constexpr int TMAX = L < 2 * MAXA ? L : 2 * MAXA;  // last E index an axis can reach
-  extern __shared__ double sD[];         // ntuv(L) x NG: one density column per group
-  const int sub = threadIdx.x % S, grp = threadIdx.x / S;
+  extern __shared__ double sD[];         // ntuv(L) x NG
+  const int gsub = threadIdx.x % G;      // thread within the quartet's group
+  const int sub = gsub % S, part = gsub / S, grp = threadIdx.x / S;
   const int lane = threadIdx.x & 31;
-  const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
-  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane - gsub));
+  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
   // whole groups leave together (S divides 32)
   if (qi >= A.qend) return;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
@@ -264,8 +271,9 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
   const int sj = A.gstart[Q.gj], nj = A.gcount[Q.gj];
   const int sk = A.gstart[Q.gk], nk = A.gcount[Q.gk];
   const int sr = A.gstart[Q.gr], nr = A.gcount[Q.gr];
-  for (int ia = 0; ia < ni; ++ia) {
-    for (int ib = 0; ib < nj; ++ib) {
+  for (int ab = part; ab < ni * nj; ab += PP) {
+    {
+      const int ia = ab / nj, ib = ab - ia * nj;
       const int fa = si + ia, fb = sj + ib;
       const int la = A.flmn[fa], lb = A.flmn[fb];
       const int64_t rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
@@ -358,8 +366,20 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
           if (S == 1 || V <= L - T - U) col[dindex<L>(T, U, V) * NG] = D[e];
         }
   }
-  if (S > 1) __syncwarp(gmask);
-  stage1_finish<L, KIND, S>(A, Q, col, NG, qi, sub, gmask);
+  if (G > 1) __syncwarp(gmask);
+  if (PP > 1) {
+    // fixed-order sum of the P partial densities into the first part's column
+    double *col0 = sD + (threadIdx.x - gsub) / S;
+    for (int k = gsub; k < ntuv(L); k += G) {
+      double t = col0[k * NG];
+#pragma unroll
+      for (int p = 1; p < PP; ++p) t += col0[k * NG + p];
+      col0[k * NG] = t;
+    }
+    __syncwarp(gmask);
+    col = col0;
+  }
+  stage1_finish<L, KIND, G>(A, Q, col, NG, qi, gsub, gmask);
 }
 
 // ---------------------------------------------------------------------------
@@ -500,7 +520,7 @@ static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t 
     cudaError_t e =
         cudaFuncSetAttribute(stage1_reg_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    int64_t threads = n * S;
+    int64_t threads = n * S * stage1_reg_parts(L);
     stage1_reg_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
   } else {
     constexpr int S = stage1_smem_split(L);
