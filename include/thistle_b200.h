@@ -50,7 +50,7 @@ int thistle_version(void);
  * files: mat/total/nmat are read_twordm's rows (src/one_rdm.f90:2112-2147),
  * onerdm is read_onerdm's matrix (:2072-2108).
  *
- *   type          1 total j0, 2 elastic j0, 7 total j2
+ *   type          1 total j0, 2 elastic j0, 3 total aligned, 7 total j2
  *   Zn, geom      atomic numbers and (natoms,3) geometry; not used by these
  *                 types (kept for the reference's argument list), may be NULL
  *   maxl          maxval(l) as the reference passes it (checked, not trusted)
@@ -64,6 +64,12 @@ int thistle_version(void);
  *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (type 2)
  *   q_abs_out     nq doubles, set to q (the reference returns |q| here)
  *   result_out    nq doubles, I(q)
+ * Type 3 (CASE(3), src/main_calculation.f90:156-217) evaluates the aligned
+ * intensity on the reference's own QCOORD3 grid (k0 = 10.583544175): nq must
+ * be 3131, q is not read, q_abs_out gets |q| of the grid vectors and
+ * result_out the real part of I(q) (the reference writes it, with the
+ * imaginary part, to result_aligned.dat; the imaginary part is zero, see
+ * thistle_plan_execute_aligned).
  * All pointers are host pointers.
  */
 int thistle_total_scattering(int32_t type, const double *Zn, const double *geom, int32_t natoms,
@@ -91,6 +97,18 @@ int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const d
                         const double *total, int32_t nmat, const double *onerdm, int32_t nmo1,
                         const double *q, int32_t nq, double cutoffz, double cutoffmd,
                         double cutoffcentre);
+/* Type THISTLE_TOTAL_ALIGNED plans take q as nq vectors, a (3, nq)
+ * column-major array (the reference's q_al layout), and evaluate
+ * tot_integration_aligned (src/Integrals.f90:1425-1573) on them;
+ * thistle_plan_execute then returns the real part.  This returns both parts:
+ * the reference sums all ng^4 ordered quartets, whose bra-ket exchange
+ * conjugates each term, so the imaginary part is zero (written as 0.0; the
+ * reference's own is rounding noise).  im_host may be NULL. */
+int thistle_plan_execute_aligned(thistle_plan *plan, double *re_host, double *im_host);
+/* The 3131 aligned q vectors of the reference (QCOORD3,
+ * src/main_calculation.f90:864-929) for beam wavevector k0, written as a
+ * (3, 3131) column-major array.  Host-only. */
+int thistle_qcoord3(double k0, double *q_al);
 /* Run the plan on a caller-owned cudaStream_t (passed as void*); the plan
  * stops using its own stream.  The caller keeps the stream alive. */
 int thistle_plan_set_stream(thistle_plan *plan, void *stream);

@@ -27,7 +27,8 @@ EXPORTS = sorted([
     "thistle_plan_execute_device", "thistle_plan_recompute_device", "thistle_plan_execute_quartets",
     "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
     "thistle_plan_destroy", "thistle_plan_records", "thistle_bessel_sum_static",
-    "thistle_release_device_cache", "thistle_device_cache_bytes",
+    "thistle_release_device_cache", "thistle_device_cache_bytes", "thistle_plan_execute_aligned",
+    "thistle_qcoord3",
 ])
 
 
@@ -91,6 +92,10 @@ def lib():
     L.thistle_plan_timings.argtypes = [VP, D]
     L.thistle_plan_destroy.restype = C.c_int
     L.thistle_plan_destroy.argtypes = [VP]
+    L.thistle_plan_execute_aligned.restype = C.c_int
+    L.thistle_plan_execute_aligned.argtypes = [VP, D, D]
+    L.thistle_qcoord3.restype = C.c_int
+    L.thistle_qcoord3.argtypes = [C.c_double, D]
     L.thistle_release_device_cache.restype = C.c_int
     L.thistle_release_device_cache.argtypes = []
     L.thistle_device_cache_bytes.restype = C.c_int

@@ -371,9 +371,10 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st) {
-  // instantiated in tb_stage1_total.cu, tb_stage1_elastic.cu, tb_stage1_j2.cu
+  // instantiated in tb_stage1_{total,elastic,j2,aligned}.cu
   if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, st);
   if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_k<KIND_ALIGNED>(L, a, st);
   return launch_stage1_k<KIND_J2>(L, a, st);
 }
 

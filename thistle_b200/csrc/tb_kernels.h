@@ -74,6 +74,18 @@ int stage2_quartets_per_warp(int LB);
 int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
 cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st);
 
+// Aligned intensity of one LLmax class on q vectors (tb_aligned.cu).
+struct AlignedArgs {
+  const double *rec;          // class records [Hx, Hy, Hz, s, w K K' D_TUV...]
+  int rs;
+  int64_t nquart;
+  const double *qv;           // nq vectors, (qx, qy, qz) interleaved
+  int nq;
+  double *partial;            // gridDim.y rows of pstride doubles, accumulated (+=)
+  int64_t pstride;
+};
+cudaError_t launch_aligned(int L, const AlignedArgs &a, int slices, cudaStream_t st);
+
 // Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
 cudaError_t pool_malloc(void **p, size_t bytes);
 void pool_free(void *p);

@@ -43,7 +43,7 @@ constexpr int SER_K = 24;
 #define TB_SKIP30 1.0000000031710769e-30
 #define TB_PI 3.141592653589793
 
-enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2 };
+enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2, KIND_ALIGNED = 3 };
 enum RecKind { REC_BESSEL = 0, REC_BESSEL_J2 = 1, REC_P0 = 2 };
 
 // number of (T,U,V) with T+U+V <= L

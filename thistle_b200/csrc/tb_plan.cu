@@ -91,7 +91,8 @@ struct thistle_plan {
   int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nq = 0, maxa = 0, nmat = 0;
   double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
   std::vector<int> gstart, gcount, gL, flmn;
-  std::vector<double> hq;            // host copy of the q grid
+  std::vector<double> hq;            // host copy of the q grid (aligned: interleaved q vectors)
+  int qdim = 1;                      // 3 for aligned plans (q vectors)
   int64_t nquart = 0, np = 0;
   int ncls = 0;
   int cls_L[MAXCLS];
@@ -258,9 +259,9 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
     P->cls_L[k] = LL;
     P->cls_begin[k] = pos;
     P->cls_end[k] = pos + c;
-    int rs = LL + 7;  // [H, s, kind, order] + up to LL+3 coefficients
+    // [H, s, kind, order] + up to LL+3 coefficients; aligned: [H vector, s] + D_TUV
+    int rs = kind == KIND_ALIGNED ? 4 + ntuv(LL) : LL + 7;
     rs += rs & 1;
-    (void)kind;
     P->cls_rs[k] = rs;
     P->cls_recoff[k] = recoff;
     recoff += c * rs;
@@ -486,14 +487,21 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
                        int32_t nq, double cutoffz, double cutoffmd, double cutoffcentre) {
   if (!out) return fail(THISTLE_ERR_ARG, "null plan pointer");
   *out = nullptr;
-  if (type != THISTLE_TOTAL_J0 && type != THISTLE_ELASTIC_J0 && type != THISTLE_TOTAL_J2)
+  if (type != THISTLE_TOTAL_J0 && type != THISTLE_ELASTIC_J0 && type != THISTLE_TOTAL_J2 &&
+      type != THISTLE_TOTAL_ALIGNED)
     return fail(THISTLE_ERR_TYPE, "calculation type " + std::to_string(type) + " is not provided by this entry");
   thistle_plan *P = new thistle_plan();
   int rc = THISTLE_OK;
   std::vector<int64_t> cnt;
   PhaseTrace tr;
   TB_TRY(check_basis(P, ngto, ga, l, m, n, xx, yy, zz, group));
-  TB_TRY(check_q(q, nq));
+  if (type == THISTLE_TOTAL_ALIGNED) {
+    // q holds nq vectors, (3, nq) column-major like the reference's q_al
+    if (!q || nq <= 0) { rc = fail(THISTLE_ERR_ARG, "empty q-vector list"); goto done; }
+    if (!finite_all(q, 3 * (int64_t)nq)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite q vector"); goto done; }
+  } else {
+    TB_TRY(check_q(q, nq));
+  }
   if (!std::isfinite(cutoffz) || !std::isfinite(cutoffmd) || !std::isfinite(cutoffcentre) || cutoffz < 0 ||
       cutoffmd < 0 || cutoffcentre < 0) {
     rc = fail(THISTLE_ERR_ARG, "cutoffs must be finite and non-negative");
@@ -502,9 +510,12 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   if (!mmod || norbs <= 0) { rc = fail(THISTLE_ERR_ARG, "missing MO coefficients"); goto done; }
   if (!finite_all(mmod, (int64_t)norbs * ngto)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite MO coefficient"); goto done; }
   P->type = type;
-  P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL : (type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC : KIND_J2);
+  P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL
+            : type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC
+            : type == THISTLE_TOTAL_ALIGNED ? KIND_ALIGNED : KIND_J2;
   P->nq = nq;
-  P->hq.assign(q, q + nq);
+  P->qdim = type == THISTLE_TOTAL_ALIGNED ? 3 : 1;
+  P->hq.assign(q, q + (int64_t)P->qdim * nq);
   P->nmo = norbs;
   P->cutoffz = cutoffz;
   P->cutoffmd = cutoffmd;
@@ -549,7 +560,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(dalloc(&P->d_flmn, (size_t)ngto, "functions"));
   TB_TRY(dalloc(&P->d_ga, (size_t)ngto, "exponents"));
   TB_TRY(dalloc(&P->d_xyz, (size_t)ngto * 3, "centres"));
-  TB_TRY(dalloc(&P->d_q, (size_t)nq, "q"));
+  TB_TRY(dalloc(&P->d_q, (size_t)P->qdim * nq, "q"));
   TB_TRY(dalloc(&P->d_result, (size_t)nq, "result"));
   TB_TRY(dalloc(&P->d_pairtab, (size_t)npairs(P->ng) * PAIR_STRIDE, "pair tables"));
   TB_TRY(dalloc(&P->d_esoa, (size_t)esoa_doubles(P->ng, P->maxa), "transposed E tables"));
@@ -558,7 +569,12 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRYC(cudaMemcpyAsync(P->d_gcount, P->gcount.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_flmn, P->flmn.data(), sizeof(int) * ngto, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_ga, ga, sizeof(double) * ngto, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
+  if (P->qdim == 3) {
+    // (3, nq) column-major = the vectors' components interleaved
+    TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice, P->st));
+  } else {
+    TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
+  }
   TB_TRY(upload_centres(P, xx, yy, zz));
   tr.mark("small buffers, uploads");
   TB_TRY(density_alloc(P));
@@ -574,12 +590,14 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     P->s2_qtile = std::min(nq, STAGE2_QTILE);
     int maxbps = 1;
     for (int b = 0; b <= LMAXB; ++b) P->s2_bps[b] = 0;
-    for (int c = 0; c < P->ncls; ++c) {
+    for (int c = 0; c < P->ncls && P->kind != KIND_ALIGNED; ++c) {
       int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
       P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, P->kind == KIND_J2, P->s2_qtile);
       maxbps = std::max(maxbps, P->s2_bps[LB]);
     }
-    P->s2_rows = P->nsm * maxbps;
+    // aligned: quartet slices of the q-vector kernel (one partial row each)
+    P->s2_rows = P->kind == KIND_ALIGNED ? std::max(1, 4 * P->nsm / std::max(1, (nq + 127) / 128)) : P->nsm * maxbps;
+    if (P->kind == KIND_ALIGNED) P->s2_rows = std::min(P->s2_rows, 4 * P->nsm);
     TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_rows * nq, "partial sums"));
     const int64_t n = std::max<int64_t>(P->nquart, 1);
     TB_TRY(dalloc(&P->d_s2key, (size_t)n, "stage-2 keys"));
@@ -670,13 +688,34 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.recbase = recoff[c];
     a.rs = rs[c];
     a.p0count = (unsigned long long *)(P->d_p0count + c);
-    a.s2key = order ? P->d_s2key : nullptr;
+    a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
     TB_CK(launch_stage1(P->kind, cL[c], a, P->st));
     P->launches += 1;
   }
   TB_CK(cudaEventRecord(E[2], P->st));
   int64_t nall = ncls > 0 ? ce[ncls - 1] : 0;
+  if (P->kind == KIND_ALIGNED) {
+    TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
+    for (int c = 0; c < ncls; ++c) {
+      AlignedArgs s;
+      s.rec = d_rec + recoff[c];
+      s.rs = rs[c];
+      s.nquart = ce[c] - cb[c];
+      s.qv = P->d_q;
+      s.nq = P->nq;
+      s.partial = P->d_partial;
+      s.pstride = P->nq;
+      const int slices = (int)std::max<int64_t>(1, std::min<int64_t>(P->s2_rows, (s.nquart + 31) / 32));
+      TB_CK(launch_aligned(cL[c], s, slices, P->st));
+      P->launches += 1;
+    }
+    TB_CK(cudaEventRecord(E[3], P->st));
+    TB_CK(launch_reduce(P->d_partial, P->s2_rows, P->nq, d_out, P->st));
+    P->launches += 1;
+    TB_CK(cudaEventRecord(E[4], P->st));
+    return THISTLE_OK;
+  }
   if (order && nall > 0) {
     size_t bytes = P->s2sort_bytes;
     TB_CK(cub::DeviceRadixSort::SortPairs(P->d_s2sort_tmp, bytes, P->d_s2key, P->d_s2key_sorted, P->d_iota,
@@ -743,10 +782,70 @@ static void read_timings(thistle_plan *P) {
   }
 }
 
+// The reference's aligned q grid (QCOORD3, src/main_calculation.f90:864-929):
+// the origin, one point on the +y axis, a hexagon of radius dk, then rings of
+// radius i dk (i = 2..31) with ceil(pi / asin(1/(2i))) points each starting on
+// +y, every point lifted onto the Ewald sphere of radius k0; dk =
+// sqrt(3)/2 k0/31.  Unused slots and zero components are 1e-10, as there.
+static void qcoord3_grid(double k0, double *qal /* (3, 3131) column-major */) {
+  const int nring = 30, npts = 3131;
+  const double pi = std::acos(-1.0);
+  const double dk = std::sqrt(3.0) / 2.0 * k0 / (nring + 1.0);
+  double *qx = qal, *qy = qal + 1, *qz = qal + 2;  // stride 3
+  for (int t = 0; t < npts; ++t) qx[3 * t] = qy[3 * t] = qz[3 * t] = 1.0e-10;
+  auto lift = [&](double x, double y) { return k0 * (1.0 - std::sqrt(std::fabs(1.0 - (x * x + y * y) / (k0 * k0)))); };
+  int pos = 1;  // 0-based slot of the +y point
+  qy[3 * pos] = dk;
+  qz[3 * pos] = k0 * (1.0 - std::sqrt(1.0 - 1.0 / ((nring + 1.0) * (nring + 1.0))));
+  for (int i = 1; i <= 5; ++i) {
+    ++pos;
+    const double x = std::sin(i * pi / 3.0) * dk, y = std::cos(i * pi / 3.0) * dk;
+    qx[3 * pos] = x;
+    qy[3 * pos] = y;
+    qz[3 * pos] = k0 * (1.0 - std::sqrt(1.0 - (x * x + y * y) / (k0 * k0)));
+  }
+  for (int i = 2; i <= nring + 1; ++i) {
+    const int np = (int)std::ceil(pi / std::asin(1.0 / (2.0 * i)));
+    const double rc = i * dk, ang = 2.0 * pi / np;
+    ++pos;
+    qy[3 * pos] = rc;
+    qz[3 * pos] = k0 * (1.0 - std::sqrt(std::fabs(1.0 - std::pow((double)i, 2.0) / ((nring + 1.0) * (nring + 1.0)))));
+    for (int j = 1; j <= np - 1; ++j) {
+      ++pos;
+      const double x = std::sin(j * ang) * rc, y = std::cos(j * ang) * rc;
+      qx[3 * pos] = x;
+      qy[3 * pos] = y;
+      qz[3 * pos] = lift(x, y);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+int thistle_qcoord3(double k0, double *q_al) {
+  if (!q_al) return fail(THISTLE_ERR_ARG, "null argument");
+  if (!std::isfinite(k0) || !(k0 > 0.0)) return fail(THISTLE_ERR_ARG, "k0 must be finite and positive");
+  qcoord3_grid(k0, q_al);
+  return THISTLE_OK;
+}
+
+int thistle_plan_execute_aligned(thistle_plan *P, double *re_host, double *im_host) {
+  if (!P || !re_host) return fail(THISTLE_ERR_ARG, "null argument");
+  if (P->kind != KIND_ALIGNED) return fail(THISTLE_ERR_TYPE, "not an aligned plan (type 3)");
+  P->launches = 0;
+  int rc = plan_exec(P, P->d_result);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaMemcpyAsync(re_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
+  TB_CK(cudaStreamSynchronize(P->st));
+  // the ordered quartet sum is real: bra-ket exchange conjugates each term
+  if (im_host)
+    for (int i = 0; i < P->nq; ++i) im_host[i] = 0.0;
+  read_timings(P);
+  return THISTLE_OK;
+}
 
 const char *thistle_last_error_string(void) { return g_err.c_str(); }
 
@@ -836,7 +935,8 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
     int64_t u = t;
     while (u < nquart && items[u].first / 625 == LL) ++u;
     cb[ncls] = t; ce[ncls] = u; cL[ncls] = LL;
-    rs[ncls] = (LL + 7) + ((LL + 7) & 1);
+    rs[ncls] = P->kind == KIND_ALIGNED ? 4 + ntuv(LL) : LL + 7;
+    rs[ncls] += rs[ncls] & 1;
     ro[ncls] = roff;
     roff += (u - t) * rs[ncls];
     ++ncls;
@@ -948,6 +1048,15 @@ int thistle_total_scattering(int32_t type, const double *Zn, const double *geom,
   (void)Zn; (void)geom; (void)natoms;
   if (!result_out) return fail(THISTLE_ERR_ARG, "null result");
   if (maxl < 0) return fail(THISTLE_ERR_ARG, "maxl must be >= 0");
+  // type 3 evaluates on the reference's own aligned grid (QCOORD3 with
+  // k0 = 10.583544175, 3131 vectors), whatever q holds; q_abs_out gets |q|
+  std::vector<double> qal;
+  if (type == THISTLE_TOTAL_ALIGNED) {
+    if (nq != 3131) return fail(THISTLE_ERR_SHAPE, "type 3 runs on the 3131-vector QCOORD3 grid: nq must be 3131");
+    qal.resize(3 * 3131);
+    qcoord3_grid(10.583544175, qal.data());
+    q = qal.data();
+  }
   thistle_plan *P = nullptr;
   int rc = plan_create(&P, type, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, mat, total, nmat, onerdm, nmo1,
                        q, nq, cutoffz, cutoffmd, cutoffcentre);
@@ -959,8 +1068,12 @@ int thistle_total_scattering(int32_t type, const double *Zn, const double *geom,
   PhaseTrace tr;
   rc = thistle_plan_execute(P, result_out);
   tr.mark("execute");
-  if (rc == THISTLE_OK && q_abs_out)
-    for (int i = 0; i < nq; ++i) q_abs_out[i] = q[i];
+  if (rc == THISTLE_OK && q_abs_out) {
+    for (int i = 0; i < nq; ++i)
+      q_abs_out[i] = type == THISTLE_TOTAL_ALIGNED
+                         ? std::sqrt(q[3 * i] * q[3 * i] + q[3 * i + 1] * q[3 * i + 1] + q[3 * i + 2] * q[3 * i + 2])
+                         : q[i];
+  }
   thistle_plan_destroy(P);
   return rc;
 }

@@ -101,10 +101,11 @@ __device__ __forceinline__ QuartetHead quartet_head(const Stage1Args &A, int64_t
   Q.Hz = Q.tk[2] - Q.tb[2];
   Q.h = sqrt(Q.Hx * Q.Hx + Q.Hy * Q.Hy + Q.Hz * Q.Hz);
   Q.loop = quartet_loop(Q.gi, Q.gj, Q.gk, Q.gr);
-  Q.p0 = Q.loop == 5 || Q.h < A.cutoffcentre;
+  // the aligned kernel has no P = Q branch (tot_integral_k_ijkr_alig, src/Integrals.f90:5588-5727)
+  Q.p0 = KIND == KIND_ALIGNED ? false : (Q.loop == 5 || Q.h < A.cutoffcentre);
   // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
   // a skipped factor removes every term it multiplies, i.e. it is a zero.
-  Q.skip = Q.p0 ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : (KIND == KIND_ELASTIC ? 0x1f : 0x0f));
+  Q.skip = (Q.p0 || KIND == KIND_ALIGNED || KIND == KIND_ELASTIC) ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : 0x0f);
   return Q;
 }
 
@@ -125,6 +126,17 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
   const double pre = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
   double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
   const bool leader = sub == 0;
+  if (KIND == KIND_ALIGNED) {
+    // [Hx, Hy, Hz, 1/4p+1/4p', w K K' D_TUV...]: the q-vector kernel forms
+    // sum_TUV D_TUV (i qx)^T (i qy)^U (i qz)^V exp(i q.H) itself
+    if (!leader) return;
+    r[0] = Q.Hx;
+    r[1] = Q.Hy;
+    r[2] = Q.Hz;
+    r[3] = Q.tb[5] + Q.tk[5];
+    for (int k = 0; k < ntuv(L); ++k) r[4 + k] = pre * D[k * dstride];
+    return;
+  }
   if (Q.p0) {
     // F(q) = sum_s c_s q^{2s}, c_s = (-1)^s sum_{T+U+V=2s, even} D P0-factor
     constexpr int NS = L / 2 + 1;

@@ -1,0 +1,7 @@
+// Stage-1 kernels of one calculation kind (see tb_stage1.cuh); one
+// translation unit per kind so that the builds run in parallel.
+#include "tb_stage1.cuh"
+
+namespace tb {
+template cudaError_t launch_stage1_k<KIND_ALIGNED>(int L, const Stage1Args &a, cudaStream_t st);
+}  // namespace tb

@@ -49,7 +49,11 @@ def read_onerdm(filename):
 def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
                                  mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=None, total=None,
                                  onerdm=None):
-    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 7 total j2).
+    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 7 total j2).
+
+    Type 3 runs on the reference's QCOORD3 grid (``nq`` must be 3131; ``q``
+    is not read): ``q_abs`` is |q| of the grid vectors and ``result`` the real
+    part of the aligned intensity.
 
     ``mmod`` is (norbs, ngto) as the reference passes it; ``mat``/``total``
     are the 2-RDM rows (types 1 and 7), ``onerdm`` the 1-RDM (type 2).
@@ -111,8 +115,13 @@ class ScatteringPlan:
         ga, l, m, n, xx, yy, zz, group = self._keep
         mmod = np.asarray(mmod, dtype=np.float64)
         self.ngto = int(ga.size)
-        self.q = _abi.as_f64(q)
-        self.nq = int(self.q.size)
+        if self.type == TOTAL_ALIGNED:
+            # nq vectors; the C side takes them (3, nq) column-major = rows of (qx, qy, qz)
+            self.q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(-1, 3))
+            self.nq = int(self.q.shape[0])
+        else:
+            self.q = _abi.as_f64(q)
+            self.nq = int(self.q.size)
         mcm = colmajor_f64(mmod)
         matcm = colmajor_i32(mat) if mat is not None else None
         tot = _abi.as_f64(total) if total is not None else None
@@ -140,6 +149,12 @@ class ScatteringPlan:
         out = np.zeros(self.nq) if out is None else out
         check(_abi.lib().thistle_plan_execute(self._p, dptr(out)))
         return out
+
+    def execute_aligned(self):
+        """Aligned plans: (Re, Im) of I(q) per q vector (Im is identically zero)."""
+        re, im = np.zeros(self.nq), np.zeros(self.nq)
+        check(_abi.lib().thistle_plan_execute_aligned(self._p, dptr(re), dptr(im)))
+        return re, im
 
     def execute_device(self, ptr: int):
         """Integrator only, I(q) to the device address ``ptr`` (stream-ordered)."""
@@ -215,6 +230,20 @@ class ScatteringPlan:
             self.close()
         except Exception:
             pass
+
+
+def qcoord3(k0: float = 10.583544175) -> np.ndarray:
+    """The reference's 3131 aligned q vectors (QCOORD3), shape (3131, 3)."""
+    out = np.zeros((3131, 3))
+    check(_abi.lib().thistle_qcoord3(float(k0), dptr(out)))
+    return out
+
+
+def aligned(prob, qvec=None):
+    """Aligned total intensity (Re, Im) of a Problem on q vectors (default: the QCOORD3 grid)."""
+    qv = qcoord3() if qvec is None else np.asarray(qvec, dtype=np.float64).reshape(-1, 3)
+    with ScatteringPlan.from_problem(prob, TOTAL_ALIGNED, q=qv) as pl:
+        return pl.execute_aligned()
 
 
 def scattering(prob, type=TOTAL_J0, q=None):
