@@ -105,6 +105,19 @@ int thistle_plan_create(thistle_plan **plan, int32_t type, int32_t ngto, const d
  * conjugates each term, so the imaginary part is zero (written as 0.0; the
  * reference's own is rounding noise).  im_host may be NULL. */
 int thistle_plan_execute_aligned(thistle_plan *plan, double *re_host, double *im_host);
+/* Adjoint of total j0 (type 1) with respect to the Gaussian centres.  No
+ * counterpart in the reference.  For a cotangent v (nq doubles) it returns
+ * grad[3 g + axis] = sum_q v(q) dI(q)/dA_g,axis for every group g (ng x 3,
+ * row-major): the centre of group g is A_g; a nuclear gradient is the sum over
+ * the groups on that atom.  The pair density (MO coefficients and RDM) is held
+ * fixed; McMurchie-Davidson coefficients, Gaussian-product prefactors and the
+ * Bessel argument |P_kr - P_ij| carry the geometry.  Quartets on the P = Q
+ * branch contribute through their prefactors and coefficients only (that
+ * branch does not depend on H).  Runs the forward stages first unless the
+ * last execution used the current centres.  LLmax <= 8 (s, p, d shells). */
+int thistle_plan_vjp(thistle_plan *plan, const double *v_host, double *grad_host);
+/* Same with device pointers, on the plan's stream (no synchronisation). */
+int thistle_plan_vjp_device(thistle_plan *plan, const double *v_dev, double *grad_dev);
 /* The 3131 aligned q vectors of the reference (QCOORD3,
  * src/main_calculation.f90:864-929) for beam wavevector k0, written as a
  * (3, 3131) column-major array.  Host-only. */

@@ -28,7 +28,7 @@ EXPORTS = sorted([
     "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
     "thistle_plan_destroy", "thistle_plan_records", "thistle_bessel_sum_static",
     "thistle_release_device_cache", "thistle_device_cache_bytes", "thistle_plan_execute_aligned",
-    "thistle_qcoord3",
+    "thistle_qcoord3", "thistle_plan_vjp", "thistle_plan_vjp_device",
 ])
 
 
@@ -94,6 +94,10 @@ def lib():
     L.thistle_plan_destroy.argtypes = [VP]
     L.thistle_plan_execute_aligned.restype = C.c_int
     L.thistle_plan_execute_aligned.argtypes = [VP, D, D]
+    L.thistle_plan_vjp.restype = C.c_int
+    L.thistle_plan_vjp.argtypes = [VP, D, D]
+    L.thistle_plan_vjp_device.restype = C.c_int
+    L.thistle_plan_vjp_device.argtypes = [VP, VP, VP]
     L.thistle_qcoord3.restype = C.c_int
     L.thistle_qcoord3.argtypes = [C.c_double, D]
     L.thistle_release_device_cache.restype = C.c_int

@@ -1,0 +1,456 @@
+// Adjoint of the total-j0 intensity with respect to the Gaussian centres: for
+// a cotangent v(q) the vector-Jacobian product
+//   g_c = sum_q v(q) dI(q)/dA_c        (A_c the centre of group c, 3 numbers)
+// No reference counterpart (THISTLE computes I(q) only); the derivatives are
+// those of the forward path of tot_integration (src/Integrals.f90:8-472,
+// 5068-5226).  Per group quartet the forward value is
+//   I_Q(q) = w K K' exp(-q^2 s) sum_TUV D_TUV G_TUV(q; H),
+//   G_TUV = d^T/dHx d^U/dHy d^V/dHz j0(q|H|) = sum_k a_x a_y a_z J_b(q),
+//   J_b(q) = j_b(qH) (q/H)^b,  b = (T-k1) + (U-k2) + (V-k3)
+// (a the rrdj0 Hermite-like tables), or the P = Q polynomial when H is below
+// cutoffcentre.  The geometry enters through K K' (the Gaussian-product
+// prefactors), H = P_kr - P_ij and the McMurchie-Davidson coefficients inside
+// D; the pair density rho is fixed.
+//
+// Stage A (q side, per quartet): Jbar_b = H^{-2b} sum_q v(q) exp(-q^2 s)
+//   g_b(qH) for b <= LLmax + 1 (g_b = j_b x^b from the same generator as the
+//   forward stage 2), or the moments M_s = sum_q v exp(-q^2 s) q^{2s} for
+//   P = Q quartets.  Lanes over quartets, no cross-lane sums.
+// Stage B (function-quartet side, thread per quartet):
+//   Abar_TUV = w K K' sum_k a a a Jbar_b   (T+U+V <= LLmax + 1), then over the
+//   function quartets, with the convolutions C of the forward stage 1 and
+//   their centre derivatives dC (from dE/dA_i = 2 a_i E^{la+1,lb} - la
+//   E^{la-1,lb} - (a_i/p) E^{la,lb}_{t-1} + 2 mu X E^{la,lb}, K excluded):
+//     S0   = sum rho Abar.C C C             (-> d(K K')/dA: -2 mu X S0)
+//     gH   = sum rho Abar_{TUV+e}.C C C      (-> dH/dA = -a_i/p, +a_k/p'), 0 for P = Q
+//     gE_i = sum rho Abar.dC_i C C, gE_k likewise (dE/dA_j = -dE/dA_i)
+//   and the four centres' gradients go into per-warp rows of shared memory
+//   in a fixed order (deterministic), then into per-block partial rows.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_kernels.h"
+#include "tb_math.cuh"
+#include "tb_stage1.cuh"
+
+namespace tb {
+
+namespace {
+
+constexpr int DE_T = 2 * MAXA + 2;  // t = 0 .. 2 MAXA + 1
+
+__device__ void emd(int l1, int l2, double PA, double PB, double a, double *out) {
+  if (l1 >= l2) md_chain(l1, l2, PA, PB, a, out);
+  else md_chain(l2, l1, PB, PA, a, out);
+}
+
+// dE^{la,lb}_t / dA_i (first centre of the pair), transposed like the E table:
+// element t of (axis, la, lb) at dsoa[((axis (maxa+1) + la) (maxa+1) + lb) DE_T + t][pair].
+__global__ void pair_dtables_kernel(int ng, int maxa, const int *__restrict__ gstart, const double *__restrict__ ga,
+                                    const double *__restrict__ xyz, double *__restrict__ dsoa) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t npair = npairs(ng);
+  if (p >= npair) return;
+  int i = 0, rem = p;
+  while (rem >= ng - i) { rem -= ng - i; ++i; }
+  const int j = i + rem;
+  const int fi = gstart[i], fj = gstart[j];
+  const double ai = ga[fi], aj = ga[fj], gp = ai + aj, mu = ai * aj / gp;
+  for (int ax = 0; ax < 3; ++ax) {
+    const double xi = xyz[3 * fi + ax], xj = xyz[3 * fj + ax];
+    const double P = (ai * xi + aj * xj) / gp, X = xi - xj;
+    const double PA = P - xi, PB = P - xj, a = 0.5 / gp;
+    double E0[DE_T], Ep[DE_T], Em[DE_T];
+    for (int la = 0; la <= maxa; ++la)
+      for (int lb = 0; lb <= maxa; ++lb) {
+        emd(la, lb, PA, PB, a, E0);
+        emd(la + 1, lb, PA, PB, a, Ep);
+        if (la > 0) emd(la - 1, lb, PA, PB, a, Em);
+        const int64_t slot = ((int64_t)(ax * (maxa + 1) + la) * (maxa + 1) + lb) * DE_T;
+        for (int t = 0; t < DE_T; ++t) {
+          double d = 0.0;
+          if (t <= la + lb + 1) d = 2.0 * ai * Ep[t];
+          if (la > 0 && t <= la + lb - 1) d -= la * Em[t];
+          if (t >= 1 && t - 1 <= la + lb) d -= ai / gp * E0[t - 1];
+          if (t <= la + lb) d += 2.0 * mu * X * E0[t];
+          dsoa[(slot + t) * npair + p] = d;
+        }
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage A
+// ---------------------------------------------------------------------------
+template <int N, int NK>
+__device__ __forceinline__ double series_un(double y) {
+  double p = series_coef(N, NK);
+#pragma unroll
+  for (int k = NK - 1; k >= 0; --k) p = fma(p, y, series_coef(N, k));
+  return p;
+}
+
+// g_b = j_b(x) x^b for b = 0..LB1 below the crossover: series for the top two
+// orders, downward recurrence, g_b = y^b / (2b+1)!! u_b.
+template <int LB1>
+__device__ __noinline__ void gb_small(double y, double *g) {
+  constexpr int NK = series_terms(LB1);
+  double uhi = series_un<LB1 + 1, NK>(y);
+  double umid = series_un<LB1, NK>(y);
+  double u[LB1 + 1];
+  u[LB1] = umid;
+#pragma unroll
+  for (int b = LB1; b >= 1; --b) {
+    double ulo = umid - (y * (1.0 / ((2.0 * b + 1.0) * (2.0 * b + 3.0)))) * uhi;
+    u[b - 1] = ulo;
+    uhi = umid;
+    umid = ulo;
+  }
+  double w = 1.0;
+#pragma unroll
+  for (int b = 0; b <= LB1; ++b) {
+    g[b] = w * u[b];
+    w *= y / (2.0 * b + 3.0);
+  }
+}
+
+template <int LB1>
+__global__ void __launch_bounds__(128) adjoint_q_kernel(AdjointQArgs A) {
+  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= A.nquart) return;
+  const int64_t idx = A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot;
+  const double *rec = A.rec + idx * A.rs;
+  double *out = A.adj + idx * A.rs;
+  const bool p0 = (int)rec[2] == REC_P0;
+  const double H = p0 ? 1.0 : rec[0], s = rec[1], invH = 1.0 / H;
+  constexpr double XC = bessel_crossover(LB1);
+  double acc[LB1 + 1];
+#pragma unroll
+  for (int b = 0; b <= LB1; ++b) acc[b] = 0.0;
+  const double dq = A.dq;
+  double sd = 0.0, cd = 1.0;
+  sincos(dq * H, &sd, &cd);
+  const double kk = exp(-2.0 * dq * dq * s);
+  double sn = 0.0, cs = 0.0, g = 0.0, r = 0.0;
+  int next_seed = 0;
+  for (int m = 0; m < A.nq; ++m) {
+    const double q = A.q[m], vq = A.v[m];
+    if (m == next_seed) {
+      sincos(q * H, &sn, &cs);
+      g = exp(-(q * q) * s);
+      r = exp(-(2.0 * q * dq + dq * dq) * s);
+      next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + 64);
+    }
+    const double w = vq * g;
+    if (p0) {
+      // moments sum_q v exp(-q^2 s) q^{2s}
+      const double q2 = q * q;
+      double t = w;
+#pragma unroll
+      for (int b = 0; b <= LB1; ++b) {
+        acc[b] += t;
+        t *= q2;
+      }
+    } else {
+      const double x = q * H;
+      double gb[LB1 + 1];
+      if (x >= XC) {
+        gb[0] = sn * ((1.0 / q) * invH);
+        gb[1] = gb[0] - cs;
+        const double y = x * x;
+#pragma unroll
+        for (int b = 1; b < LB1; ++b) gb[b + 1] = fma((double)(2 * b + 1), gb[b], -y * gb[b - 1]);
+      } else {
+        gb_small<LB1>(x * x, gb);
+      }
+#pragma unroll
+      for (int b = 0; b <= LB1; ++b) acc[b] = fma(w, gb[b], acc[b]);
+    }
+    const double s2 = fma(sn, cd, cs * sd);
+    cs = fma(cs, cd, -sn * sd);
+    sn = s2;
+    g *= r;
+    r *= kk;
+  }
+  if (p0) {
+#pragma unroll
+    for (int b = 0; b <= LB1; ++b) out[b] = acc[b];
+  } else {
+    const double ih2 = invH * invH;
+    double f = 1.0;
+#pragma unroll
+    for (int b = 0; b <= LB1; ++b) {
+      out[b] = acc[b] * f;
+      f *= ih2;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage B
+// ---------------------------------------------------------------------------
+constexpr int ADJ_THREADS = 64;
+
+template <int L>
+__device__ __forceinline__ int adx(int T, int U, int V) {  // simplex index of order L+1
+  return ntuv(L + 1) - ntuv(L + 1 - T) + U * (L + 2 - T) - (U * (U - 1)) / 2 + V;
+}
+
+__device__ __forceinline__ const double *dsoa_slot(const AdjointFArgs &A, int axis, int la, int lb, int pair) {
+  const int m1 = A.s1.emaxa + 1;
+  return A.dsoa + (int64_t)((axis * m1 + la) * m1 + lb) * DE_T * A.s1.npair + pair;
+}
+
+template <int L>
+__global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) {
+  constexpr int L1 = L + 1;
+  constexpr int NA = ntuv(L1);
+  constexpr int TM = L < 2 * MAXA ? L : 2 * MAXA;          // last E index
+  constexpr int TD = L1 < 2 * MAXA + 1 ? L1 : 2 * MAXA + 1;  // last dE index
+  extern __shared__ double sm[];
+  const int ng = A.s1.ng;
+  double *gw = sm + (size_t)ADJ_THREADS * NA + (threadIdx.x >> 5) * 3 * ng;  // this warp's gradient row
+  for (int i = threadIdx.x; i < (ADJ_THREADS / 32) * 3 * ng; i += ADJ_THREADS) sm[(size_t)ADJ_THREADS * NA + i] = 0.0;
+  __syncthreads();
+  const Stage1Args &S = A.s1;
+  const int64_t n = S.qend - S.qbegin;
+  const int lane = threadIdx.x & 31;
+  double *Ab = sm + threadIdx.x;  // Abar_TUV at Ab[adx * ADJ_THREADS]
+  for (int64_t base = (int64_t)blockIdx.x * ADJ_THREADS; base < n; base += (int64_t)gridDim.x * ADJ_THREADS) {
+    const int64_t qi = S.qbegin + base + threadIdx.x;
+    const bool act = base + threadIdx.x < n;
+    double gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0}, gk[3] = {0, 0, 0}, gr[3] = {0, 0, 0};
+    int ci = 0, cj = 0, ck = 0, cr = 0;
+    if (act) {
+      const QuartetHead Q = quartet_head<KIND_TOTAL>(S, qi);
+      ci = Q.gi; cj = Q.gj; ck = Q.gk; cr = Q.gr;
+      const double *jb = A.adj + S.recbase + (qi - S.qbegin) * (int64_t)S.rs;
+      const double wpp = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
+      // Abar up to order L+1
+      if (Q.p0) {
+        for (int T = 0; T <= L1; ++T)
+          for (int U = 0; U <= L1 - T; ++U)
+            for (int V = 0; V <= L1 - T - U; ++V) {
+              double a = 0.0;
+              if (!((T | U | V) & 1)) {
+                const int k = (T + U + V) / 2;
+                a = p0_factor(T, U, V, false) * jb[k];
+                if (k & 1) a = -a;
+              }
+              Ab[adx<L>(T, U, V) * ADJ_THREADS] = wpp * a;
+            }
+      } else {
+        double ax[tp_size(L1)], ay[tp_size(L1)], az[tp_size(L1)];
+        hermite_table(L1, Q.Hx, ax);
+        hermite_table(L1, Q.Hy, ay);
+        hermite_table(L1, Q.Hz, az);
+        for (int T = 0; T <= L1; ++T)
+          for (int U = 0; U <= L1 - T; ++U)
+            for (int V = 0; V <= L1 - T - U; ++V) {
+              double a = 0.0;
+              for (int k1 = 0; 2 * k1 <= T; ++k1)
+                for (int k2 = 0; 2 * k2 <= U; ++k2)
+                  for (int k3 = 0; 2 * k3 <= V; ++k3)
+                    a += ax[tp_off(T) + k1] * ay[tp_off(U) + k2] * az[tp_off(V) + k3] *
+                         jb[(T - k1) + (U - k2) + (V - k3)];
+              Ab[adx<L>(T, U, V) * ADJ_THREADS] = wpp * a;
+            }
+      }
+      const int pb = pair_index(Q.gi, Q.gj, ng), pk = pair_index(Q.gk, Q.gr, ng);
+      const int64_t np = S.npair;
+      double S0 = 0.0, gH[3] = {0, 0, 0}, gEi[3] = {0, 0, 0}, gEk[3] = {0, 0, 0};
+      const int si = S.gstart[Q.gi], ni = S.gcount[Q.gi];
+      const int sj = S.gstart[Q.gj], nj = S.gcount[Q.gj];
+      const int sk = S.gstart[Q.gk], nk = S.gcount[Q.gk];
+      const int sr = S.gstart[Q.gr], nr = S.gcount[Q.gr];
+      for (int ab = 0; ab < ni * nj; ++ab) {
+        const int fa = si + ab / nj, fb = sj + ab % nj;
+        const int la = S.flmn[fa], lb = S.flmn[fb];
+        const int64_t rowp = fpair(min(fa, fb), max(fa, fb)) * S.np;
+        const int lab[3][2] = {{la & 0xff, lb & 0xff}, {(la >> 8) & 0xff, (lb >> 8) & 0xff},
+                               {(la >> 16) & 0xff, (lb >> 16) & 0xff}};
+        // bra E (signed, skips as forward) and bra dE/dA_i (signed)
+        double be[3][L + 1], bd[3][L1 + 1];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          const double *e = esoa_slot(S, Q.skip & (1 << ax), ax, lab[ax][0], lab[ax][1], pb);
+          const double *d = dsoa_slot(A, ax, lab[ax][0], lab[ax][1], pb);
+#pragma unroll
+          for (int t = 0; t <= L; ++t) {
+            const double v = t <= TM ? e[t * np] : 0.0;
+            be[ax][t] = (t & 1) ? -v : v;
+          }
+#pragma unroll
+          for (int t = 0; t <= L1; ++t) {
+            const double v = t <= TD ? d[t * np] : 0.0;
+            bd[ax][t] = (t & 1) ? -v : v;
+          }
+        }
+        for (int cd = 0; cd < nk * nr; ++cd) {
+          const int fc = sk + cd / nr, fd = sr + cd % nr;
+          double z = S.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+          z = fabs(z) < S.cutoffz ? 0.0 : z;
+          const int lc = S.flmn[fc], ld = S.flmn[fd];
+          const int lcd[3][2] = {{lc & 0xff, ld & 0xff}, {(lc >> 8) & 0xff, (ld >> 8) & 0xff},
+                                 {(lc >> 16) & 0xff, (ld >> 16) & 0xff}};
+          // per axis: C (forward), dCi (bra centre), dCk (ket centre), orders 0..L+1
+          double C[3][L1 + 1], Ci[3][L1 + 1], Ck[3][L1 + 1];
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax) {
+            const bool sk2 = ax == 0 ? (Q.skip & 8) : (ax == 1 ? (Q.skip & 16) : false);
+            const double *e = esoa_slot(S, sk2, ax, lcd[ax][0], lcd[ax][1], pk);
+            const double *d = dsoa_slot(A, ax, lcd[ax][0], lcd[ax][1], pk);
+            double ke[L + 1], kd[L1 + 1];
+#pragma unroll
+            for (int t = 0; t <= L; ++t) ke[t] = t <= TM ? e[t * np] : 0.0;
+#pragma unroll
+            for (int t = 0; t <= L1; ++t) kd[t] = t <= TD ? d[t * np] : 0.0;
+#pragma unroll
+            for (int T = 0; T <= L1; ++T) {
+              double c = 0.0, c1 = 0.0, c2 = 0.0;
+#pragma unroll
+              for (int t = 0; t <= T; ++t) {
+                if (t <= L && T - t <= L) c = fma(be[ax][t], ke[T - t], c);
+                c1 = fma(bd[ax][t], T - t <= L ? ke[T - t] : 0.0, c1);
+                if (t <= L) c2 = fma(be[ax][t], kd[T - t], c2);
+              }
+              C[ax][T] = c;
+              Ci[ax][T] = c1;
+              Ck[ax][T] = c2;
+            }
+          }
+          // contractions of Abar with two of the three convolutions
+          double Yx[L1 + 1], Yy[L1 + 1], Yz[L1 + 1];
+#pragma unroll
+          for (int i = 0; i <= L1; ++i) Yx[i] = Yy[i] = Yz[i] = 0.0;
+#pragma unroll
+          for (int T = 0; T <= L1; ++T)
+#pragma unroll
+            for (int U = 0; U <= L1 - T; ++U) {
+              double w = 0.0;
+              const double cxy = C[0][T] * C[1][U];
+#pragma unroll
+              for (int V = 0; V <= L1 - T - U; ++V) {
+                const double a = Ab[adx<L>(T, U, V) * ADJ_THREADS];
+                w = fma(a, C[2][V], w);
+                Yz[V] = fma(a, cxy, Yz[V]);
+              }
+              Yx[T] = fma(w, C[1][U], Yx[T]);
+              Yy[U] = fma(w, C[0][T], Yy[U]);
+            }
+          double s0 = 0.0, h0 = 0.0, h1 = 0.0, h2 = 0.0;
+#pragma unroll
+          for (int T = 0; T <= L; ++T) {
+            s0 = fma(C[0][T], Yx[T], s0);
+            h0 = fma(C[0][T], Yx[T + 1], h0);
+            h1 = fma(C[1][T], Yy[T + 1], h1);
+            h2 = fma(C[2][T], Yz[T + 1], h2);
+          }
+          double e0 = 0.0, e1 = 0.0, e2 = 0.0, k0 = 0.0, k1 = 0.0, k2 = 0.0;
+#pragma unroll
+          for (int T = 0; T <= L1; ++T) {
+            e0 = fma(Ci[0][T], Yx[T], e0);
+            e1 = fma(Ci[1][T], Yy[T], e1);
+            e2 = fma(Ci[2][T], Yz[T], e2);
+            k0 = fma(Ck[0][T], Yx[T], k0);
+            k1 = fma(Ck[1][T], Yy[T], k1);
+            k2 = fma(Ck[2][T], Yz[T], k2);
+          }
+          S0 = fma(z, s0, S0);
+          gH[0] = fma(z, h0, gH[0]);
+          gH[1] = fma(z, h1, gH[1]);
+          gH[2] = fma(z, h2, gH[2]);
+          gEi[0] = fma(z, e0, gEi[0]);
+          gEi[1] = fma(z, e1, gEi[1]);
+          gEi[2] = fma(z, e2, gEi[2]);
+          gEk[0] = fma(z, k0, gEk[0]);
+          gEk[1] = fma(z, k1, gEk[1]);
+          gEk[2] = fma(z, k2, gEk[2]);
+        }
+      }
+      if (Q.p0) gH[0] = gH[1] = gH[2] = 0.0;  // the P = Q polynomial does not depend on H
+      const double pij = Q.tb[3], pkr = Q.tk[3];
+      const int hi = S.gstart[Q.gi], hj = S.gstart[Q.gj], hk = S.gstart[Q.gk], hr = S.gstart[Q.gr];
+      const double ai = A.ga[hi], aj = A.ga[hj], ak = A.ga[hk], ar = A.ga[hr];
+      const double muij = ai * aj / pij, mukr = ak * ar / pkr;
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const double Xij = A.xyz[3 * hi + ax] - A.xyz[3 * hj + ax];
+        const double Xkr = A.xyz[3 * hk + ax] - A.xyz[3 * hr + ax];
+        gi[ax] = -2.0 * muij * Xij * S0 - ai / pij * gH[ax] + gEi[ax];
+        gj[ax] = 2.0 * muij * Xij * S0 - aj / pij * gH[ax] - gEi[ax];
+        gk[ax] = -2.0 * mukr * Xkr * S0 + ak / pkr * gH[ax] + gEk[ax];
+        gr[ax] = 2.0 * mukr * Xkr * S0 + ar / pkr * gH[ax] - gEk[ax];
+      }
+    }
+    // fixed-order accumulation into the warp's row: lane 0 adds lane 0's
+    // twelve values, then lane 1's, ...
+    for (int l = 0; l < 32; ++l) {
+      const int c4[4] = {__shfl_sync(0xffffffffu, ci, l), __shfl_sync(0xffffffffu, cj, l),
+                         __shfl_sync(0xffffffffu, ck, l), __shfl_sync(0xffffffffu, cr, l)};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const double v0 = __shfl_sync(0xffffffffu, gi[ax], l), v1 = __shfl_sync(0xffffffffu, gj[ax], l);
+        const double v2 = __shfl_sync(0xffffffffu, gk[ax], l), v3 = __shfl_sync(0xffffffffu, gr[ax], l);
+        if (lane == 0) {
+          gw[3 * c4[0] + ax] += v0;
+          gw[3 * c4[1] + ax] += v1;
+          gw[3 * c4[2] + ax] += v2;
+          gw[3 * c4[3] + ax] += v3;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * ng; i += ADJ_THREADS) {
+    double t = 0.0;
+    for (int w = 0; w < ADJ_THREADS / 32; ++w) t += sm[(size_t)ADJ_THREADS * NA + w * 3 * ng + i];
+    A.gpart[(size_t)blockIdx.x * A.gstride + i] += t;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const double *ga, const double *xyz,
+                                double *dsoa, cudaStream_t st) {
+  const int n = npairs(ng);
+  pair_dtables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, ga, xyz, dsoa);
+  return cudaGetLastError();
+}
+
+int64_t dsoa_doubles(int ng, int maxa) { return (int64_t)3 * (maxa + 1) * (maxa + 1) * DE_T * npairs(ng); }
+
+cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, cudaStream_t st) {
+  if (a.nquart <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((a.nquart + 127) / 128);
+  switch (LB1) {
+#define TB_Q(n) case n: adjoint_q_kernel<n><<<grid, 128, 0, st>>>(a); break;
+    TB_Q(1) TB_Q(2) TB_Q(3) TB_Q(4) TB_Q(5) TB_Q(6) TB_Q(7) TB_Q(8) TB_Q(9)
+#undef TB_Q
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t launch_adjoint_f_l(const AdjointFArgs &a, int grid, cudaStream_t st) {
+  const size_t smem = sizeof(double) * ((size_t)ADJ_THREADS * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng);
+  cudaError_t e = cudaFuncSetAttribute(adjoint_f_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  adjoint_f_kernel<L><<<grid, ADJ_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+int adjoint_f_threads() { return ADJ_THREADS; }
+
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, cudaStream_t st) {
+  if (a.s1.qend <= a.s1.qbegin) return cudaSuccess;
+  switch (L) {
+#define TB_F(n) case n: return launch_adjoint_f_l<n>(a, grid, st);
+    TB_F(0) TB_F(1) TB_F(2) TB_F(3) TB_F(4) TB_F(5) TB_F(6) TB_F(7) TB_F(8)
+#undef TB_F
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace tb

@@ -86,6 +86,34 @@ struct AlignedArgs {
 };
 cudaError_t launch_aligned(int L, const AlignedArgs &a, int slices, cudaStream_t st);
 
+// Adjoint (tb_adjoint.cu): vector-Jacobian product of total j0 w.r.t. the centres.
+struct AdjointQArgs {
+  const double *rec;          // the class's forward records
+  double *adj;                // per quartet: Jbar_b (b <= LLmax+1) or P = Q moments, same slots as rec
+  int rs;
+  int64_t nquart;
+  const uint32_t *perm;       // optional visiting order (as stage 2)
+  int64_t pbase;
+  const double *q, *v;        // q grid and cotangent, nq each
+  int nq;
+  int uniform, first_on_grid;
+  double dq;
+};
+struct AdjointFArgs {
+  Stage1Args s1;              // the class's quartets, tables and density (as stage 1)
+  const double *adj;          // stage-A output
+  const double *dsoa;         // dE/dA_i table
+  const double *ga, *xyz;     // per function
+  double *gpart;              // gridDim.x rows of gstride doubles (3 per group), accumulated (+=)
+  int64_t gstride;
+};
+int64_t dsoa_doubles(int ng, int maxa);
+int adjoint_f_threads();
+cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const double *ga, const double *xyz,
+                                double *dsoa, cudaStream_t st);
+cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, cudaStream_t st);
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, cudaStream_t st);
+
 // Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
 cudaError_t pool_malloc(void **p, size_t bytes);
 void pool_free(void *p);

@@ -138,6 +138,11 @@ struct thistle_plan {
   bool have_ev = false;
   float ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t launches = 0;              // own kernels launched by the last call
+  std::vector<double> hxyz;          // host copy of the centres (interleaved)
+  bool fwd_valid = false;            // records and visiting order match the current centres
+  // adjoint workspaces (allocated by the first vector-Jacobian product)
+  double *d_dsoa = nullptr, *d_adj = nullptr, *d_gpart = nullptr, *d_v = nullptr, *d_grad = nullptr;
+  int adj_rows = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -456,6 +461,7 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_gk0); dfree(P->d_gk1); dfree(P->d_gv0); dfree(P->d_gv1); dfree(P->d_gsort_tmp);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
   dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
+  dfree(P->d_dsoa); dfree(P->d_adj); dfree(P->d_gpart); dfree(P->d_v); dfree(P->d_grad);
   dfree(P->d_s2sort_tmp);
   dfree(P->d_sort_tmp);
   if (P->cb) pool_cublas_release(P->cb);
@@ -475,8 +481,11 @@ static int upload_centres(thistle_plan *P, const double *xx, const double *yy, c
     xyz[3 * i + 1] = yy[i];
     xyz[3 * i + 2] = zz[i];
   }
+  if (xyz == P->hxyz) return THISTLE_OK;  // unchanged: records stay valid
   TB_CK(cudaMemcpyAsync(P->d_xyz, xyz.data(), sizeof(double) * xyz.size(), cudaMemcpyHostToDevice, P->st));
   TB_CK(cudaStreamSynchronize(P->st));
+  P->hxyz.swap(xyz);
+  P->fwd_valid = false;
   return THISTLE_OK;
 }
 
@@ -652,6 +661,38 @@ static void grid_info(const double *q, int n, int &uniform, int &first_on_grid, 
 
 // Pair tables, stage 1 per class, the stage-2 visiting order (when `order`),
 // stage 2 per class and q tile, and the fixed-order reduction into d_out.
+// Stage-1 arguments of one class of a quartet list.
+static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t qbegin, int64_t qend,
+                              double *d_rec, int64_t recbase, int rs) {
+  Stage1Args a;
+  a.quartets = d_quart;
+  a.qbegin = qbegin;
+  a.qend = qend;
+  a.pairtab = P->d_pairtab;
+  a.ng = P->ng;
+  a.gstart = P->d_gstart;
+  a.gcount = P->d_gcount;
+  a.flmn = P->d_flmn;
+  a.rho = P->d_rho;
+  a.np = P->np;
+  a.zao = P->d_zao;
+  a.ngto = P->ngto;
+  a.cutoffz = P->cutoffz;
+  a.cutoffmd = P->cutoffmd;
+  a.cutoffcentre = P->cutoffcentre;
+  a.esoa = P->d_esoa;
+  a.eskip = esoa_doubles(P->ng, P->maxa) / 2;
+  a.emaxa = P->maxa;
+  a.npair = npairs(P->ng);
+  a.rec = d_rec;
+  a.recbase = recbase;
+  a.rs = rs;
+  a.p0count = nullptr;
+  a.s2key = nullptr;
+  a.cls = 0;
+  return a;
+}
+
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
                       double *d_out, bool order) {
@@ -664,29 +705,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
   TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS, P->st));
   TB_CK(cudaEventRecord(E[1], P->st));
   for (int c = 0; c < ncls; ++c) {
-    Stage1Args a;
-    a.quartets = d_quart;
-    a.qbegin = cb[c];
-    a.qend = ce[c];
-    a.pairtab = P->d_pairtab;
-    a.ng = P->ng;
-    a.gstart = P->d_gstart;
-    a.gcount = P->d_gcount;
-    a.flmn = P->d_flmn;
-    a.rho = P->d_rho;
-    a.np = P->np;
-    a.zao = P->d_zao;
-    a.ngto = P->ngto;
-    a.cutoffz = P->cutoffz;
-    a.cutoffmd = P->cutoffmd;
-    a.cutoffcentre = P->cutoffcentre;
-    a.esoa = P->d_esoa;
-    a.eskip = esoa_doubles(P->ng, P->maxa) / 2;
-    a.emaxa = P->maxa;
-    a.npair = npairs(P->ng);
-    a.rec = d_rec;
-    a.recbase = recoff[c];
-    a.rs = rs[c];
+    Stage1Args a = stage1_args(P, d_quart, cb[c], ce[c], d_rec, recoff[c], rs[c]);
     a.p0count = (unsigned long long *)(P->d_p0count + c);
     a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
@@ -769,8 +788,70 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
 }
 
 static int plan_exec(thistle_plan *P, double *d_out) {
-  return run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                    P->cls_rs, d_out, true);
+  int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
+                      P->cls_rs, d_out, true);
+  P->fwd_valid = rc == THISTLE_OK;
+  return rc;
+}
+
+// Vector-Jacobian product of total j0 with respect to the group centres:
+// grad[3 g + axis] = sum_q v(q) dI(q)/dA_g (tb_adjoint.cu).  Runs the forward
+// stages first when the records are not those of the current centres.
+static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
+  if (P->kind != KIND_TOTAL) return fail(THISTLE_ERR_TYPE, "the adjoint is provided for total j0 (type 1)");
+  for (int c = 0; c < P->ncls; ++c)
+    if (P->cls_L[c] > 8) return fail(THISTLE_ERR_ANGMOM, "the adjoint covers LLmax <= 8 (s, p, d shells)");
+  int rc = THISTLE_OK;
+  if (!P->d_dsoa) {
+    TB_TRY(dalloc(&P->d_dsoa, (size_t)dsoa_doubles(P->ng, P->maxa), "dE tables"));
+    TB_TRY(dalloc(&P->d_adj, (size_t)std::max<int64_t>(P->rec_total, 1), "adjoint records"));
+    P->adj_rows = 2 * P->nsm;
+    TB_TRY(dalloc(&P->d_gpart, (size_t)P->adj_rows * 3 * P->ng, "gradient rows"));
+  }
+  if (!P->fwd_valid) TB_TRY(plan_exec(P, P->d_result));
+  TB_TRYC(launch_pair_dtables(P->ng, P->maxa, P->d_gstart, P->d_ga, P->d_xyz, P->d_dsoa, P->st));
+  P->launches += 1;
+  {
+    int uniform = 0, first_on_grid = 0;
+    double dq = 0.0;
+    grid_info(P->hq.data(), P->nq, uniform, first_on_grid, dq);
+    for (int c = 0; c < P->ncls; ++c) {
+      AdjointQArgs a;
+      a.rec = P->d_rec + P->cls_recoff[c];
+      a.adj = P->d_adj + P->cls_recoff[c];
+      a.rs = P->cls_rs[c];
+      a.nquart = P->cls_end[c] - P->cls_begin[c];
+      a.perm = P->d_perm;
+      a.pbase = P->cls_begin[c];
+      a.q = P->d_q;
+      a.v = d_v;
+      a.nq = P->nq;
+      a.uniform = uniform;
+      a.first_on_grid = first_on_grid;
+      a.dq = dq;
+      TB_TRYC(launch_adjoint_q(P->cls_L[c] + 1, a, P->st));
+      P->launches += 1;
+    }
+  }
+  TB_TRYC(cudaMemsetAsync(P->d_gpart, 0, sizeof(double) * (size_t)P->adj_rows * 3 * P->ng, P->st));
+  for (int c = 0; c < P->ncls; ++c) {
+    AdjointFArgs a;
+    a.s1 = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c], P->cls_rs[c]);
+    a.adj = P->d_adj;
+    a.dsoa = P->d_dsoa;
+    a.ga = P->d_ga;
+    a.xyz = P->d_xyz;
+    a.gpart = P->d_gpart;
+    a.gstride = 3 * P->ng;
+    const int64_t n = P->cls_end[c] - P->cls_begin[c];
+    const int grid = (int)std::min<int64_t>(P->adj_rows, (n + adjoint_f_threads() - 1) / adjoint_f_threads());
+    TB_TRYC(launch_adjoint_f(P->cls_L[c], a, grid, P->st));
+    P->launches += 1;
+  }
+  TB_TRYC(launch_reduce(P->d_gpart, P->adj_rows, 3 * P->ng, d_grad, P->st));
+  P->launches += 1;
+done:
+  return rc;
 }
 
 static void read_timings(thistle_plan *P) {
@@ -830,6 +911,29 @@ int thistle_qcoord3(double k0, double *q_al) {
   if (!std::isfinite(k0) || !(k0 > 0.0)) return fail(THISTLE_ERR_ARG, "k0 must be finite and positive");
   qcoord3_grid(k0, q_al);
   return THISTLE_OK;
+}
+
+int thistle_plan_vjp(thistle_plan *P, const double *v_host, double *grad_host) {
+  if (!P || !v_host || !grad_host) return fail(THISTLE_ERR_ARG, "null argument");
+  if (!finite_all(v_host, P->nq)) return fail(THISTLE_ERR_NONFINITE, "non-finite cotangent");
+  P->launches = 0;
+  int rc = THISTLE_OK;
+  if (!P->d_v) {
+    TB_TRY(dalloc(&P->d_v, (size_t)P->nq, "cotangent"));
+    TB_TRY(dalloc(&P->d_grad, (size_t)3 * P->ng, "gradient"));
+  }
+  TB_TRYC(cudaMemcpyAsync(P->d_v, v_host, sizeof(double) * P->nq, cudaMemcpyHostToDevice, P->st));
+  TB_TRY(plan_vjp(P, P->d_v, P->d_grad));
+  TB_TRYC(cudaMemcpyAsync(grad_host, P->d_grad, sizeof(double) * 3 * P->ng, cudaMemcpyDeviceToHost, P->st));
+  TB_TRYC(cudaStreamSynchronize(P->st));
+done:
+  return rc;
+}
+
+int thistle_plan_vjp_device(thistle_plan *P, const double *v_dev, double *grad_dev) {
+  if (!P || !v_dev || !grad_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  return plan_vjp(P, v_dev, grad_dev);
 }
 
 int thistle_plan_execute_aligned(thistle_plan *P, double *re_host, double *im_host) {

@@ -115,6 +115,9 @@ class ScatteringPlan:
         ga, l, m, n, xx, yy, zz, group = self._keep
         mmod = np.asarray(mmod, dtype=np.float64)
         self.ngto = int(ga.size)
+        self.ng = int(group.max())
+        # first function of each group (its centre is the group's)
+        self.group_first = np.array([int(np.argmax(group == k + 1)) for k in range(self.ng)])
         if self.type == TOTAL_ALIGNED:
             # nq vectors; the C side takes them (3, nq) column-major = rows of (qx, qy, qz)
             self.q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(-1, 3))
@@ -155,6 +158,19 @@ class ScatteringPlan:
         re, im = np.zeros(self.nq), np.zeros(self.nq)
         check(_abi.lib().thistle_plan_execute_aligned(self._p, dptr(re), dptr(im)))
         return re, im
+
+    def vjp(self, v):
+        """Total j0: sum_q v(q) dI(q)/dA_g for every group centre A_g, shape (ng, 3)."""
+        v = _abi.as_f64(v)
+        if v.size != self.nq:
+            raise ValueError(f"cotangent has {v.size} entries, the plan {self.nq} q points")
+        g = np.zeros((self.ng, 3))
+        check(_abi.lib().thistle_plan_vjp(self._p, dptr(v), dptr(g)))
+        return g
+
+    def vjp_device(self, v_ptr: int, grad_ptr: int):
+        """Device pointers (nq and 3 ng doubles), on the plan's stream."""
+        check(_abi.lib().thistle_plan_vjp_device(self._p, C.c_void_p(v_ptr), C.c_void_p(grad_ptr)))
 
     def execute_device(self, ptr: int):
         """Integrator only, I(q) to the device address ``ptr`` (stream-ordered)."""
@@ -230,6 +246,14 @@ class ScatteringPlan:
             self.close()
         except Exception:
             pass
+
+
+def atom_gradient(prob, group_grad):
+    """Sum per-group centre gradients (ng, 3) onto the atoms carrying them."""
+    g0 = np.array([np.argmax(prob.group == k + 1) for k in range(prob.ng)])
+    out = np.zeros((prob.atoms.shape[0], 3))
+    np.add.at(out, prob.atom_of[g0], np.asarray(group_grad))
+    return out
 
 
 def qcoord3(k0: float = 10.583544175) -> np.ndarray:
