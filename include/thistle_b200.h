@@ -118,6 +118,32 @@ int thistle_plan_execute_aligned(thistle_plan *plan, double *re_host, double *im
 int thistle_plan_vjp(thistle_plan *plan, const double *v_host, double *grad_host);
 /* Same with device pointers, on the plan's stream (no synchronisation). */
 int thistle_plan_vjp_device(thistle_plan *plan, const double *v_dev, double *grad_dev);
+/*
+ * Geometry batches (no reference counterpart; the reference evaluates one
+ * geometry per call).  A plan can hold ngeom geometries of its basis that
+ * share its density, quartet list and stage-2 visiting order; every kernel
+ * then runs over all of them in one launch (the geometry is the grid's second
+ * dimension).  set_batch replicates geometry 0's centres into all slots;
+ * set_centres_batch takes ngeom x ngto x 3 interleaved host coordinates.
+ * execute_batch returns ngeom x nq doubles, vjp_batch takes ngeom x nq
+ * cotangents and returns ngeom x ng x 3 group-centre gradients (type 1).
+ * The single-geometry entry points work on geometry 0 of a batch.
+ * use_graph makes the batch entry points capture their launches once in a
+ * CUDA graph (forward, and the adjoint stages) and replay it; the graph is
+ * dropped when the batch size changes.
+ * autotune_batch times forward + adjoint per geometry for ngeom = 1, 2, 4, ..
+ * <= gmax and two stage-2 q tiles, keeps the fastest (ngeom, q tile) in the
+ * plan and reports it with its geometries per second.
+ */
+int thistle_plan_set_batch(thistle_plan *plan, int32_t ngeom);
+int thistle_plan_set_centres_batch(thistle_plan *plan, const double *xyz);
+int thistle_plan_execute_batch(thistle_plan *plan, double *result_host);
+int thistle_plan_execute_batch_device(thistle_plan *plan, double *result_dev);
+int thistle_plan_vjp_batch(thistle_plan *plan, const double *v_host, double *grad_host);
+int thistle_plan_vjp_batch_device(thistle_plan *plan, const double *v_dev, double *grad_dev);
+int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);
+int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom_best, int32_t *qtile_best,
+                                double *geoms_per_s);
 /* The 3131 aligned q vectors of the reference (QCOORD3,
  * src/main_calculation.f90:864-929) for beam wavevector k0, written as a
  * (3, 3131) column-major array.  Host-only. */

@@ -28,7 +28,10 @@ EXPORTS = sorted([
     "thistle_plan_info", "thistle_plan_class_counts", "thistle_plan_timings", "thistle_plan_stage_totals",
     "thistle_plan_destroy", "thistle_plan_records", "thistle_bessel_sum_static",
     "thistle_release_device_cache", "thistle_device_cache_bytes", "thistle_plan_execute_aligned",
-    "thistle_qcoord3", "thistle_plan_vjp", "thistle_plan_vjp_device",
+    "thistle_qcoord3", "thistle_plan_vjp", "thistle_plan_vjp_device", "thistle_plan_set_batch",
+    "thistle_plan_set_centres_batch", "thistle_plan_execute_batch", "thistle_plan_execute_batch_device",
+    "thistle_plan_vjp_batch", "thistle_plan_vjp_batch_device", "thistle_plan_use_graph",
+    "thistle_plan_autotune_batch",
 ])
 
 
@@ -98,6 +101,13 @@ def lib():
     L.thistle_plan_vjp.argtypes = [VP, D, D]
     L.thistle_plan_vjp_device.restype = C.c_int
     L.thistle_plan_vjp_device.argtypes = [VP, VP, VP]
+    for name, args in (("thistle_plan_set_batch", [VP, C.c_int32]), ("thistle_plan_set_centres_batch", [VP, D]),
+                       ("thistle_plan_execute_batch", [VP, D]), ("thistle_plan_execute_batch_device", [VP, VP]),
+                       ("thistle_plan_vjp_batch", [VP, D, D]), ("thistle_plan_vjp_batch_device", [VP, VP, VP]),
+                       ("thistle_plan_use_graph", [VP, C.c_int32]),
+                       ("thistle_plan_autotune_batch", [VP, C.c_int32, I32, I32, D])):
+        getattr(L, name).restype = C.c_int
+        getattr(L, name).argtypes = args
     L.thistle_qcoord3.restype = C.c_int
     L.thistle_qcoord3.argtypes = [C.c_double, D]
     L.thistle_release_device_cache.restype = C.c_int

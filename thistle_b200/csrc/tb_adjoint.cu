@@ -47,10 +47,13 @@ __device__ void emd(int l1, int l2, double PA, double PB, double a, double *out)
 // dE^{la,lb}_t / dA_i (first centre of the pair), transposed like the E table:
 // element t of (axis, la, lb) at dsoa[((axis (maxa+1) + la) (maxa+1) + lb) DE_T + t][pair].
 __global__ void pair_dtables_kernel(int ng, int maxa, const int *__restrict__ gstart, const double *__restrict__ ga,
-                                    const double *__restrict__ xyz, double *__restrict__ dsoa) {
+                                    const double *__restrict__ xyz, double *__restrict__ dsoa, int64_t gs_xyz,
+                                    int64_t gs_dsoa) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t npair = npairs(ng);
   if (p >= npair) return;
+  xyz += blockIdx.y * gs_xyz;
+  dsoa += blockIdx.y * gs_dsoa;
   int i = 0, rem = p;
   while (rem >= ng - i) { rem -= ng - i; ++i; }
   const int j = i + rem;
@@ -116,6 +119,9 @@ __device__ __noinline__ void gb_small(double y, double *g) {
 
 template <int LB1>
 __global__ void __launch_bounds__(128) adjoint_q_kernel(AdjointQArgs A) {
+  A.rec += blockIdx.y * A.gs_rec;
+  A.adj += blockIdx.y * A.gs_rec;
+  A.v += (int64_t)blockIdx.y * A.nq;
   const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= A.nquart) return;
   const int64_t idx = A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot;
@@ -203,6 +209,15 @@ __device__ __forceinline__ const double *dsoa_slot(const AdjointFArgs &A, int ax
 
 template <int L>
 __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) {
+  {
+    const int64_t g = blockIdx.y;  // geometry of a batch
+    A.s1.pairtab += g * A.s1.gs_pair;
+    A.s1.esoa += g * A.s1.gs_esoa;
+    A.adj += g * A.s1.gs_rec;
+    A.dsoa += g * A.gs_dsoa;
+    A.xyz += g * A.gs_xyz;
+    A.gpart += g * A.gs_gpart;
+  }
   constexpr int L1 = L + 1;
   constexpr int NA = ntuv(L1);
   constexpr int TM = L < 2 * MAXA ? L : 2 * MAXA;          // last E index
@@ -412,17 +427,18 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
 }  // namespace
 
 cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const double *ga, const double *xyz,
-                                double *dsoa, cudaStream_t st) {
+                                double *dsoa, int ngeom, int64_t gs_xyz, int64_t gs_dsoa, cudaStream_t st) {
   const int n = npairs(ng);
-  pair_dtables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, ga, xyz, dsoa);
+  pair_dtables_kernel<<<dim3((n + 127) / 128, ngeom), 128, 0, st>>>(ng, maxa, gstart, ga, xyz, dsoa, gs_xyz,
+                                                                     gs_dsoa);
   return cudaGetLastError();
 }
 
 int64_t dsoa_doubles(int ng, int maxa) { return (int64_t)3 * (maxa + 1) * (maxa + 1) * DE_T * npairs(ng); }
 
-cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, cudaStream_t st) {
+cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStream_t st) {
   if (a.nquart <= 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((a.nquart + 127) / 128);
+  const dim3 grid((unsigned)((a.nquart + 127) / 128), ngeom);
   switch (LB1) {
 #define TB_Q(n) case n: adjoint_q_kernel<n><<<grid, 128, 0, st>>>(a); break;
     TB_Q(1) TB_Q(2) TB_Q(3) TB_Q(4) TB_Q(5) TB_Q(6) TB_Q(7) TB_Q(8) TB_Q(9)
@@ -433,20 +449,20 @@ cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, cudaStream_t st) {
 }
 
 template <int L>
-static cudaError_t launch_adjoint_f_l(const AdjointFArgs &a, int grid, cudaStream_t st) {
+static cudaError_t launch_adjoint_f_l(const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st) {
   const size_t smem = sizeof(double) * ((size_t)ADJ_THREADS * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng);
   cudaError_t e = cudaFuncSetAttribute(adjoint_f_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  adjoint_f_kernel<L><<<grid, ADJ_THREADS, smem, st>>>(a);
+  adjoint_f_kernel<L><<<dim3(grid, ngeom), ADJ_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 int adjoint_f_threads() { return ADJ_THREADS; }
 
-cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, cudaStream_t st) {
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st) {
   if (a.s1.qend <= a.s1.qbegin) return cudaSuccess;
   switch (L) {
-#define TB_F(n) case n: return launch_adjoint_f_l<n>(a, grid, st);
+#define TB_F(n) case n: return launch_adjoint_f_l<n>(a, grid, ngeom, st);
     TB_F(0) TB_F(1) TB_F(2) TB_F(3) TB_F(4) TB_F(5) TB_F(6) TB_F(7) TB_F(8)
 #undef TB_F
     default: return cudaErrorInvalidValue;

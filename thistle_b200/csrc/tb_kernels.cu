@@ -32,10 +32,14 @@ int64_t esoa_doubles(int ng, int maxa) {
 __global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gstart,
                                    const int *__restrict__ flmn, const double *__restrict__ ga,
                                    const double *__restrict__ xyz, double *__restrict__ tab,
-                                   double *__restrict__ esoa) {
+                                   double *__restrict__ esoa, int64_t gs_xyz, int64_t gs_tab, int64_t gs_esoa) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t npair = npairs(ng);
   if (p >= npair) return;
+  // geometry blockIdx.y of a batch
+  xyz += blockIdx.y * gs_xyz;
+  tab += blockIdx.y * gs_tab;
+  esoa += blockIdx.y * gs_esoa;
   const int64_t skipoff = (int64_t)3 * (maxa + 1) * (maxa + 1) * E_T * npair;
   int i = 0, rem = p;
   while (rem >= ng - i) { rem -= ng - i; ++i; }
@@ -259,9 +263,12 @@ __global__ void __launch_bounds__(256) stage2_kernel(Stage2Args A) {
   }
 }
 
-__global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out) {
+__global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out,
+                              int64_t gs_in) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
+  partial += blockIdx.y * gs_in;
+  out += (int64_t)blockIdx.y * nq;
   double t = 0.0;
   for (int b = 0; b < nblocks; ++b) t += partial[(size_t)b * nq + i];
   out[i] = t;
@@ -364,18 +371,20 @@ __global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off,
 // host-side launchers
 // ---------------------------------------------------------------------------
 cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
-                               const double *xyz, double *tab, double *esoa, cudaStream_t st) {
+                               const double *xyz, double *tab, double *esoa, int ngeom, int64_t gs_xyz,
+                               int64_t gs_tab, int64_t gs_esoa, cudaStream_t st) {
   int n = npairs(ng);
-  pair_tables_kernel<<<(n + 127) / 128, 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab, esoa);
+  pair_tables_kernel<<<dim3((n + 127) / 128, ngeom), 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab, esoa,
+                                                                    gs_xyz, gs_tab, gs_esoa);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st) {
+cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st) {
   // instantiated in tb_stage1_{total,elastic,j2,aligned}.cu
-  if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, st);
-  if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, st);
-  if (kind == KIND_ALIGNED) return launch_stage1_k<KIND_ALIGNED>(L, a, st);
-  return launch_stage1_k<KIND_J2>(L, a, st);
+  if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, ngeom, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, ngeom, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_k<KIND_ALIGNED>(L, a, ngeom, st);
+  return launch_stage1_k<KIND_J2>(L, a, ngeom, st);
 }
 
 size_t stage2_smem_bytes(int nqp, int nwarps) { return sizeof(double) * (size_t)nqp * (3 + nwarps); }
@@ -389,7 +398,13 @@ cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_
 }
 
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st) {
-  reduce_kernel<<<(nq + 127) / 128, 128, 0, st>>>(partial, nblocks, nq, out);
+  reduce_kernel<<<(nq + 127) / 128, 128, 0, st>>>(partial, nblocks, nq, out, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_batch(const double *partial, int nblocks, int nq, int64_t gs_in, double *out, int ngeom,
+                                cudaStream_t st) {
+  reduce_kernel<<<dim3((nq + 127) / 128, ngeom), 128, 0, st>>>(partial, nblocks, nq, out, gs_in);
   return cudaGetLastError();
 }
 

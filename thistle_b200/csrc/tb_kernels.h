@@ -31,6 +31,9 @@ struct Stage1Args {
   unsigned long long *p0count; // P=Q quartets counted for this launch's class
   uint32_t *s2key;            // optional: stage-2 order key per quartet, (cls << 6) | h bucket
   int cls;                    // this launch's class index (for s2key)
+  // geometry batches: blockIdx.y is the geometry; its tables, records and
+  // counters sit these many elements after geometry 0's
+  int64_t gs_pair, gs_esoa, gs_rec;
 };
 
 constexpr int MAXCLS = 20;
@@ -66,13 +69,14 @@ struct Stage2ClassArgs {
   int j2;                     // Bessel records are j2 (F / q^2)
   double *partial;            // gridDim.x rows of pstride doubles, accumulated (+=)
   int64_t pstride;
+  int64_t gs_rec, gs_partial; // per-geometry strides (blockIdx.y is the geometry)
 };
 constexpr int STAGE2_WARPS = 8;
 // q points a stage-2 block holds in shared memory at once
 constexpr int STAGE2_QTILE = 1024;
 int stage2_quartets_per_warp(int LB);
 int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
-cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st);
 
 // Aligned intensity of one LLmax class on q vectors (tb_aligned.cu).
 struct AlignedArgs {
@@ -98,6 +102,7 @@ struct AdjointQArgs {
   int nq;
   int uniform, first_on_grid;
   double dq;
+  int64_t gs_rec;             // per-geometry record stride (blockIdx.y; v advances by nq)
 };
 struct AdjointFArgs {
   Stage1Args s1;              // the class's quartets, tables and density (as stage 1)
@@ -106,13 +111,14 @@ struct AdjointFArgs {
   const double *ga, *xyz;     // per function
   double *gpart;              // gridDim.x rows of gstride doubles (3 per group), accumulated (+=)
   int64_t gstride;
+  int64_t gs_dsoa, gs_xyz, gs_gpart;  // per-geometry strides (blockIdx.y); adj uses s1.gs_rec
 };
 int64_t dsoa_doubles(int ng, int maxa);
 int adjoint_f_threads();
 cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const double *ga, const double *xyz,
-                                double *dsoa, cudaStream_t st);
-cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, cudaStream_t st);
-cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, cudaStream_t st);
+                                double *dsoa, int ngeom, int64_t gs_xyz, int64_t gs_dsoa, cudaStream_t st);
+cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStream_t st);
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st);
 
 // Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
 cudaError_t pool_malloc(void **p, size_t bytes);
@@ -126,13 +132,17 @@ int set_error(int code, const std::string &msg);
 // Doubles of the transposed E table (both variants) for ng groups.
 int64_t esoa_doubles(int ng, int maxa);
 cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *flmn, const double *ga,
-                               const double *xyz, double *tab, double *esoa, cudaStream_t st);
+                               const double *xyz, double *tab, double *esoa, int ngeom, int64_t gs_xyz,
+                               int64_t gs_tab, int64_t gs_esoa, cudaStream_t st);
 template <int K>
-cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st);
-cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, cudaStream_t st);
+cudaError_t launch_stage1_k(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
+cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);
+// geometry batches: ngeom independent (nblocks x nq) partial arrays, gs_in apart, into ngeom rows of out
+cudaError_t launch_reduce_batch(const double *partial, int nblocks, int nq, int64_t gs_in, double *out, int ngeom,
+                                cudaStream_t st);
 cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int n, int *keys, double *vals,
                              cudaStream_t st);
 cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st);

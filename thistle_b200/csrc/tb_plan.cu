@@ -138,7 +138,12 @@ struct thistle_plan {
   bool have_ev = false;
   float ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t launches = 0;              // own kernels launched by the last call
-  std::vector<double> hxyz;          // host copy of the centres (interleaved)
+  // geometry batches: ngeom copies of the centres, tables, records and results
+  int ngeom = 1;
+  bool capturing = false;            // inside a CUDA-graph capture (no event records)
+  bool use_graph = false;
+  cudaGraphExec_t gx_fwd = nullptr, gx_vjp = nullptr;
+  std::vector<double> hxyz;          // host copy of the centres (interleaved, ngeom x ngto x 3)
   bool fwd_valid = false;            // records and visiting order match the current centres
   // adjoint workspaces (allocated by the first vector-Jacobian product)
   double *d_dsoa = nullptr, *d_adj = nullptr, *d_gpart = nullptr, *d_v = nullptr, *d_grad = nullptr;
@@ -462,6 +467,8 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
   dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
   dfree(P->d_dsoa); dfree(P->d_adj); dfree(P->d_gpart); dfree(P->d_v); dfree(P->d_grad);
+  if (P->gx_fwd) cudaGraphExecDestroy(P->gx_fwd);
+  if (P->gx_vjp) cudaGraphExecDestroy(P->gx_vjp);
   dfree(P->d_s2sort_tmp);
   dfree(P->d_sort_tmp);
   if (P->cb) pool_cublas_release(P->cb);
@@ -474,6 +481,37 @@ static void plan_free(thistle_plan *P) {
   delete P;
 }
 
+static int64_t gs_pair(const thistle_plan *P) { return (int64_t)npairs(P->ng) * PAIR_STRIDE; }
+static int64_t gs_esoa(const thistle_plan *P) { return esoa_doubles(P->ng, P->maxa); }
+static int64_t gs_rec(const thistle_plan *P) { return std::max<int64_t>(P->rec_total, 1); }
+
+static void drop_graphs(thistle_plan *P) {
+  if (P->gx_fwd) cudaGraphExecDestroy(P->gx_fwd);
+  if (P->gx_vjp) cudaGraphExecDestroy(P->gx_vjp);
+  P->gx_fwd = P->gx_vjp = nullptr;
+}
+
+// (Re)allocates the per-geometry buffers for G geometries (the adjoint's on
+// its next use); the partial-row count s2_rows must be set.
+static int geo_alloc(thistle_plan *P, int G) {
+  int rc = THISTLE_OK;
+  drop_graphs(P);
+  dfree(P->d_xyz); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rec); dfree(P->d_partial);
+  dfree(P->d_p0count); dfree(P->d_result);
+  dfree(P->d_dsoa); dfree(P->d_adj); dfree(P->d_gpart); dfree(P->d_v); dfree(P->d_grad);
+  P->ngeom = G;
+  TB_TRY(dalloc(&P->d_xyz, (size_t)G * 3 * P->ngto, "centres"));
+  TB_TRY(dalloc(&P->d_pairtab, (size_t)G * gs_pair(P), "pair tables"));
+  TB_TRY(dalloc(&P->d_esoa, (size_t)G * gs_esoa(P), "transposed E tables"));
+  TB_TRY(dalloc(&P->d_rec, (size_t)G * gs_rec(P), "quartet records"));
+  TB_TRY(dalloc(&P->d_partial, (size_t)G * P->s2_rows * P->nq, "partial sums"));
+  TB_TRY(dalloc(&P->d_p0count, (size_t)G * MAXCLS, "P0 counters"));
+  TB_TRY(dalloc(&P->d_result, (size_t)G * P->nq, "result"));
+  P->fwd_valid = false;
+done:
+  return rc;
+}
+
 static int upload_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
   std::vector<double> xyz((size_t)P->ngto * 3);
   for (int i = 0; i < P->ngto; ++i) {
@@ -481,10 +519,24 @@ static int upload_centres(thistle_plan *P, const double *xx, const double *yy, c
     xyz[3 * i + 1] = yy[i];
     xyz[3 * i + 2] = zz[i];
   }
-  if (xyz == P->hxyz) return THISTLE_OK;  // unchanged: records stay valid
+  // geometry 0 (the only one outside batches)
+  if (P->hxyz.size() >= xyz.size() && std::equal(xyz.begin(), xyz.end(), P->hxyz.begin()))
+    return THISTLE_OK;  // unchanged: records stay valid
   TB_CK(cudaMemcpyAsync(P->d_xyz, xyz.data(), sizeof(double) * xyz.size(), cudaMemcpyHostToDevice, P->st));
   TB_CK(cudaStreamSynchronize(P->st));
-  P->hxyz.swap(xyz);
+  if (P->hxyz.size() < xyz.size()) P->hxyz.resize(xyz.size());
+  std::copy(xyz.begin(), xyz.end(), P->hxyz.begin());
+  P->fwd_valid = false;
+  return THISTLE_OK;
+}
+
+// All geometries of a batch from one host array (ngeom x ngto x 3, interleaved).
+static int upload_centres_batch(thistle_plan *P, const double *xyz) {
+  const size_t n = (size_t)P->ngeom * 3 * P->ngto;
+  if (P->hxyz.size() == n && std::equal(xyz, xyz + n, P->hxyz.begin())) return THISTLE_OK;
+  TB_CK(cudaMemcpyAsync(P->d_xyz, xyz, sizeof(double) * n, cudaMemcpyHostToDevice, P->st));
+  TB_CK(cudaStreamSynchronize(P->st));
+  P->hxyz.assign(xyz, xyz + n);
   P->fwd_valid = false;
   return THISTLE_OK;
 }
@@ -568,12 +620,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_flmn, (size_t)ngto, "functions"));
   TB_TRY(dalloc(&P->d_ga, (size_t)ngto, "exponents"));
-  TB_TRY(dalloc(&P->d_xyz, (size_t)ngto * 3, "centres"));
   TB_TRY(dalloc(&P->d_q, (size_t)P->qdim * nq, "q"));
-  TB_TRY(dalloc(&P->d_result, (size_t)nq, "result"));
-  TB_TRY(dalloc(&P->d_pairtab, (size_t)npairs(P->ng) * PAIR_STRIDE, "pair tables"));
-  TB_TRY(dalloc(&P->d_esoa, (size_t)esoa_doubles(P->ng, P->maxa), "transposed E tables"));
-  TB_TRY(dalloc(&P->d_p0count, (size_t)MAXCLS, "P0 counters"));
   TB_TRYC(cudaMemcpyAsync(P->d_gstart, P->gstart.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_gcount, P->gcount.data(), sizeof(int) * P->ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_flmn, P->flmn.data(), sizeof(int) * ngto, cudaMemcpyHostToDevice, P->st));
@@ -584,13 +631,11 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   } else {
     TB_TRYC(cudaMemcpyAsync(P->d_q, q, sizeof(double) * nq, cudaMemcpyHostToDevice, P->st));
   }
-  TB_TRY(upload_centres(P, xx, yy, zz));
   tr.mark("small buffers, uploads");
   TB_TRY(density_alloc(P));
   TB_TRY(density_upload(P, mmod, mat, total, onerdm));
   tr.mark("density buffers");
   TB_TRY(quartets_alloc(P));
-  TB_TRY(dalloc(&P->d_rec, (size_t)P->rec_total, "quartet records"));
   tr.mark("quartet buffers");
   {
     int dev = 0;
@@ -607,7 +652,8 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     // aligned: quartet slices of the q-vector kernel (one partial row each)
     P->s2_rows = P->kind == KIND_ALIGNED ? std::max(1, 4 * P->nsm / std::max(1, (nq + 127) / 128)) : P->nsm * maxbps;
     if (P->kind == KIND_ALIGNED) P->s2_rows = std::min(P->s2_rows, 4 * P->nsm);
-    TB_TRY(dalloc(&P->d_partial, (size_t)P->s2_rows * nq, "partial sums"));
+    TB_TRY(geo_alloc(P, 1));
+    TB_TRY(upload_centres(P, xx, yy, zz));
     const int64_t n = std::max<int64_t>(P->nquart, 1);
     TB_TRY(dalloc(&P->d_s2key, (size_t)n, "stage-2 keys"));
     TB_TRY(dalloc(&P->d_s2key_sorted, (size_t)n, "stage-2 keys"));
@@ -690,29 +736,34 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
   a.p0count = nullptr;
   a.s2key = nullptr;
   a.cls = 0;
+  a.gs_pair = gs_pair(P);
+  a.gs_esoa = gs_esoa(P);
+  a.gs_rec = gs_rec(P);
   return a;
 }
 
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
-                      double *d_out, bool order) {
+                      double *d_out, bool order, int ngeom) {
+  // stage events (not while a graph is being captured)
   cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
-  P->ring_next += 1;
-  TB_CK(cudaEventRecord(E[0], P->st));
+  auto mark = [&](int i) -> cudaError_t { return P->capturing ? cudaSuccess : cudaEventRecord(E[i], P->st); };
+  if (!P->capturing) P->ring_next += 1;
+  TB_CK(mark(0));
   TB_CK(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa,
-                           P->st));
+                           ngeom, 3 * (int64_t)P->ngto, gs_pair(P), gs_esoa(P), P->st));
   P->launches += 1;
-  TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS, P->st));
-  TB_CK(cudaEventRecord(E[1], P->st));
+  TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS * ngeom, P->st));
+  TB_CK(mark(1));
   for (int c = 0; c < ncls; ++c) {
     Stage1Args a = stage1_args(P, d_quart, cb[c], ce[c], d_rec, recoff[c], rs[c]);
     a.p0count = (unsigned long long *)(P->d_p0count + c);
     a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
-    TB_CK(launch_stage1(P->kind, cL[c], a, P->st));
+    TB_CK(launch_stage1(P->kind, cL[c], a, ngeom, P->st));
     P->launches += 1;
   }
-  TB_CK(cudaEventRecord(E[2], P->st));
+  TB_CK(mark(2));
   int64_t nall = ncls > 0 ? ce[ncls - 1] : 0;
   if (P->kind == KIND_ALIGNED) {
     TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
@@ -729,10 +780,10 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       TB_CK(launch_aligned(cL[c], s, slices, P->st));
       P->launches += 1;
     }
-    TB_CK(cudaEventRecord(E[3], P->st));
+    TB_CK(mark(3));
     TB_CK(launch_reduce(P->d_partial, P->s2_rows, P->nq, d_out, P->st));
     P->launches += 1;
-    TB_CK(cudaEventRecord(E[4], P->st));
+    TB_CK(mark(4));
     return THISTLE_OK;
   }
   if (order && nall > 0) {
@@ -741,7 +792,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
                                           P->d_perm, (int)nall, 0, 11, P->st));
     P->launches += 1;
   }
-  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
+  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq * ngeom, P->st));
   for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
     const int tn = std::min(P->s2_qtile, P->nq - q0);
     int uniform = 0, first_on_grid = 0;
@@ -754,6 +805,8 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       s.rs = rs[c];
       s.nquart = ce[c] - cb[c];
       s.perm = order ? P->d_perm : nullptr;
+      s.gs_rec = gs_rec(P);
+      s.gs_partial = (int64_t)P->s2_rows * P->nq;
       s.pbase = cb[c];
       s.q = P->d_q + q0;
       s.nq = tn;
@@ -768,48 +821,76 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       const int64_t per_warp = stage2_quartets_per_warp(LB);
       const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
       const int64_t resident = (int64_t)P->nsm * bps * STAGE2_WARPS;
-      const int64_t nbatch = (s.nquart + per_warp - 1) / per_warp;
+      const int64_t nbatch = (s.nquart + per_warp - 1) / per_warp * ngeom;
       const int nseg = (tn + 63) / 64;
       int nch = (int)std::min<int64_t>(nseg, std::max<int64_t>(1, (8 * resident + nbatch - 1) / nbatch));
       s.chunk = nch <= 1 ? 0 : 64 * ((nseg + nch - 1) / nch);
       if (s.chunk > 0) nch = (tn + s.chunk - 1) / s.chunk;
-      const int64_t items = nbatch * nch;
+      const int64_t items = nbatch / ngeom * nch;
       const int64_t nblk = (items + STAGE2_WARPS - 1) / STAGE2_WARPS;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
-      TB_CK(launch_stage2_class(LB, s, grid, P->st));
+      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->st));
       P->launches += 1;
     }
   }
-  TB_CK(cudaEventRecord(E[3], P->st));
-  TB_CK(launch_reduce(P->d_partial, P->s2_rows, P->nq, d_out, P->st));
+  TB_CK(mark(3));
+  TB_CK(launch_reduce_batch(P->d_partial, P->s2_rows, P->nq, (int64_t)P->s2_rows * P->nq, d_out, ngeom, P->st));
   P->launches += 1;
-  TB_CK(cudaEventRecord(E[4], P->st));
+  TB_CK(mark(4));
   return THISTLE_OK;
 }
 
 static int plan_exec(thistle_plan *P, double *d_out) {
   int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                      P->cls_rs, d_out, true);
+                      P->cls_rs, d_out, true, P->ngeom);
   P->fwd_valid = rc == THISTLE_OK;
   return rc;
 }
 
+static void read_timings(thistle_plan *P) {
+  if (P->ring_next == 0) return;
+  cudaEvent_t *E = P->rev[(P->ring_next - 1) % thistle_plan::NRING];
+  for (int i = 0; i < 4; ++i) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, E[i], E[i + 1]) == cudaSuccess) P->ms[i] = t;
+  }
+}
+
 // Vector-Jacobian product of total j0 with respect to the group centres:
-// grad[3 g + axis] = sum_q v(q) dI(q)/dA_g (tb_adjoint.cu).  Runs the forward
-// stages first when the records are not those of the current centres.
-static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
+// grad[g][3 c + axis] = sum_q v[g](q) dI_g(q)/dA_c for every geometry g of the
+// batch (tb_adjoint.cu).  The forward records must be those of the current
+// centres (adjoint_ready runs the forward stages otherwise).
+static int adjoint_check(thistle_plan *P) {
   if (P->kind != KIND_TOTAL) return fail(THISTLE_ERR_TYPE, "the adjoint is provided for total j0 (type 1)");
   for (int c = 0; c < P->ncls; ++c)
     if (P->cls_L[c] > 8) return fail(THISTLE_ERR_ANGMOM, "the adjoint covers LLmax <= 8 (s, p, d shells)");
+  return THISTLE_OK;
+}
+
+static int adjoint_alloc(thistle_plan *P) {
   int rc = THISTLE_OK;
+  const int G = P->ngeom;
   if (!P->d_dsoa) {
-    TB_TRY(dalloc(&P->d_dsoa, (size_t)dsoa_doubles(P->ng, P->maxa), "dE tables"));
-    TB_TRY(dalloc(&P->d_adj, (size_t)std::max<int64_t>(P->rec_total, 1), "adjoint records"));
+    TB_TRY(dalloc(&P->d_dsoa, (size_t)G * dsoa_doubles(P->ng, P->maxa), "dE tables"));
+    TB_TRY(dalloc(&P->d_adj, (size_t)G * gs_rec(P), "adjoint records"));
     P->adj_rows = 2 * P->nsm;
-    TB_TRY(dalloc(&P->d_gpart, (size_t)P->adj_rows * 3 * P->ng, "gradient rows"));
+    TB_TRY(dalloc(&P->d_gpart, (size_t)G * P->adj_rows * 3 * P->ng, "gradient rows"));
   }
-  if (!P->fwd_valid) TB_TRY(plan_exec(P, P->d_result));
-  TB_TRYC(launch_pair_dtables(P->ng, P->maxa, P->d_gstart, P->d_ga, P->d_xyz, P->d_dsoa, P->st));
+  if (!P->d_v) {
+    TB_TRY(dalloc(&P->d_v, (size_t)G * P->nq, "cotangent"));
+    TB_TRY(dalloc(&P->d_grad, (size_t)G * 3 * P->ng, "gradient"));
+  }
+done:
+  return rc;
+}
+
+// The adjoint stages proper (no allocation, no synchronisation: capturable).
+static int adjoint_stages(thistle_plan *P, const double *d_v, double *d_grad) {
+  int rc = THISTLE_OK;
+  const int G = P->ngeom;
+  const int64_t gs_dsoa = dsoa_doubles(P->ng, P->maxa), gs_gpart = (int64_t)P->adj_rows * 3 * P->ng;
+  TB_TRYC(launch_pair_dtables(P->ng, P->maxa, P->d_gstart, P->d_ga, P->d_xyz, P->d_dsoa, G, 3 * (int64_t)P->ngto,
+                              gs_dsoa, P->st));
   P->launches += 1;
   {
     int uniform = 0, first_on_grid = 0;
@@ -829,11 +910,12 @@ static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
       a.uniform = uniform;
       a.first_on_grid = first_on_grid;
       a.dq = dq;
-      TB_TRYC(launch_adjoint_q(P->cls_L[c] + 1, a, P->st));
+      a.gs_rec = gs_rec(P);
+      TB_TRYC(launch_adjoint_q(P->cls_L[c] + 1, a, G, P->st));
       P->launches += 1;
     }
   }
-  TB_TRYC(cudaMemsetAsync(P->d_gpart, 0, sizeof(double) * (size_t)P->adj_rows * 3 * P->ng, P->st));
+  TB_TRYC(cudaMemsetAsync(P->d_gpart, 0, sizeof(double) * (size_t)G * gs_gpart, P->st));
   for (int c = 0; c < P->ncls; ++c) {
     AdjointFArgs a;
     a.s1 = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c], P->cls_rs[c]);
@@ -843,24 +925,74 @@ static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
     a.xyz = P->d_xyz;
     a.gpart = P->d_gpart;
     a.gstride = 3 * P->ng;
+    a.gs_dsoa = gs_dsoa;
+    a.gs_xyz = 3 * (int64_t)P->ngto;
+    a.gs_gpart = gs_gpart;
     const int64_t n = P->cls_end[c] - P->cls_begin[c];
     const int grid = (int)std::min<int64_t>(P->adj_rows, (n + adjoint_f_threads() - 1) / adjoint_f_threads());
-    TB_TRYC(launch_adjoint_f(P->cls_L[c], a, grid, P->st));
+    TB_TRYC(launch_adjoint_f(P->cls_L[c], a, grid, G, P->st));
     P->launches += 1;
   }
-  TB_TRYC(launch_reduce(P->d_gpart, P->adj_rows, 3 * P->ng, d_grad, P->st));
+  TB_TRYC(launch_reduce_batch(P->d_gpart, P->adj_rows, 3 * P->ng, gs_gpart, d_grad, G, P->st));
   P->launches += 1;
 done:
   return rc;
 }
 
-static void read_timings(thistle_plan *P) {
-  if (P->ring_next == 0) return;
-  cudaEvent_t *E = P->rev[(P->ring_next - 1) % thistle_plan::NRING];
-  for (int i = 0; i < 4; ++i) {
-    float t = 0;
-    if (cudaEventElapsedTime(&t, E[i], E[i + 1]) == cudaSuccess) P->ms[i] = t;
+// Forward stages of the batch into d_result, through the captured graph when enabled.
+static int forward_batch(thistle_plan *P) {
+  if (!P->use_graph) return plan_exec(P, P->d_result);
+  if (!P->gx_fwd) {
+    // capture once (all buffers exist); replays use the same pointers
+    cudaGraph_t g = nullptr;
+    TB_CK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
+    P->capturing = true;
+    int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
+                        P->cls_rs, P->d_result, true, P->ngeom);
+    P->capturing = false;
+    cudaError_t e = cudaStreamEndCapture(P->st, &g);
+    if (rc != THISTLE_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    TB_CK(e);
+    e = cudaGraphInstantiate(&P->gx_fwd, g, 0);
+    cudaGraphDestroy(g);
+    TB_CK(e);
   }
+  TB_CK(cudaGraphLaunch(P->gx_fwd, P->st));
+  P->fwd_valid = true;
+  return THISTLE_OK;
+}
+
+static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
+  int rc = adjoint_check(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_TRY(adjoint_alloc(P));
+  if (!P->fwd_valid) TB_TRY(forward_batch(P));
+  if (!P->use_graph || d_v != P->d_v || d_grad != P->d_grad) {
+    TB_TRY(adjoint_stages(P, d_v, d_grad));
+  } else {
+    if (!P->gx_vjp) {
+      cudaGraph_t g = nullptr;
+      TB_TRYC(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
+      P->capturing = true;
+      rc = adjoint_stages(P, d_v, d_grad);
+      P->capturing = false;
+      cudaError_t e = cudaStreamEndCapture(P->st, &g);
+      if (rc != THISTLE_OK) {
+        if (g) cudaGraphDestroy(g);
+        goto done;
+      }
+      TB_TRYC(e);
+      e = cudaGraphInstantiate(&P->gx_vjp, g, 0);
+      cudaGraphDestroy(g);
+      TB_TRYC(e);
+    }
+    TB_TRYC(cudaGraphLaunch(P->gx_vjp, P->st));
+  }
+done:
+  return rc;
 }
 
 // The reference's aligned q grid (QCOORD3, src/main_calculation.f90:864-929):
@@ -917,11 +1049,10 @@ int thistle_plan_vjp(thistle_plan *P, const double *v_host, double *grad_host) {
   if (!P || !v_host || !grad_host) return fail(THISTLE_ERR_ARG, "null argument");
   if (!finite_all(v_host, P->nq)) return fail(THISTLE_ERR_NONFINITE, "non-finite cotangent");
   P->launches = 0;
-  int rc = THISTLE_OK;
-  if (!P->d_v) {
-    TB_TRY(dalloc(&P->d_v, (size_t)P->nq, "cotangent"));
-    TB_TRY(dalloc(&P->d_grad, (size_t)3 * P->ng, "gradient"));
-  }
+  int rc = adjoint_check(P);
+  if (rc != THISTLE_OK) return rc;
+  if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "plan holds a geometry batch: use thistle_plan_vjp_batch");
+  TB_TRY(adjoint_alloc(P));
   TB_TRYC(cudaMemcpyAsync(P->d_v, v_host, sizeof(double) * P->nq, cudaMemcpyHostToDevice, P->st));
   TB_TRY(plan_vjp(P, P->d_v, P->d_grad));
   TB_TRYC(cudaMemcpyAsync(grad_host, P->d_grad, sizeof(double) * 3 * P->ng, cudaMemcpyDeviceToHost, P->st));
@@ -930,8 +1061,179 @@ done:
   return rc;
 }
 
+int thistle_plan_set_batch(thistle_plan *P, int32_t ngeom) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  if (ngeom < 1 || ngeom > 65535) return fail(THISTLE_ERR_ARG, "ngeom must be 1..65535");
+  if (P->kind == KIND_ALIGNED && ngeom != 1) return fail(THISTLE_ERR_TYPE, "aligned plans hold one geometry");
+  if (ngeom == P->ngeom) return THISTLE_OK;
+  TB_CK(cudaStreamSynchronize(P->st));
+  // every geometry starts at geometry 0's centres
+  std::vector<double> g0(P->hxyz.begin(), P->hxyz.begin() + 3 * (size_t)P->ngto);
+  int rc = geo_alloc(P, ngeom);
+  if (rc != THISTLE_OK) return rc;
+  std::vector<double> all((size_t)ngeom * g0.size());
+  for (int g = 0; g < ngeom; ++g) std::copy(g0.begin(), g0.end(), all.begin() + (size_t)g * g0.size());
+  P->hxyz.clear();
+  return upload_centres_batch(P, all.data());
+}
+
+int thistle_plan_set_centres_batch(thistle_plan *P, const double *xyz) {
+  if (!P || !xyz) return fail(THISTLE_ERR_ARG, "null argument");
+  const int64_t n = (int64_t)P->ngeom * 3 * P->ngto;
+  if (!finite_all(xyz, n)) return fail(THISTLE_ERR_NONFINITE, "non-finite centre");
+  for (int g = 0; g < P->ngeom; ++g)
+    for (int k = 0; k < P->ng; ++k) {
+      const double *h = xyz + ((size_t)g * P->ngto + P->gstart[k]) * 3;
+      for (int i = P->gstart[k]; i < P->gstart[k] + P->gcount[k]; ++i)
+        for (int ax = 0; ax < 3; ++ax)
+          if (xyz[((size_t)g * P->ngto + i) * 3 + ax] != h[ax])
+            return fail(THISTLE_ERR_SHAPE, "functions of one group must share a centre");
+    }
+  return upload_centres_batch(P, xyz);
+}
+
+int thistle_plan_execute_batch_device(thistle_plan *P, double *result_dev) {
+  if (!P || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  int rc = forward_batch(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaMemcpyAsync(result_dev, P->d_result, sizeof(double) * P->ngeom * P->nq, cudaMemcpyDeviceToDevice,
+                        P->st));
+  return THISTLE_OK;
+}
+
+int thistle_plan_execute_batch(thistle_plan *P, double *result_host) {
+  if (!P || !result_host) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  int rc = forward_batch(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->ngeom * P->nq, cudaMemcpyDeviceToHost,
+                        P->st));
+  TB_CK(cudaStreamSynchronize(P->st));
+  return THISTLE_OK;
+}
+
+int thistle_plan_vjp_batch(thistle_plan *P, const double *v_host, double *grad_host) {
+  if (!P || !v_host || !grad_host) return fail(THISTLE_ERR_ARG, "null argument");
+  if (!finite_all(v_host, (int64_t)P->ngeom * P->nq)) return fail(THISTLE_ERR_NONFINITE, "non-finite cotangent");
+  P->launches = 0;
+  int rc = adjoint_check(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_TRY(adjoint_alloc(P));
+  TB_TRYC(cudaMemcpyAsync(P->d_v, v_host, sizeof(double) * P->ngeom * P->nq, cudaMemcpyHostToDevice, P->st));
+  TB_TRY(plan_vjp(P, P->d_v, P->d_grad));
+  TB_TRYC(cudaMemcpyAsync(grad_host, P->d_grad, sizeof(double) * P->ngeom * 3 * P->ng, cudaMemcpyDeviceToHost,
+                          P->st));
+  TB_TRYC(cudaStreamSynchronize(P->st));
+done:
+  return rc;
+}
+
+int thistle_plan_vjp_batch_device(thistle_plan *P, const double *v_dev, double *grad_dev) {
+  if (!P || !v_dev || !grad_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  P->launches = 0;
+  int rc = adjoint_check(P);
+  if (rc != THISTLE_OK) return rc;
+  TB_TRY(adjoint_alloc(P));
+  TB_TRYC(cudaMemcpyAsync(P->d_v, v_dev, sizeof(double) * P->ngeom * P->nq, cudaMemcpyDeviceToDevice, P->st));
+  TB_TRY(plan_vjp(P, P->d_v, P->d_grad));
+  TB_TRYC(cudaMemcpyAsync(grad_dev, P->d_grad, sizeof(double) * P->ngeom * 3 * P->ng, cudaMemcpyDeviceToDevice,
+                          P->st));
+done:
+  return rc;
+}
+
+// Stage-2 q tile (points per shared-memory tile): recomputes the resident
+// blocks per class and the partial-row count; buffers are reallocated.
+static int set_qtile(thistle_plan *P, int qt) {
+  P->s2_qtile = std::max(1, std::min(qt, std::min(P->nq, STAGE2_QTILE)));
+  int maxbps = 1;
+  for (int c = 0; c < P->ncls; ++c) {
+    const int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
+    P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, P->kind == KIND_J2, P->s2_qtile);
+    maxbps = std::max(maxbps, P->s2_bps[LB]);
+  }
+  P->s2_rows = P->nsm * maxbps;
+  std::vector<double> keep = P->hxyz;
+  const int G = P->ngeom;
+  int rc = geo_alloc(P, G);
+  if (rc != THISTLE_OK) return rc;
+  P->hxyz.clear();
+  return upload_centres_batch(P, keep.data());
+}
+
+int thistle_plan_autotune_batch(thistle_plan *P, int32_t gmax, int32_t *g_best, int32_t *qtile_best,
+                                double *geoms_per_s) {
+  if (!P || !g_best || !qtile_best || !geoms_per_s) return fail(THISTLE_ERR_ARG, "null argument");
+  if (gmax < 1) return fail(THISTLE_ERR_ARG, "gmax must be >= 1");
+  int rc = adjoint_check(P);
+  if (rc != THISTLE_OK) return rc;
+  const int qfull = std::min(P->nq, STAGE2_QTILE);
+  int qts[2] = {qfull, std::max(64, (qfull / 2 + 63) / 64 * 64)};
+  const int nqt = qts[1] < qfull ? 2 : 1;
+  double best = -1.0;
+  int bestG = 1, bestQ = qfull;
+  cudaEvent_t e0, e1;
+  TB_CK(cudaEventCreate(&e0));
+  TB_CK(cudaEventCreate(&e1));
+  for (int G = 1; G <= gmax; G *= 2) {
+    bool fits = true;
+    for (int t = 0; t < nqt && fits; ++t) {
+      rc = thistle_plan_set_batch(P, G);
+      if (rc == THISTLE_OK) rc = set_qtile(P, qts[t]);
+      if (rc == THISTLE_OK) rc = adjoint_alloc(P);
+      if (rc != THISTLE_OK) {
+        fits = false;  // no room for this batch: keep the best so far
+        break;
+      }
+      cudaMemsetAsync(P->d_v, 0, sizeof(double) * G * P->nq, P->st);
+      const int reps = 3;
+      for (int w = 0; w < 2 + reps && rc == THISTLE_OK; ++w) {
+        if (w == 2) cudaEventRecord(e0, P->st);
+        P->fwd_valid = false;
+        rc = forward_batch(P);
+        if (rc == THISTLE_OK) rc = plan_vjp(P, P->d_v, P->d_grad);
+      }
+      cudaEventRecord(e1, P->st);
+      if (cudaEventSynchronize(e1) != cudaSuccess || rc != THISTLE_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc != THISTLE_OK ? rc : fail(THISTLE_ERR_CUDA, "autotune run failed");
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double gps = ms > 0 ? G * reps / (ms * 1e-3) : 0.0;
+      if (gps > best) {
+        best = gps;
+        bestG = G;
+        bestQ = qts[t];
+      }
+    }
+    if (!fits) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  rc = thistle_plan_set_batch(P, bestG);
+  if (rc == THISTLE_OK) rc = set_qtile(P, bestQ);
+  if (rc != THISTLE_OK) return rc;
+  *g_best = bestG;
+  *qtile_best = bestQ;
+  *geoms_per_s = best;
+  return THISTLE_OK;
+}
+
+int thistle_plan_use_graph(thistle_plan *P, int32_t enable) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  TB_CK(cudaStreamSynchronize(P->st));
+  drop_graphs(P);
+  P->use_graph = enable != 0;
+  return THISTLE_OK;
+}
+
 int thistle_plan_vjp_device(thistle_plan *P, const double *v_dev, double *grad_dev) {
   if (!P || !v_dev || !grad_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "plan holds a geometry batch: use thistle_plan_vjp_batch_device");
   P->launches = 0;
   return plan_vjp(P, v_dev, grad_dev);
 }
@@ -1058,7 +1360,7 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
   if (nquart == 0) {
     TB_TRYC(cudaMemsetAsync(P->d_result, 0, sizeof(double) * P->nq, P->st));
   } else {
-    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result, false));
+    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result, false, 1));
   }
   TB_TRYC(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));

@@ -255,8 +255,21 @@ __device__ __forceinline__ const double *esoa_slot(const Stage1Args &A, bool ski
   return A.esoa + (skipped ? A.eskip : 0) + (int64_t)slot * E_T * A.npair + pair;
 }
 
+// Geometry blockIdx.y of a batch: its pair tables, E tables, records and
+// P = Q counter; the stage-2 order keys are written for geometry 0 only.
+__device__ __forceinline__ void stage1_geometry(Stage1Args &A) {
+  const int64_t g = blockIdx.y;
+  if (g == 0) return;
+  A.pairtab += g * A.gs_pair;
+  A.esoa += g * A.gs_esoa;
+  A.rec += g * A.gs_rec;
+  if (A.p0count) A.p0count += g * MAXCLS;
+  A.s2key = nullptr;
+}
+
 template <int L, int KIND>
 __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kernel(Stage1Args A) {
+  stage1_geometry(A);
   constexpr int S = stage1_reg_split(L);
   constexpr int PP = stage1_reg_parts(L);
   constexpr int G = S * PP;              // threads per quartet
@@ -399,6 +412,7 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
 // ---------------------------------------------------------------------------
 template <int L, int KIND>
 __global__ void stage1_smem_kernel(Stage1Args A) {
+  stage1_geometry(A);
   // Each thread owns a column of the block's shared array; element k of its
   // (partial) Hermite density sits at sD[k * blockDim.x + threadIdx.x].
   constexpr int S = stage1_smem_split(L);
@@ -524,7 +538,7 @@ static inline int stage1_smem_threads(int L) {
 }
 
 template <int L, int K>
-static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t st) {
+static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, int ngeom, cudaStream_t st) {
   if constexpr (L <= STAGE1_REG_MAXL) {
     constexpr int S = stage1_reg_split(L);
     const int thr = 128;
@@ -533,7 +547,7 @@ static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t 
         cudaFuncSetAttribute(stage1_reg_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int64_t threads = n * S * stage1_reg_parts(L);
-    stage1_reg_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
+    stage1_reg_kernel<L, K><<<dim3((unsigned)((threads + thr - 1) / thr), ngeom), thr, smem, st>>>(a);
   } else {
     constexpr int S = stage1_smem_split(L);
     int thr = stage1_smem_threads(L);
@@ -542,17 +556,17 @@ static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, cudaStream_t 
         cudaFuncSetAttribute(stage1_smem_kernel<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int64_t threads = n * S;
-    stage1_smem_kernel<L, K><<<(unsigned)((threads + thr - 1) / thr), thr, smem, st>>>(a);
+    stage1_smem_kernel<L, K><<<dim3((unsigned)((threads + thr - 1) / thr), ngeom), thr, smem, st>>>(a);
   }
   return cudaGetLastError();
 }
 
 template <int K>
-cudaError_t launch_stage1_k(int L, const Stage1Args &a, cudaStream_t st) {
+cudaError_t launch_stage1_k(int L, const Stage1Args &a, int ngeom, cudaStream_t st) {
   int64_t n = a.qend - a.qbegin;
   if (n <= 0) return cudaSuccess;
   switch (L) {
-#define TB_S1(l) case l: return launch_stage1_l<l, K>(a, n, st);
+#define TB_S1(l) case l: return launch_stage1_l<l, K>(a, n, ngeom, st);
     TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
     TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
 #undef TB_S1

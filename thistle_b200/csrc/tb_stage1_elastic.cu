@@ -3,5 +3,5 @@
 #include "tb_stage1.cuh"
 
 namespace tb {
-template cudaError_t launch_stage1_k<KIND_ELASTIC>(int L, const Stage1Args &a, cudaStream_t st);
+template cudaError_t launch_stage1_k<KIND_ELASTIC>(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 }  // namespace tb

@@ -123,6 +123,9 @@ TB_HD constexpr int padded_nq(int nq) { return (nq + QB - 1) / QB * QB; }
 template <int LB, int K, bool J2>
 __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
   extern __shared__ double sm[];
+  // geometry blockIdx.y of a batch
+  A.rec += blockIdx.y * A.gs_rec;
+  A.partial += blockIdx.y * A.gs_partial;
   const int nq = A.nq, nqb = padded_nq(nq);
   double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q), padded with the last point
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -258,13 +261,13 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
 size_t class_smem(int nq) { return sizeof(double) * (size_t)padded_nq(nq) * (2 + STAGE2_WARPS); }
 
 template <int LB, bool J2>
-cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, cudaStream_t st) {
+cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st) {
   constexpr int K = stage2_k(LB);
   size_t smem = class_smem(a.nq);
   cudaError_t e =
       cudaFuncSetAttribute(stage2_class_kernel<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  stage2_class_kernel<LB, K, J2><<<grid, STAGE2_WARPS * 32, smem, st>>>(a);
+  stage2_class_kernel<LB, K, J2><<<dim3(grid, ngeom), STAGE2_WARPS * 32, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -314,11 +317,11 @@ int stage2_class_blocks_per_sm(int LB, bool j2, int nq) {
   }
 }
 
-cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cudaStream_t st) {
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st) {
   if (a.nquart <= 0 || grid <= 0) return cudaSuccess;
   if (a.j2) {
     switch (LB) {
-#define TB_L(n) case n: return launch_class_l<n, true>(a, grid, st);
+#define TB_L(n) case n: return launch_class_l<n, true>(a, grid, ngeom, st);
       TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8) TB_L(9) TB_L(10)
       TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16) TB_L(17) TB_L(18)
 #undef TB_L
@@ -326,7 +329,7 @@ cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, cuda
     }
   }
   switch (LB) {
-#define TB_L(n) case n: return launch_class_l<n, false>(a, grid, st);
+#define TB_L(n) case n: return launch_class_l<n, false>(a, grid, ngeom, st);
     TB_L(0) TB_L(1) TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8)
     TB_L(9) TB_L(10) TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16)
 #undef TB_L

@@ -118,6 +118,7 @@ class ScatteringPlan:
         self.ng = int(group.max())
         # first function of each group (its centre is the group's)
         self.group_first = np.array([int(np.argmax(group == k + 1)) for k in range(self.ng)])
+        self.ngeom = 1
         if self.type == TOTAL_ALIGNED:
             # nq vectors; the C side takes them (3, nq) column-major = rows of (qx, qy, qz)
             self.q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(-1, 3))
@@ -171,6 +172,38 @@ class ScatteringPlan:
     def vjp_device(self, v_ptr: int, grad_ptr: int):
         """Device pointers (nq and 3 ng doubles), on the plan's stream."""
         check(_abi.lib().thistle_plan_vjp_device(self._p, C.c_void_p(v_ptr), C.c_void_p(grad_ptr)))
+
+    # --- geometry batches -------------------------------------------------
+    def set_batch(self, ngeom: int):
+        """Hold ngeom geometries (all at geometry 0's centres until set_centres_batch)."""
+        check(_abi.lib().thistle_plan_set_batch(self._p, int(ngeom)))
+        self.ngeom = int(ngeom)
+
+    def set_centres_batch(self, xyz):
+        """Centres of every geometry: array (ngeom, ngto, 3)."""
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(self.ngeom, self.ngto, 3))
+        check(_abi.lib().thistle_plan_set_centres_batch(self._p, dptr(xyz)))
+
+    def execute_batch(self):
+        out = np.zeros((self.ngeom, self.nq))
+        check(_abi.lib().thistle_plan_execute_batch(self._p, dptr(out)))
+        return out
+
+    def vjp_batch(self, v):
+        v = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(self.ngeom, self.nq))
+        g = np.zeros((self.ngeom, self.ng, 3))
+        check(_abi.lib().thistle_plan_vjp_batch(self._p, dptr(v), dptr(g)))
+        return g
+
+    def use_graph(self, enable: bool = True):
+        check(_abi.lib().thistle_plan_use_graph(self._p, int(bool(enable))))
+
+    def autotune_batch(self, gmax: int):
+        """Pick the batch size and stage-2 q tile by timing forward + adjoint; returns (ngeom, qtile, geoms/s)."""
+        g, qt, gps = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
+        check(_abi.lib().thistle_plan_autotune_batch(self._p, int(gmax), C.byref(g), C.byref(qt), C.byref(gps)))
+        self.ngeom = g.value
+        return g.value, qt.value, gps.value
 
     def execute_device(self, ptr: int):
         """Integrator only, I(q) to the device address ``ptr`` (stream-ordered)."""
