@@ -219,6 +219,83 @@ def e2e_entry1(p, steps, warmup):
     return dt, res
 
 
+def run_fit(args):
+    """Configuration 5: a 6-atom ring (configuration-2 basis per atom, 30 MOs,
+    dense 2-RDM, 400 q) at 512 geometries; per geometry the forward I(q) and
+    the adjoint dLoss/dR for Loss = sum_q (I(q; R) - I_ref(q))^2.  The plain
+    path runs one geometry per call (set_centres, execute, vjp); the batched
+    path holds an autotuned number of geometries per plan, replays CUDA graphs
+    and runs every stage once per batch.  Both from the same plan set-up."""
+    import torch
+    from thistle_b200 import inputs as I
+    from thistle_b200 import main_calculation as MC
+    torch.cuda.set_device(0)
+    p = I.config5_fit()
+    geos = I.config5_geometries(p, args.fit_geometries)
+    probs = [p.with_geometry(R) for R in geos]
+    xyz = np.stack([np.stack([q.xx, q.yy, q.zz], axis=1) for q in probs])
+    ng = len(probs)
+    with MC.ScatteringPlan.from_problem(p, 1) as pl:
+        iref = pl.execute()
+        nquart = pl.info()["nquart"]
+        # plain per-geometry path
+        nplain = min(ng, args.fit_plain)
+        for k in range(3):
+            pl.set_centres(*xyz[k].T)
+            I0 = pl.execute()
+            pl.vjp(2 * (I0 - iref))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(nplain):
+            pl.set_centres(*xyz[k].T)
+            Ik = pl.execute()
+            pl.vjp(2 * (Ik - iref))
+        torch.cuda.synchronize()
+        t_plain = (time.perf_counter() - t0) / nplain
+        # batched path
+        pl.use_graph(True)
+        G, qt, gps_tune = pl.autotune_batch(args.fit_gmax)
+        nb = (ng + G - 1) // G
+        gbuf = np.zeros((nb * G, p.ng, 3))
+        ibuf = np.zeros((nb * G, p.nq))
+        pad = np.concatenate([xyz, np.repeat(xyz[:1], nb * G - ng, axis=0)])
+        for b in range(min(nb, 2)):
+            pl.set_centres_batch(pad[b * G:(b + 1) * G])
+            Ib = pl.execute_batch()
+            pl.vjp_batch(2 * (Ib - iref))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for b in range(nb):
+            pl.set_centres_batch(pad[b * G:(b + 1) * G])
+            Ib = pl.execute_batch()
+            ibuf[b * G:(b + 1) * G] = Ib
+            gbuf[b * G:(b + 1) * G] = pl.vjp_batch(2 * (Ib - iref))
+        torch.cuda.synchronize()
+        t_batch = (time.perf_counter() - t0) / ng
+        # spot check: the batched answer of the last geometry against the plain path
+        pl.set_batch(1)
+        pl.set_centres(*xyz[ng - 1].T)
+        Ichk = pl.execute()
+        gchk = pl.vjp(2 * (Ichk - iref))
+    err_i = float(np.max(np.abs(ibuf[ng - 1] - Ichk)) / np.max(np.abs(Ichk)))
+    err_g = float(np.max(np.abs(gbuf[ng - 1] - gchk)) / np.max(np.abs(gchk)))
+    line = {
+        "metric": "geometries/s, forward I(q) + adjoint dLoss/dR (fit6, 400 q)", "value": 1.0 / t_batch,
+        "unit": "geometries/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded; BASELINE configuration 5 shapes)",
+        "config": {"workload": f"fit6: 6-atom ring, {p.ngto} primitives ({p.ng} shells), {p.nmo} MOs, dense 2-RDM "
+                               f"({p.mat.shape[0]} rows), {p.nq} q, {ng} geometries (sigma 0.1 bohr)",
+                   "quartets_per_geometry": int(nquart), "autotuned_batch": G, "autotuned_qtile": qt},
+        "plain_geometries_per_s": 1.0 / t_plain, "plain_sample_geometries": nplain,
+        "batched_over_plain": t_plain / t_batch,
+        "quartet_q_per_s_forward_and_adjoint": nquart * p.nq / t_batch,
+        "check_vs_plain": {"I_rel": err_i, "grad_rel": err_g},
+        "path": "host arrays in and out per batch (set_centres_batch, execute_batch, vjp_batch)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,9 +304,15 @@ def main():
     ap.add_argument("--impl", default="thistle", choices=["thistle", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="ab6", choices=["ab6", "ab6_4atom"],
-                    help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis")
+    ap.add_argument("--workload", default="ab6", choices=["ab6", "ab6_4atom", "fit6"],
+                    help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis; "
+                         "fit6: batched forward + adjoint over geometries (configuration 5)")
+    ap.add_argument("--fit-geometries", type=int, default=512)
+    ap.add_argument("--fit-plain", type=int, default=32, help="geometries timed on the plain path")
+    ap.add_argument("--fit-gmax", type=int, default=64)
     args = ap.parse_args()
+    if args.workload == "fit6" and args.impl == "thistle":
+        return run_fit(args)
     global WORKLOAD
     WORKLOAD = args.workload
     args.warmup = max(args.warmup, 3) if args.impl == "thistle" else args.warmup
