@@ -55,6 +55,21 @@ def workload():
     return I.config3_ab6()
 
 
+def max_over_ranks(ms: float, device: str) -> float:
+    """The slowest rank's time (every rank calls this, in the same order)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world: int, units_per_step: int, steps: int, ms: float) -> float:
+    """Replicas: every rank processes units_per_step per step; the job's rate
+    is all ranks' units over the slowest rank's time."""
+    return world * units_per_step * steps / (ms * 1e-3)
+
+
 def workload_config(p, nquart):
     return {
         "workload": f"ab6_total_j0: {len(p.atoms)} atoms, {p.ngto} primitives ({p.ng} shells), {p.nmo} MOs, "
@@ -371,13 +386,11 @@ def main():
     ms = e0.elapsed_time(e1)
     st = plan.stage_totals()
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, "cuda")
     result = out.cpu().numpy()
 
     qq_step = nquart * p.nq
-    value = world * qq_step * args.steps / (ms * 1e-3)
+    value = whole_job_value(world, qq_step, args.steps, ms)
     # roofline of the dominant kernel (stage 2, the Bessel sum), averaged over the timed launches
     n2 = max(st["executions"], 1)
     s2_ms = st["stage2"] / n2
