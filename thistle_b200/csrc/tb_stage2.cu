@@ -139,6 +139,10 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
   __syncthreads();
 
   constexpr double XC = bessel_crossover(LB);
+  // polynomial form for the orders whose float64 accuracy it matches (LB <= 8)
+  constexpr bool POLY = LB <= 8;
+  constexpr int NA = LB / 2 + 1;                   // A: powers q^0, q^2, .., q^{2 (NA-1)}
+  constexpr int NB = LB >= 1 ? (LB - 1) / 2 + 1 : 1;  // B: q times powers of q^2
   const int64_t per = 32 * K;
   const int64_t nb = (A.nquart + per - 1) / per;
   // work item = (batch of 32 K quartets, chunk of the q tile); chunks start
@@ -151,7 +155,10 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
   for (int64_t it = (int64_t)blockIdx.x * NW + warp; it < nitems; it += (int64_t)gridDim.x * NW) {
     const int64_t bt = it / nch;
     const int m0 = (int)(it - bt * nch) * chunk, m1 = min(nqb, m0 + chunk);
-    double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K], hh[K][LB + 1];
+    double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K];
+    double hh[POLY ? 1 : K][POLY ? 1 : LB + 1];  // recurrence form: hhat_b
+    double pa[POLY ? K : 1][NA], pb[POLY ? K : 1][NB];  // polynomial form
+    long long qcb[K];  // bits of x_c / H: below it the series branch
     const double *hm[K];
     int p0n[K];  // P = Q polynomial order, or -1 for a Bessel quartet
 #pragma unroll
@@ -160,17 +167,78 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
       const double *rec = kZeroRecord;
       double h = 1.0;
       p0n[k] = -1;
+      bool bessel = false;
       if (slot < A.nquart) {
         const int64_t idx = A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot;
         rec = A.rec + idx * A.rs;
         if ((int)rec[2] == REC_P0) p0n[k] = (int)rec[3];
-        else h = rec[0];
+        else {
+          h = rec[0];
+          bessel = true;
+        }
       }
       hm[k] = rec + 4;
       H[k] = h;
       invH[k] = 1.0 / h;
+      qcb[k] = bessel ? __double_as_longlong(XC / h) : 0;
+      if constexpr (POLY) {
+        // sum_b hhat_b g_b(x) = (A(x) sin x + B(x) cos x) / x with
+        // x g_b = P_b(x^2) sin x + x Q_b(x^2) cos x, P_0 = 1, Q_0 = 0,
+        // P_1 = 1, Q_1 = -1 and (P, Q)_{b+1} = (2b+1) (P, Q)_b - x^2 (P, Q)_{b-1};
+        // in q (x = qH, the 1/q left to the warp):
+        //   F q = sum_j A_j H^{2j-1} q^{2j} sin + q sum_j B_j H^{2j} q^{2j} cos
+        double Ac[NA], Bc[NB], Pm[NA], Pc[NA], Qm[NB], Qc[NB];
 #pragma unroll
-      for (int b = 0; b <= LB; ++b) hh[k][b] = p0n[k] < 0 ? hm[k][b] : 0.0;
+        for (int j = 0; j < NA; ++j) Ac[j] = Pm[j] = Pc[j] = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) Bc[j] = Qm[j] = Qc[j] = 0.0;
+        if (bessel) {
+          Pm[0] = 1.0;  // b = 0
+          Ac[0] = hm[k][0];
+          if (LB >= 1) {
+            Pc[0] = 1.0;  // b = 1
+            Qc[0] = -1.0;
+            Ac[0] += hm[k][1];
+            Bc[0] = -hm[k][1];
+          }
+#pragma unroll
+          for (int bb = 1; bb < LB; ++bb) {
+            const double c = (double)(2 * bb + 1), hb = hm[k][bb + 1];
+            double Pn[NA], Qn[NB];
+#pragma unroll
+            for (int j = 0; j < NA; ++j) Pn[j] = c * Pc[j] - (j > 0 ? Pm[j - 1] : 0.0);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) Qn[j] = c * Qc[j] - (j > 0 ? Qm[j - 1] : 0.0);
+#pragma unroll
+            for (int j = 0; j < NA; ++j) {
+              Ac[j] = fma(hb, Pn[j], Ac[j]);
+              Pm[j] = Pc[j];
+              Pc[j] = Pn[j];
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+              Bc[j] = fma(hb, Qn[j], Bc[j]);
+              Qm[j] = Qc[j];
+              Qc[j] = Qn[j];
+            }
+          }
+        }
+        double hp = invH[k];  // H^{2j-1}
+#pragma unroll
+        for (int j = 0; j < NA; ++j) {
+          pa[k][j] = Ac[j] * hp;
+          hp *= h * h;
+        }
+        hp = 1.0;  // H^{2j}
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+          pb[k][j] = Bc[j] * hp;
+          hp *= h * h;
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b <= LB; ++b) hh[k][b] = p0n[k] < 0 ? hm[k][b] : 0.0;
+      }
       const double s = rec[1];
       sincos(dq * h, &sd[k], &cd[k]);
       kk[k] = exp(-2.0 * dq * dq * s);
@@ -195,26 +263,39 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
           }
           next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + RESEED);
         }
-        // the upward recurrence for all K quartets as straight-line code,
-        // then the rare lanes below the crossover or with P = Q patched in
+        // all K quartets as straight-line code, then the rare lanes below the
+        // crossover or on the P = Q branch patched in.  Polynomial form: the
+        // values are F q (J2: F q^3), the common 1/q (1/q^3) is applied once.
+        const long long qb = __double_as_longlong(q);
         double F[K];
         bool special = false;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const double x = q * H[k];
-          F[k] = bessel_up<LB>(hh[k], x, sn[k], cs[k], iq * invH[k]);
-          if (J2) F[k] *= iq * iq;
-          special |= (x < XC) | (p0n[k] >= 0);
+          if constexpr (POLY) {
+            const double y = q * q;
+            double ae = pa[k][NA - 1], bo = pb[k][NB - 1];
+#pragma unroll
+            for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
+#pragma unroll
+            for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
+            F[k] = fma(ae, sn[k], bo * (cs[k] * q));
+          } else {
+            F[k] = bessel_up<LB>(hh[k], q * H[k], sn[k], cs[k], iq * invH[k]);
+            if (J2) F[k] *= iq * iq;
+          }
+          special |= (qb < qcb[k]) | (p0n[k] >= 0);
         }
         if (special) {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const double x = q * H[k];
             if (p0n[k] >= 0) {
               F[k] = p0_poly(hm[k], p0n[k], q * q);
-            } else if (x < XC) {
+              if (POLY) F[k] *= J2 ? q * q * q : q;
+            } else if (qb < qcb[k]) {
+              const double x = q * H[k];
               F[k] = bessel_small<LB>(hm[k], x * x);
-              if (J2) F[k] *= iq * iq;
+              if (POLY) F[k] *= q;            // total: F q; j2: (F / q^2) q^3
+              else if (J2) F[k] *= iq * iq;
             }
           }
         }
@@ -228,6 +309,7 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
           g[k] *= r[k];
           r[k] *= kk[k];
         }
+        if constexpr (POLY) Fs *= J2 ? iq * iq * iq : iq;
         Fv[j] = Fs;
       }
       // reduce-scatter: after the halving rounds over lane bits 4, 3, 2 the
