@@ -244,6 +244,26 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
       kk[k] = exp(-2.0 * dq * dq * s);
       sn[k] = cs[k] = g[k] = r[k] = 0.0;
     }
+    // last point (exclusive) at which any lane of the warp may need a patch:
+    // on an ascending uniform tile the series region of a quartet is a
+    // prefix of its points (q < x_c / H), P = Q lanes need every point
+    int mse = 0;
+    {
+      int lane_end = 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (p0n[k] >= 0) lane_end = nqb;
+        else if (qcb[k] > 0) {
+          int e = nqb;
+          if (A.uniform && nq > 1) {
+            const double q1 = qs[1].x, qc = __longlong_as_double(qcb[k]);
+            e = qc <= q1 ? 2 : (int)min((double)nqb, ceil((qc - q1) / dq) + 3.0);
+          }
+          lane_end = max(lane_end, e);
+        }
+      }
+      mse = (int)__reduce_max_sync(0xffffffffu, (unsigned)lane_end);
+    }
     int next_seed = m0;
     for (int mb = m0; mb < m1; mb += QB) {
       double Fv[QB];
@@ -268,7 +288,6 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
         // values are F q (J2: F q^3), the common 1/q (1/q^3) is applied once.
         const long long qb = __double_as_longlong(q);
         double F[K];
-        bool special = false;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           if constexpr (POLY) {
@@ -283,7 +302,11 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
             F[k] = bessel_up<LB>(hh[k], q * H[k], sn[k], cs[k], iq * invH[k]);
             if (J2) F[k] *= iq * iq;
           }
-          special |= (qb < qcb[k]) | (p0n[k] >= 0);
+        }
+        bool special = false;
+        if (m < mse) {  // warp-uniform
+#pragma unroll
+          for (int k = 0; k < K; ++k) special |= (qb < qcb[k]) | (p0n[k] >= 0);
         }
         if (special) {
 #pragma unroll
