@@ -111,6 +111,15 @@ __device__ __noinline__ Seed seed_point(double q, double H, double s, double dq)
 #endif
 TB_HD constexpr int stage2_k(int LB) { return LB <= 2 ? TB_S2_K_LO : (LB <= 8 ? TB_S2_K_MID : 1); }
 
+// Crossover of the polynomial form: the smallest x at which its float64 error
+// stays within ~2e-13 of the largest term |hhat_b g_b| -- the level the same
+// form (and the upward recurrence) has at large x -- from a simulation against
+// 40-digit values over random coefficients spanning the H^{-2b} scales.
+TB_HD constexpr double poly_crossover(int LB) {
+  return LB == 0 ? 0.0 : LB == 1 ? 0.1 : LB == 2 ? 0.5 : LB == 3 ? 1.25 : LB == 4 ? 2.0 : LB == 5 ? 3.0
+       : LB == 6 ? 4.0 : LB == 7 ? 5.0 : 6.0;
+}
+
 // q points per reduction block: the warp sums QB points at once with a
 // reduce-scatter (3 halving rounds over lane bits 4..2, then 2 butterfly
 // rounds), so the shuffle latency is paid once per QB points.
@@ -138,9 +147,9 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
   for (int i = threadIdx.x; i < NW * nqb; i += blockDim.x) sm[2 * nqb + i] = 0.0;
   __syncthreads();
 
-  constexpr double XC = bessel_crossover(LB);
   // polynomial form for the orders whose float64 accuracy it matches (LB <= 8)
   constexpr bool POLY = LB <= 8;
+  constexpr double XC = POLY ? poly_crossover(LB) : bessel_crossover(LB);
   constexpr int NA = LB / 2 + 1;                   // A: powers q^0, q^2, .., q^{2 (NA-1)}
   constexpr int NB = LB >= 1 ? (LB - 1) / 2 + 1 : 1;  // B: q times powers of q^2
   const int64_t per = 32 * K;
