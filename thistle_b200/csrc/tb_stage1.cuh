@@ -58,6 +58,15 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
   return v;
 }
 
+#ifndef TB_S1_PF_MAXL
+#define TB_S1_PF_MAXL -1
+#endif
+#ifndef TB_S1_MB_LO
+#define TB_S1_MB_LO 2
+#endif
+#ifndef TB_S1_MB_3
+#define TB_S1_MB_3 3
+#endif
 // Largest LLmax handled by the register kernel, and its threads per quartet.
 constexpr int STAGE1_REG_MAXL = 8;
 TB_HD constexpr int stage1_reg_split(int L) { return L <= 4 ? 1 : (L == 5 ? 2 : (L == 6 ? 4 : 8)); }
@@ -72,7 +81,11 @@ TB_HD constexpr int stage1_split(int L) {
 }
 // Resident blocks asked of the register allocator: the largest count whose
 // register cap (65536 / (128 x blocks)) still holds the kernel without spills.
-TB_HD constexpr int stage1_reg_minblocks(int L) { return L <= 2 ? 4 : (L == 3 ? 3 : 2); }
+TB_HD constexpr int stage1_reg_minblocks(int L) { return L <= TB_S1_MB_LO ? 4 : (L == 3 ? TB_S1_MB_3 : 2); }
+// Classes whose density and ket coefficients of the next function quartet are
+// loaded before the current one is used (a one-deep software pipeline hiding
+// the gather latency where registers allow it).
+TB_HD constexpr int stage1_prefetch(int L) { return L <= TB_S1_PF_MAXL; }
 // Register entries of one thread: (T, U, j) with V = S j + s <= L - T - U for some s.
 TB_HD constexpr int reg_entries(int L, int S) {
   int n = 0;
@@ -319,25 +332,49 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
           bz[t] = (t & 1) ? -vz : vz;
         }
       }
-      for (int ic = 0; ic < nk; ++ic) {
-        for (int id = 0; id < nr; ++id) {
-          const int fc = sk + ic, fd = sr + id;
-          double z;
-          if (KIND == KIND_ELASTIC) z = A.zao[(size_t)fc * A.ngto + fd] * zab;
-          else z = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+      // ket function pairs; the density and ket coefficients of the next pair
+      // are loaded before the current one is used (one-deep software pipeline)
+      const int ncd = nk * nr;
+      auto fetch = [&](int ic, int id, double &zo, double *kxo, double *kyo, double *kzo) {
+        const int fc = sk + ic, fd = sr + id;
+        if (KIND == KIND_ELASTIC) zo = A.zao[(size_t)fc * A.ngto + fd] * zab;
+        else zo = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+        const int lc = A.flmn[fc], ld = A.flmn[fd];
+        const double *ex = esoa_slot(A, Q.skip & 8, 0, lc & 0xff, ld & 0xff, pk);
+        const double *ey = esoa_slot(A, Q.skip & 16, 1, (lc >> 8) & 0xff, (ld >> 8) & 0xff, pk);
+        const double *ez = esoa_slot(A, false, 2, (lc >> 16) & 0xff, (ld >> 16) & 0xff, pk);
+#pragma unroll
+        for (int t = 0; t <= TMAX; ++t) {
+          kxo[t] = ex[t * np];
+          kyo[t] = ey[t * np];
+          kzo[t] = ez[t * np];
+        }
+      };
+      constexpr bool PF = stage1_prefetch(L);
+      double zn = 0.0, kxn[TMAX + 1], kyn[TMAX + 1], kzn[TMAX + 1];
+      if (PF) fetch(0, 0, zn, kxn, kyn, kzn);
+      int icn = 0, idn = 0;
+      for (int cd = 0; cd < ncd; ++cd) {
+        {
+          double z, kx[TMAX + 1], ky[TMAX + 1], kz[TMAX + 1];
+          if constexpr (PF) {
+            z = zn;
+#pragma unroll
+            for (int t = 0; t <= TMAX; ++t) {
+              kx[t] = kxn[t];
+              ky[t] = kyn[t];
+              kz[t] = kzn[t];
+            }
+          } else {
+            fetch(icn, idn, z, kx, ky, kz);
+          }
+          if (++idn == nr) {
+            idn = 0;
+            ++icn;
+          }
+          if (PF && cd + 1 < ncd) fetch(icn, idn, zn, kxn, kyn, kzn);
           // the reference skips primitive quartets with |ztot| < cutoffz
           z = fabs(z) < A.cutoffz ? 0.0 : z;
-          const int lc = A.flmn[fc], ld = A.flmn[fd];
-          const double *ex = esoa_slot(A, Q.skip & 8, 0, lc & 0xff, ld & 0xff, pk);
-          const double *ey = esoa_slot(A, Q.skip & 16, 1, (lc >> 8) & 0xff, (ld >> 8) & 0xff, pk);
-          const double *ez = esoa_slot(A, false, 2, (lc >> 16) & 0xff, (ld >> 16) & 0xff, pk);
-          double kx[TMAX + 1], ky[TMAX + 1], kz[TMAX + 1];
-#pragma unroll
-          for (int t = 0; t <= TMAX; ++t) {
-            kx[t] = ex[t * np];
-            ky[t] = ey[t * np];
-            kz[t] = ez[t * np];
-          }
           // C_axis[T] = sum_t b[t] k[T - t] over the full (zero-padded) range
           double Cx[L + 1], Cy[L + 1], Cz[L + 1];
 #pragma unroll
