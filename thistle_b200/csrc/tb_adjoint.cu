@@ -196,6 +196,10 @@ __global__ void __launch_bounds__(128) adjoint_q_kernel(AdjointQArgs A) {
 // stage B
 // ---------------------------------------------------------------------------
 constexpr int ADJ_THREADS = 64;
+// Threads per quartet of stage B: PA x PC split the bra x ket function pairs
+// of the heavy classes (their partial sums are combined in a fixed order).
+TB_HD constexpr int adj_pa(int L) { return L >= 6 ? 4 : (L >= 4 ? 2 : 1); }
+TB_HD constexpr int adj_pc(int L) { return L >= 6 ? 4 : (L >= 4 ? 2 : 1); }
 
 template <int L>
 __device__ __forceinline__ int adx(int T, int U, int V) {  // simplex index of order L+1
@@ -207,7 +211,7 @@ __device__ __forceinline__ const double *dsoa_slot(const AdjointFArgs &A, int ax
   return A.dsoa + (int64_t)((axis * m1 + la) * m1 + lb) * DE_T * A.s1.npair + pair;
 }
 
-template <int L>
+template <int L, bool SPLIT>
 __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) {
   {
     const int64_t g = blockIdx.y;  // geometry of a batch
@@ -224,16 +228,21 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
   constexpr int TD = L1 < 2 * MAXA + 1 ? L1 : 2 * MAXA + 1;  // last dE index
   extern __shared__ double sm[];
   const int ng = A.s1.ng;
-  double *gw = sm + (size_t)ADJ_THREADS * NA + (threadIdx.x >> 5) * 3 * ng;  // this warp's gradient row
-  for (int i = threadIdx.x; i < (ADJ_THREADS / 32) * 3 * ng; i += ADJ_THREADS) sm[(size_t)ADJ_THREADS * NA + i] = 0.0;
+  constexpr int QPB0 = SPLIT ? ADJ_THREADS / (adj_pa(L) * adj_pc(L)) : ADJ_THREADS;
+  double *gw = sm + (size_t)QPB0 * NA + (threadIdx.x >> 5) * 3 * ng;  // this warp's gradient row
+  for (int i = threadIdx.x; i < (ADJ_THREADS / 32) * 3 * ng; i += ADJ_THREADS) sm[(size_t)QPB0 * NA + i] = 0.0;
   __syncthreads();
   const Stage1Args &S = A.s1;
   const int64_t n = S.qend - S.qbegin;
   const int lane = threadIdx.x & 31;
-  double *Ab = sm + threadIdx.x;  // Abar_TUV at Ab[adx * ADJ_THREADS]
-  for (int64_t base = (int64_t)blockIdx.x * ADJ_THREADS; base < n; base += (int64_t)gridDim.x * ADJ_THREADS) {
-    const int64_t qi = S.qbegin + base + threadIdx.x;
-    const bool act = base + threadIdx.x < n;
+  constexpr int PA = SPLIT ? adj_pa(L) : 1, PC = SPLIT ? adj_pc(L) : 1, P = PA * PC;
+  constexpr int QPB = ADJ_THREADS / P;  // quartets per block and round
+  const int gsub = threadIdx.x % P, grp = threadIdx.x / P, pa = gsub % PA, pc = gsub / PA;
+  const unsigned gmask = P == 32 ? 0xffffffffu : (((1u << P) - 1u) << (lane - gsub));
+  double *Ab = sm + grp;  // the group's Abar_TUV at Ab[adx * QPB]
+  for (int64_t base = (int64_t)blockIdx.x * QPB; base < n; base += (int64_t)gridDim.x * QPB) {
+    const int64_t qi = S.qbegin + base + grp;
+    const bool act = base + grp < n;  // whole groups
     double gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0}, gk[3] = {0, 0, 0}, gr[3] = {0, 0, 0};
     int ci = 0, cj = 0, ck = 0, cr = 0;
     if (act) {
@@ -241,18 +250,20 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
       ci = Q.gi; cj = Q.gj; ck = Q.gk; cr = Q.gr;
       const double *jb = A.adj + S.recbase + (qi - S.qbegin) * (int64_t)S.rs;
       const double wpp = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
-      // Abar up to order L+1
+      // Abar up to order L+1, entries shared out over the group
+      int cnt = 0;
       if (Q.p0) {
         for (int T = 0; T <= L1; ++T)
           for (int U = 0; U <= L1 - T; ++U)
             for (int V = 0; V <= L1 - T - U; ++V) {
+              if ((cnt++ % P) != gsub) continue;
               double a = 0.0;
               if (!((T | U | V) & 1)) {
                 const int k = (T + U + V) / 2;
                 a = p0_factor(T, U, V, false) * jb[k];
                 if (k & 1) a = -a;
               }
-              Ab[adx<L>(T, U, V) * ADJ_THREADS] = wpp * a;
+              Ab[adx<L>(T, U, V) * QPB] = wpp * a;
             }
       } else {
         double ax[tp_size(L1)], ay[tp_size(L1)], az[tp_size(L1)];
@@ -262,15 +273,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
         for (int T = 0; T <= L1; ++T)
           for (int U = 0; U <= L1 - T; ++U)
             for (int V = 0; V <= L1 - T - U; ++V) {
+              if ((cnt++ % P) != gsub) continue;
               double a = 0.0;
               for (int k1 = 0; 2 * k1 <= T; ++k1)
                 for (int k2 = 0; 2 * k2 <= U; ++k2)
                   for (int k3 = 0; 2 * k3 <= V; ++k3)
                     a += ax[tp_off(T) + k1] * ay[tp_off(U) + k2] * az[tp_off(V) + k3] *
                          jb[(T - k1) + (U - k2) + (V - k3)];
-              Ab[adx<L>(T, U, V) * ADJ_THREADS] = wpp * a;
+              Ab[adx<L>(T, U, V) * QPB] = wpp * a;
             }
       }
+      if (P > 1) __syncwarp(gmask);
       const int pb = pair_index(Q.gi, Q.gj, ng), pk = pair_index(Q.gk, Q.gr, ng);
       const int64_t np = S.npair;
       double S0 = 0.0, gH[3] = {0, 0, 0}, gEi[3] = {0, 0, 0}, gEk[3] = {0, 0, 0};
@@ -278,7 +291,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
       const int sj = S.gstart[Q.gj], nj = S.gcount[Q.gj];
       const int sk = S.gstart[Q.gk], nk = S.gcount[Q.gk];
       const int sr = S.gstart[Q.gr], nr = S.gcount[Q.gr];
-      for (int ab = 0; ab < ni * nj; ++ab) {
+      for (int ab = pa; ab < ni * nj; ab += PA) {
         const int fa = si + ab / nj, fb = sj + ab % nj;
         const int la = S.flmn[fa], lb = S.flmn[fb];
         const int64_t rowp = fpair(min(fa, fb), max(fa, fb)) * S.np;
@@ -301,7 +314,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
             bd[ax][t] = (t & 1) ? -v : v;
           }
         }
-        for (int cd = 0; cd < nk * nr; ++cd) {
+        for (int cd = pc; cd < nk * nr; cd += PC) {
           const int fc = sk + cd / nr, fd = sr + cd % nr;
           double z = S.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
           z = fabs(z) < S.cutoffz ? 0.0 : z;
@@ -346,7 +359,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
               const double cxy = C[0][T] * C[1][U];
 #pragma unroll
               for (int V = 0; V <= L1 - T - U; ++V) {
-                const double a = Ab[adx<L>(T, U, V) * ADJ_THREADS];
+                const double a = Ab[adx<L>(T, U, V) * QPB];
                 w = fma(a, C[2][V], w);
                 Yz[V] = fma(a, cxy, Yz[V]);
               }
@@ -382,6 +395,18 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
           gEk[1] = fma(z, k1, gEk[1]);
           gEk[2] = fma(z, k2, gEk[2]);
         }
+      }
+      if (P > 1) {
+        // fixed-order sum of the group's partial sums (in its first thread)
+        S0 = group_sum<P>(S0, gmask);
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          gH[ax] = group_sum<P>(gH[ax], gmask);
+          gEi[ax] = group_sum<P>(gEi[ax], gmask);
+          gEk[ax] = group_sum<P>(gEk[ax], gmask);
+        }
+        if (gsub != 0) S0 = gH[0] = gH[1] = gH[2] = gEi[0] = gEi[1] = gEi[2] = gEk[0] = gEk[1] = gEk[2] = 0.0;
+        __syncwarp(gmask);  // Abar is rewritten by the next round
       }
       if (Q.p0) gH[0] = gH[1] = gH[2] = 0.0;  // the P = Q polynomial does not depend on H
       const double pij = Q.tb[3], pkr = Q.tk[3];
@@ -419,7 +444,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
   __syncthreads();
   for (int i = threadIdx.x; i < 3 * ng; i += ADJ_THREADS) {
     double t = 0.0;
-    for (int w = 0; w < ADJ_THREADS / 32; ++w) t += sm[(size_t)ADJ_THREADS * NA + w * 3 * ng + i];
+    for (int w = 0; w < ADJ_THREADS / 32; ++w) t += sm[(size_t)QPB0 * NA + w * 3 * ng + i];
     A.gpart[(size_t)blockIdx.x * A.gstride + i] += t;
   }
 }
@@ -448,21 +473,28 @@ cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStre
   return cudaGetLastError();
 }
 
-template <int L>
+template <int L, bool SPLIT>
 static cudaError_t launch_adjoint_f_l(const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st) {
-  const size_t smem = sizeof(double) * ((size_t)ADJ_THREADS * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng);
-  cudaError_t e = cudaFuncSetAttribute(adjoint_f_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int qpb = SPLIT ? ADJ_THREADS / (adj_pa(L) * adj_pc(L)) : ADJ_THREADS;
+  const size_t smem = sizeof(double) * ((size_t)qpb * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng);
+  cudaError_t e =
+      cudaFuncSetAttribute(adjoint_f_kernel<L, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  adjoint_f_kernel<L><<<dim3(grid, ngeom), ADJ_THREADS, smem, st>>>(a);
+  adjoint_f_kernel<L, SPLIT><<<dim3(grid, ngeom), ADJ_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
-int adjoint_f_threads() { return ADJ_THREADS; }
+int adjoint_f_quartets_per_block(int L, bool split) {
+  return split ? ADJ_THREADS / (adj_pa(L) * adj_pc(L)) : ADJ_THREADS;
+}
 
-cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st) {
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, bool split, cudaStream_t st) {
   if (a.s1.qend <= a.s1.qbegin) return cudaSuccess;
   switch (L) {
-#define TB_F(n) case n: return launch_adjoint_f_l<n>(a, grid, ngeom, st);
+#define TB_F(n)                                                                     \
+  case n:                                                                           \
+    return split ? launch_adjoint_f_l<n, true>(a, grid, ngeom, st)                  \
+                 : launch_adjoint_f_l<n, false>(a, grid, ngeom, st);
     TB_F(0) TB_F(1) TB_F(2) TB_F(3) TB_F(4) TB_F(5) TB_F(6) TB_F(7) TB_F(8)
 #undef TB_F
     default: return cudaErrorInvalidValue;

@@ -114,11 +114,11 @@ struct AdjointFArgs {
   int64_t gs_dsoa, gs_xyz, gs_gpart;  // per-geometry strides (blockIdx.y); adj uses s1.gs_rec
 };
 int64_t dsoa_doubles(int ng, int maxa);
-int adjoint_f_threads();
+int adjoint_f_quartets_per_block(int L, bool split);
 cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const double *ga, const double *xyz,
                                 double *dsoa, int ngeom, int64_t gs_xyz, int64_t gs_dsoa, cudaStream_t st);
 cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStream_t st);
-cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st);
+cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, bool split, cudaStream_t st);
 
 // Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
 cudaError_t pool_malloc(void **p, size_t bytes);

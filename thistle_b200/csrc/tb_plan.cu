@@ -929,8 +929,12 @@ static int adjoint_stages(thistle_plan *P, const double *d_v, double *d_grad) {
     a.gs_xyz = 3 * (int64_t)P->ngto;
     a.gs_gpart = gs_gpart;
     const int64_t n = P->cls_end[c] - P->cls_begin[c];
-    const int grid = (int)std::min<int64_t>(P->adj_rows, (n + adjoint_f_threads() - 1) / adjoint_f_threads());
-    TB_TRYC(launch_adjoint_f(P->cls_L[c], a, grid, G, P->st));
+    // a class with too few quartets (over all geometries) to keep every SM
+    // busy several times over splits each quartet across a thread group
+    const bool split = n * G < (int64_t)4 * P->nsm * 64;
+    const int qpb = adjoint_f_quartets_per_block(P->cls_L[c], split);
+    const int grid = (int)std::min<int64_t>(P->adj_rows, (n + qpb - 1) / qpb);
+    TB_TRYC(launch_adjoint_f(P->cls_L[c], a, grid, G, split, P->st));
     P->launches += 1;
   }
   TB_TRYC(launch_reduce_batch(P->d_gpart, P->adj_rows, 3 * P->ng, gs_gpart, d_grad, G, P->st));
