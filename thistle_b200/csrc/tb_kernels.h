@@ -71,7 +71,10 @@ struct Stage2ClassArgs {
   int64_t pstride;
   int64_t gs_rec, gs_partial; // per-geometry strides (blockIdx.y is the geometry)
 };
-constexpr int STAGE2_WARPS = 8;
+#ifndef TB_S2_WARPS
+#define TB_S2_WARPS 4
+#endif
+constexpr int STAGE2_WARPS = TB_S2_WARPS;
 // q points a stage-2 block holds in shared memory at once
 constexpr int STAGE2_QTILE = 1024;
 int stage2_quartets_per_warp(int LB);

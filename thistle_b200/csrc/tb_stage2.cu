@@ -21,7 +21,8 @@
 //                 Horner in x^2 / (2b+1).
 // On uniform q grids sin/cos(qH) advance by a rotation through dq H and
 // exp(-q^2 s) by g <- g r, r <- r k (r = exp(-(2 q dq + dq^2) s),
-// k = exp(-2 dq^2 s)), both restarted from direct values every 64 points.
+// k = exp(-2 dq^2 s)), both restarted from direct values every 128 points
+// (and at the start of every q chunk).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -32,7 +33,10 @@ namespace tb {
 
 namespace {
 
-constexpr int RESEED = 64;
+#ifndef TB_S2_RESEED
+#define TB_S2_RESEED 128
+#endif
+constexpr int RESEED = TB_S2_RESEED;
 
 // Coefficients that lanes without a quartet point at: a zero record body,
 // with room for the [H, s, kind, order] head in front of it.
@@ -107,7 +111,7 @@ __device__ __noinline__ Seed seed_point(double q, double H, double s, double dq)
 #define TB_S2_K_MID 2
 #endif
 #ifndef TB_S2_MINB
-#define TB_S2_MINB 2
+#define TB_S2_MINB 4
 #endif
 TB_HD constexpr int stage2_k(int LB) { return LB <= 2 ? TB_S2_K_LO : (LB <= 8 ? TB_S2_K_MID : 1); }
 
