@@ -364,7 +364,7 @@ __global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off,
   }
   quart[qi] = (uint64_t)i | ((uint64_t)j << 16) | ((uint64_t)k << 32) | ((uint64_t)r << 48);
   int Li = gL[i], Lj = gL[j], Lk = gL[k], Lr = gL[r];
-  keys[qi] = (uint32_t)(((((Li + Lj + Lk + Lr) * 5 + Li) * 5 + Lj) * 5 + Lk) * 5 + Lr);
+  keys[qi] = quartet_key(Li, Lj, Lk, Lr);
 }
 
 // ---------------------------------------------------------------------------
@@ -377,6 +377,21 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
   pair_tables_kernel<<<dim3((n + 127) / 128, ngeom), 128, 0, st>>>(ng, maxa, gstart, flmn, ga, xyz, tab, esoa,
                                                                     gs_xyz, gs_tab, gs_esoa);
   return cudaGetLastError();
+}
+
+#ifndef TB_S1_XK_MIN
+#define TB_S1_XK_MIN 4
+#endif
+#ifndef TB_S1_XK_MAX
+#define TB_S1_XK_MAX 6
+#endif
+bool stage1_xk(int L) { return L >= TB_S1_XK_MIN && L <= TB_S1_XK_MAX; }
+
+cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_xk_k<KIND_TOTAL>(L, LK, XB, a, ngeom, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_xk_k<KIND_ELASTIC>(L, LK, XB, a, ngeom, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_xk_k<KIND_ALIGNED>(L, LK, XB, a, ngeom, st);
+  return launch_stage1_xk_k<KIND_J2>(L, LK, XB, a, ngeom, st);
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st) {

@@ -140,6 +140,12 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
 template <int K>
 cudaError_t launch_stage1_k(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st);
+template <int K>
+cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
+// LLmax classes whose quartets go through the contracted-side kernel, by
+// sub-range of equal (LK = min(L_bra, L_ket), XB = L_bra < L_ket)
+bool stage1_xk(int L);
+cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);

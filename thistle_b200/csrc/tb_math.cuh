@@ -131,6 +131,17 @@ TB_HD int npairs(int ng) { return ng * (ng + 1) / 2; }
 // function-pair index for a <= b, ordered by b then a
 TB_HD int64_t fpair(int a, int b) { return (int64_t)b * (b + 1) / 2 + a; }
 
+// Sort key of a group quartet from its shells' angular momenta: LLmax first
+// (classes), then LK = min(L_bra, L_ket) and whether that is the bra (the
+// contracted side of stage 1), then the four shells.  18 bits.
+TB_HD uint32_t quartet_key(int Li, int Lj, int Lk, int Lr) {
+  const int LL = Li + Lj + Lk + Lr, lb = Li + Lj, lk = Lk + Lr;
+  const int LK = lb < lk ? lb : lk, XB = lb < lk ? 1 : 0;
+  return (uint32_t)(((LL * 9 + LK) * 2 + XB) * 625 + ((Li * 5 + Lj) * 5 + Lk) * 5 + Lr);
+}
+constexpr uint32_t KEY_CLASS_DIV = 9 * 2 * 625;  // LLmax = key / KEY_CLASS_DIV
+constexpr int KEY_BITS = 18;
+
 // Series coefficients of u_n(x) = j_n(x) (2n+1)!!/x^n = sum_k c_{n,k} y^k,
 // y = x^2: c_{n,0} = 1, c_{n,k} = c_{n,k-1} (-1/2) / (k (2n+2k+1)).
 TB_HD constexpr double series_coef(int n, int k) {

@@ -86,6 +86,12 @@ static void dfree(T *&p) {
   p = nullptr;
 }
 
+// Quartets of one LLmax class with equal (LK, XB) (see quartet_key).
+struct SubRange {
+  int LK, XB;
+  int64_t begin, end;
+};
+
 struct thistle_plan {
   int type = 0, kind = 0;
   int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nq = 0, maxa = 0, nmat = 0;
@@ -98,6 +104,7 @@ struct thistle_plan {
   int cls_L[MAXCLS];
   int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
   int cls_rs[MAXCLS];
+  std::vector<SubRange> cls_sub[MAXCLS];
   int64_t rec_total = 0;
   int *d_gstart = nullptr, *d_gcount = nullptr, *d_flmn = nullptr;
   double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr, *d_esoa = nullptr;
@@ -280,6 +287,21 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
     rs += rs & 1;
     P->cls_rs[k] = rs;
     P->cls_recoff[k] = recoff;
+    // sub-ranges in key order: (LK, XB) ascending
+    P->cls_sub[k].clear();
+    int64_t sp = pos;
+    for (int LK = 0; LK <= 8; ++LK)
+      for (int XB = 0; XB <= 1; ++XB) {
+        int64_t sc = 0;
+        for (int t = 0; t < 625; ++t) {
+          const int Li = t / 125, Lj = (t / 25) % 5, Lk = (t / 5) % 5, Lr = t % 5;
+          const uint32_t key = quartet_key(Li, Lj, Lk, Lr);
+          if ((int)(key / KEY_CLASS_DIV) != LL || (int)((key / 625) % 18) != LK * 2 + XB) continue;
+          sc += cnt[LL * 625 + t];
+        }
+        if (sc > 0) P->cls_sub[k].push_back(SubRange{LK, XB, sp, sp + sc});
+        sp += sc;
+      }
     recoff += c * rs;
     pos += c;
   }
@@ -477,7 +499,7 @@ static int quartets_alloc(thistle_plan *P) {
   TB_TRYC(cudaMemcpyAsync(P->d_braoff, off.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cudaMemcpyAsync(P->d_gL, P->gL.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, P->st));
   TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->sort_tmp_bytes, P->d_k0, P->d_k1, P->d_v0, P->d_quart,
-                                          (int)acc, 0, 14, P->st));
+                                          (int)acc, 0, KEY_BITS, P->st));
   TB_TRY(dalloc((char **)&P->d_sort_tmp, P->sort_tmp_bytes, "sort scratch"));
 done:
   return rc;
@@ -488,7 +510,7 @@ static int quartets_run(thistle_plan *P) {
   TB_TRYC(launch_quartet_fill(P->ng, P->d_braoff, P->nquart, P->d_gL, P->d_v0, P->d_k0, P->st));
   P->launches += 1;
   TB_TRYC(cub::DeviceRadixSort::SortPairs(P->d_sort_tmp, P->sort_tmp_bytes, P->d_k0, P->d_k1, P->d_v0, P->d_quart,
-                                          (int)P->nquart, 0, 14, P->st));
+                                          (int)P->nquart, 0, KEY_BITS, P->st));
 done:
   return rc;
 }
@@ -785,7 +807,7 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
 
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
-                      double *d_out, bool order, int ngeom) {
+                      const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom) {
   // stage events (not while a graph is being captured)
   cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
   auto mark = [&](int i) -> cudaError_t { return P->capturing ? cudaSuccess : cudaEventRecord(E[i], P->st); };
@@ -801,8 +823,19 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.p0count = (unsigned long long *)(P->d_p0count + c);
     a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
-    TB_CK(launch_stage1(P->kind, cL[c], a, ngeom, P->st));
-    P->launches += 1;
+    if (stage1_xk(cL[c])) {
+      for (const SubRange &u : subs[c]) {
+        Stage1Args b = a;
+        b.qbegin = u.begin;
+        b.qend = u.end;
+        b.recbase = recoff[c] + (u.begin - cb[c]) * (int64_t)rs[c];
+        TB_CK(launch_stage1_xk(P->kind, cL[c], u.LK, u.XB != 0, b, ngeom, P->st));
+        P->launches += 1;
+      }
+    } else {
+      TB_CK(launch_stage1(P->kind, cL[c], a, ngeom, P->st));
+      P->launches += 1;
+    }
   }
   TB_CK(mark(2));
   int64_t nall = ncls > 0 ? ce[ncls - 1] : 0;
@@ -883,7 +916,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
 
 static int plan_exec(thistle_plan *P, double *d_out) {
   int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                      P->cls_rs, d_out, true, P->ngeom);
+                      P->cls_rs, P->cls_sub, d_out, true, P->ngeom);
   P->fwd_valid = rc == THISTLE_OK;
   return rc;
 }
@@ -993,7 +1026,7 @@ static int forward_batch(thistle_plan *P) {
     TB_CK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
     P->capturing = true;
     int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                        P->cls_rs, P->d_result, true, P->ngeom);
+                        P->cls_rs, P->cls_sub, P->d_result, true, P->ngeom);
     P->capturing = false;
     cudaError_t e = cudaStreamEndCapture(P->st, &g);
     if (rc != THISTLE_OK) {
@@ -1373,18 +1406,26 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
     if (gi < 0 || gj < 0 || gk < 0 || gr < 0 || gi >= P->ng || gj >= P->ng || gk >= P->ng || gr >= P->ng ||
         gi > gj || gk > gr)
       return fail(THISTLE_ERR_SHAPE, "quartet " + std::to_string(t) + " needs 0 <= gi <= gj < ng, 0 <= gk <= gr < ng");
-    int key = class_key(P->gL[gi], P->gL[gj], P->gL[gk], P->gL[gr]);
+    int key = (int)quartet_key(P->gL[gi], P->gL[gj], P->gL[gk], P->gL[gr]);
     items[t] = {key, (uint64_t)gi | ((uint64_t)gj << 16) | ((uint64_t)gk << 32) | ((uint64_t)gr << 48)};
   }
   std::stable_sort(items.begin(), items.end(),
                    [](const std::pair<int, uint64_t> &a, const std::pair<int, uint64_t> &b) { return a.first < b.first; });
   int64_t cb[MAXCLS], ce[MAXCLS], ro[MAXCLS];
   int cL[MAXCLS], rs[MAXCLS], ncls = 0;
+  std::vector<SubRange> sub[MAXCLS];
   int64_t roff = 0;
   for (int64_t t = 0; t < nquart;) {
-    int LL = items[t].first / 625;
+    int LL = items[t].first / (int)KEY_CLASS_DIV;
     int64_t u = t;
-    while (u < nquart && items[u].first / 625 == LL) ++u;
+    while (u < nquart && items[u].first / (int)KEY_CLASS_DIV == LL) ++u;
+    for (int64_t w = t; w < u;) {
+      const int sk = (items[w].first / 625) % 18;
+      int64_t x = w;
+      while (x < u && (items[x].first / 625) % 18 == sk) ++x;
+      sub[ncls].push_back(SubRange{sk / 2, sk % 2, w, x});
+      w = x;
+    }
     cb[ncls] = t; ce[ncls] = u; cL[ncls] = LL;
     rs[ncls] = P->kind == KIND_ALIGNED ? 4 + ntuv(LL) : LL + 7;
     rs[ncls] += rs[ncls] & 1;
@@ -1405,7 +1446,7 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
   if (nquart == 0) {
     TB_TRYC(cudaMemsetAsync(P->d_result, 0, sizeof(double) * P->nq, P->st));
   } else {
-    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, P->d_result, false, 1));
+    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, sub, P->d_result, false, 1));
   }
   TB_TRYC(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));

@@ -564,6 +564,137 @@ __global__ void stage1_smem_kernel(Stage1Args A) {
 }
 
 // ---------------------------------------------------------------------------
+// contracted-side kernel (LLmax 4..6), thread per quartet
+// ---------------------------------------------------------------------------
+// The quartets of one launch share LK = min(L_bra, L_ket) and which side it
+// is (XB: the bra).  That side is contracted with the pair density first,
+//   X_o(t'u'v') = sum_c rho(o, c) E_c^x(t') E_c^y(u') E_c^z(v')   (o on the other side),
+// and its Hermite box then convolved once per function pair of the other side,
+//   D(T U V) += sum B_o(t u v) X_o(T-t, U-u, V-v),
+// every shape compile-time (the other side has order L - LK), so a function
+// quartet costs ntuv(LK) FMAs instead of the three zero-padded convolutions
+// and the outer product of stage1_reg_kernel.
+
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128, 2) stage1_xk_kernel(Stage1Args A) {
+  stage1_geometry(A);
+  constexpr int LO = L - LK;  // order of the convolved (outer) side
+  constexpr int NT = ntuv(L), NX = ntuv(LK);
+  constexpr int NG = 128;
+  extern __shared__ double sD[];
+  const int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= A.qend) return;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const int pb = pair_index(Q.gi, Q.gj, A.ng), pk = pair_index(Q.gk, Q.gr, A.ng);
+  const int64_t np = A.npair;
+  double D[NT];
+#pragma unroll
+  for (int e = 0; e < NT; ++e) D[e] = 0.0;
+  const int si = A.gstart[Q.gi], ni = A.gcount[Q.gi];
+  const int sj = A.gstart[Q.gj], nj = A.gcount[Q.gj];
+  const int sk = A.gstart[Q.gk], nk = A.gcount[Q.gk];
+  const int sr = A.gstart[Q.gr], nr = A.gcount[Q.gr];
+  const int nab = ni * nj, ncd = nk * nr;
+  // the bra side's E coefficients carry the (-1)^t sign of src/Integrals.f90:5181
+  const int nout = XB ? ncd : nab, nin = XB ? nab : ncd;
+  for (int o = 0; o < nout; ++o) {
+    // the outer pair's functions and coefficients (order LO)
+    int fa, fb, fc, fd;
+    if (XB) { fc = sk + o / nr; fd = sr + o % nr; fa = fb = 0; }
+    else { fa = si + o / nj; fb = sj + o % nj; fc = fd = 0; }
+    double ox[LO + 1], oy[LO + 1], oz[LO + 1];
+    {
+      const int l1 = XB ? A.flmn[fc] : A.flmn[fa], l2 = XB ? A.flmn[fd] : A.flmn[fb];
+      const int pr = XB ? pk : pb;
+      const double *ex = esoa_slot(A, XB ? (Q.skip & 8) : (Q.skip & 1), 0, l1 & 0xff, l2 & 0xff, pr);
+      const double *ey = esoa_slot(A, XB ? (Q.skip & 16) : (Q.skip & 2), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
+      const double *ez = esoa_slot(A, XB ? false : (Q.skip & 4), 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
+#pragma unroll
+      for (int t = 0; t <= LO; ++t) {
+        const double sg = (!XB && (t & 1)) ? -1.0 : 1.0;
+        ox[t] = sg * ex[t * np];
+        oy[t] = sg * ey[t * np];
+        oz[t] = sg * ez[t * np];
+      }
+    }
+    // X over the contracted side's function pairs
+    double X[NX];
+#pragma unroll
+    for (int e = 0; e < NX; ++e) X[e] = 0.0;
+    int64_t rowp = 0;
+    double zo = 0.0;
+    if (!XB) {
+      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+    } else {
+      zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
+    }
+    for (int c = 0; c < nin; ++c) {
+      int ga, gb2, gc, gd;
+      if (XB) { ga = si + c / nj; gb2 = sj + c % nj; gc = fc; gd = fd; }
+      else { gc = sk + c / nr; gd = sr + c % nr; ga = fa; gb2 = fb; }
+      double z;
+      if (KIND == KIND_ELASTIC) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
+      else {
+        const int64_t rp = XB ? fpair(min(ga, gb2), max(ga, gb2)) * A.np : rowp;
+        z = A.rho[rp + fpair(min(gc, gd), max(gc, gd))];
+      }
+      // the reference skips primitive quartets with |ztot| < cutoffz
+      z = fabs(z) < A.cutoffz ? 0.0 : z;
+      const int l1 = XB ? A.flmn[ga] : A.flmn[gc], l2 = XB ? A.flmn[gb2] : A.flmn[gd];
+      const int pr = XB ? pb : pk;
+      const double *ex = esoa_slot(A, XB ? (Q.skip & 1) : (Q.skip & 8), 0, l1 & 0xff, l2 & 0xff, pr);
+      const double *ey = esoa_slot(A, XB ? (Q.skip & 2) : (Q.skip & 16), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
+      const double *ez = esoa_slot(A, XB ? (Q.skip & 4) : false, 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
+      double cx[LK + 1], cy[LK + 1], cz[LK + 1];
+#pragma unroll
+      for (int t = 0; t <= LK; ++t) {
+        const double sg = (XB && (t & 1)) ? -1.0 : 1.0;
+        cx[t] = sg * ex[t * np];
+        cy[t] = sg * ey[t * np];
+        cz[t] = sg * ez[t * np];
+      }
+      int e = 0;
+#pragma unroll
+      for (int t = 0; t <= LK; ++t) {
+        const double w1 = z * cx[t];
+#pragma unroll
+        for (int u = 0; u <= LK - t; ++u) {
+          const double w2 = w1 * cy[u];
+#pragma unroll
+          for (int v = 0; v <= LK - t - u; ++v, ++e) X[e] = fma(w2, cz[v], X[e]);
+        }
+      }
+    }
+    // D += O (x) X over the two simplices
+#pragma unroll
+    for (int t = 0; t <= LO; ++t)
+#pragma unroll
+      for (int u = 0; u <= LO - t; ++u) {
+        const double oxy = ox[t] * oy[u];
+#pragma unroll
+        for (int v = 0; v <= LO - t - u; ++v) {
+          const double b = oxy * oz[v];
+          int e = 0;
+#pragma unroll
+          for (int t2 = 0; t2 <= LK; ++t2)
+#pragma unroll
+            for (int u2 = 0; u2 <= LK - t2; ++u2)
+#pragma unroll
+              for (int v2 = 0; v2 <= LK - t2 - u2; ++v2, ++e) {
+                const int k = dindex<L>(t + t2, u + u2, v + v2);
+                D[k] = fma(b, X[e], D[k]);
+              }
+        }
+      }
+  }
+  double *col = sD + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NT; ++k) col[k * NG] = D[k];
+  stage1_finish<L, KIND, 1>(A, Q, col, NG, qi, 0, 0xffffffffu);
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 // threads per block of the shared-memory kernel so that the Hermite densities
@@ -596,6 +727,33 @@ static cudaError_t launch_stage1_l(const Stage1Args &a, int64_t n, int ngeom, cu
     stage1_smem_kernel<L, K><<<dim3((unsigned)((threads + thr - 1) / thr), ngeom), thr, smem, st>>>(a);
   }
   return cudaGetLastError();
+}
+
+template <int L, int K, int LK, bool XB>
+static cudaError_t launch_stage1_xk_l(const Stage1Args &a, int64_t n, int ngeom, cudaStream_t st) {
+  const int thr = 128;
+  const size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
+  cudaError_t e =
+      cudaFuncSetAttribute(stage1_xk_kernel<L, K, LK, XB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage1_xk_kernel<L, K, LK, XB><<<dim3((unsigned)((n + thr - 1) / thr), ngeom), thr, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st) {
+  const int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+#define TB_XK(l, lk)                                                                         \
+  if (L == l && LK == lk)                                                                   \
+    return XB ? launch_stage1_xk_l<l, K, lk, true>(a, n, ngeom, st)                         \
+              : launch_stage1_xk_l<l, K, lk, false>(a, n, ngeom, st);
+  TB_XK(3, 0) TB_XK(3, 1)
+  TB_XK(4, 0) TB_XK(4, 1) TB_XK(4, 2)
+  TB_XK(5, 0) TB_XK(5, 1) TB_XK(5, 2)
+  TB_XK(6, 0) TB_XK(6, 1) TB_XK(6, 2) TB_XK(6, 3)
+#undef TB_XK
+  return cudaErrorInvalidValue;
 }
 
 template <int K>

@@ -4,4 +4,6 @@
 
 namespace tb {
 template cudaError_t launch_stage1_k<KIND_TOTAL>(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
+template cudaError_t launch_stage1_xk_k<KIND_TOTAL>(int L, int LK, bool XB, const Stage1Args &a, int ngeom,
+                                                      cudaStream_t st);
 }  // namespace tb
