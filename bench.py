@@ -311,6 +311,85 @@ def run_fit(args):
     return 0
 
 
+def run_batch4(args):
+    """Configuration 4: uneven molecules (2-12 atoms, s4p2d1 per atom, 4-24
+    MOs, sparse 2-RDMs, total j0 on 256 q).  Molecules are taken in chunks that
+    fit the device; per chunk every molecule gets its plan (density transform,
+    quartet list), then the chunk's I(q) is computed twice: once plan by plan
+    (the plain GPU path, one integrator call per molecule) and once as a
+    molecule batch (one launch per stage and class, replayed from a CUDA
+    graph).  Both integrator paths start from the same plans and copy I(q) to
+    host memory; set-up time is reported separately."""
+    import torch
+    from thistle_b200 import _abi
+    from thistle_b200 import inputs as I
+    from thistle_b200 import main_calculation as MC
+    import ctypes as C
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    mols = I.config4_batch(nmol=args.batch_molecules)
+    t_gen = time.perf_counter() - t0
+    budget = args.batch_gb * 1e9
+    t_setup = t_plain = t_batch = 0.0
+    qq = 0
+    nchunks, launches, err = 0, [], 0.0
+    i = 0
+    while i < len(mols):
+        plans = []
+        cached, used = C.c_int64(0), C.c_int64(0)
+        while i < len(mols) and len(plans) < args.batch_chunk:
+            t0 = time.perf_counter()
+            pl = MC.ScatteringPlan.from_problem(mols[i], MC.TOTAL_J0)
+            pl.execute()  # first execution allocates the records
+            t_setup += time.perf_counter() - t0
+            plans.append(pl)
+            qq += pl.info()["nquart"] * pl.nq
+            i += 1
+            _abi.check(_abi.lib().thistle_device_cache_bytes(C.byref(cached), C.byref(used)))
+            if used.value > budget:
+                break
+        # plain: one integrator call per molecule
+        for pl in plans[:2]:
+            pl.execute()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        singles = [pl.execute() for pl in plans]
+        t_plain += time.perf_counter() - t0
+        # batched: every molecule of the chunk in one launch per stage and class
+        with MC.MoleculeBatch(plans) as b:
+            b.use_graph(True)
+            for _ in range(2):
+                b.execute()
+            torch.cuda.synchronize()
+            reps = max(1, args.steps)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                out = b.execute()
+            t_batch += (time.perf_counter() - t0) / reps
+            launches.append(b.info()["launches"])
+        err = max(err, max(float(np.max(np.abs(o - s)) / np.max(np.abs(s))) for o, s in zip(out, singles)))
+        for pl in plans:
+            pl.close()
+        nchunks += 1
+    n = len(mols)
+    line = {
+        "metric": "molecules/s, total j0 I(q) of an uneven molecule batch (256 q)", "value": n / t_batch,
+        "unit": "molecules/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded; BASELINE configuration 4 shapes)",
+        "config": {"workload": f"batch4: {n} molecules of 2-12 atoms, s(4)+p(2)+d(1) per atom, 4-24 MOs, "
+                               f"sparse 2-RDMs (1-10 %), 256 q", "chunks": nchunks,
+                   "max_molecules_per_chunk": args.batch_chunk, "chunk_budget_gb": args.batch_gb},
+        "plain_molecules_per_s": n / t_plain, "batched_over_plain": t_plain / t_batch,
+        "quartet_q_per_s_batched": qq / t_batch, "quartet_q_per_s_plain": qq / t_plain,
+        "setup_s_per_molecule": t_setup / n, "input_generation_s": t_gen,
+        "kernel_launches_per_chunk": launches[:4], "check_vs_plain_max_rel": err,
+        "path": "integrator only, from plans already built; host I(q) out (MoleculeBatch.execute vs "
+                "ScatteringPlan.execute per molecule)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,15 +398,21 @@ def main():
     ap.add_argument("--impl", default="thistle", choices=["thistle", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="ab6", choices=["ab6", "ab6_4atom", "fit6"],
+    ap.add_argument("--workload", default="ab6", choices=["ab6", "ab6_4atom", "fit6", "batch4"],
                     help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis; "
-                         "fit6: batched forward + adjoint over geometries (configuration 5)")
+                         "fit6: batched forward + adjoint over geometries (configuration 5); "
+                         "batch4: uneven molecule batches (configuration 4)")
     ap.add_argument("--fit-geometries", type=int, default=512)
     ap.add_argument("--fit-plain", type=int, default=32, help="geometries timed on the plain path")
     ap.add_argument("--fit-gmax", type=int, default=64)
+    ap.add_argument("--batch-molecules", type=int, default=1024)
+    ap.add_argument("--batch-chunk", type=int, default=128, help="molecules per batch at most")
+    ap.add_argument("--batch-gb", type=float, default=60.0, help="device memory held per chunk of plans")
     args = ap.parse_args()
     if args.workload == "fit6" and args.impl == "thistle":
         return run_fit(args)
+    if args.workload == "batch4" and args.impl == "thistle":
+        return run_batch4(args)
     global WORKLOAD
     WORKLOAD = args.workload
     args.warmup = max(args.warmup, 3) if args.impl == "thistle" else args.warmup

@@ -144,6 +144,25 @@ int thistle_plan_vjp_batch_device(thistle_plan *plan, const double *v_dev, doubl
 int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);
 int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom_best, int32_t *qtile_best,
                                 double *geoms_per_s);
+/*
+ * Molecule batches (no reference counterpart).  Several plans -- any bases,
+ * one geometry each, the same calculation type, nq <= 1024 -- executed
+ * together: pair tables, stage 1 per class, stage 2 per class and the
+ * reductions each run as one launch over every plan, its blocks spread over
+ * the plans in proportion to their work.  batch_create runs every plan once
+ * (records and stage-2 visiting order) and builds the launch tables; the
+ * plans must outlive the batch and keep their stream.  execute writes the
+ * plans' I(q) one after the other (sum of their nq doubles).  use_graph
+ * captures the launches once in a CUDA graph and replays it.  info: [0]
+ * plans, [1] total q points, [2] kernels launched by the last execution.
+ */
+typedef struct thistle_batch thistle_batch;
+int thistle_batch_create(thistle_batch **batch, thistle_plan *const *plans, int32_t nplans);
+int thistle_batch_use_graph(thistle_batch *batch, int32_t enable);
+int thistle_batch_execute(thistle_batch *batch, double *result_host);
+int thistle_batch_execute_device(thistle_batch *batch, double *result_dev);
+int thistle_batch_info(const thistle_batch *batch, int64_t *info);
+int thistle_batch_destroy(thistle_batch *batch);
 /* The 3131 aligned q vectors of the reference (QCOORD3,
  * src/main_calculation.f90:864-929) for beam wavevector k0, written as a
  * (3, 3131) column-major array.  Host-only. */

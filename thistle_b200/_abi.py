@@ -31,7 +31,8 @@ EXPORTS = sorted([
     "thistle_qcoord3", "thistle_plan_vjp", "thistle_plan_vjp_device", "thistle_plan_set_batch",
     "thistle_plan_set_centres_batch", "thistle_plan_execute_batch", "thistle_plan_execute_batch_device",
     "thistle_plan_vjp_batch", "thistle_plan_vjp_batch_device", "thistle_plan_use_graph",
-    "thistle_plan_autotune_batch",
+    "thistle_plan_autotune_batch", "thistle_batch_create", "thistle_batch_use_graph", "thistle_batch_execute",
+    "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy",
 ])
 
 
@@ -105,7 +106,11 @@ def lib():
                        ("thistle_plan_execute_batch", [VP, D]), ("thistle_plan_execute_batch_device", [VP, VP]),
                        ("thistle_plan_vjp_batch", [VP, D, D]), ("thistle_plan_vjp_batch_device", [VP, VP, VP]),
                        ("thistle_plan_use_graph", [VP, C.c_int32]),
-                       ("thistle_plan_autotune_batch", [VP, C.c_int32, I32, I32, D])):
+                       ("thistle_plan_autotune_batch", [VP, C.c_int32, I32, I32, D]),
+                       ("thistle_batch_create", [C.POINTER(VP), C.POINTER(VP), C.c_int32]),
+                       ("thistle_batch_use_graph", [VP, C.c_int32]), ("thistle_batch_execute", [VP, D]),
+                       ("thistle_batch_execute_device", [VP, VP]), ("thistle_batch_info", [VP, I64]),
+                       ("thistle_batch_destroy", [VP])):
         getattr(L, name).restype = C.c_int
         getattr(L, name).argtypes = args
     L.thistle_qcoord3.restype = C.c_int

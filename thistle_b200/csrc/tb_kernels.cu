@@ -29,17 +29,12 @@ int64_t esoa_doubles(int ng, int maxa) {
 // transposed E table: element t of (axis, la, lb) at
 // esoa[((axis (maxa+1) + la) (maxa+1) + lb) E_T + t][pair], zero for
 // t > la + lb, and a second copy with |E| < 1e-30 set to zero (the MD skips).
-__global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gstart,
-                                   const int *__restrict__ flmn, const double *__restrict__ ga,
-                                   const double *__restrict__ xyz, double *__restrict__ tab,
-                                   double *__restrict__ esoa, int64_t gs_xyz, int64_t gs_tab, int64_t gs_esoa) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pair_table_one(int p, int ng, int maxa, const int *__restrict__ gstart,
+                                               const int *__restrict__ flmn, const double *__restrict__ ga,
+                                               const double *__restrict__ xyz, double *__restrict__ tab,
+                                               double *__restrict__ esoa) {
   const int64_t npair = npairs(ng);
   if (p >= npair) return;
-  // geometry blockIdx.y of a batch
-  xyz += blockIdx.y * gs_xyz;
-  tab += blockIdx.y * gs_tab;
-  esoa += blockIdx.y * gs_esoa;
   const int64_t skipoff = (int64_t)3 * (maxa + 1) * (maxa + 1) * E_T * npair;
   int i = 0, rem = p;
   while (rem >= ng - i) { rem -= ng - i; ++i; }
@@ -77,6 +72,41 @@ __global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gst
   t[5] = 0.25 / gaP;
   t[6] = 0.0;
   t[7] = 0.0;
+}
+
+__global__ void pair_tables_kernel(int ng, int maxa, const int *__restrict__ gstart,
+                                   const int *__restrict__ flmn, const double *__restrict__ ga,
+                                   const double *__restrict__ xyz, double *__restrict__ tab,
+                                   double *__restrict__ esoa, int64_t gs_xyz, int64_t gs_tab, int64_t gs_esoa) {
+  // geometry blockIdx.y of a batch
+  pair_table_one(blockIdx.x * blockDim.x + threadIdx.x, ng, maxa, gstart, flmn, ga, xyz + blockIdx.y * gs_xyz,
+                 tab + blockIdx.y * gs_tab, esoa + blockIdx.y * gs_esoa);
+}
+
+__device__ __forceinline__ int desc_item(const int64_t *__restrict__ pre, int n, int64_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void pair_tables_batch_kernel(const PairDesc *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = desc_item(pre, n, blockIdx.x);
+  const PairDesc D = d[it];
+  pair_table_one((int)(blockIdx.x - pre[it]) * blockDim.x + threadIdx.x, D.ng, D.maxa, D.gstart, D.flmn, D.ga, D.xyz,
+                 D.tab, D.esoa);
+}
+
+__global__ void reduce_desc_kernel(const ReduceDesc *__restrict__ d) {
+  const ReduceDesc D = d[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.nq) return;
+  double t = 0.0;
+  for (int b = 0; b < D.rows; ++b) t += D.partial[(size_t)b * D.nq + i];
+  D.out[i] = t;
 }
 
 // ---------------------------------------------------------------------------
@@ -392,6 +422,26 @@ cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args 
   if (kind == KIND_ELASTIC) return launch_stage1_xk_k<KIND_ELASTIC>(L, LK, XB, a, ngeom, st);
   if (kind == KIND_ALIGNED) return launch_stage1_xk_k<KIND_ALIGNED>(L, LK, XB, a, ngeom, st);
   return launch_stage1_xk_k<KIND_J2>(L, LK, XB, a, ngeom, st);
+}
+
+cudaError_t launch_pair_tables_batch(const PairDesc *d, const int64_t *pre, int n, int64_t blocks, cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+  pair_tables_batch_kernel<<<(unsigned)blocks, 128, 0, st>>>(d, pre, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_desc(const ReduceDesc *d, int n, int nqmax, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  reduce_desc_kernel<<<dim3((nqmax + 127) / 128, n), 128, 0, st>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
+                                int64_t blocks, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_batch_k<KIND_TOTAL>(L, LK, XB, d, pre, n, blocks, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_batch_k<KIND_ELASTIC>(L, LK, XB, d, pre, n, blocks, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_batch_k<KIND_ALIGNED>(L, LK, XB, d, pre, n, blocks, st);
+  return launch_stage1_batch_k<KIND_J2>(L, LK, XB, d, pre, n, blocks, st);
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st) {

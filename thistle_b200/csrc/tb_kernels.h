@@ -80,6 +80,9 @@ constexpr int STAGE2_QTILE = 1024;
 int stage2_quartets_per_warp(int LB);
 int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
 cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st);
+// molecule batches: n items (device descriptors d), item i's blocks pre[i] .. pre[i+1]-1
+cudaError_t launch_stage2_class_batch(int LB, bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n,
+                                      int64_t blocks, int nqmax, cudaStream_t st);
 
 // Aligned intensity of one LLmax class on q vectors (tb_aligned.cu).
 struct AlignedArgs {
@@ -145,6 +148,12 @@ cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int 
 // LLmax classes whose quartets go through the contracted-side kernel, by
 // sub-range of equal (LK = min(L_bra, L_ket), XB = L_bra < L_ket)
 bool stage1_xk(int L);
+template <int K>
+cudaError_t launch_stage1_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
+                                  int64_t blocks, cudaStream_t st);
+cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
+                                int64_t blocks, cudaStream_t st);
+int64_t stage1_item_blocks(int L, bool xk, int64_t n);
 cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
@@ -157,6 +166,21 @@ cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int 
 cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st);
 cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
+// molecule batches: pair tables of every item (blocks pre[i] .. pre[i+1]-1 of 128 pairs)
+struct PairDesc {
+  int ng, maxa;
+  const int *gstart, *flmn;
+  const double *ga, *xyz;
+  double *tab, *esoa;
+};
+cudaError_t launch_pair_tables_batch(const PairDesc *d, const int64_t *pre, int n, int64_t blocks, cudaStream_t st);
+// molecule batches: item i sums rows[i] partial rows of nq[i] points into out[i]
+struct ReduceDesc {
+  const double *partial;
+  int rows, nq;
+  double *out;
+};
+cudaError_t launch_reduce_desc(const ReduceDesc *d, int n, int nqmax, cudaStream_t st);
 cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st);
 int stage2_blocks_per_sm(int nqp, int nwarps);
 cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,

@@ -170,7 +170,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
 #pragma unroll
     for (int k = 0; k < NS; ++k) cs[k] = group_sum<S>(cs[k], gmask);
     if (!leader) return;
-    atomicAdd(A.p0count, 1ull);
+    if (A.p0count) atomicAdd(A.p0count, 1ull);
     const double fj2 = sqrt(5.0 / TB_PI);
     r[0] = 0.0;
     r[1] = Q.tb[5] + Q.tk[5];
@@ -268,6 +268,18 @@ __device__ __forceinline__ const double *esoa_slot(const Stage1Args &A, bool ski
   return A.esoa + (skipped ? A.eskip : 0) + (int64_t)slot * E_T * A.npair + pair;
 }
 
+// Molecule batches: launch blocks are spread over items (one plan's quartet
+// range each); pre[i] is item i's first block, pre[n] the total.
+__device__ __forceinline__ int batch_item(const int64_t *__restrict__ pre, int n, int64_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Geometry blockIdx.y of a batch: its pair tables, E tables, records and
 // P = Q counter; the stage-2 order keys are written for geometry 0 only.
 __device__ __forceinline__ void stage1_geometry(Stage1Args &A) {
@@ -281,8 +293,7 @@ __device__ __forceinline__ void stage1_geometry(Stage1Args &A) {
 }
 
 template <int L, int KIND>
-__global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kernel(Stage1Args A) {
-  stage1_geometry(A);
+__device__ __forceinline__ void stage1_reg_body(Stage1Args &A, int64_t vb) {
   constexpr int S = stage1_reg_split(L);
   constexpr int PP = stage1_reg_parts(L);
   constexpr int G = S * PP;              // threads per quartet
@@ -294,7 +305,7 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
   const int sub = gsub % S, part = gsub / S, grp = threadIdx.x / S;
   const int lane = threadIdx.x & 31;
   const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane - gsub));
-  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int64_t qi = A.qbegin + (vb * blockDim.x + threadIdx.x) / G;
   // whole groups leave together (S divides 32)
   if (qi >= A.qend) return;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
@@ -444,12 +455,25 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kerne
   stage1_finish<L, KIND, G>(A, Q, col, NG, qi, gsub, gmask);
 }
 
+template <int L, int KIND>
+__global__ void __launch_bounds__(128, stage1_reg_minblocks(L)) stage1_reg_kernel(Stage1Args A) {
+  stage1_geometry(A);
+  stage1_reg_body<L, KIND>(A, blockIdx.x);
+}
+
+template <int L, int KIND>
+__global__ void __launch_bounds__(128, stage1_reg_minblocks(L))
+    stage1_reg_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  Stage1Args A = d[it];
+  stage1_reg_body<L, KIND>(A, blockIdx.x - pre[it]);
+}
+
 // ---------------------------------------------------------------------------
 // shared-memory kernel (LLmax 9..16)
 // ---------------------------------------------------------------------------
 template <int L, int KIND>
-__global__ void stage1_smem_kernel(Stage1Args A) {
-  stage1_geometry(A);
+__device__ __forceinline__ void stage1_smem_body(Stage1Args &A, int64_t vb) {
   // Each thread owns a column of the block's shared array; element k of its
   // (partial) Hermite density sits at sD[k * blockDim.x + threadIdx.x].
   constexpr int S = stage1_smem_split(L);
@@ -458,7 +482,7 @@ __global__ void stage1_smem_kernel(Stage1Args A) {
   const int sub = threadIdx.x % S;
   const int lane = threadIdx.x & 31;
   const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane - sub));
-  const int64_t qi = A.qbegin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S;
+  const int64_t qi = A.qbegin + (vb * blockDim.x + threadIdx.x) / S;
   if (qi >= A.qend) return;
   double *D = sD + threadIdx.x;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
@@ -563,6 +587,19 @@ __global__ void stage1_smem_kernel(Stage1Args A) {
   stage1_finish<L, KIND, S>(A, Q, sD + base, nthr, qi, sub, gmask);
 }
 
+template <int L, int KIND>
+__global__ void stage1_smem_kernel(Stage1Args A) {
+  stage1_geometry(A);
+  stage1_smem_body<L, KIND>(A, blockIdx.x);
+}
+
+template <int L, int KIND>
+__global__ void stage1_smem_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  Stage1Args A = d[it];
+  stage1_smem_body<L, KIND>(A, blockIdx.x - pre[it]);
+}
+
 // ---------------------------------------------------------------------------
 // contracted-side kernel (LLmax 4..6), thread per quartet
 // ---------------------------------------------------------------------------
@@ -576,13 +613,12 @@ __global__ void stage1_smem_kernel(Stage1Args A) {
 // and the outer product of stage1_reg_kernel.
 
 template <int L, int KIND, int LK, bool XB>
-__global__ void __launch_bounds__(128, 2) stage1_xk_kernel(Stage1Args A) {
-  stage1_geometry(A);
+__device__ __forceinline__ void stage1_xk_body(Stage1Args &A, int64_t vb) {
   constexpr int LO = L - LK;  // order of the convolved (outer) side
   constexpr int NT = ntuv(L), NX = ntuv(LK);
   constexpr int NG = 128;
   extern __shared__ double sD[];
-  const int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t qi = A.qbegin + vb * blockDim.x + threadIdx.x;
   if (qi >= A.qend) return;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
   const int pb = pair_index(Q.gi, Q.gj, A.ng), pk = pair_index(Q.gk, Q.gr, A.ng);
@@ -694,6 +730,20 @@ __global__ void __launch_bounds__(128, 2) stage1_xk_kernel(Stage1Args A) {
   stage1_finish<L, KIND, 1>(A, Q, col, NG, qi, 0, 0xffffffffu);
 }
 
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128, 2) stage1_xk_kernel(Stage1Args A) {
+  stage1_geometry(A);
+  stage1_xk_body<L, KIND, LK, XB>(A, blockIdx.x);
+}
+
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128, 2)
+    stage1_xk_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  Stage1Args A = d[it];
+  stage1_xk_body<L, KIND, LK, XB>(A, blockIdx.x - pre[it]);
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -754,6 +804,63 @@ cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int 
   TB_XK(6, 0) TB_XK(6, 1) TB_XK(6, 2) TB_XK(6, 3)
 #undef TB_XK
   return cudaErrorInvalidValue;
+}
+
+// Molecule batches: one launch over every item (one plan's quartet range of
+// class L, and for the contracted-side kernel of one (LK, XB)); item i owns
+// blocks pre[i] .. pre[i+1]-1 (stage1_item_blocks of its quartets).
+template <int L, int K>
+static cudaError_t launch_stage1_batch_l(int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
+                                         int64_t blocks, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  if constexpr (L >= 3 && L <= 6) {
+    if (LK >= 0) {
+#define TB_XB(lk)                                                                                         \
+  if (LK == lk && lk <= L / 2) {                                                                        \
+    const size_t smem = (size_t)ntuv(L) * sizeof(double) * 128;                                         \
+    if (XB) {                                                                                           \
+      e = cudaFuncSetAttribute(stage1_xk_batch<L, K, lk, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               (int)smem);                                                              \
+      if (e == cudaSuccess) stage1_xk_batch<L, K, lk, true><<<(unsigned)blocks, 128, smem, st>>>(d, pre, n); \
+    } else {                                                                                            \
+      e = cudaFuncSetAttribute(stage1_xk_batch<L, K, lk, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               (int)smem);                                                              \
+      if (e == cudaSuccess) stage1_xk_batch<L, K, lk, false><<<(unsigned)blocks, 128, smem, st>>>(d, pre, n); \
+    }                                                                                                   \
+    return e != cudaSuccess ? e : cudaGetLastError();                                                   \
+  }
+      TB_XB(0) TB_XB(1) TB_XB(2) TB_XB(3)
+#undef TB_XB
+      return cudaErrorInvalidValue;
+    }
+  }
+  if constexpr (L <= STAGE1_REG_MAXL) {
+    constexpr int S = stage1_reg_split(L);
+    const size_t smem = (size_t)ntuv(L) * sizeof(double) * (128 / S);
+    e = cudaFuncSetAttribute(stage1_reg_batch<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    stage1_reg_batch<L, K><<<(unsigned)blocks, 128, smem, st>>>(d, pre, n);
+  } else {
+    const int thr = stage1_smem_threads(L);
+    const size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
+    e = cudaFuncSetAttribute(stage1_smem_batch<L, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    stage1_smem_batch<L, K><<<(unsigned)blocks, thr, smem, st>>>(d, pre, n);
+  }
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_stage1_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
+                                  int64_t blocks, cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+  switch (L) {
+#define TB_S1(l) case l: return launch_stage1_batch_l<l, K>(LK, XB, d, pre, n, blocks, st);
+    TB_S1(0) TB_S1(1) TB_S1(2) TB_S1(3) TB_S1(4) TB_S1(5) TB_S1(6) TB_S1(7) TB_S1(8)
+    TB_S1(9) TB_S1(10) TB_S1(11) TB_S1(12) TB_S1(13) TB_S1(14) TB_S1(15) TB_S1(16)
+#undef TB_S1
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <int K>

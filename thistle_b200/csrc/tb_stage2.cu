@@ -134,11 +134,8 @@ constexpr int QB = TB_S2_QB;
 TB_HD constexpr int padded_nq(int nq) { return (nq + QB - 1) / QB * QB; }
 
 template <int LB, int K, bool J2>
-__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
+__device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb, int64_t vgrid) {
   extern __shared__ double sm[];
-  // geometry blockIdx.y of a batch
-  A.rec += blockIdx.y * A.gs_rec;
-  A.partial += blockIdx.y * A.gs_partial;
   const int nq = A.nq, nqb = padded_nq(nq);
   double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q), padded with the last point
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -165,7 +162,7 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
   const int64_t nitems = nb * nch;
   const double dq = A.dq;
   const int jsel = (lane / (32 / QB)) & (QB - 1);
-  for (int64_t it = (int64_t)blockIdx.x * NW + warp; it < nitems; it += (int64_t)gridDim.x * NW) {
+  for (int64_t it = vb * NW + warp; it < nitems; it += vgrid * NW) {
     const int64_t bt = it / nch;
     const int m0 = (int)(it - bt * nch) * chunk, m1 = min(nqb, m0 + chunk);
     double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K];
@@ -372,8 +369,35 @@ __global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_ke
     double t = 0.0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) t += sm[2 * nqb + w * nqb + i];
-    A.partial[(size_t)blockIdx.x * A.pstride + i] += t;
+    A.partial[(size_t)vb * A.pstride + i] += t;
   }
+}
+
+template <int LB, int K, bool J2>
+__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
+  // geometry blockIdx.y of a batch
+  A.rec += blockIdx.y * A.gs_rec;
+  A.partial += blockIdx.y * A.gs_partial;
+  stage2_class_body<LB, K, J2>(A, blockIdx.x, gridDim.x);
+}
+
+// Molecule batches: item i's blocks are pre[i] .. pre[i+1]-1 (its vgrid).
+__device__ __forceinline__ int s2_batch_item(const int64_t *__restrict__ pre, int n, int64_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int LB, int K, bool J2>
+__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB)
+    stage2_class_batch(const Stage2ClassArgs *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = s2_batch_item(pre, n, blockIdx.x);
+  Stage2ClassArgs A = d[it];
+  stage2_class_body<LB, K, J2>(A, blockIdx.x - pre[it], pre[it + 1] - pre[it]);
 }
 
 size_t class_smem(int nq) { return sizeof(double) * (size_t)padded_nq(nq) * (2 + STAGE2_WARPS); }
@@ -403,7 +427,40 @@ int blocks_per_sm_l(int nq) {
   return nb > 0 ? nb : 1;
 }
 
+template <int LB, bool J2>
+cudaError_t launch_class_batch_l(const Stage2ClassArgs *d, const int64_t *pre, int n, int64_t blocks, int nqmax,
+                                 cudaStream_t st) {
+  constexpr int K = stage2_k(LB);
+  size_t smem = class_smem(nqmax);
+  cudaError_t e =
+      cudaFuncSetAttribute(stage2_class_batch<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage2_class_batch<LB, K, J2><<<(unsigned)blocks, STAGE2_WARPS * 32, smem, st>>>(d, pre, n);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_stage2_class_batch(int LB, bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n,
+                                      int64_t blocks, int nqmax, cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+  if (j2) {
+    switch (LB) {
+#define TB_L(n_) case n_: return launch_class_batch_l<n_, true>(d, pre, n, blocks, nqmax, st);
+      TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8) TB_L(9) TB_L(10)
+      TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16) TB_L(17) TB_L(18)
+#undef TB_L
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (LB) {
+#define TB_L(n_) case n_: return launch_class_batch_l<n_, false>(d, pre, n, blocks, nqmax, st);
+    TB_L(0) TB_L(1) TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8)
+    TB_L(9) TB_L(10) TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16)
+#undef TB_L
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 int stage2_quartets_per_warp(int LB) {
   switch (LB) {

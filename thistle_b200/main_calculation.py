@@ -281,6 +281,57 @@ class ScatteringPlan:
             pass
 
 
+class MoleculeBatch:
+    """Several plans (different molecules and bases, one geometry each, the
+    same calculation type, at most 1024 q points each) executed together:
+    each stage and class runs as one launch over all of them.  The plans must
+    stay open while the batch is used; ``execute`` returns one I(q) array per
+    plan, for each plan's current centres."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        self._b = C.c_void_p()
+        arr = (C.c_void_p * len(self.plans))(*[p._p.value for p in self.plans])
+        check(_abi.lib().thistle_batch_create(C.byref(self._b), arr, len(self.plans)))
+        self._split = np.cumsum([p.nq for p in self.plans])[:-1]
+        self._nq = int(sum(p.nq for p in self.plans))
+
+    def use_graph(self, enable: bool = True):
+        check(_abi.lib().thistle_batch_use_graph(self._b, int(bool(enable))))
+
+    def execute(self):
+        out = np.zeros(self._nq)
+        check(_abi.lib().thistle_batch_execute(self._b, dptr(out)))
+        return np.split(out, self._split)
+
+    def execute_device(self, ptr: int):
+        """All plans' I(q), one after the other, to the device address ``ptr``
+        (stream-ordered on the first plan's stream)."""
+        check(_abi.lib().thistle_batch_execute_device(self._b, C.c_void_p(ptr)))
+
+    def info(self):
+        a = np.zeros(3, dtype=np.int64)
+        check(_abi.lib().thistle_batch_info(self._b, a.ctypes.data_as(_abi.I64)))
+        return dict(plans=int(a[0]), nq=int(a[1]), launches=int(a[2]))
+
+    def close(self):
+        if self._b:
+            _abi.lib().thistle_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def atom_gradient(prob, group_grad):
     """Sum per-group centre gradients (ng, 3) onto the atoms carrying them."""
     g0 = np.array([np.argmax(prob.group == k + 1) for k in range(prob.ng)])
