@@ -95,6 +95,11 @@ struct Seed {
   double sn, cs, g, r;
 };
 
+template <bool B>
+struct BoolTag {
+  static constexpr bool value = B;
+};
+
 __device__ __noinline__ Seed seed_point(double q, double H, double s, double dq) {
   Seed z;
   sincos(q * H, &z.sn, &z.cs);
@@ -274,50 +279,35 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
       }
       mse = (int)__reduce_max_sync(0xffffffffu, (unsigned)lane_end);
     }
-    int next_seed = m0;
-    for (int mb = m0; mb < m1; mb += QB) {
-      double Fv[QB];
+    // One point of the tile for the warp's 32 K quartets: all K as
+    // straight-line code; CHECKED points (before mse) then patch the rare
+    // lanes below the crossover or on the P = Q branch.  Polynomial form: the
+    // values are F q (J2: F q^3), the common 1/q (1/q^3) is applied once.
+    auto point = [&](const int m, auto checked) -> double {
+      constexpr bool CHECKED = decltype(checked)::value;
+      const double2 qq = qs[m];
+      const double q = qq.x, iq = qq.y;
+      double F[K];
 #pragma unroll
-      for (int j = 0; j < QB; ++j) {
-        const int m = mb + j;
-        const double2 qq = qs[m];
-        const double q = qq.x, iq = qq.y;
-        if (m == next_seed) {
+      for (int k = 0; k < K; ++k) {
+        if constexpr (POLY) {
+          const double y = q * q;
+          double ae = pa[k][NA - 1], bo = pb[k][NB - 1];
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const Seed z = seed_point(q, H[k], hm[k][-3], dq);
-            sn[k] = z.sn;
-            cs[k] = z.cs;
-            g[k] = z.g;
-            r[k] = z.r;
-          }
-          next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + RESEED);
+          for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
+#pragma unroll
+          for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
+          F[k] = fma(ae, sn[k], bo * (cs[k] * q));
+        } else {
+          F[k] = bessel_up<LB>(hh[k], q * H[k], sn[k], cs[k], iq * invH[k]);
+          if (J2) F[k] *= iq * iq;
         }
-        // all K quartets as straight-line code, then the rare lanes below the
-        // crossover or on the P = Q branch patched in.  Polynomial form: the
-        // values are F q (J2: F q^3), the common 1/q (1/q^3) is applied once.
+      }
+      if constexpr (CHECKED) {
         const long long qb = __double_as_longlong(q);
-        double F[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          if constexpr (POLY) {
-            const double y = q * q;
-            double ae = pa[k][NA - 1], bo = pb[k][NB - 1];
-#pragma unroll
-            for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
-#pragma unroll
-            for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
-            F[k] = fma(ae, sn[k], bo * (cs[k] * q));
-          } else {
-            F[k] = bessel_up<LB>(hh[k], q * H[k], sn[k], cs[k], iq * invH[k]);
-            if (J2) F[k] *= iq * iq;
-          }
-        }
         bool special = false;
-        if (m < mse) {  // warp-uniform
 #pragma unroll
-          for (int k = 0; k < K; ++k) special |= (qb < qcb[k]) | (p0n[k] >= 0);
-        }
+        for (int k = 0; k < K; ++k) special |= (qb < qcb[k]) | (p0n[k] >= 0);
         if (special) {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
@@ -332,18 +322,50 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
             }
           }
         }
-        double Fs = 0.0;
+      }
+      double Fs = 0.0;
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          Fs = fma(F[k], g[k], Fs);
-          const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
-          cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
-          sn[k] = s2;
-          g[k] *= r[k];
-          r[k] *= kk[k];
+      for (int k = 0; k < K; ++k) {
+        Fs = fma(F[k], g[k], Fs);
+        const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
+        cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
+        sn[k] = s2;
+        g[k] *= r[k];
+        r[k] *= kk[k];
+      }
+      if constexpr (POLY) Fs *= J2 ? iq * iq * iq : iq;
+      return Fs;
+    };
+    auto seed = [&](const int m) {
+      const double q = qs[m].x;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const Seed z = seed_point(q, H[k], hm[k][-3], dq);
+        sn[k] = z.sn;
+        cs[k] = z.cs;
+        g[k] = z.g;
+        r[k] = z.r;
+      }
+    };
+    // Seeds (direct sincos / exp) at the chunk start and every RESEED points
+    // after it, all on block boundaries; on a non-uniform tile at every
+    // point, and when q[0] lies off the grid (the drivers' 1e-10) again at
+    // point 1.  Blocks without a patch or an in-block seed take the lean path.
+    const bool every = !A.uniform;
+    const bool off0 = m0 == 0 && !A.first_on_grid;
+    for (int mb = m0; mb < m1; mb += QB) {
+      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb);
+      double Fv[QB];
+      if (mb < mse || every || (off0 && mb == 0)) {
+#pragma unroll
+        for (int j = 0; j < QB; ++j) {
+          const int m = mb + j;
+          if (every ? (j > 0 || ((mb - m0) & (RESEED - 1)) != 0) : (off0 && m == 1)) seed(m);
+          Fv[j] = point(m, BoolTag<true>());
         }
-        if constexpr (POLY) Fs *= J2 ? iq * iq * iq : iq;
-        Fv[j] = Fs;
+      } else {
+#pragma unroll
+        for (int j = 0; j < QB; ++j) Fv[j] = point(mb + j, BoolTag<false>());
       }
       // reduce-scatter: after the halving rounds over lane bits 4, 3, 2 the
       // lane holds point jsel summed over 8 lanes; two butterfly rounds finish
