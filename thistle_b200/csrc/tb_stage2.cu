@@ -92,21 +92,29 @@ __device__ __noinline__ double p0_poly(const double *__restrict__ c, int n, doub
 }
 
 struct Seed {
-  double sn, cs, g, r;
+  double S, C, wr, wi, g, r;
 };
+
+// Direct values at point q: z = g e^{i q H}, the step w = r e^{i dq H}, g
+// and r (g = exp(-q^2 s), r = exp(-(2 q dq + dq^2) s)).
+__device__ __noinline__ Seed seed_point(double q, double H, double s, double dq) {
+  Seed z;
+  double sn, cs, sd, cd;
+  sincos(q * H, &sn, &cs);
+  sincos(dq * H, &sd, &cd);
+  z.g = exp(-(q * q) * s);
+  z.r = exp(-(2.0 * q * dq + dq * dq) * s);
+  z.S = z.g * sn;
+  z.C = z.g * cs;
+  z.wr = z.r * cd;
+  z.wi = z.r * sd;
+  return z;
+}
 
 template <bool B>
 struct BoolTag {
   static constexpr bool value = B;
 };
-
-__device__ __noinline__ Seed seed_point(double q, double H, double s, double dq) {
-  Seed z;
-  sincos(q * H, &z.sn, &z.cs);
-  z.g = exp(-(q * q) * s);
-  z.r = exp(-(2.0 * q * dq + dq * dq) * s);
-  return z;
-}
 
 // quartets per lane, and the resident blocks per SM the register allocation aims at
 #ifndef TB_S2_K_LO
@@ -170,7 +178,10 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
   for (int64_t it = vb * NW + warp; it < nitems; it += vgrid * NW) {
     const int64_t bt = it / nch;
     const int m0 = (int)(it - bt * nch) * chunk, m1 = min(nqb, m0 + chunk);
-    double H[K], invH[K], sd[K], cd[K], kk[K], sn[K], cs[K], g[K], r[K];
+    // per quartet: z = exp(-q^2 s) e^{i q H} = C + i S advances by z <- z w,
+    // w = r e^{i dq H}, w <- w kk (r, kk the Gaussian's ratios); the Gaussian
+    // g itself (g <- g rg, rg <- rg kk) only through the patched prefix
+    double H[K], invH[K], kk[K], S[K], C[K], wr[K], wi[K], g[K], rg[K];
     double hh[POLY ? 1 : K][POLY ? 1 : LB + 1];  // recurrence form: hhat_b
     double pa[POLY ? K : 1][NA], pb[POLY ? K : 1][NB];  // polynomial form
     long long qcb[K];  // bits of x_c / H: below it the series branch
@@ -254,10 +265,8 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
 #pragma unroll
         for (int b = 0; b <= LB; ++b) hh[k][b] = p0n[k] < 0 ? hm[k][b] : 0.0;
       }
-      const double s = rec[1];
-      sincos(dq * h, &sd[k], &cd[k]);
-      kk[k] = exp(-2.0 * dq * dq * s);
-      sn[k] = cs[k] = g[k] = r[k] = 0.0;
+      kk[k] = exp(-2.0 * dq * dq * rec[1]);
+      S[k] = C[k] = wr[k] = wi[k] = g[k] = rg[k] = 0.0;
     }
     // last point (exclusive) at which any lane of the warp may need a patch:
     // on an ascending uniform tile the series region of a quartet is a
@@ -279,15 +288,27 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
       }
       mse = (int)__reduce_max_sync(0xffffffffu, (unsigned)lane_end);
     }
-    // One point of the tile for the warp's 32 K quartets: all K as
-    // straight-line code; CHECKED points (before mse) then patch the rare
-    // lanes below the crossover or on the P = Q branch.  Polynomial form: the
-    // values are F q (J2: F q^3), the common 1/q (1/q^3) is applied once.
+    // One point of the tile for the warp's 32 K quartets, all K as
+    // straight-line code.  Polynomial form: sum_k (A_k S_k + q B_k C_k) is
+    // F q summed over the lanes' quartets (J2: F q^3), the common 1/q (1/q^3)
+    // applied once.  CHECKED points (the prefix before mse) first find the
+    // lanes below the crossover or on the P = Q branch and replace their
+    // terms by the series / polynomial value times the Gaussian g.
     auto point = [&](const int m, auto checked) -> double {
       constexpr bool CHECKED = decltype(checked)::value;
       const double2 qq = qs[m];
       const double q = qq.x, iq = qq.y;
-      double F[K];
+      bool sp[K];
+      bool any = false;
+      if constexpr (CHECKED) {
+        const long long qb = __double_as_longlong(q);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          sp[k] = (qb < qcb[k]) | (p0n[k] >= 0);
+          any |= sp[k];
+        }
+      }
+      double FA = 0.0, FB = 0.0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if constexpr (POLY) {
@@ -297,76 +318,68 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
           for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
 #pragma unroll
           for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
-          F[k] = fma(ae, sn[k], bo * (cs[k] * q));
+          if (CHECKED && sp[k]) ae = bo = 0.0;
+          FA = fma(ae, S[k], FA);
+          FB = fma(bo, C[k], FB);
         } else {
-          F[k] = bessel_up<LB>(hh[k], q * H[k], sn[k], cs[k], iq * invH[k]);
-          if (J2) F[k] *= iq * iq;
+          // the recurrence is linear in (sin, cos): fed z it gives F g
+          double f = bessel_up<LB>(hh[k], q * H[k], S[k], C[k], iq * invH[k]);
+          if (J2) f *= iq * iq;
+          if (CHECKED && sp[k]) f = 0.0;
+          FA += f;
         }
       }
+      double X = 0.0;
       if constexpr (CHECKED) {
-        const long long qb = __double_as_longlong(q);
-        bool special = false;
-#pragma unroll
-        for (int k = 0; k < K; ++k) special |= (qb < qcb[k]) | (p0n[k] >= 0);
-        if (special) {
+        if (any) {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
+            if (!sp[k]) continue;
+            double v;
             if (p0n[k] >= 0) {
-              F[k] = p0_poly(hm[k], p0n[k], q * q);
-              if (POLY) F[k] *= J2 ? q * q * q : q;
-            } else if (qb < qcb[k]) {
+              v = p0_poly(hm[k], p0n[k], q * q);
+              if (POLY) v *= J2 ? q * q * q : q;
+            } else {
               const double x = q * H[k];
-              F[k] = bessel_small<LB>(hm[k], x * x);
-              if (POLY) F[k] *= q;            // total: F q; j2: (F / q^2) q^3
-              else if (J2) F[k] *= iq * iq;
+              v = bessel_small<LB>(hm[k], x * x);
+              if (POLY) v *= q;            // total: F q; j2: (F / q^2) q^3
+              else if (J2) v *= iq * iq;
             }
+            X = fma(v, g[k], X);
           }
         }
       }
-      double Fs = 0.0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        Fs = fma(F[k], g[k], Fs);
-        const double s2 = fma(sn[k], cd[k], cs[k] * sd[k]);
-        cs[k] = fma(cs[k], cd[k], -sn[k] * sd[k]);
-        sn[k] = s2;
-        g[k] *= r[k];
-        r[k] *= kk[k];
+        const double s2 = fma(S[k], wr[k], C[k] * wi[k]);
+        C[k] = fma(C[k], wr[k], -S[k] * wi[k]);
+        S[k] = s2;
+        wr[k] *= kk[k];
+        wi[k] *= kk[k];
+        if constexpr (CHECKED) {
+          g[k] *= rg[k];
+          rg[k] *= kk[k];
+        }
       }
-      if constexpr (POLY) Fs *= J2 ? iq * iq * iq : iq;
-      return Fs;
+      if constexpr (POLY) return (fma(q, FB, FA) + X) * (J2 ? iq * iq * iq : iq);
+      else return FA + X;
     };
-    auto seed = [&](const int m) {
+    auto seed = [&](const int m, auto checked) {
       const double q = qs[m].x;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const Seed z = seed_point(q, H[k], hm[k][-3], dq);
-        sn[k] = z.sn;
-        cs[k] = z.cs;
-        g[k] = z.g;
-        r[k] = z.r;
+        S[k] = z.S;
+        C[k] = z.C;
+        wr[k] = z.wr;
+        wi[k] = z.wi;
+        if constexpr (decltype(checked)::value) {
+          g[k] = z.g;
+          rg[k] = z.r;
+        }
       }
     };
-    // Seeds (direct sincos / exp) at the chunk start and every RESEED points
-    // after it, all on block boundaries; on a non-uniform tile at every
-    // point, and when q[0] lies off the grid (the drivers' 1e-10) again at
-    // point 1.  Blocks without a patch or an in-block seed take the lean path.
-    const bool every = !A.uniform;
-    const bool off0 = m0 == 0 && !A.first_on_grid;
-    for (int mb = m0; mb < m1; mb += QB) {
-      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb);
-      double Fv[QB];
-      if (mb < mse || every || (off0 && mb == 0)) {
-#pragma unroll
-        for (int j = 0; j < QB; ++j) {
-          const int m = mb + j;
-          if (every ? (j > 0 || ((mb - m0) & (RESEED - 1)) != 0) : (off0 && m == 1)) seed(m);
-          Fv[j] = point(m, BoolTag<true>());
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < QB; ++j) Fv[j] = point(mb + j, BoolTag<false>());
-      }
+    auto reduce = [&](double *Fv, const int mb) {
       // reduce-scatter: after the halving rounds over lane bits 4, 3, 2 the
       // lane holds point jsel summed over 8 lanes; two butterfly rounds finish
 #pragma unroll
@@ -383,6 +396,32 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
 #pragma unroll
       for (int bit = 32 / QB / 2; bit >= 1; bit >>= 1) t += __shfl_xor_sync(0xffffffffu, t, bit);
       if ((lane & (32 / QB - 1)) == 0) acc[mb + jsel] += t;
+    };
+    // Seeds (direct sincos / exp) at the chunk start and every RESEED points
+    // after it, all on block boundaries; on a non-uniform tile at every
+    // point, and when q[0] lies off the grid (the drivers' 1e-10) again at
+    // point 1.  The checked blocks come first (mse bounds a prefix); the rest
+    // take the lean path, without the Gaussian g.
+    const bool every = !A.uniform;
+    const bool off0 = m0 == 0 && !A.first_on_grid;
+    int mb = m0;
+    for (; mb < m1 && (mb < mse || every || (off0 && mb == 0)); mb += QB) {
+      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb, BoolTag<true>());
+      double Fv[QB];
+#pragma unroll
+      for (int j = 0; j < QB; ++j) {
+        const int m = mb + j;
+        if (every ? (j > 0 || ((mb - m0) & (RESEED - 1)) != 0) : (off0 && m == 1)) seed(m, BoolTag<true>());
+        Fv[j] = point(m, BoolTag<true>());
+      }
+      reduce(Fv, mb);
+    }
+    for (; mb < m1; mb += QB) {
+      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb, BoolTag<false>());
+      double Fv[QB];
+#pragma unroll
+      for (int j = 0; j < QB; ++j) Fv[j] = point(mb + j, BoolTag<false>());
+      reduce(Fv, mb);
     }
   }
   __syncthreads();
