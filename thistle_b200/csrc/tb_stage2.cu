@@ -19,10 +19,10 @@
 //   x <  x_c(LB): power series of u_n = j_n (2n+1)!! / x^n for the top two
 //                 orders, then the stable downward recurrence, accumulated by
 //                 Horner in x^2 / (2b+1).
-// On uniform q grids sin/cos(qH) advance by a rotation through dq H and
-// exp(-q^2 s) by g <- g r, r <- r k (r = exp(-(2 q dq + dq^2) s),
-// k = exp(-2 dq^2 s)), both restarted from direct values every 128 points
-// (and at the start of every q chunk).
+// On uniform q grids z = exp(-q^2 s) e^{i q H} advances by z <- z w,
+// w <- w k (w = r e^{i dq H}, r = exp(-(2 q dq + dq^2) s), k = exp(-2 dq^2 s)),
+// restarted from direct values every 128 points (and at the start of every q
+// chunk).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -42,11 +42,30 @@ constexpr int RESEED = TB_S2_RESEED;
 // with room for the [H, s, kind, order] head in front of it.
 __device__ const double kZeroRecord[4 + LMAXB + 4] = {0};
 
+// Series coefficients c_{n,k} and the downward-recurrence factors in constant
+// memory: FP64 instructions read them as constant-bank operands, where
+// literals would first be moved into registers at every use.
+struct SeriesTable {
+  double c[LMAXB + 2][SER_K + 1];
+  double r1[LMAXB + 2];  // 1 / ((2b + 1) (2b + 3))
+  double r2[LMAXB + 2];  // 1 / (2b + 1)
+};
+constexpr SeriesTable make_series_table() {
+  SeriesTable t{};
+  for (int n = 0; n < LMAXB + 2; ++n) {
+    for (int k = 0; k <= SER_K; ++k) t.c[n][k] = series_coef(n, k);
+    t.r1[n] = 1.0 / ((2.0 * n + 1.0) * (2.0 * n + 3.0));
+    t.r2[n] = 1.0 / (2.0 * n + 1.0);
+  }
+  return t;
+}
+__constant__ SeriesTable kSeries = make_series_table();
+
 template <int N, int NK>
 __device__ __forceinline__ double series_u(double y) {
-  double p = series_coef(N, NK);
+  double p = kSeries.c[N][NK];
 #pragma unroll
-  for (int k = NK - 1; k >= 0; --k) p = fma(p, y, series_coef(N, k));
+  for (int k = NK - 1; k >= 0; --k) p = fma(p, y, kSeries.c[N][k]);
   return p;
 }
 
@@ -59,8 +78,8 @@ __device__ __noinline__ double bessel_small(const double *__restrict__ h, double
   double acc = h[LB] * umid;
 #pragma unroll
   for (int b = LB; b >= 1; --b) {
-    double ulo = umid - (y * (1.0 / ((2.0 * b + 1.0) * (2.0 * b + 3.0)))) * uhi;
-    acc = fma(acc, y * (1.0 / (2.0 * b + 1.0)), h[b - 1] * ulo);
+    double ulo = umid - (y * kSeries.r1[b]) * uhi;
+    acc = fma(acc, y * kSeries.r2[b], h[b - 1] * ulo);
     uhi = umid;
     umid = ulo;
   }
