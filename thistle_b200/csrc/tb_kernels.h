@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 namespace tb {
 
@@ -165,6 +166,11 @@ cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int 
                              cudaStream_t st);
 cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st);
 cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
+// last pass of the density transform: rho[fpair(a, b)][r] = sum_i T3[i][b][r] C(i, a);
+// Ct is scratch of rho_rows_ct_doubles(n, ngto) doubles
+size_t rho_rows_ct_doubles(int n, int ngto);
+cudaError_t launch_rho_rows(const double *T3, const double *C, double *Ct, int n, int ngto, int64_t np, double *rho,
+                            cudaStream_t st);
 cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
 // molecule batches: pair tables of every item (blocks pre[i] .. pre[i+1]-1 of 128 pairs)
 struct PairDesc {

@@ -114,7 +114,7 @@ struct thistle_plan {
   // device-resident density inputs and transform workspaces
   int *d_mat = nullptr;
   double *d_C = nullptr, *d_tot = nullptr, *d_D = nullptr, *d_Ds = nullptr, *d_Y = nullptr;
-  double *d_G = nullptr, *d_T1 = nullptr, *d_T2 = nullptr, *d_V = nullptr, *d_T3 = nullptr;
+  double *d_G = nullptr, *d_T1 = nullptr, *d_T2 = nullptr, *d_V = nullptr, *d_T3 = nullptr, *d_Ct = nullptr;
   // Ghat build: (index, value) per row placement, sorted by index
   int *d_gk0 = nullptr, *d_gk1 = nullptr;
   double *d_gv0 = nullptr, *d_gv1 = nullptr;
@@ -122,11 +122,6 @@ struct thistle_plan {
   size_t gsort_bytes = 0;
   int gbits = 0;
   // grouped GEMM of the transform's last pass (one group per b)
-  bool gg_ok = false;
-  std::vector<cublasOperation_t> gg_ta;
-  std::vector<int> gg_m, gg_n, gg_k, gg_lda, gg_ldb, gg_ldc, gg_size;
-  std::vector<double> gg_one, gg_zero;
-  void **d_gg_ptr = nullptr;
   // quartet enumeration workspaces
   int64_t *d_braoff = nullptr;
   int *d_gL = nullptr;
@@ -362,6 +357,7 @@ static int density_alloc(thistle_plan *P) {
     TB_TRY(dalloc(&P->d_T2, (size_t)(n2 * ngto * ngto), "transform T2"));
     TB_TRY(dalloc(&P->d_V, (size_t)(n2 * np), "transform V"));
     TB_TRY(dalloc(&P->d_T3, (size_t)((int64_t)n * ngto * np), "transform T3"));
+    TB_TRY(dalloc(&P->d_Ct, rho_rows_ct_doubles(n, ngto), "transform C^T"));
     const int64_t m = std::max<int64_t>(8 * (int64_t)P->nmat, 1);
     TB_TRY(dalloc(&P->d_gk0, (size_t)m, "Ghat keys"));
     TB_TRY(dalloc(&P->d_gk1, (size_t)m, "Ghat keys"));
@@ -372,29 +368,6 @@ static int density_alloc(thistle_plan *P) {
     TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->gsort_bytes, P->d_gk0, P->d_gk1, P->d_gv0, P->d_gv1,
                                             (int)m, 0, P->gbits, P->st));
     TB_TRY(dalloc((char **)&P->d_gsort_tmp, P->gsort_bytes, "Ghat sort scratch"));
-    {
-      std::vector<void *> ptr((size_t)3 * ngto);
-      P->gg_ta.assign(ngto, CUBLAS_OP_N);
-      P->gg_m.assign(ngto, (int)np);
-      P->gg_k.assign(ngto, n);
-      P->gg_lda.assign(ngto, (int)((int64_t)ngto * np));
-      P->gg_ldb.assign(ngto, n);
-      P->gg_ldc.assign(ngto, (int)np);
-      P->gg_size.assign(ngto, 1);
-      P->gg_one.assign(ngto, 1.0);
-      P->gg_zero.assign(ngto, 0.0);
-      P->gg_n.resize(ngto);
-      for (int b = 0; b < ngto; ++b) {
-        P->gg_n[b] = b + 1;
-        ptr[b] = P->d_T3 + (size_t)b * np;
-        ptr[ngto + b] = P->d_C;
-        ptr[2 * ngto + b] = P->d_rho + (size_t)fpair(0, b) * np;
-      }
-      TB_TRY(dalloc((char **)&P->d_gg_ptr, ptr.size() * sizeof(void *), "GEMM pointer arrays"));
-      TB_TRYC(cudaMemcpyAsync(P->d_gg_ptr, ptr.data(), ptr.size() * sizeof(void *), cudaMemcpyHostToDevice, P->st));
-      TB_TRYC(cudaStreamSynchronize(P->st));
-      P->gg_ok = true;
-    }
   }
 done:
   return rc;
@@ -429,8 +402,11 @@ static int density_run(thistle_plan *P) {
                         ngto));
     goto done;
   }
-  TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
-  if (P->nmat == 0) goto done;
+  if (P->nmat == 0) {
+    // otherwise the last pass writes every element
+    TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
+    goto done;
+  }
   TB_TRYC(cudaMemsetAsync(P->d_G, 0, sizeof(double) * (size_t)n4, P->st));
   {
     const int64_t m = 8 * (int64_t)P->nmat;
@@ -454,21 +430,9 @@ static int density_run(thistle_plan *P) {
   TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, ngto, n, &one, P->d_V, (int)np,
                                     (long long)n * np, P->d_C, n, 0, &zero, P->d_T3, (int)np, (long long)ngto * np,
                                     n));
-  // rho rows (a<=b, b fixed): (np x b+1) = T3[:,b,:]' C[:,0..b], all b in one
-  // grouped GEMM (one group per b)
-  if (P->gg_ok) {
-    cublasStatus_t st = cublasDgemmGroupedBatched(
-        P->cb, P->gg_ta.data(), P->gg_ta.data(), P->gg_m.data(), P->gg_n.data(), P->gg_k.data(), P->gg_one.data(),
-        (const double *const *)P->d_gg_ptr, P->gg_lda.data(), (const double *const *)(P->d_gg_ptr + ngto),
-        P->gg_ldb.data(), P->gg_zero.data(), (double *const *)(P->d_gg_ptr + 2 * ngto), P->gg_ldc.data(), ngto,
-        P->gg_size.data());
-    if (st != CUBLAS_STATUS_SUCCESS) P->gg_ok = false;  // this cuBLAS lacks it: row GEMMs below
-  }
-  if (!P->gg_ok)
-    for (int b = 0; b < ngto; ++b)
-      TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, b + 1, n, &one, P->d_T3 + (size_t)b * np,
-                          (int)((int64_t)ngto * np), P->d_C, n, &zero, P->d_rho + (size_t)fpair(0, b) * np,
-                          (int)np));
+  // rho rows (a <= b, b fixed) = T3[:,b,:]' C[:,0..b] for every b (rho_rows_kernel)
+  TB_TRYC(launch_rho_rows(P->d_T3, P->d_C, P->d_Ct, n, ngto, np, P->d_rho, P->st));
+  P->launches += 2;  // C^T and the rows
 done:
   return rc;
 }
@@ -525,9 +489,8 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
   dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
-  dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3);
+  dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3); dfree(P->d_Ct);
   dfree(P->d_gk0); dfree(P->d_gk1); dfree(P->d_gv0); dfree(P->d_gv1); dfree(P->d_gsort_tmp);
-  dfree(P->d_gg_ptr);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
   dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
   dfree(P->d_dsoa); dfree(P->d_adj); dfree(P->d_gpart); dfree(P->d_v); dfree(P->d_grad);
