@@ -540,10 +540,18 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
 #ifndef TB_S1_XK_MIN
 #define TB_S1_XK_MIN 4
 #endif
-#ifndef TB_S1_XK_MAX
-#define TB_S1_XK_MAX 6
+// LLmax 4-6 always; 7-8 (a thread per quartet holding 120 / 165 density
+// entries, one block of 128 per SM) only with at least this many quartets
+// per SM, below which the register kernel's 32 threads per quartet fill the
+// GPU better
+#ifndef TB_S1_XK_HIGH_PER_SM
+#define TB_S1_XK_HIGH_PER_SM 512
 #endif
-bool stage1_xk(int L) { return L >= TB_S1_XK_MIN && L <= TB_S1_XK_MAX; }
+bool stage1_xk(int L, int64_t nquart, int nsm) {
+  if (L < TB_S1_XK_MIN) return false;
+  if (L <= 6) return true;
+  return L <= 8 && nquart >= (int64_t)TB_S1_XK_HIGH_PER_SM * nsm;
+}
 
 cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st) {
   if (kind == KIND_TOTAL) return launch_stage1_xk_k<KIND_TOTAL>(L, LK, XB, a, ngeom, st);

@@ -146,9 +146,10 @@ cudaError_t launch_stage1_k(int L, const Stage1Args &a, int ngeom, cudaStream_t 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 template <int K>
 cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
-// LLmax classes whose quartets go through the contracted-side kernel, by
-// sub-range of equal (LK = min(L_bra, L_ket), XB = L_bra < L_ket)
-bool stage1_xk(int L);
+// Whether a class of LLmax L with nquart quartets (summed over the plans of a
+// molecule batch) goes through the contracted-side kernel, by sub-range of
+// equal (LK = min(L_bra, L_ket), XB = L_bra < L_ket)
+bool stage1_xk(int L, int64_t nquart, int nsm);
 template <int K>
 cudaError_t launch_stage1_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
                                   int64_t blocks, cudaStream_t st);

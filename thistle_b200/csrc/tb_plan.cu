@@ -787,7 +787,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.p0count = (unsigned long long *)(P->d_p0count + c);
     a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
-    if (stage1_xk(cL[c])) {
+    if (stage1_xk(cL[c], (ce[c] - cb[c]) * ngeom, P->nsm)) {
       for (const SubRange &u : subs[c]) {
         Stage1Args b = a;
         b.qbegin = u.begin;
@@ -1184,14 +1184,18 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
     TB_TRY(upload_vec(&B->d_pair, pd, B->st, "batch pair descriptors"));
     TB_TRY(upload_vec(&B->d_pair_pre, ppre, B->st, "batch pair prefix"));
     TB_TRY(upload_vec(&B->d_red, rd, B->st, "batch reduce descriptors"));
-    // stage 1: items grouped by (L, LK, XB)
+    // stage 1: items grouped by (L, LK, XB); the kernel choice per L counts
+    // the quartets of every plan
+    int64_t ltot[LMAXQ + 1] = {0};
+    for (thistle_plan *P : B->plans)
+      for (int c = 0; c < P->ncls; ++c) ltot[P->cls_L[c]] += P->cls_end[c] - P->cls_begin[c];
     std::vector<std::pair<std::array<int, 3>, Stage1Args>> items;
     for (thistle_plan *P : B->plans)
       for (int c = 0; c < P->ncls; ++c) {
         Stage1Args a = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c],
                                    P->cls_rs[c]);
         const int L = P->cls_L[c];
-        if (stage1_xk(L)) {
+        if (stage1_xk(L, ltot[L], P->nsm)) {
           for (const SubRange &u : P->cls_sub[c]) {
             Stage1Args b = a;
             b.qbegin = u.begin;

@@ -61,6 +61,10 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
 #ifndef TB_S1_PF_MAXL
 #define TB_S1_PF_MAXL -1
 #endif
+// contracted-side kernel instances for LLmax 7 and 8 as well
+#ifndef TB_S1_XK_HIGH
+#define TB_S1_XK_HIGH 1
+#endif
 #ifndef TB_S1_MB_LO
 #define TB_S1_MB_LO 2
 #endif
@@ -802,6 +806,10 @@ cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int 
   TB_XK(4, 0) TB_XK(4, 1) TB_XK(4, 2)
   TB_XK(5, 0) TB_XK(5, 1) TB_XK(5, 2)
   TB_XK(6, 0) TB_XK(6, 1) TB_XK(6, 2) TB_XK(6, 3)
+#if TB_S1_XK_HIGH
+  TB_XK(7, 0) TB_XK(7, 1) TB_XK(7, 2) TB_XK(7, 3)
+  TB_XK(8, 0) TB_XK(8, 1) TB_XK(8, 2) TB_XK(8, 3) TB_XK(8, 4)
+#endif
 #undef TB_XK
   return cudaErrorInvalidValue;
 }
@@ -813,10 +821,11 @@ template <int L, int K>
 static cudaError_t launch_stage1_batch_l(int LK, int XB, const Stage1Args *d, const int64_t *pre, int n,
                                          int64_t blocks, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
-  if constexpr (L >= 3 && L <= 6) {
+  if constexpr (L >= 3 && L <= (TB_S1_XK_HIGH ? 8 : 6)) {
     if (LK >= 0) {
 #define TB_XB(lk)                                                                                         \
-  if (LK == lk && lk <= L / 2) {                                                                        \
+  if constexpr (lk <= L / 2)                                                                            \
+    if (LK == lk) {                                                                                     \
     const size_t smem = (size_t)ntuv(L) * sizeof(double) * 128;                                         \
     if (XB) {                                                                                           \
       e = cudaFuncSetAttribute(stage1_xk_batch<L, K, lk, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
@@ -829,7 +838,7 @@ static cudaError_t launch_stage1_batch_l(int LK, int XB, const Stage1Args *d, co
     }                                                                                                   \
     return e != cudaSuccess ? e : cudaGetLastError();                                                   \
   }
-      TB_XB(0) TB_XB(1) TB_XB(2) TB_XB(3)
+      TB_XB(0) TB_XB(1) TB_XB(2) TB_XB(3) TB_XB(4)
 #undef TB_XB
       return cudaErrorInvalidValue;
     }
