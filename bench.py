@@ -167,7 +167,13 @@ def run_reference(args, rank, world):
     ncores = os.cpu_count() or 1
     qs = O.enum_quartets(p.ng)
     rng = np.random.default_rng(17)
-    per_step = 24
+    # each step a random sample of about two seconds of work on all host
+    # threads, sized from a first untimed call
+    per_step = 256
+    idx = np.sort(rng.choice(len(qs), size=per_step, replace=False))
+    t0 = time.perf_counter()
+    O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
+    per_step = int(min(len(qs), max(256, per_step * 2.0 / max(time.perf_counter() - t0, 1e-3))))
     times = []
     for s in range(args.warmup + args.steps):
         idx = np.sort(rng.choice(len(qs), size=per_step, replace=False))
@@ -485,7 +491,7 @@ def main():
     achieved = flops / (s2_ms * 1e-3) / 1e12
     traffic = None
     prof = os.path.join(ROOT, "profiles", "stage2_ab6_dram.json")
-    if os.path.exists(prof):
+    if WORKLOAD == "ab6" and os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
         except Exception:
