@@ -560,6 +560,14 @@ cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args 
   return launch_stage1_xk_k<KIND_J2>(L, LK, XB, a, ngeom, st);
 }
 
+cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+                                 cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_xsplit_k<KIND_TOTAL>(L, LK, XB, a, xbuf, nout, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_xsplit_k<KIND_ELASTIC>(L, LK, XB, a, xbuf, nout, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_xsplit_k<KIND_ALIGNED>(L, LK, XB, a, xbuf, nout, st);
+  return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, st);
+}
+
 cudaError_t launch_pair_tables_batch(const PairDesc *d, const int64_t *pre, int n, int64_t blocks, cudaStream_t st) {
   if (n <= 0 || blocks <= 0) return cudaSuccess;
   pair_tables_batch_kernel<<<(unsigned)blocks, 128, 0, st>>>(d, pre, n);

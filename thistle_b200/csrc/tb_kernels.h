@@ -157,6 +157,13 @@ cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Arg
                                 int64_t blocks, cudaStream_t st);
 int64_t stage1_item_blocks(int L, bool xk, int64_t n);
 cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
+// the same sub-range of one geometry as two kernels through xbuf (at least
+// (qend - qbegin) * nout * ntuv(LK) doubles; nout = most outer function pairs)
+template <int K>
+cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+                                   cudaStream_t st);
+cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+                                 cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);

@@ -91,6 +91,7 @@ static void dfree(T *&p) {
 struct SubRange {
   int LK, XB;
   int64_t begin, end;
+  int nout = 0;  // most function pairs of an outer (convolved) side; 0: unknown
 };
 
 struct thistle_plan {
@@ -106,6 +107,8 @@ struct thistle_plan {
   int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
   int cls_rs[MAXCLS];
   std::vector<SubRange> cls_sub[MAXCLS];
+  double *d_xbuf = nullptr;  // contraction output of the split contracted-side stage 1
+  int64_t xbuf_len = 0;
   int64_t rec_total = 0;
   int *d_gstart = nullptr, *d_gcount = nullptr, *d_flmn = nullptr;
   double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr, *d_esoa = nullptr;
@@ -269,6 +272,9 @@ static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt) 
 static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
   int64_t pos = 0, recoff = 0;
   P->ncls = 0;
+  int maxg[5] = {0, 0, 0, 0, 0};  // most functions of a group, per shell L
+  for (int g = 0; g < P->ng; ++g)
+    if (P->gL[g] >= 0 && P->gL[g] <= 4) maxg[P->gL[g]] = std::max(maxg[P->gL[g]], P->gcount[g]);
   for (int LL = 0; LL <= LMAXQ; ++LL) {
     int64_t c = 0;
     for (int t = 0; t < 625; ++t) c += cnt[LL * 625 + t];
@@ -289,13 +295,17 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
     for (int LK = 0; LK <= 8; ++LK)
       for (int XB = 0; XB <= 1; ++XB) {
         int64_t sc = 0;
+        int nout = 0;
         for (int t = 0; t < 625; ++t) {
           const int Li = t / 125, Lj = (t / 25) % 5, Lk = (t / 5) % 5, Lr = t % 5;
           const uint32_t key = quartet_key(Li, Lj, Lk, Lr);
           if ((int)(key / KEY_CLASS_DIV) != LL || (int)((key / 625) % 18) != LK * 2 + XB) continue;
+          if (cnt[LL * 625 + t] == 0) continue;
           sc += cnt[LL * 625 + t];
+          // the outer side is the ket when LK is the bra's
+          nout = std::max(nout, XB ? maxg[Lk] * maxg[Lr] : maxg[Li] * maxg[Lj]);
         }
-        if (sc > 0) P->cls_sub[k].push_back(SubRange{LK, XB, sp, sp + sc});
+        if (sc > 0) P->cls_sub[k].push_back(SubRange{LK, XB, sp, sp + sc, nout});
         sp += sc;
       }
     recoff += c * rs;
@@ -491,6 +501,7 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
   dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3); dfree(P->d_Ct);
   dfree(P->d_gk0); dfree(P->d_gk1); dfree(P->d_gv0); dfree(P->d_gv1); dfree(P->d_gsort_tmp);
+  dfree(P->d_xbuf);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
   dfree(P->d_s2key); dfree(P->d_s2key_sorted); dfree(P->d_iota); dfree(P->d_perm);
   dfree(P->d_dsoa); dfree(P->d_adj); dfree(P->d_gpart); dfree(P->d_v); dfree(P->d_grad);
@@ -679,6 +690,23 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     // aligned: quartet slices of the q-vector kernel (one partial row each)
     P->s2_rows = P->kind == KIND_ALIGNED ? std::max(1, 4 * P->nsm / std::max(1, (nq + 127) / 128)) : P->nsm * maxbps;
     if (P->kind == KIND_ALIGNED) P->s2_rows = std::min(P->s2_rows, 4 * P->nsm);
+    // contraction buffer of the split contracted-side stage 1: the largest
+    // sub-range's quartets x outer pairs x ntuv(LK), up to 2 GB (larger
+    // sub-ranges keep the fused kernel)
+    {
+      int64_t need = 0;
+      for (int c = 0; c < P->ncls; ++c) {
+        if (!stage1_xk(P->cls_L[c], P->cls_end[c] - P->cls_begin[c], P->nsm)) continue;
+        for (const SubRange &u : P->cls_sub[c]) {
+          const int64_t x = (u.end - u.begin) * (int64_t)u.nout * ntuv(u.LK);
+          if (x <= (int64_t(1) << 28)) need = std::max(need, x);
+        }
+      }
+      if (need > 0) {
+        TB_TRY(dalloc(&P->d_xbuf, (size_t)need, "stage-1 contraction buffer"));
+        P->xbuf_len = need;
+      }
+    }
     TB_TRY(geo_alloc(P, 1));
     TB_TRY(upload_centres(P, xx, yy, zz));
     const int64_t n = std::max<int64_t>(P->nquart, 1);
@@ -793,8 +821,14 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
         b.qbegin = u.begin;
         b.qend = u.end;
         b.recbase = recoff[c] + (u.begin - cb[c]) * (int64_t)rs[c];
-        TB_CK(launch_stage1_xk(P->kind, cL[c], u.LK, u.XB != 0, b, ngeom, P->st));
-        P->launches += 1;
+        const int64_t need = (u.end - u.begin) * (int64_t)u.nout * ntuv(u.LK);
+        if (ngeom == 1 && u.nout > 0 && P->d_xbuf && need <= P->xbuf_len) {
+          TB_CK(launch_stage1_xsplit(P->kind, cL[c], u.LK, u.XB != 0, b, P->d_xbuf, u.nout, P->st));
+          P->launches += 2;
+        } else {
+          TB_CK(launch_stage1_xk(P->kind, cL[c], u.LK, u.XB != 0, b, ngeom, P->st));
+          P->launches += 1;
+        }
       }
     } else {
       TB_CK(launch_stage1(P->kind, cL[c], a, ngeom, P->st));

@@ -616,8 +616,140 @@ __global__ void stage1_smem_batch(const Stage1Args *__restrict__ d, const int64_
 // quartet costs ntuv(LK) FMAs instead of the three zero-padded convolutions
 // and the outer product of stage1_reg_kernel.
 
+// The function pairs of a quartet's two sides, and the outer pair o's
+// functions: (fa, fb) on the bra (XB false) or (fc, fd) on the ket (XB true).
+struct XkSides {
+  int si, ni, sj, nj, sk, nk, sr, nr, pb, pk, nout, nin;
+};
+
+template <bool XB>
+__device__ __forceinline__ XkSides xk_sides(const Stage1Args &A, const QuartetHead &Q) {
+  XkSides S;
+  S.pb = pair_index(Q.gi, Q.gj, A.ng);
+  S.pk = pair_index(Q.gk, Q.gr, A.ng);
+  S.si = A.gstart[Q.gi]; S.ni = A.gcount[Q.gi];
+  S.sj = A.gstart[Q.gj]; S.nj = A.gcount[Q.gj];
+  S.sk = A.gstart[Q.gk]; S.nk = A.gcount[Q.gk];
+  S.sr = A.gstart[Q.gr]; S.nr = A.gcount[Q.gr];
+  const int nab = S.ni * S.nj, ncd = S.nk * S.nr;
+  S.nout = XB ? ncd : nab;
+  S.nin = XB ? nab : ncd;
+  return S;
+}
+
+// Outer pair o's E coefficients (order LO), with the bra's (-1)^t sign of
+// src/Integrals.f90:5181 when the outer side is the bra.
+template <int LO, bool XB>
+__device__ __forceinline__ void xk_outer(const Stage1Args &A, const QuartetHead &Q, const XkSides &S, int o, int &fa,
+                                         int &fb, int &fc, int &fd, double *ox, double *oy, double *oz) {
+  if (XB) { fc = S.sk + o / S.nr; fd = S.sr + o % S.nr; fa = fb = 0; }
+  else { fa = S.si + o / S.nj; fb = S.sj + o % S.nj; fc = fd = 0; }
+  if (ox == nullptr) return;
+  const int64_t np = A.npair;
+  const int l1 = XB ? A.flmn[fc] : A.flmn[fa], l2 = XB ? A.flmn[fd] : A.flmn[fb];
+  const int pr = XB ? S.pk : S.pb;
+  const double *ex = esoa_slot(A, XB ? (Q.skip & 8) : (Q.skip & 1), 0, l1 & 0xff, l2 & 0xff, pr);
+  const double *ey = esoa_slot(A, XB ? (Q.skip & 16) : (Q.skip & 2), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
+  const double *ez = esoa_slot(A, XB ? false : (Q.skip & 4), 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
+#pragma unroll
+  for (int t = 0; t <= LO; ++t) {
+    const double sg = (!XB && (t & 1)) ? -1.0 : 1.0;
+    ox[t] = sg * ex[t * np];
+    oy[t] = sg * ey[t * np];
+    oz[t] = sg * ez[t * np];
+  }
+}
+
+// X_o over the contracted side's function pairs c:
+//   X_o(t'u'v') = sum_c rho(o, c) E_c^x(t') E_c^y(u') E_c^z(v')
+template <int LK, int KIND, bool XB>
+__device__ __forceinline__ void xk_contract(const Stage1Args &A, const QuartetHead &Q, const XkSides &S, int fa,
+                                            int fb, int fc, int fd, double *X) {
+  constexpr int NX = ntuv(LK);
+  const int64_t np = A.npair;
+#pragma unroll
+  for (int e = 0; e < NX; ++e) X[e] = 0.0;
+  int64_t rowp = 0;
+  double zo = 0.0;
+  if (!XB) {
+    rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+    zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+  } else {
+    zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
+  }
+  for (int c = 0; c < S.nin; ++c) {
+    int ga, gb2, gc, gd;
+    if (XB) { ga = S.si + c / S.nj; gb2 = S.sj + c % S.nj; gc = fc; gd = fd; }
+    else { gc = S.sk + c / S.nr; gd = S.sr + c % S.nr; ga = fa; gb2 = fb; }
+    double z;
+    if (KIND == KIND_ELASTIC) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
+    else {
+      const int64_t rp = XB ? fpair(min(ga, gb2), max(ga, gb2)) * A.np : rowp;
+      z = A.rho[rp + fpair(min(gc, gd), max(gc, gd))];
+    }
+    // the reference skips primitive quartets with |ztot| < cutoffz
+    z = fabs(z) < A.cutoffz ? 0.0 : z;
+    const int l1 = XB ? A.flmn[ga] : A.flmn[gc], l2 = XB ? A.flmn[gb2] : A.flmn[gd];
+    const int pr = XB ? S.pb : S.pk;
+    const double *ex = esoa_slot(A, XB ? (Q.skip & 1) : (Q.skip & 8), 0, l1 & 0xff, l2 & 0xff, pr);
+    const double *ey = esoa_slot(A, XB ? (Q.skip & 2) : (Q.skip & 16), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
+    const double *ez = esoa_slot(A, XB ? (Q.skip & 4) : false, 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
+    double cx[LK + 1], cy[LK + 1], cz[LK + 1];
+#pragma unroll
+    for (int t = 0; t <= LK; ++t) {
+      const double sg = (XB && (t & 1)) ? -1.0 : 1.0;
+      cx[t] = sg * ex[t * np];
+      cy[t] = sg * ey[t * np];
+      cz[t] = sg * ez[t * np];
+    }
+    int e = 0;
+#pragma unroll
+    for (int t = 0; t <= LK; ++t) {
+      const double w1 = z * cx[t];
+#pragma unroll
+      for (int u = 0; u <= LK - t; ++u) {
+        const double w2 = w1 * cy[u];
+#pragma unroll
+        for (int v = 0; v <= LK - t - u; ++v, ++e) X[e] = fma(w2, cz[v], X[e]);
+      }
+    }
+  }
+}
+
+// D += O (x) X over the two simplices
+template <int L, int LK>
+__device__ __forceinline__ void xk_convolve(double *D, const double *ox, const double *oy, const double *oz,
+                                            const double *X) {
+  constexpr int LO = L - LK;
+#pragma unroll
+  for (int t = 0; t <= LO; ++t)
+#pragma unroll
+    for (int u = 0; u <= LO - t; ++u) {
+      const double oxy = ox[t] * oy[u];
+#pragma unroll
+      for (int v = 0; v <= LO - t - u; ++v) {
+        const double b = oxy * oz[v];
+        int e = 0;
+#pragma unroll
+        for (int t2 = 0; t2 <= LK; ++t2)
+#pragma unroll
+          for (int u2 = 0; u2 <= LK - t2; ++u2)
+#pragma unroll
+            for (int v2 = 0; v2 <= LK - t2 - u2; ++v2, ++e) {
+              const int k = dindex<L>(t + t2, u + u2, v + v2);
+              D[k] = fma(b, X[e], D[k]);
+            }
+      }
+    }
+}
+
+// Fused form: a thread per quartet, contraction and convolution per outer
+// pair (geometry and molecule batches).  With xbuf given, X_o is read from
+// the contraction kernel's buffer instead (stage1_xc_kernel, row stride
+// xstride doubles per quartet).
 template <int L, int KIND, int LK, bool XB>
-__device__ __forceinline__ void stage1_xk_body(Stage1Args &A, int64_t vb) {
+__device__ __forceinline__ void stage1_xk_body(Stage1Args &A, int64_t vb, const double *__restrict__ xbuf = nullptr,
+                                               int xstride = 0) {
   constexpr int LO = L - LK;  // order of the convolved (outer) side
   constexpr int NT = ntuv(L), NX = ntuv(LK);
   constexpr int NG = 128;
@@ -625,113 +757,58 @@ __device__ __forceinline__ void stage1_xk_body(Stage1Args &A, int64_t vb) {
   const int64_t qi = A.qbegin + vb * blockDim.x + threadIdx.x;
   if (qi >= A.qend) return;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
-  const int pb = pair_index(Q.gi, Q.gj, A.ng), pk = pair_index(Q.gk, Q.gr, A.ng);
-  const int64_t np = A.npair;
+  const XkSides S = xk_sides<XB>(A, Q);
   double D[NT];
 #pragma unroll
   for (int e = 0; e < NT; ++e) D[e] = 0.0;
-  const int si = A.gstart[Q.gi], ni = A.gcount[Q.gi];
-  const int sj = A.gstart[Q.gj], nj = A.gcount[Q.gj];
-  const int sk = A.gstart[Q.gk], nk = A.gcount[Q.gk];
-  const int sr = A.gstart[Q.gr], nr = A.gcount[Q.gr];
-  const int nab = ni * nj, ncd = nk * nr;
-  // the bra side's E coefficients carry the (-1)^t sign of src/Integrals.f90:5181
-  const int nout = XB ? ncd : nab, nin = XB ? nab : ncd;
-  for (int o = 0; o < nout; ++o) {
-    // the outer pair's functions and coefficients (order LO)
+  const double *xq = xbuf ? xbuf + (qi - A.qbegin) * (int64_t)xstride : nullptr;
+  for (int o = 0; o < S.nout; ++o) {
     int fa, fb, fc, fd;
-    if (XB) { fc = sk + o / nr; fd = sr + o % nr; fa = fb = 0; }
-    else { fa = si + o / nj; fb = sj + o % nj; fc = fd = 0; }
     double ox[LO + 1], oy[LO + 1], oz[LO + 1];
-    {
-      const int l1 = XB ? A.flmn[fc] : A.flmn[fa], l2 = XB ? A.flmn[fd] : A.flmn[fb];
-      const int pr = XB ? pk : pb;
-      const double *ex = esoa_slot(A, XB ? (Q.skip & 8) : (Q.skip & 1), 0, l1 & 0xff, l2 & 0xff, pr);
-      const double *ey = esoa_slot(A, XB ? (Q.skip & 16) : (Q.skip & 2), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
-      const double *ez = esoa_slot(A, XB ? false : (Q.skip & 4), 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
-#pragma unroll
-      for (int t = 0; t <= LO; ++t) {
-        const double sg = (!XB && (t & 1)) ? -1.0 : 1.0;
-        ox[t] = sg * ex[t * np];
-        oy[t] = sg * ey[t * np];
-        oz[t] = sg * ez[t * np];
-      }
-    }
-    // X over the contracted side's function pairs
+    xk_outer<LO, XB>(A, Q, S, o, fa, fb, fc, fd, ox, oy, oz);
     double X[NX];
+    if (xq) {
 #pragma unroll
-    for (int e = 0; e < NX; ++e) X[e] = 0.0;
-    int64_t rowp = 0;
-    double zo = 0.0;
-    if (!XB) {
-      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-      zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      for (int e = 0; e < NX; ++e) X[e] = xq[o * NX + e];
     } else {
-      zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
+      xk_contract<LK, KIND, XB>(A, Q, S, fa, fb, fc, fd, X);
     }
-    for (int c = 0; c < nin; ++c) {
-      int ga, gb2, gc, gd;
-      if (XB) { ga = si + c / nj; gb2 = sj + c % nj; gc = fc; gd = fd; }
-      else { gc = sk + c / nr; gd = sr + c % nr; ga = fa; gb2 = fb; }
-      double z;
-      if (KIND == KIND_ELASTIC) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
-      else {
-        const int64_t rp = XB ? fpair(min(ga, gb2), max(ga, gb2)) * A.np : rowp;
-        z = A.rho[rp + fpair(min(gc, gd), max(gc, gd))];
-      }
-      // the reference skips primitive quartets with |ztot| < cutoffz
-      z = fabs(z) < A.cutoffz ? 0.0 : z;
-      const int l1 = XB ? A.flmn[ga] : A.flmn[gc], l2 = XB ? A.flmn[gb2] : A.flmn[gd];
-      const int pr = XB ? pb : pk;
-      const double *ex = esoa_slot(A, XB ? (Q.skip & 1) : (Q.skip & 8), 0, l1 & 0xff, l2 & 0xff, pr);
-      const double *ey = esoa_slot(A, XB ? (Q.skip & 2) : (Q.skip & 16), 1, (l1 >> 8) & 0xff, (l2 >> 8) & 0xff, pr);
-      const double *ez = esoa_slot(A, XB ? (Q.skip & 4) : false, 2, (l1 >> 16) & 0xff, (l2 >> 16) & 0xff, pr);
-      double cx[LK + 1], cy[LK + 1], cz[LK + 1];
-#pragma unroll
-      for (int t = 0; t <= LK; ++t) {
-        const double sg = (XB && (t & 1)) ? -1.0 : 1.0;
-        cx[t] = sg * ex[t * np];
-        cy[t] = sg * ey[t * np];
-        cz[t] = sg * ez[t * np];
-      }
-      int e = 0;
-#pragma unroll
-      for (int t = 0; t <= LK; ++t) {
-        const double w1 = z * cx[t];
-#pragma unroll
-        for (int u = 0; u <= LK - t; ++u) {
-          const double w2 = w1 * cy[u];
-#pragma unroll
-          for (int v = 0; v <= LK - t - u; ++v, ++e) X[e] = fma(w2, cz[v], X[e]);
-        }
-      }
-    }
-    // D += O (x) X over the two simplices
-#pragma unroll
-    for (int t = 0; t <= LO; ++t)
-#pragma unroll
-      for (int u = 0; u <= LO - t; ++u) {
-        const double oxy = ox[t] * oy[u];
-#pragma unroll
-        for (int v = 0; v <= LO - t - u; ++v) {
-          const double b = oxy * oz[v];
-          int e = 0;
-#pragma unroll
-          for (int t2 = 0; t2 <= LK; ++t2)
-#pragma unroll
-            for (int u2 = 0; u2 <= LK - t2; ++u2)
-#pragma unroll
-              for (int v2 = 0; v2 <= LK - t2 - u2; ++v2, ++e) {
-                const int k = dindex<L>(t + t2, u + u2, v + v2);
-                D[k] = fma(b, X[e], D[k]);
-              }
-        }
-      }
+    xk_convolve<L, LK>(D, ox, oy, oz, X);
   }
   double *col = sD + threadIdx.x;
 #pragma unroll
   for (int k = 0; k < NT; ++k) col[k * NG] = D[k];
   stage1_finish<L, KIND, 1>(A, Q, col, NG, qi, 0, 0xffffffffu);
+}
+
+// Contraction alone, at high occupancy: G threads per quartet (G a power of
+// two >= its outer pairs), thread o computing X_o; the G threads of a quartet
+// read the same inner-pair coefficients (one transaction per warp).  X_o goes
+// to xbuf[(qi - qbegin) * xstride + o * NX + e].
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride) {
+  constexpr int NX = ntuv(LK);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t qi = A.qbegin + t / G;
+  const int o = (int)(t % G);
+  if (qi >= A.qend) return;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const XkSides S = xk_sides<XB>(A, Q);
+  if (o >= S.nout) return;
+  int fa, fb, fc, fd;
+  xk_outer<L - LK, XB>(A, Q, S, o, fa, fb, fc, fd, nullptr, nullptr, nullptr);
+  double X[NX];
+  xk_contract<LK, KIND, XB>(A, Q, S, fa, fb, fc, fd, X);
+  double *xo = xbuf + (qi - A.qbegin) * (int64_t)xstride + o * NX;
+#pragma unroll
+  for (int e = 0; e < NX; ++e) xo[e] = X[e];
+}
+
+// Convolution and epilogue from the contraction kernel's X.
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128, 2) stage1_xb_kernel(Stage1Args A, const double *__restrict__ xbuf,
+                                                           int xstride) {
+  stage1_xk_body<L, KIND, LK, XB>(A, blockIdx.x, xbuf, xstride);
 }
 
 template <int L, int KIND, int LK, bool XB>
@@ -811,6 +888,45 @@ cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int 
   TB_XK(8, 0) TB_XK(8, 1) TB_XK(8, 2) TB_XK(8, 3) TB_XK(8, 4)
 #endif
 #undef TB_XK
+  return cudaErrorInvalidValue;
+}
+
+// Contracted-side classes of a single geometry in two kernels: the
+// contraction into xbuf (G threads per quartet), then convolution + epilogue.
+template <int L, int K, int LK, bool XB>
+static cudaError_t launch_stage1_xsplit_l(const Stage1Args &a, int64_t n, double *xbuf, int nout, cudaStream_t st) {
+  int G = 1;
+  while (G < nout) G *= 2;
+  const int xstride = nout * ntuv(LK);
+  const int64_t nthr = n * G;
+  stage1_xc_kernel<L, K, LK, XB><<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(a, xbuf, G, xstride);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int thr = 128;
+  const size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
+  e = cudaFuncSetAttribute(stage1_xb_kernel<L, K, LK, XB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage1_xb_kernel<L, K, LK, XB><<<(unsigned)((n + thr - 1) / thr), thr, smem, st>>>(a, xbuf, xstride);
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+                                   cudaStream_t st) {
+  const int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+#define TB_XS(l, lk)                                                                         \
+  if (L == l && LK == lk)                                                                   \
+    return XB ? launch_stage1_xsplit_l<l, K, lk, true>(a, n, xbuf, nout, st)                 \
+              : launch_stage1_xsplit_l<l, K, lk, false>(a, n, xbuf, nout, st);
+  TB_XS(4, 0) TB_XS(4, 1) TB_XS(4, 2)
+  TB_XS(5, 0) TB_XS(5, 1) TB_XS(5, 2)
+  TB_XS(6, 0) TB_XS(6, 1) TB_XS(6, 2) TB_XS(6, 3)
+#if TB_S1_XK_HIGH
+  TB_XS(7, 0) TB_XS(7, 1) TB_XS(7, 2) TB_XS(7, 3)
+  TB_XS(8, 0) TB_XS(8, 1) TB_XS(8, 2) TB_XS(8, 3) TB_XS(8, 4)
+#endif
+#undef TB_XS
   return cudaErrorInvalidValue;
 }
 
