@@ -190,3 +190,16 @@ def test_device_cache_reuses_buffers():
     assert np.array_equal(a, b)
     _abi.release_device_cache()
     assert _abi.device_cache_bytes()[0] == 0
+
+
+@pytest.mark.parametrize("type_", [1, 2, 7])
+def test_split_contraction_matches_fused(oracle, type_):
+    """A plan's own execution runs the contracted-side classes (LLmax 4-6) as
+    a contraction kernel plus a convolution kernel; an explicit quartet list
+    takes the fused one-thread-per-quartet kernel.  Both must agree."""
+    p = I.config3_ab6(natoms=3)
+    qs = oracle.enum_quartets(p.ng)
+    with MC.ScatteringPlan.from_problem(p, type_) as pl:
+        split = pl.execute()
+        fused = pl.execute_quartets(qs[:, :4])
+    assert np.max(rel_err(split, fused)) < 1e-12
