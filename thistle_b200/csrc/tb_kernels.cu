@@ -568,6 +568,17 @@ cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1A
   return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, st);
 }
 
+cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
+                                       int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,
+                                       cudaStream_t st) {
+#define TB_K(k) return launch_stage1_xsplit_batch_k<k>(L, LK, XB, d, prexc, blocksxc, pre, blocks, n, xbuf, st)
+  if (kind == KIND_TOTAL) TB_K(KIND_TOTAL);
+  if (kind == KIND_ELASTIC) TB_K(KIND_ELASTIC);
+  if (kind == KIND_ALIGNED) TB_K(KIND_ALIGNED);
+  TB_K(KIND_J2);
+#undef TB_K
+}
+
 cudaError_t launch_pair_tables_batch(const PairDesc *d, const int64_t *pre, int n, int64_t blocks, cudaStream_t st) {
   if (n <= 0 || blocks <= 0) return cudaSuccess;
   pair_tables_batch_kernel<<<(unsigned)blocks, 128, 0, st>>>(d, pre, n);

@@ -35,6 +35,11 @@ struct Stage1Args {
   // geometry batches: blockIdx.y is the geometry; its tables, records and
   // counters sit these many elements after geometry 0's
   int64_t gs_pair, gs_esoa, gs_rec;
+  // molecule batches, split contracted side: this item's X rows start xoff
+  // doubles into the batch's contraction buffer, xstride per quartet, xg
+  // contraction threads per quartet
+  int64_t xoff;
+  int xstride, xg;
 };
 
 constexpr int MAXCLS = 20;
@@ -164,6 +169,15 @@ cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, 
                                    cudaStream_t st);
 cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
                                  cudaStream_t st);
+// molecule batches: the contraction (blocks from prexc) then the convolution
+// (blocks from pre, as the fused kernel) over every item of one (L, LK, XB)
+template <int K>
+cudaError_t launch_stage1_xsplit_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
+                                         int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,
+                                         cudaStream_t st);
+cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
+                                       int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,
+                                       cudaStream_t st);
 size_t stage2_smem_bytes(int nqp, int nwarps);
 cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_t st);
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st);

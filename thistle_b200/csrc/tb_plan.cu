@@ -794,6 +794,9 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
   a.gs_pair = gs_pair(P);
   a.gs_esoa = gs_esoa(P);
   a.gs_rec = gs_rec(P);
+  a.xoff = 0;
+  a.xstride = 0;
+  a.xg = 0;
   return a;
 }
 
@@ -1086,6 +1089,8 @@ struct thistle_batch {
     int L, LK, XB, n;
     Stage1Args *d;
     int64_t *pre, blocks;
+    bool split;            // contraction kernel + convolution kernel through d_xbuf
+    int64_t *prexc, blocksxc;
   };
   struct S2 {
     int LB, n;
@@ -1095,7 +1100,7 @@ struct thistle_batch {
   std::vector<S1> s1;
   std::vector<S2> s2;
   ReduceDesc *d_red = nullptr;
-  double *d_partial = nullptr, *d_out = nullptr;
+  double *d_partial = nullptr, *d_out = nullptr, *d_xbuf = nullptr;
   int64_t partial_len = 0;
   bool use_graph = false;
   cudaGraphExec_t gx = nullptr;
@@ -1105,7 +1110,8 @@ struct thistle_batch {
 static void batch_free(thistle_batch *B) {
   if (!B) return;
   dfree(B->d_pair); dfree(B->d_pair_pre); dfree(B->d_red); dfree(B->d_partial); dfree(B->d_out);
-  for (auto &x : B->s1) { dfree(x.d); dfree(x.pre); }
+  for (auto &x : B->s1) { dfree(x.d); dfree(x.pre); dfree(x.prexc); }
+  dfree(B->d_xbuf);
   for (auto &x : B->s2) { dfree(x.d); dfree(x.pre); }
   if (B->gx) cudaGraphExecDestroy(B->gx);
   delete B;
@@ -1125,8 +1131,14 @@ static int batch_run(thistle_batch *B) {
   TB_CK(launch_pair_tables_batch(B->d_pair, B->d_pair_pre, (int)B->plans.size(), B->pair_blocks, st));
   B->launches += 1;
   for (auto &x : B->s1) {
-    TB_CK(launch_stage1_batch(B->kind, x.L, x.LK, x.XB, x.d, x.pre, x.n, x.blocks, st));
-    B->launches += 1;
+    if (x.split) {
+      TB_CK(launch_stage1_xsplit_batch(B->kind, x.L, x.LK, x.XB, x.d, x.prexc, x.blocksxc, x.pre, x.blocks, x.n,
+                                       B->d_xbuf, st));
+      B->launches += 2;
+    } else {
+      TB_CK(launch_stage1_batch(B->kind, x.L, x.LK, x.XB, x.d, x.pre, x.n, x.blocks, st));
+      B->launches += 1;
+    }
   }
   TB_CK(cudaMemsetAsync(B->d_partial, 0, sizeof(double) * B->partial_len, st));
   for (auto &x : B->s2) {
@@ -1223,7 +1235,7 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
     int64_t ltot[LMAXQ + 1] = {0};
     for (thistle_plan *P : B->plans)
       for (int c = 0; c < P->ncls; ++c) ltot[P->cls_L[c]] += P->cls_end[c] - P->cls_begin[c];
-    std::vector<std::pair<std::array<int, 3>, Stage1Args>> items;
+    std::vector<std::pair<std::array<int, 4>, Stage1Args>> items;  // (L, LK, XB, nout)
     for (thistle_plan *P : B->plans)
       for (int c = 0; c < P->ncls; ++c) {
         Stage1Args a = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c],
@@ -1235,31 +1247,59 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
             b.qbegin = u.begin;
             b.qend = u.end;
             b.recbase = P->cls_recoff[c] + (u.begin - P->cls_begin[c]) * (int64_t)P->cls_rs[c];
-            items.push_back({{L, u.LK, u.XB}, b});
+            items.push_back({{L, u.LK, u.XB, u.nout}, b});
           }
         } else {
-          items.push_back({{L, -1, 0}, a});
+          items.push_back({{L, -1, 0, 0}, a});
         }
       }
-    std::stable_sort(items.begin(), items.end(),
-                     [](const auto &x, const auto &y) { return x.first < y.first; });
+    auto same = [](const std::array<int, 4> &x, const std::array<int, 4> &y) {
+      return x[0] == y[0] && x[1] == y[1] && x[2] == y[2];
+    };
+    std::stable_sort(items.begin(), items.end(), [](const auto &x, const auto &y) {
+      return std::array<int, 3>{x.first[0], x.first[1], x.first[2]} <
+             std::array<int, 3>{y.first[0], y.first[1], y.first[2]};
+    });
+    int64_t xneed = 0;
     for (size_t i = 0; i < items.size();) {
       size_t j = i;
       std::vector<Stage1Args> d;
-      std::vector<int64_t> pre(1, 0);
-      while (j < items.size() && items[j].first == items[i].first) {
-        d.push_back(items[j].second);
-        pre.push_back(pre.back() + stage1_item_blocks(items[j].first[0], items[j].first[1] >= 0,
-                                                      items[j].second.qend - items[j].second.qbegin));
+      std::vector<int64_t> pre(1, 0), prexc(1, 0);
+      const int L = items[i].first[0], LK = items[i].first[1];
+      // contracted side: split through the batch's contraction buffer when
+      // every item knows its outer-pair count and the group fits in 2 GB
+      bool split = LK >= 0;
+      int64_t xoff = 0;
+      while (j < items.size() && same(items[j].first, items[i].first)) {
+        Stage1Args a = items[j].second;
+        const int64_t nq = a.qend - a.qbegin;
+        const int nout = items[j].first[3];
+        if (LK >= 0 && nout > 0) {
+          int G = 1;
+          while (G < nout) G *= 2;
+          a.xg = G;
+          a.xstride = nout * ntuv(LK);
+          a.xoff = xoff;
+          xoff += nq * a.xstride;
+          prexc.push_back(prexc.back() + (nq * G + 127) / 128);
+        } else {
+          split = false;
+        }
+        d.push_back(a);
+        pre.push_back(pre.back() + stage1_item_blocks(L, LK >= 0, nq));
         ++j;
       }
-      thistle_batch::S1 x{items[i].first[0], items[i].first[1], items[i].first[2], (int)d.size(), nullptr, nullptr,
-                          pre.back()};
+      if (xoff > (int64_t(1) << 28)) split = false;
+      if (split) xneed = std::max(xneed, xoff);
+      thistle_batch::S1 x{L, LK, items[i].first[2], (int)d.size(), nullptr, nullptr, pre.back(), split, nullptr,
+                          split ? prexc.back() : 0};
       TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-1 descriptors"));
       TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-1 prefix"));
+      if (split) TB_TRY(upload_vec(&x.prexc, prexc, B->st, "batch contraction prefix"));
       B->s1.push_back(x);
       i = j;
     }
+    if (xneed > 0) TB_TRY(dalloc(&B->d_xbuf, (size_t)xneed, "batch contraction buffer"));
     // stage 2: items grouped by Bessel order
     std::vector<std::pair<int, std::pair<Stage2ClassArgs, int64_t>>> s2items;
     for (int i = 0; i < n; ++i) {

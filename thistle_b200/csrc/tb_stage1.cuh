@@ -786,9 +786,9 @@ __device__ __forceinline__ void stage1_xk_body(Stage1Args &A, int64_t vb, const 
 // read the same inner-pair coefficients (one transaction per warp).  X_o goes
 // to xbuf[(qi - qbegin) * xstride + o * NX + e].
 template <int L, int KIND, int LK, bool XB>
-__global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride) {
+__device__ __forceinline__ void stage1_xc_body(const Stage1Args &A, int64_t t, double *__restrict__ xbuf, int G,
+                                               int xstride) {
   constexpr int NX = ntuv(LK);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t qi = A.qbegin + t / G;
   const int o = (int)(t % G);
   if (qi >= A.qend) return;
@@ -804,11 +804,36 @@ __global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__
   for (int e = 0; e < NX; ++e) xo[e] = X[e];
 }
 
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride) {
+  stage1_xc_body<L, KIND, LK, XB>(A, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, xbuf, G, xstride);
+}
+
+// Molecule batches: item i's contraction threads in blocks prexc[i] ..
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128)
+    stage1_xc_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ prexc, int n,
+                    double *__restrict__ xbuf) {
+  const int it = batch_item(prexc, n, blockIdx.x);
+  const Stage1Args A = d[it];
+  stage1_xc_body<L, KIND, LK, XB>(A, (blockIdx.x - prexc[it]) * blockDim.x + threadIdx.x, xbuf + A.xoff, A.xg,
+                                  A.xstride);
+}
+
 // Convolution and epilogue from the contraction kernel's X.
 template <int L, int KIND, int LK, bool XB>
 __global__ void __launch_bounds__(128, 2) stage1_xb_kernel(Stage1Args A, const double *__restrict__ xbuf,
                                                            int xstride) {
   stage1_xk_body<L, KIND, LK, XB>(A, blockIdx.x, xbuf, xstride);
+}
+
+template <int L, int KIND, int LK, bool XB>
+__global__ void __launch_bounds__(128, 2)
+    stage1_xb_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n,
+                    const double *__restrict__ xbuf) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  Stage1Args A = d[it];
+  stage1_xk_body<L, KIND, LK, XB>(A, blockIdx.x - pre[it], xbuf + A.xoff, A.xstride);
 }
 
 template <int L, int KIND, int LK, bool XB>
@@ -927,6 +952,40 @@ cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, 
   TB_XS(8, 0) TB_XS(8, 1) TB_XS(8, 2) TB_XS(8, 3) TB_XS(8, 4)
 #endif
 #undef TB_XS
+  return cudaErrorInvalidValue;
+}
+
+template <int L, int K, int LK, bool XB>
+static cudaError_t launch_stage1_xsplit_batch_l(const Stage1Args *d, const int64_t *prexc, int64_t blocksxc,
+                                                const int64_t *pre, int64_t blocks, int n, double *xbuf,
+                                                cudaStream_t st) {
+  stage1_xc_batch<L, K, LK, XB><<<(unsigned)blocksxc, 128, 0, st>>>(d, prexc, n, xbuf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = (size_t)ntuv(L) * sizeof(double) * 128;
+  e = cudaFuncSetAttribute(stage1_xb_batch<L, K, LK, XB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  stage1_xb_batch<L, K, LK, XB><<<(unsigned)blocks, 128, smem, st>>>(d, pre, n, xbuf);
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_stage1_xsplit_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
+                                         int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,
+                                         cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+#define TB_XSB(l, lk)                                                                                   \
+  if (L == l && LK == lk)                                                                             \
+    return XB ? launch_stage1_xsplit_batch_l<l, K, lk, true>(d, prexc, blocksxc, pre, blocks, n, xbuf, st) \
+              : launch_stage1_xsplit_batch_l<l, K, lk, false>(d, prexc, blocksxc, pre, blocks, n, xbuf, st);
+  TB_XSB(4, 0) TB_XSB(4, 1) TB_XSB(4, 2)
+  TB_XSB(5, 0) TB_XSB(5, 1) TB_XSB(5, 2)
+  TB_XSB(6, 0) TB_XSB(6, 1) TB_XSB(6, 2) TB_XSB(6, 3)
+#if TB_S1_XK_HIGH
+  TB_XSB(7, 0) TB_XSB(7, 1) TB_XSB(7, 2) TB_XSB(7, 3)
+  TB_XSB(8, 0) TB_XSB(8, 1) TB_XSB(8, 2) TB_XSB(8, 3) TB_XSB(8, 4)
+#endif
+#undef TB_XSB
   return cudaErrorInvalidValue;
 }
 
