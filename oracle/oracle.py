@@ -169,3 +169,55 @@ def md_chain(l1, l2, PA, PB, a) -> np.ndarray:
     lib().orc_md_chain(C.c_int(l1), C.c_int(l2), C.c_double(PA), C.c_double(PB), C.c_double(a),
                        out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
+
+
+def nuclear(prob, Zn, *, bessel_mode: int = 1, q=None) -> np.ndarray:
+    """Nuclear-electron term Ine(q) of electron scattering (nuclei_electron_integration)
+    with the AO density of the problem's 1-RDM; atoms at prob.atoms with charges Zn."""
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
+    out = np.zeros(qv.size)
+    geom = np.asfortranarray(np.asarray(prob.atoms, dtype=np.float64)).ravel(order="F")
+    rc = lib().orc_nuclear(
+        C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n), d(prob.xx), d(prob.yy), d(prob.zz),
+        i(prob.group), d(np.asfortranarray(prob.mmod).ravel(order="F")), C.c_int(prob.nmo),
+        d(np.asfortranarray(prob.onerdm).ravel(order="F")), C.c_int(prob.onerdm.shape[0]), d(qv),
+        C.c_int(qv.size), C.c_double(prob.cutoffz), C.c_double(prob.cutoffmd), C.c_double(prob.cutoffcentre),
+        d(np.asarray(Zn, dtype=np.float64)), d(geom), C.c_int(len(prob.atoms)), C.c_int(bessel_mode),
+        out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_nuclear failed with code {rc}")
+    return out
+
+
+def nuclear_nuclear(prob, Zn, q=None) -> np.ndarray:
+    """Inn(q) = sum_ij Zn_i Zn_j sinc(q R_ij) (src/main_calculation.f90:302-311; sinc(0) = 1)."""
+    qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
+    R = np.asarray(prob.atoms, dtype=np.float64)
+    Zn = np.asarray(Zn, dtype=np.float64)
+    out = np.zeros(qv.size)
+    for a in range(len(R)):
+        for b in range(len(R)):
+            x = qv * np.sqrt(np.sum((R[a] - R[b]) ** 2))
+            s = np.where(np.abs(x) < 1e-10, 1.0, np.sin(x) / np.where(np.abs(x) < 1e-10, 1.0, x))
+            out += Zn[a] * Zn[b] * s
+    return out
+
+
+def electron(prob, type_: int, Zn, *, bessel_mode: int = 1, nthreads: int = 0) -> np.ndarray:
+    """Electron scattering, types 5 (total) and 6 (elastic) of main_calculation
+    (src/main_calculation.f90:277-329, 330-...): I_e - 2 Ine + Inn with I_e the
+    total (type 5) or elastic (type 6) j0 intensity."""
+    Ie = scattering(prob, 1 if type_ == 5 else 2, bessel_mode=bessel_mode, nthreads=nthreads)
+    return Ie - 2.0 * nuclear(prob, Zn, bessel_mode=bessel_mode) + nuclear_nuclear(prob, Zn)

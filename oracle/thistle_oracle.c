@@ -1084,3 +1084,129 @@ void orc_bessels0rr(int order, const double *mu, int nq, double H, const double 
 void orc_md_chain(int l1, int l2, double PA, double PB, double a, double *out) {
     md_chain(l1, l2, PA, PB, a, out);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Nuclear-electron term of electron scattering (types 5 and 6)              */
+/* ------------------------------------------------------------------------ */
+
+/* BesselSum (src/Integrals.f90:6328-6366): F = sum_b h_b j_b(qH) (q/H)^b.
+ * bessel_mode 0 keeps the reference's upward recurrence
+ *   h_r = ((2r-1)/(qH) h_{r-1} - h_{r-2} q/H) q/H,
+ * bessel_mode 1 takes the j_b of the stable backward recurrence instead (the
+ * quantity the upward form approximates; it loses digits for qH below ~b). */
+static void bessel_sum(double *f, const double *mu, int nq, double H, int LLmax, const double *h_saved,
+                       int bessel_mode, double *scratch) {
+    if (bessel_mode != 0) {
+        bessels0rr(f, LLmax, mu, nq, H, h_saved, 1, scratch);
+        return;
+    }
+    for (int iq = 0; iq < nq; ++iq) {
+        double Pmu = H * mu[iq];
+        double h0 = sin(Pmu) / Pmu;
+        double sum = h0 * h_saved[0];
+        if (LLmax >= 1) {
+            double muOH = mu[iq] / H;
+            double h1 = (sin(Pmu) / (Pmu * Pmu) - cos(Pmu) / Pmu) * muOH;
+            sum = sum + h_saved[1] * h1;
+            for (int ra = 2; ra <= LLmax; ++ra) {
+                double hr = ((double)(2 * ra - 1) / Pmu * h1 - h0 * muOH) * muOH;
+                sum = sum + hr * h_saved[ra];
+                h0 = h1;
+                h1 = hr;
+            }
+        }
+        f[iq] = sum;
+    }
+}
+
+/*
+ * nuclei_electron_integration (src/Integrals.f90:2493-2596) with
+ * integral_k_ij (:6192-6326) and integral_ij_pzero (:4865-4953):
+ *   Ine(q) = sum_a sum_{group pairs (i,k), ordered} Zn_a F_ik(q) e12(q,i,k),
+ * H = R_a - P_ik, F from the pair's Hermite expansion against the AO density
+ * Z of the 1-RDM (variables_elastic).  geom is (natoms,3) column-major.
+ */
+int orc_nuclear(int ngto, const double *ga, const int *l, const int *m, const int *n,
+                const double *xx, const double *yy, const double *zz, const int *group,
+                const double *mmod, int nmo, const double *onerdm, int nmo1, const double *q, int nq,
+                double cutoffz, double cutoffmd, double cutoffcentre, const double *Zn, const double *geom,
+                int natoms, int bessel_mode, double *ine) {
+    (void)cutoffz;  /* integral_k_ij has its |ztot| < cutoff1 test commented out (:6268-6273) */
+    if (nmo1 > nmo || natoms < 0) return ORC_ERR_ARG;
+    setup_t S;
+    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, q, nq, 1);
+    if (e != ORC_OK) { free_setup(&S); return e; }
+    dens_t D;
+    memset(&D, 0, sizeof D);
+    D.mmod = mmod; D.nmo = nmo;
+    D.zao = malloc(sizeof(double) * (size_t)ngto * ngto);
+    build_zao(&S, &D, onerdm, nmo1);
+    for (int iq = 0; iq < nq; ++iq) ine[iq] = 0.0;
+    double *f = malloc(sizeof(double) * (size_t)nq);
+    double *scratch = malloc(sizeof(double) * 4096);
+    double *h_pre2 = malloc(sizeof(double) * (size_t)DIM * 21 * 21 * 21);
+    const size_t N = (size_t)ngto;
+    for (int na = 0; na < natoms; ++na)
+        for (int gi = 0; gi < S.ng; ++gi)
+            for (int gk = 0; gk < S.ng; ++gk) {
+                double hx = geom[na] - PX(&S, gi, gk);
+                double hy = geom[na + natoms] - PY(&S, gi, gk);
+                double hz = geom[na + 2 * natoms] - PZ(&S, gi, gk);
+                double h = sqrt(hx * hx + hy * hy + hz * hz);
+                const double *dx1 = DDP(&S, S.ddx, gk, gi), *dy1 = DDP(&S, S.ddy, gk, gi),
+                             *dz1 = DDP(&S, S.ddz, gk, gi);
+                int i0 = S.gs[gi] - 1, k0 = S.gs[gk] - 1;
+                int LLmax = S.l[i0] + S.m[i0] + S.n[i0] + S.l[k0] + S.m[k0] + S.n[k0];
+                int Ld = LLmax + 1;
+                double a[DIM][DIM], b[DIM][DIM], c[DIM][DIM], h_saved[DIM];
+                int pzero = h < cutoffcentre;
+                if (!pzero) {
+                    hermite_like(a, LLmax, hx); hermite_like(b, LLmax, hy); hermite_like(c, LLmax, hz);
+                    double BD[DIM];
+                    for (int kk = 0; kk <= LLmax; ++kk)
+                        for (int jj = 0; jj <= LLmax - kk; ++jj)
+                            for (int ii = 0; ii <= LLmax - kk - jj; ++ii) {
+                                bessel_deriv(BD, ii, jj, kk, a, b, c, LLmax);
+                                double *row = h_pre2 + (size_t)DIM * (ii + Ld * (jj + (size_t)Ld * kk));
+                                for (int t = 0; t < DIM; ++t) row[t] = BD[t];
+                            }
+                    for (int t = 0; t < DIM; ++t) h_saved[t] = 0.0;
+                } else {
+                    for (int iq = 0; iq < nq; ++iq) f[iq] = 0.0;
+                }
+                for (int pi = 0; pi < S.gc[gi]; ++pi)
+                    for (int pk = 0; pk < S.gc[gk]; ++pk) {
+                        int fi = i0 + pi, fk = k0 + pk;
+                        double ztot = D.zao[fi + N * fk];
+                        for (int ll = 0; ll <= l[fi] + l[fk]; ++ll) {
+                            double MDL = dx1[ll + S.dt * (l[fi] + S.dl * l[fk])];
+                            if (fabs(MDL) < SKIP30) continue;
+                            double prod1 = MDL * ztot;
+                            for (int mm = 0; mm <= m[fi] + m[fk]; ++mm) {
+                                double MDM = dy1[mm + S.dt * (m[fi] + S.dl * m[fk])];
+                                if (fabs(MDM) < SKIP30) continue;
+                                double prod2 = MDM * prod1;
+                                for (int nn = 0; nn <= n[fi] + n[fk]; ++nn) {
+                                    double H1 = ((ll + mm + nn) & 1) ? -1.0 : 1.0;
+                                    double MDN = dz1[nn + S.dt * (n[fi] + S.dl * n[fk])];
+                                    if (fabs(MDN) < SKIP30) continue;
+                                    double prod3 = MDN * H1 * prod2;
+                                    if (!(fabs(prod3) > cutoffmd)) continue;
+                                    if (pzero) {
+                                        for (int iq = 0; iq < nq; ++iq) f[iq] += prod3 * P0AT(&S, iq, ll, mm, nn);
+                                    } else {
+                                        const double *row = h_pre2 + (size_t)DIM * (ll + Ld * (mm + (size_t)Ld * nn));
+                                        for (int t = 0; t < DIM; ++t) h_saved[t] += row[t] * prod3;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                if (!pzero) bessel_sum(f, q, nq, h, LLmax, h_saved, bessel_mode, scratch);
+                for (int iq = 0; iq < nq; ++iq) ine[iq] = ine[iq] + Zn[na] * f[iq] * E12(&S, iq, gi, gk);
+            }
+    free(f); free(scratch); free(h_pre2);
+    free_dens(&D);
+    free_setup(&S);
+    return ORC_OK;
+}
