@@ -38,6 +38,13 @@ int thistle_probe_fp64_peak(int32_t reps, double *tflops);
 #define THISTLE_ELASTIC_J0 2
 #define THISTLE_TOTAL_ALIGNED 3
 #define THISTLE_TOTAL_J2 7
+/* electron scattering: I_e - 2 Ine + Inn (src/main_calculation.f90:277-329,
+ * 330-...), I_e the total (5) or elastic (6) j0 intensity, Ine the
+ * nuclear-electron term, Inn the nuclear-nuclear sinc sum; Entry 1 only.
+ * Needs Zn (natoms), geom (natoms x 3, column-major) and the 1-RDM; type 5
+ * also the 2-RDM rows.  q_abs_out receives q. */
+#define THISTLE_TOTAL_ELECTRON 5
+#define THISTLE_ELASTIC_ELECTRON 6
 
 const char *thistle_last_error_string(void);
 int thistle_version(void);
@@ -144,6 +151,18 @@ int thistle_plan_vjp_batch_device(thistle_plan *plan, const double *v_dev, doubl
 int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);
 int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom_best, int32_t *qtile_best,
                                 double *geoms_per_s);
+/*
+ * Nuclear-electron term of an elastic plan (type 2) for its current centres:
+ * ine_host[q] = sum_a Zn_a sum over ordered group pairs (i,k) of the pair's
+ * Hermite expansion against the plan's AO density at H = R_a - P_ik, times
+ * e12 (nuclei_electron_integration, src/Integrals.f90:2493-2596, with
+ * integral_k_ij :6192-6326 and integral_ij_pzero :4865-4953).  geom is
+ * (natoms, 3) column-major.  Entry 1 types 5 and 6 combine it as
+ * I_e - 2 Ine + Inn.
+ */
+int thistle_plan_nuclear(thistle_plan *plan, const double *Zn, const double *geom, int32_t natoms,
+                         double *ine_host);
+
 /*
  * Molecule batches (no reference counterpart).  Several plans -- any bases,
  * one geometry each, the same calculation type, nq <= 1024 -- executed

@@ -32,7 +32,7 @@ EXPORTS = sorted([
     "thistle_plan_set_centres_batch", "thistle_plan_execute_batch", "thistle_plan_execute_batch_device",
     "thistle_plan_vjp_batch", "thistle_plan_vjp_batch_device", "thistle_plan_use_graph",
     "thistle_plan_autotune_batch", "thistle_batch_create", "thistle_batch_use_graph", "thistle_batch_execute",
-    "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy",
+    "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy", "thistle_plan_nuclear",
 ])
 
 
@@ -110,7 +110,7 @@ def lib():
                        ("thistle_batch_create", [C.POINTER(VP), C.POINTER(VP), C.c_int32]),
                        ("thistle_batch_use_graph", [VP, C.c_int32]), ("thistle_batch_execute", [VP, D]),
                        ("thistle_batch_execute_device", [VP, VP]), ("thistle_batch_info", [VP, I64]),
-                       ("thistle_batch_destroy", [VP])):
+                       ("thistle_batch_destroy", [VP]), ("thistle_plan_nuclear", [VP, D, D, C.c_int32, D])):
         getattr(L, name).restype = C.c_int
         getattr(L, name).argtypes = args
     L.thistle_qcoord3.restype = C.c_int

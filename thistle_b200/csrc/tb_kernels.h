@@ -162,6 +162,10 @@ cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Arg
                                 int64_t blocks, cudaStream_t st);
 int64_t stage1_item_blocks(int L, bool xk, int64_t n);
 cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);
+// nuclear-electron records of items a | gi << 16 | gk << 40 in [a.qbegin, a.qend)
+// of pair order L (tb_nuclear.cu); nucrec holds [R_a, 0, Zn_a, 0, 0, 0] per nucleus
+cudaError_t launch_nuclear(int L, const Stage1Args &a, const uint64_t *items, const double *nucrec,
+                           cudaStream_t st);
 // the same sub-range of one geometry as two kernels through xbuf (at least
 // (qend - qbegin) * nout * ntuv(LK) doubles; nout = most outer function pairs)
 template <int K>

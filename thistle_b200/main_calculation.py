@@ -26,6 +26,8 @@ TOTAL_J0 = 1
 ELASTIC_J0 = 2
 TOTAL_ALIGNED = 3
 TOTAL_J2 = 7
+TOTAL_ELECTRON = 5
+ELASTIC_ELECTRON = 6
 
 
 def read_twordm(filename):
@@ -49,7 +51,13 @@ def read_onerdm(filename):
 def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
                                  mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=None, total=None,
                                  onerdm=None):
-    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 7 total j2).
+    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 5 total electron,
+    6 elastic electron, 7 total j2).
+
+    Types 5 and 6 return I_e - 2 Ine + Inn (I_e the total or elastic j0
+    intensity, Ine the nuclear-electron term, Inn the nuclear-nuclear sinc
+    sum) and need ``Zn`` (natoms,), ``geom`` (natoms, 3) and ``onerdm``; type
+    5 also the 2-RDM rows.
 
     Type 3 runs on the reference's QCOORD3 grid (``nq`` must be 3131; ``q``
     is not read): ``q_abs`` is |q| of the grid vectors and ``result`` the real
@@ -73,8 +81,13 @@ def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng,
     one = colmajor_f64(onerdm) if onerdm is not None else None
     nmo1 = 0 if onerdm is None else int(np.asarray(onerdm).shape[0])
     Zn = _abi.as_f64(Zn) if Zn is not None else None
-    geom = colmajor_f64(geom) if geom is not None else None
-    natoms = 0 if geom is None else int(np.asarray(geom).shape[0]) if np.asarray(geom).ndim == 2 else 0
+    natoms = 0
+    if geom is not None:
+        geom = np.asarray(geom, dtype=np.float64).reshape(-1, 3)
+        natoms = int(geom.shape[0])
+        if Zn is not None and Zn.size != natoms:
+            raise ValueError(f"{Zn.size} nuclear charges for {natoms} atoms")
+        geom = colmajor_f64(geom)
     q_abs = np.zeros(int(nq))
     result = np.zeros(int(nq))
     rc = _abi.lib().thistle_total_scattering(
@@ -168,6 +181,15 @@ class ScatteringPlan:
         g = np.zeros((self.ng, 3))
         check(_abi.lib().thistle_plan_vjp(self._p, dptr(v), dptr(g)))
         return g
+
+    def nuclear(self, Zn, geom):
+        """Elastic plans: the nuclear-electron term Ine(q) for nuclei at geom
+        (natoms, 3) with charges Zn, at the plan's current centres."""
+        Zn = _abi.as_f64(Zn)
+        g = colmajor_f64(np.asarray(geom, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(self.nq)
+        check(_abi.lib().thistle_plan_nuclear(self._p, dptr(Zn), dptr(g), int(Zn.size), dptr(out)))
+        return out
 
     def vjp_device(self, v_ptr: int, grad_ptr: int):
         """Device pointers (nq and 3 ng doubles), on the plan's stream."""
@@ -354,13 +376,16 @@ def aligned(prob, qvec=None):
         return pl.execute_aligned()
 
 
-def scattering(prob, type=TOTAL_J0, q=None):
-    """I(q) of an :class:`thistle_b200.inputs.Problem` through Entry 1."""
+def scattering(prob, type=TOTAL_J0, q=None, Zn=None):
+    """I(q) of an :class:`thistle_b200.inputs.Problem` through Entry 1
+    (types 5 and 6: nuclei at ``prob.atoms`` with charges ``Zn``)."""
     qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
+    two = type in (TOTAL_J0, TOTAL_J2, TOTAL_ELECTRON)
+    one = type in (ELASTIC_J0, TOTAL_ELECTRON, ELASTIC_ELECTRON)
     _, res = total_scattering_calculation(
-        type, None, prob.atoms, 0, 0, int(max(prob.l.max(), prob.m.max(), prob.n.max())), prob.ngto, prob.ng,
+        type, Zn, prob.atoms, 0, 0, int(max(prob.l.max(), prob.m.max(), prob.n.max())), prob.ngto, prob.ng,
         prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.mmod, qv, qv.size, prob.group,
         prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
-        mat=prob.mat if type != ELASTIC_J0 else None, total=prob.total if type != ELASTIC_J0 else None,
-        onerdm=prob.onerdm if type == ELASTIC_J0 else None)
+        mat=prob.mat if two else None, total=prob.total if two else None,
+        onerdm=prob.onerdm if one else None)
     return res
