@@ -222,7 +222,9 @@ int thistle_plan_stage_totals(thistle_plan *plan, double *ms4, int64_t *nexec);
  * class c < *ncls (at most 20 classes; the arrays need that room): quartets
  * [cls_begin[c], cls_end[c]) in class order, their records at cls_recoff[c]
  * doubles with stride cls_rs[c].  A record is [H, 1/4p+1/4p', kind (0 Bessel
- * j0, 1 Bessel j2, 2 P=Q polynomial in q^2), order, coefficients...]. */
+ * j0, 1 Bessel j2, 2 P=Q polynomial in q^2), order, coefficients...].
+ * Total, elastic and j2 plans only: aligned plans hold Hermite densities
+ * instead and return THISTLE_ERR_TYPE. */
 int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32_t *ncls,
                          int64_t *cls_begin, int64_t *cls_end, int64_t *cls_recoff,
                          int32_t *cls_rs, const double **q_dev);
@@ -253,9 +255,14 @@ int thistle_device_cache_bytes(int64_t *cached, int64_t *in_use);
  * points), so nq is limited to 1024 per call; larger nq is rejected with
  * THISTLE_ERR_ARG.  The first call on a device looks up that array's device
  * address (cudaGetSymbolAddress) with the device current; make that first call
- * before any stream capture.  All calls on a device share the array and it
+ * before any stream capture.  The address is kept for the life of the
+ * process: a cudaDeviceReset (or anything else that destroys the device's
+ * primary context) makes it stale, so do not call this entry point on a
+ * device after resetting it.  All calls on a device share the array and it
  * keeps the last call's contents: calls that overlap on the GPU (different
- * streams, or threads) race and must be serialised by the caller.
+ * streams, or threads) race and must be serialised by the caller.  The class
+ * table must start at quartet 0 (cls_begin[0] == 0) and its ranges must be
+ * contiguous; otherwise THISTLE_ERR_SHAPE.
  */
 int thistle_bessel_sum_static(const double *rec_dev, int32_t ncls, const int64_t *cls_begin,
                               const int64_t *cls_end, const int64_t *cls_recoff,

@@ -99,3 +99,18 @@ def test_rdm_index_out_of_range_rejected(h2):
 
 def test_elastic_needs_onerdm(h2):
     assert code_of(lambda: _call(h2, type=2, onerdm=None)) == -1
+
+
+def test_static_bessel_sum_rejects_table_not_starting_at_zero():
+    """thistle_bessel_sum_static walks quartets from 0: a class table whose
+    first range starts later is rejected before any device work."""
+    import ctypes as C
+    b = np.array([5], np.int64)
+    e = np.array([9], np.int64)
+    o = np.zeros(1, np.int64)
+    s = np.full(1, 8, np.int32)
+    rc = _abi.lib().thistle_bessel_sum_static(
+        C.c_void_p(8), 1, b.ctypes.data_as(_abi.I64), e.ctypes.data_as(_abi.I64), o.ctypes.data_as(_abi.I64),
+        s.ctypes.data_as(_abi.I32), C.c_void_p(8), 16, C.c_void_p(8), C.c_void_p(0))
+    assert rc == -2
+    assert b"quartet 0" in _abi.lib().thistle_last_error_string()

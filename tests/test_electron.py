@@ -102,3 +102,12 @@ def test_electron_rejects_mismatched_nuclei():
     p = I.config1_h2()
     with pytest.raises((ThistleError, ValueError)):
         MC.scattering(p, 6, Zn=np.ones(3))
+
+
+@pytest.mark.gpu
+def test_plan_nuclear_rejects_short_geometry():
+    from thistle_b200 import main_calculation as MC
+    p = I.config1_h2()
+    with MC.ScatteringPlan.from_problem(p, MC.ELASTIC_J0) as pl:
+        with pytest.raises(ValueError):
+            pl.nuclear(np.ones(2), p.atoms[:1])

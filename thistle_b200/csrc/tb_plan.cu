@@ -1917,6 +1917,8 @@ int thistle_plan_records(const thistle_plan *P, const double **rec_dev, int32_t 
                          int64_t *cls_end, int64_t *cls_recoff, int32_t *cls_rs, const double **q_dev) {
   if (!P || !rec_dev || !ncls || !cls_begin || !cls_end || !cls_recoff || !cls_rs || !q_dev)
     return fail(THISTLE_ERR_ARG, "null argument");
+  if (P->kind == KIND_ALIGNED)
+    return fail(THISTLE_ERR_TYPE, "aligned plans hold Hermite-density records, not Bessel-sum records");
   *rec_dev = P->d_rec;
   *q_dev = P->d_q;
   *ncls = P->ncls;

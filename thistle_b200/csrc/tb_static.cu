@@ -36,6 +36,10 @@ extern "C" int thistle_bessel_sum_static(const double *rec_dev, int32_t ncls, co
   if (nq < 1 || nq > kStaticMaxQ)
     return tb::set_error(THISTLE_ERR_ARG, "nq = " + std::to_string(nq) + " exceeds the static scratch (at most " +
                                               std::to_string(kStaticMaxQ) + " q points per call)");
+  // the stage-2 kernel walks quartets 0 .. cls_end[ncls-1]: the table must start at 0
+  if (cls_begin[0] != 0)
+    return tb::set_error(THISTLE_ERR_SHAPE, "the first class must begin at quartet 0 (cls_begin[0] = " +
+                                                std::to_string(cls_begin[0]) + ")");
   int64_t nquart = 0;
   for (int c = 0; c < ncls; ++c) {
     if (cls_begin[c] < 0 || cls_end[c] < cls_begin[c] || (c > 0 && cls_begin[c] != cls_end[c - 1]) ||

@@ -186,7 +186,10 @@ class ScatteringPlan:
         """Elastic plans: the nuclear-electron term Ine(q) for nuclei at geom
         (natoms, 3) with charges Zn, at the plan's current centres."""
         Zn = _abi.as_f64(Zn)
-        g = colmajor_f64(np.asarray(geom, dtype=np.float64).reshape(-1, 3))
+        g3 = np.asarray(geom, dtype=np.float64).reshape(-1, 3)
+        if g3.shape[0] != Zn.size:
+            raise ValueError(f"geom has {g3.shape[0]} atoms, Zn {Zn.size}")
+        g = colmajor_f64(g3)
         out = np.zeros(self.nq)
         check(_abi.lib().thistle_plan_nuclear(self._p, dptr(Zn), dptr(g), int(Zn.size), dptr(out)))
         return out
