@@ -133,30 +133,62 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(p, target_s: float = 12.0, seed: int = 11):
-    """The oracle (C restatement of the reference's loops and per-quartet dgemm)
-    on a random sample of the workload's quartets, all host threads."""
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def llmax_of_quartets(p, qs):
+    heads = np.searchsorted(p.group, np.arange(1, p.ng + 1))
+    gl = (p.l + p.m + p.n)[heads]
+    return gl[qs[:, 0]] + gl[qs[:, 1]] + gl[qs[:, 2]] + gl[qs[:, 3]]
+
+
+def stratified_indices(L, frac, rng):
+    """A proportional sample stratified by LLmax class: round(frac x class
+    size) quartets of every class (at least one), so the sample's mix of
+    classes is the workload's and its rate estimates the whole run's."""
+    pick = []
+    for LL in np.unique(L):
+        idx = np.flatnonzero(L == LL)
+        k = max(1, int(round(frac * idx.size)))
+        pick.append(rng.choice(idx, size=min(k, idx.size), replace=False))
+    return np.sort(np.concatenate(pick))
+
+
+def cpu_baseline(p, target_s: float = 15.0, seed: int = 11):
+    """The oracle (C restatement of the reference's five loops with its
+    per-quartet dgemm contraction of the 2-RDM rows, dphrec Bessel functions)
+    on a sample of the workload's quartets stratified by LLmax class, all host
+    threads; the rate is extrapolated to the whole workload."""
     from oracle import oracle as O
     ncores = os.cpu_count() or 1
     qs = O.enum_quartets(p.ng)
+    L = llmax_of_quartets(p, qs)
     rng = np.random.default_rng(seed)
-    order = rng.permutation(len(qs))
-    n = 8
-    t_per = None
+    frac = 2e-5
     while True:
-        sample = qs[np.sort(order[:n])]
+        idx = stratified_indices(L, frac, rng)
         t0 = time.perf_counter()
-        O.scattering(p, 1, quartets=sample, nthreads=ncores)
+        O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
         dt = time.perf_counter() - t0
-        t_per = dt / n
-        if dt >= target_s or n >= len(qs):
+        if dt >= 0.5 * target_s or frac >= 1.0:
             break
-        n = int(min(len(qs), max(2 * n, target_s / max(t_per, 1e-6) * 1.05)))
+        frac = min(1.0, frac * max(2.0, 1.05 * target_s / max(dt, 1e-3)))
+    n = idx.size
     value = n * p.nq / dt
-    return {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
-            "sample": f"{n} of {len(qs)} group quartets drawn uniformly at random (seed {seed}), all {p.nq} q; "
-                      f"{dt:.1f} s on {ncores} host threads; oracle/thistle_oracle.c restating "
-                      f"tot_integration with its per-quartet dgemm"}
+    return {"value": value, "unit": UNIT, "cores": ncores, "cpu_model": cpu_model(), "kind": "port",
+            "extrapolated": True,
+            "sample": f"{n} of {len(qs)} group quartets ({100 * n / len(qs):.3f} %), stratified by LLmax class "
+                      f"in proportion to the class sizes (seed {seed}), all {p.nq} q; {dt:.1f} s on {ncores} host "
+                      f"threads ({cpu_model()}); oracle/thistle_oracle.c restating tot_integration with the "
+                      f"per-quartet dgemm of the 2-RDM rows (the reference's transform) inside every quartet; "
+                      f"rate extrapolated to all quartets"}
 
 
 def run_reference(args, rank, world):
@@ -166,34 +198,41 @@ def run_reference(args, rank, world):
     p = workload()
     ncores = os.cpu_count() or 1
     qs = O.enum_quartets(p.ng)
+    L = llmax_of_quartets(p, qs)
     rng = np.random.default_rng(17)
-    # each step a random sample of about two seconds of work on all host
-    # threads, sized from a first untimed call
-    per_step = 256
-    idx = np.sort(rng.choice(len(qs), size=per_step, replace=False))
+    # each step a sample stratified by LLmax class (in proportion to the class
+    # sizes) of about two seconds of work on all host threads, sized from a
+    # first untimed call
+    frac = 2e-5
+    idx = stratified_indices(L, frac, rng)
     t0 = time.perf_counter()
     O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
-    per_step = int(min(len(qs), max(256, per_step * 2.0 / max(time.perf_counter() - t0, 1e-3))))
-    times = []
+    frac = min(1.0, frac * 2.0 / max(time.perf_counter() - t0, 1e-3))
+    times, counts = [], []
     for s in range(args.warmup + args.steps):
-        idx = np.sort(rng.choice(len(qs), size=per_step, replace=False))
+        idx = stratified_indices(L, frac, rng)
         t0 = time.perf_counter()
         O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             times.append(dt)
+            counts.append(idx.size)
     tot = sum(times)
-    value = per_step * p.nq * len(times) / tot
+    per_step = int(np.mean(counts))
+    value = sum(counts) * p.nq / tot
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded; BASELINE configuration 3 shapes)",
         "config": {"workload": workload_config(p, len(qs))["workload"],
-                   "sample_per_step": f"{per_step} random group quartets x {p.nq} q"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
-                         "sample": f"{per_step} random group quartets per step, {ncores} host threads; the C "
-                                   f"restatement of tot_integration (no Fortran compiler on this image)"},
+                   "sample_per_step": f"about {per_step} group quartets x {p.nq} q, stratified by LLmax "
+                                      f"class in proportion to the class sizes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "cpu_model": cpu_model(), "kind": "port",
+                         "extrapolated": True,
+                         "sample": f"about {per_step} group quartets per step stratified by LLmax class, {ncores} "
+                                   f"host threads ({cpu_model()}); the C restatement of tot_integration with its "
+                                   f"per-quartet dgemm (no Fortran compiler on this image)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -241,6 +280,11 @@ def e2e_entry1(p, steps, warmup):
 
 
 def run_fit(args):
+    print(json.dumps(fit6_section(args.fit_geometries, args.fit_plain, args.fit_gmax)), flush=True)
+    return 0
+
+
+def fit6_section(ngeom_total, nplain_max, gmax):
     """Configuration 5: a 6-atom ring (configuration-2 basis per atom, 30 MOs,
     dense 2-RDM, 400 q) at 512 geometries; per geometry the forward I(q) and
     the adjoint dLoss/dR for Loss = sum_q (I(q; R) - I_ref(q))^2.  The plain
@@ -252,7 +296,7 @@ def run_fit(args):
     from thistle_b200 import main_calculation as MC
     torch.cuda.set_device(0)
     p = I.config5_fit()
-    geos = I.config5_geometries(p, args.fit_geometries)
+    geos = I.config5_geometries(p, ngeom_total)
     probs = [p.with_geometry(R) for R in geos]
     xyz = np.stack([np.stack([q.xx, q.yy, q.zz], axis=1) for q in probs])
     ng = len(probs)
@@ -260,7 +304,7 @@ def run_fit(args):
         iref = pl.execute()
         nquart = pl.info()["nquart"]
         # plain per-geometry path
-        nplain = min(ng, args.fit_plain)
+        nplain = min(ng, nplain_max)
         for k in range(3):
             pl.set_centres(*xyz[k].T)
             I0 = pl.execute()
@@ -275,7 +319,7 @@ def run_fit(args):
         t_plain = (time.perf_counter() - t0) / nplain
         # batched path
         pl.use_graph(True)
-        G, qt, gps_tune = pl.autotune_batch(args.fit_gmax)
+        G, qt, gps_tune = pl.autotune_batch(gmax)
         nb = (ng + G - 1) // G
         gbuf = np.zeros((nb * G, p.ng, 3))
         ibuf = np.zeros((nb * G, p.nq))
@@ -313,11 +357,16 @@ def run_fit(args):
         "check_vs_plain": {"I_rel": err_i, "grad_rel": err_g},
         "path": "host arrays in and out per batch (set_centres_batch, execute_batch, vjp_batch)",
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_batch4(args):
+    print(json.dumps(batch4_section(args.batch_molecules, args.batch_chunk, args.batch_gb, args.steps)),
+          flush=True)
+    return 0
+
+
+def batch4_section(nmol, chunk, gb, reps_arg):
     """Configuration 4: uneven molecules (2-12 atoms, s4p2d1 per atom, 4-24
     MOs, sparse 2-RDMs, total j0 on 256 q).  Molecules are taken in chunks that
     fit the device; per chunk every molecule gets its plan (density transform,
@@ -333,9 +382,9 @@ def run_batch4(args):
     import ctypes as C
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    mols = I.config4_batch(nmol=args.batch_molecules)
+    mols = I.config4_batch(nmol=nmol)
     t_gen = time.perf_counter() - t0
-    budget = args.batch_gb * 1e9
+    budget = gb * 1e9
     t_setup = t_plain = t_batch = 0.0
     qq = 0
     nchunks, launches, err = 0, [], 0.0
@@ -343,7 +392,7 @@ def run_batch4(args):
     while i < len(mols):
         plans = []
         cached, used = C.c_int64(0), C.c_int64(0)
-        while i < len(mols) and len(plans) < args.batch_chunk:
+        while i < len(mols) and len(plans) < chunk:
             t0 = time.perf_counter()
             pl = MC.ScatteringPlan.from_problem(mols[i], MC.TOTAL_J0)
             pl.execute()  # first execution allocates the records
@@ -367,7 +416,7 @@ def run_batch4(args):
             for _ in range(2):
                 b.execute()
             torch.cuda.synchronize()
-            reps = max(1, args.steps)
+            reps = max(1, reps_arg)
             t0 = time.perf_counter()
             for _ in range(reps):
                 out = b.execute()
@@ -384,7 +433,7 @@ def run_batch4(args):
         "data": "synthetic (seeded; BASELINE configuration 4 shapes)",
         "config": {"workload": f"batch4: {n} molecules of 2-12 atoms, s(4)+p(2)+d(1) per atom, 4-24 MOs, "
                                f"sparse 2-RDMs (1-10 %), 256 q", "chunks": nchunks,
-                   "max_molecules_per_chunk": args.batch_chunk, "chunk_budget_gb": args.batch_gb},
+                   "max_molecules_per_chunk": chunk, "chunk_budget_gb": gb},
         "plain_molecules_per_s": n / t_plain, "batched_over_plain": t_plain / t_batch,
         "quartet_q_per_s_batched": qq / t_batch, "quartet_q_per_s_plain": qq / t_plain,
         "setup_s_per_molecule": t_setup / n, "input_generation_s": t_gen,
@@ -392,8 +441,64 @@ def run_batch4(args):
         "path": "integrator only, from plans already built; host I(q) out (MoleculeBatch.execute vs "
                 "ScatteringPlan.execute per molecule)",
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+def bench_extras(args, p, plan, stream, stage1_ms, peak_tf, fwd_ms):
+    """The rest of the benchmark metric on one GPU, after the timed forward
+    steps: the adjoint of the same AB6 step, the stage-1 roofline, and the
+    batched-versus-plain comparisons of configurations 5 (forward + adjoint
+    over geometries) and 4 (uneven molecules)."""
+    import torch
+    out = {}
+    # adjoint: sum_q v(q) dI(q)/dA for the 98 group centres, forward records valid
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    v = torch.randn(p.nq, dtype=torch.float64, device="cuda", generator=g)
+    grad = torch.empty(3 * p.ng, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        plan.vjp_device(v.data_ptr(), grad.data_ptr())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.vjp_device(v.data_ptr(), grad.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    adj_ms = e0.elapsed_time(e1) / args.steps
+    out["ab6_adjoint"] = {
+        "ms": adj_ms, "forward_plus_adjoint_ms": fwd_ms + adj_ms,
+        "geometries_per_s_forward_plus_adjoint": 1e3 / (fwd_ms + adj_ms),
+        "what": "thistle_plan_vjp_device: sum_q v(q) dI(q)/dA for all 98 group centres (21 nuclear "
+                "coordinates), CUDA events over the timed adjoint calls, forward records of the same centres",
+        "steps": args.steps, "grad_finite": bool(torch.isfinite(grad).all().item())}
+    # stage 1 against its algorithmic FLOPs (counted once by the oracle, oracle/stage1_flops.py)
+    prof = os.path.join(ROOT, "profiles", "stage1_ab6_flops.json")
+    if WORKLOAD == "ab6" and os.path.exists(prof):
+        fl = json.load(open(prof))["flops_per_step"]
+        npair = p.ngto * (p.ngto + 1) // 2
+        tf = fl / (stage1_ms * 1e-3) / 1e12
+        out["roofline_stage1"] = {
+            "bound": "fp64", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": tf / peak_tf if peak_tf > 0 else None, "kernel_ms": stage1_ms, "flops_per_step": fl,
+            "flops_basis": "F_E = 2 (LLmax+1) T_E per quartet (2 T_E on the P = Q branch), T_E counted by the "
+                           "oracle under the same cutoffs (profiles/stage1_ab6_flops.json)",
+            "rho_unique_half_bytes": 8 * npair * (npair + 1) // 2,
+            "hbm_floor_ms": 8 * npair * (npair + 1) / 2 / 6524e9 * 1e3}
+    t0 = time.perf_counter()
+    out["fit6"] = fit6_section(args.extra_fit_geometries, 16, 64)
+    out["fit6"]["section_s"] = time.perf_counter() - t0
+    out["fit6"]["config"]["reduction"] = (f"{args.extra_fit_geometries} of the configuration's 512 geometries, "
+                                          f"16 timed on the plain path, so the default run stays short; "
+                                          f"bench.py --workload fit6 runs all 512")
+    t0 = time.perf_counter()
+    out["batch4"] = batch4_section(args.extra_batch_molecules, 128, 60.0, 3)
+    out["batch4"]["section_s"] = time.perf_counter() - t0
+    out["batch4"]["config"]["reduction"] = (f"the first {args.extra_batch_molecules} of the configuration's 1024 "
+                                            f"seeded molecules, so the default run stays short; bench.py "
+                                            f"--workload batch4 runs all 1024")
+    return out
 
 
 def main():
@@ -408,6 +513,10 @@ def main():
                     help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis; "
                          "fit6: batched forward + adjoint over geometries (configuration 5); "
                          "batch4: uneven molecule batches (configuration 4)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the AB6 adjoint, stage-1 roofline, fit6 and batch4 keys of the default line")
+    ap.add_argument("--extra-fit-geometries", type=int, default=128)
+    ap.add_argument("--extra-batch-molecules", type=int, default=256)
     ap.add_argument("--fit-geometries", type=int, default=512)
     ap.add_argument("--fit-plain", type=int, default=32, help="geometries timed on the plain path")
     ap.add_argument("--fit-gmax", type=int, default=64)
@@ -502,6 +611,10 @@ def main():
                 "flops_per_launch": flops,
                 "peak_source": "measured FP64 FMA rate of this GPU (thistle_probe_fp64_peak, in this run)"}
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = bench_extras(args, p, plan, stream, st["stage1"] / n2, peak_tf, ms / args.steps)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -514,6 +627,7 @@ def main():
         "clocks": clocks,
         "sum_rule_check": float(result[0] / (p.nelec * (p.nelec - 1) * (float(np.float32(np.pi)) / np.pi) ** 3)),
     }
+    line.update(extras)
     if rank == 0:
         if args.e2e_steps > 0:
             dt_e2e, res_e2e = e2e_entry1(p, args.e2e_steps, 1)

@@ -49,9 +49,52 @@ def enum_quartets(ng: int) -> np.ndarray:
     return out
 
 
+def pair_density(prob) -> np.ndarray:
+    """The per-quartet contraction ztot of the 2-RDM rows, for every pair of
+    function pairs at once: rho[P(x,y), P(u,v)] = 1/8 sum_t [z11(t,x,y)
+    z22(t,u,v) + z22(t,x,y) z11(t,u,v)] with z11, z22 of variables_total
+    (src/Variables.f90:1045-1065) and P(x,y) = max(x,y)(max+1)/2 + min(x,y).
+
+    The rows enter through their eight index placements summed into a dense
+    MO-space array G[a,b,c,d] (each row adds total/8 at (m1,m2,m3,m4),
+    (m2,m1,m3,m4), (m1,m2,m4,m3), (m2,m1,m4,m3) and the four with the pairs
+    exchanged), then four contractions with the MO coefficients.  This is the
+    same quantity as the reference's per-quartet dgemm pair
+    (src/Integrals.f90:109-127) in another summation order; tests compare the
+    two modes of the oracle on configurations 1-3.  Returns (np, np)."""
+    n, ngto = prob.mmod.shape
+    C = np.asarray(prob.mmod, dtype=np.float64)
+    m = np.asarray(prob.mat, dtype=np.int64) - 1
+    v = np.asarray(prob.total, dtype=np.float64) / 8.0
+    m1, m2, m3, m4 = m[:, 0], m[:, 1], m[:, 2], m[:, 3]
+    G = np.zeros((n, n, n, n))
+    for (a, b, c, d) in ((m1, m2, m3, m4), (m2, m1, m3, m4), (m1, m2, m4, m3), (m2, m1, m4, m3),
+                         (m3, m4, m1, m2), (m4, m3, m1, m2), (m3, m4, m2, m1), (m4, m3, m2, m1)):
+        np.add.at(G, (a, b, c, d), v)
+    # x: first function of the bra pair, y second, u, v the ket pair
+    T = np.tensordot(C, G, axes=([0], [0]))            # (x, b, c, d)
+    T = np.tensordot(T, C, axes=([1], [0]))            # (x, c, d, y)
+    T = np.ascontiguousarray(T.transpose(0, 3, 1, 2))  # (x, y, c, d)
+    r, c_ = np.tril_indices(ngto)
+    V = T[r, c_]                                       # (np, c, d), P(x,y) with x >= y
+    del T
+    npair = r.size
+    out = np.empty((npair, npair))
+    blk = max(1, int(2.0e8 // max(1, ngto * ngto)))
+    for s0 in range(0, npair, blk):
+        W = np.tensordot(V[s0:s0 + blk], C, axes=([1], [0]))   # (blk, d, u)
+        W = np.tensordot(W, C, axes=([1], [0]))                # (blk, u, v)
+        out[s0:s0 + blk] = W[:, r, c_]
+    return out
+
+
 def scattering(prob, type_: int = 1, *, bessel_mode: int = 0, nthreads: int = 0,
-               quartets=None, weights=None, q=None) -> np.ndarray:
-    """Reference restatement of total_scattering_calculation_2 (types 1, 2, 7)."""
+               quartets=None, weights=None, q=None, rho=None) -> np.ndarray:
+    """Reference restatement of total_scattering_calculation_2 (types 1, 2, 7).
+
+    rho: optional ``pair_density(prob)`` for types 1 and 7; the per-quartet
+    contraction of the 2-RDM rows is then read from it (the rest of the
+    evaluation is unchanged)."""
     keep = []
 
     def d(x):
@@ -76,13 +119,19 @@ def scattering(prob, type_: int = 1, *, bessel_mode: int = 0, nthreads: int = 0,
     else:
         qptr, nqt = None, 0
     wptr = d(weights) if weights is not None else None
-    rc = lib().orc_scattering(
+    rptr = None
+    if rho is not None and type_ != 2:
+        npair = prob.ngto * (prob.ngto + 1) // 2
+        if rho.shape != (npair, npair):
+            raise ValueError("rho must be pair_density(prob)")
+        rptr = d(rho)
+    rc = lib().orc_scattering_ex(
         C.c_int(type_), C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n),
         d(prob.xx), d(prob.yy), d(prob.zz), i(prob.group), d(mmod_cm), C.c_int(prob.nmo),
         i(mat_cm), d(prob.total), C.c_int(prob.mat.shape[0]), d(one_cm), C.c_int(prob.onerdm.shape[0]),
         d(qv), C.c_int(nq), C.c_double(prob.cutoffz), C.c_double(prob.cutoffmd),
         C.c_double(prob.cutoffcentre), C.c_int(bessel_mode), C.c_int(nthreads),
-        qptr, C.c_long(nqt), wptr, out.ctypes.data_as(C.POINTER(C.c_double)))
+        qptr, C.c_long(nqt), wptr, rptr, out.ctypes.data_as(C.POINTER(C.c_double)))
     if rc != 0:
         raise RuntimeError(f"oracle orc_scattering failed with code {rc}")
     return out
@@ -115,6 +164,39 @@ def aligned(prob, qal: np.ndarray, *, nthreads: int = 0):
     if rc != 0:
         raise RuntimeError(f"oracle orc_aligned failed with code {rc}")
     return re, im
+
+
+def aligned_list(prob, qal: np.ndarray, *, quartets=None, rho=None, nthreads: int = 0) -> np.ndarray:
+    """Real part of the aligned intensity as the weighted sum over the five
+    loops' quartet list (default: all of them) instead of all ng^4 ordered
+    quartets; see orc_aligned_list.  rho as in ``scattering``."""
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qal = np.ascontiguousarray(qal, dtype=np.float64).reshape(-1, 3)
+    nq = qal.shape[0]
+    qs = enum_quartets(prob.ng) if quartets is None else np.ascontiguousarray(quartets, dtype=np.int32)
+    re = np.zeros(nq)
+    mat_cm = np.asfortranarray(prob.mat.astype(np.int32)).ravel(order="F")
+    mmod_cm = np.asfortranarray(prob.mmod).ravel(order="F")
+    rc = lib().orc_aligned_list(
+        C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n), d(prob.xx), d(prob.yy),
+        d(prob.zz), i(prob.group), d(mmod_cm), C.c_int(prob.nmo), i(mat_cm), d(prob.total),
+        C.c_int(prob.mat.shape[0]), d(rho) if rho is not None else None, d(qal), C.c_int(nq), i(qs),
+        C.c_long(qs.shape[0]), C.c_double(prob.cutoffz), C.c_double(prob.cutoffmd), C.c_int(nthreads),
+        re.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_aligned_list failed with code {rc}")
+    return re
 
 
 def qcoord3(k0: float = 10.583544175):
@@ -221,3 +303,36 @@ def electron(prob, type_: int, Zn, *, bessel_mode: int = 1, nthreads: int = 0) -
     total (type 5) or elastic (type 6) j0 intensity."""
     Ie = scattering(prob, 1 if type_ == 5 else 2, bessel_mode=bessel_mode, nthreads=nthreads)
     return Ie - 2.0 * nuclear(prob, Zn, bessel_mode=bessel_mode) + nuclear_nuclear(prob, Zn)
+
+
+def count_te(prob, quartets=None, *, rho=None, nthreads: int = 0):
+    """Per listed quartet (default: the five loops' list) the number T_E of
+    innermost Hermite-product updates of tot_integral_k_ijkr that pass both
+    cutoffs, and whether the quartet takes the P = Q branch (whose
+    tot_integral_ijkr_pzero terms are counted instead).  Returns (te, is_p0)."""
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qs = enum_quartets(prob.ng) if quartets is None else np.ascontiguousarray(quartets, dtype=np.int32)
+    te = np.zeros(qs.shape[0], dtype=np.int64)
+    p0 = np.zeros(qs.shape[0], dtype=np.int32)
+    mat_cm = np.asfortranarray(prob.mat.astype(np.int32)).ravel(order="F")
+    mmod_cm = np.asfortranarray(prob.mmod).ravel(order="F")
+    rc = lib().orc_count_te(
+        C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n), d(prob.xx), d(prob.yy), d(prob.zz),
+        i(prob.group), d(mmod_cm), C.c_int(prob.nmo), i(mat_cm), d(prob.total), C.c_int(prob.mat.shape[0]),
+        d(rho) if rho is not None else None, C.c_double(prob.cutoffz), C.c_double(prob.cutoffmd),
+        C.c_double(prob.cutoffcentre), i(qs), C.c_long(qs.shape[0]), C.c_int(nthreads),
+        te.ctypes.data_as(C.POINTER(C.c_long)), p0.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_count_te failed with code {rc}")
+    return te, p0.astype(bool)

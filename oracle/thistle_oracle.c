@@ -592,6 +592,11 @@ typedef struct {
     const double *total;
     const double *mmod;            /* (nmo, ngto) column-major */
     double *zao;                   /* elastic Z (ngto, ngto) column-major */
+    /* optional: the contracted density already summed over the rows,
+     * rho[P(x,y) * np + P(u,v)] = ztot for functions x,y (electron 1) and
+     * u,v (electron 2), P(x,y) = max(x,y)(max(x,y)+1)/2 + min(x,y) */
+    const double *rho;
+    long np;
 } dens_t;
 
 #define MMOD(D, a, b) ((D)->mmod[(a) + (size_t)(D)->nmo * (b)])
@@ -610,9 +615,25 @@ static void zvec(const dens_t *D, int x, int y, double *z1, double *z2) {
  * zcontrred(a,b,jj,ii)  = 1/8 sum_t z1(t,j'_a,i'_ii) z2(t,k'_b,r'_jj)
  * zcontrred2(jj,ii,a,b) = 1/8 sum_t z2(t,j'_a,i'_ii) z1(t,k'_b,r'_jj)
  * (the dgemm pairs of src/Integrals.f90:109-127 and the four other loops). */
+static long pair_index(int x, int y) {
+    return x >= y ? (long)x * (x + 1) / 2 + y : (long)y * (y + 1) / 2 + x;
+}
+
 static void build_total_block(const setup_t *S, const dens_t *D, int gi, int gj, int gk, int gr,
                               double *zblk, double *buf) {
     int si = S->gc[gi], sj = S->gc[gj], sk = S->gc[gk], sr = S->gc[gr];
+    if (D->rho) {
+        /* same ztot, read from the summed density */
+        for (int a = 0; a < si; ++a)
+            for (int b = 0; b < sj; ++b) {
+                const double *row = D->rho + (size_t)pair_index(S->gs[gi] - 1 + a, S->gs[gj] - 1 + b) * D->np;
+                for (int c = 0; c < sk; ++c)
+                    for (int d = 0; d < sr; ++d)
+                        zblk[(((size_t)a * sj + b) * sk + c) * sr + d] =
+                            row[pair_index(S->gs[gk] - 1 + c, S->gs[gr] - 1 + d)];
+            }
+        return;
+    }
     size_t nm = D->nmat;
     double *b1 = buf, *b2 = buf + nm * si * sj;
     double *k1 = b2 + nm * si * sj, *k2 = k1 + nm * sk * sr;
@@ -759,7 +780,7 @@ static int run_quartets(const setup_t *S, const dens_t *D, const kopts_t *o, con
 #pragma omp parallel
     {
         double *zblk = malloc(sizeof(double) * zbsz);
-        double *zbuf = o->kind == K_ELASTIC ? NULL : malloc(sizeof(double) * zbuf_sz);
+        double *zbuf = (o->kind == K_ELASTIC || D->rho) ? NULL : malloc(sizeof(double) * zbuf_sz);
         double *work = malloc(sizeof(double) * kernel_work_doubles());
         double *f = malloc(sizeof(double) * nq);
 #pragma omp for schedule(dynamic, 1)
@@ -812,12 +833,38 @@ static void free_dens(dens_t *D) { free(D->m1); free(D->m2); free(D->m3); free(D
  * (i,j,k,r,loop) with 0-based groups, evaluated with the loop's weight, or with
  * weights[c] when weights is non-NULL.  NULL runs the reference's five loops.
  */
+int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const int *m, const int *n,
+                      const double *xx, const double *yy, const double *zz, const int *group,
+                      const double *mmod, int nmo, const int *mat, const double *total, int nmat,
+                      const double *onerdm, int nmo1, const double *q, int nq,
+                      double cutoffz, double cutoffmd, double cutoffcentre, int bessel_mode, int nthreads,
+                      const int *quartets, long nquart, const double *weights, const double *rho,
+                      double *result);
+
 int orc_scattering(int type, int ngto, const double *ga, const int *l, const int *m, const int *n,
                    const double *xx, const double *yy, const double *zz, const int *group,
                    const double *mmod, int nmo, const int *mat, const double *total, int nmat,
                    const double *onerdm, int nmo1, const double *q, int nq,
                    double cutoffz, double cutoffmd, double cutoffcentre, int bessel_mode, int nthreads,
                    const int *quartets, long nquart, const double *weights, double *result) {
+    return orc_scattering_ex(type, ngto, ga, l, m, n, xx, yy, zz, group, mmod, nmo, mat, total, nmat, onerdm,
+                             nmo1, q, nq, cutoffz, cutoffmd, cutoffcentre, bessel_mode, nthreads, quartets,
+                             nquart, weights, NULL, result);
+}
+
+/* The same driver; with rho non-NULL (types 1 and 7) the per-quartet
+ * contraction of the 2-RDM rows (zcontrred, zcontrred2) is read from the
+ * summed pair density instead of being formed from the rows quartet by
+ * quartet: rho[P(x,y) np + P(u,v)] = 1/8 sum_t [z11(t,x,y) z22(t,u,v) +
+ * z22(t,x,y) z11(t,u,v)], np = ngto(ngto+1)/2 (see build_total_block).
+ * Everything after the contraction is unchanged. */
+int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const int *m, const int *n,
+                      const double *xx, const double *yy, const double *zz, const int *group,
+                      const double *mmod, int nmo, const int *mat, const double *total, int nmat,
+                      const double *onerdm, int nmo1, const double *q, int nq,
+                      double cutoffz, double cutoffmd, double cutoffcentre, int bessel_mode, int nthreads,
+                      const int *quartets, long nquart, const double *weights, const double *rho,
+                      double *result) {
     if (type != 1 && type != 2 && type != 7) return ORC_ERR_ARG;
     setup_t S;
     int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, q, nq, type == 7 ? 2 : 1);
@@ -833,6 +880,8 @@ int orc_scattering(int type, int ngto, const double *ga, const int *l, const int
     } else {
         e = build_dens(&D, mmod, nmo, mat, total, nmat);
         if (e != ORC_OK) { free_dens(&D); free_setup(&S); return e; }
+        D.rho = rho;
+        D.np = (long)ngto * (ngto + 1) / 2;
     }
     quartet_t *Qs;
     long nqt;
@@ -970,6 +1019,180 @@ int orc_aligned(int ngto, const double *ga, const int *l, const int *m, const in
         }
     free(part); free(e1r); free(e1i); free(e2r); free(e2i);
     free_dens(&D); free_setup(&S); free(qabs);
+    return ORC_OK;
+}
+
+/*
+ * The aligned intensity of orc_aligned evaluated on a quartet list with
+ * weights instead of all ng^4 ordered quartets, real part only.  Exchanging
+ * the two functions of a pair leaves a term of tot_integration_aligned
+ * unchanged, and exchanging bra and ket conjugates it (H -> -H, (iq)^L <->
+ * (-iq)^L), so the ordered sum equals the sum of w Re f over the five loops'
+ * list with their weights 8,4,4,2,1 (orc_enum_quartets).  Per quartet the
+ * hermite_loop terms of tot_integral_k_ijkr_alig (src/Integrals.f90:5588-5727)
+ * are first summed into D_TUV = sum prod6 (-1)^(ll+mm+nn) at T = ll+llp,
+ * U = mm+mmp, V = nn+nnp, since (iq)^(llp,mmp,nnp) (-iq)^(ll,mm,nn) =
+ * (-1)^(ll+mm+nn) i^(T+U+V) qx^T qy^U qz^V; then f(q) = sum D_TUV
+ * i^(T+U+V) qx^T qy^U qz^V times the three phase factors and E12 E12'.
+ * rho as in orc_scattering_ex (NULL: formed from the rows).
+ */
+typedef struct { double *D; int d; } dtctx_t;
+static void visit_dtuv(void *c, int ll, int mm, int nn, int llp, int mmp, int nnp, double prod6) {
+    dtctx_t *a = (dtctx_t *)c;
+    double sg = ((ll + mm + nn) & 1) ? -1.0 : 1.0;
+    size_t idx = (size_t)(ll + llp) + a->d * ((size_t)(mm + mmp) + a->d * (size_t)(nn + nnp));
+    a->D[idx] = a->D[idx] + sg * prod6;
+}
+
+int orc_aligned_list(int ngto, const double *ga, const int *l, const int *m, const int *n,
+                     const double *xx, const double *yy, const double *zz, const int *group,
+                     const double *mmod, int nmo, const int *mat, const double *total, int nmat,
+                     const double *rho, const double *qal, int nq, const int *quartets, long nquart,
+                     double cutoffz, double cutoffmd, int nthreads, double *result_re) {
+    double *qabs = malloc(sizeof(double) * nq);
+    for (int iq = 0; iq < nq; ++iq)
+        qabs[iq] = sqrt(pow(qal[3 * iq], 2.0) + pow(qal[3 * iq + 1], 2.0) + pow(qal[3 * iq + 2], 2.0));
+    setup_t S;
+    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, qabs, nq, 0);
+    if (e != ORC_OK) { free_setup(&S); free(qabs); return e; }
+    dens_t D;
+    e = build_dens(&D, mmod, nmo, mat, total, nmat);
+    if (e != ORC_OK) { free_dens(&D); free_setup(&S); free(qabs); return e; }
+    D.rho = rho;
+    D.np = (long)ngto * (ngto + 1) / 2;
+    int d = 4 * S.maxl + 1;
+    /* powers qx^t, qy^t, qz^t, t < d, per q vector */
+    double *pw = malloc(sizeof(double) * (size_t)nq * 3 * d);
+    for (int iq = 0; iq < nq; ++iq)
+        for (int ax = 0; ax < 3; ++ax) {
+            double v = 1.0;
+            for (int t = 0; t < d; ++t) { pw[((size_t)iq * 3 + ax) * d + t] = v; v *= qal[3 * iq + ax]; }
+        }
+    const long CH = 16;
+    long nch = (nquart + CH - 1) / CH;
+    double *part = calloc((size_t)(nch > 0 ? nch : 1) * nq, sizeof(double));
+    int mg = max_group(&S);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel
+    {
+        double *zblk = malloc(sizeof(double) * (size_t)mg * mg * mg * mg);
+        double *zbuf = rho ? NULL : malloc(sizeof(double) * (size_t)(nmat > 0 ? nmat : 1) * 4 * mg * mg);
+        double *Dt = malloc(sizeof(double) * (size_t)d * d * d);
+        int *nzi = malloc(sizeof(int) * (size_t)d * d * d * 3);
+        double *nzv = malloc(sizeof(double) * (size_t)d * d * d);
+#pragma omp for schedule(dynamic, 1)
+        for (long ch = 0; ch < nch; ++ch) {
+            double *acc = part + (size_t)ch * nq;
+            for (long c = ch * CH; c < nquart && c < (ch + 1) * CH; ++c) {
+                int i = quartets[5 * c], j = quartets[5 * c + 1], k = quartets[5 * c + 2], r = quartets[5 * c + 3];
+                double w = loop_weight[quartets[5 * c + 4]];
+                double Hx = PX(&S, k, r) - PX(&S, i, j), Hy = PY(&S, k, r) - PY(&S, i, j);
+                double Hz = PZ(&S, k, r) - PZ(&S, i, j);
+                build_total_block(&S, &D, i, j, k, r, zblk, zbuf);
+                zblock_t Z = {S.gc[i], S.gc[j], S.gc[k], S.gc[r], zblk};
+                memset(Dt, 0, sizeof(double) * (size_t)d * d * d);
+                dtctx_t dc = {Dt, d};
+                hermite_loop(&S, i, j, k, r, DDP(&S, S.ddx, j, i), DDP(&S, S.ddy, j, i), DDP(&S, S.ddz, j, i),
+                             DDP(&S, S.ddx, r, k), DDP(&S, S.ddy, r, k), DDP(&S, S.ddz, r, k), &Z,
+                             cutoffz, cutoffmd, SKIP_ALIG, 0, visit_dtuv, &dc);
+                int nnz = 0;
+                for (int V = 0; V < d; ++V) for (int U = 0; U < d; ++U) for (int T = 0; T < d; ++T) {
+                    double v = Dt[(size_t)T + d * ((size_t)U + d * (size_t)V)];
+                    if (v != 0.0) { nzi[3 * nnz] = T; nzi[3 * nnz + 1] = U; nzi[3 * nnz + 2] = V; nzv[nnz++] = v; }
+                }
+                if (nnz == 0) continue;
+                for (int iq = 0; iq < nq; ++iq) {
+                    const double *px = pw + (size_t)iq * 3 * d, *py = px + d, *pz = py + d;
+                    double hr = 0.0, hi = 0.0;
+                    for (int t = 0; t < nnz; ++t) {
+                        int T = nzi[3 * t], U = nzi[3 * t + 1], V = nzi[3 * t + 2];
+                        double term = nzv[t] * px[T] * py[U] * pz[V];
+                        switch ((T + U + V) & 3) {
+                            case 0: hr += term; break;
+                            case 1: hi += term; break;
+                            case 2: hr -= term; break;
+                            default: hi -= term; break;
+                        }
+                    }
+                    double fr = hr, fi = hi;
+                    double ang[3] = {qal[3 * iq] * Hx, qal[3 * iq + 1] * Hy, qal[3 * iq + 2] * Hz};
+                    for (int ax = 0; ax < 3; ++ax) {
+                        double cr = cos(ang[ax]), ci = sin(ang[ax]);
+                        double a = fr * cr - fi * ci, b = fr * ci + fi * cr; fr = a; fi = b;
+                    }
+                    acc[iq] += w * fr * E12(&S, iq, i, j) * E12(&S, iq, k, r);
+                }
+            }
+        }
+        free(zblk); free(zbuf); free(Dt); free(nzi); free(nzv);
+    }
+    for (int iq = 0; iq < nq; ++iq) result_re[iq] = 0.0;
+    for (long ch = 0; ch < nch; ++ch)
+        for (int iq = 0; iq < nq; ++iq) result_re[iq] += part[(size_t)ch * nq + iq];
+    free(part); free(pw);
+    free_dens(&D); free_setup(&S); free(qabs);
+    return ORC_OK;
+}
+
+/*
+ * Algorithmic work of the q-independent part of tot_integral_k_ijkr
+ * (src/Integrals.f90:5155-5219): T_E = the number of innermost h_saved
+ * updates that pass both cutoffs (|ztot| >= cutoffz, |prod6| > cutoffmd;
+ * the MD |E| < 1e-30 skips are commented out there), for each listed
+ * quartet.  Quartets on the P = Q branch (loop 5, or |H| < cutoffcentre)
+ * count the terms of tot_integral_ijkr_pzero (:4955-5067, with its active
+ * MD skips) instead and are flagged in is_p0.  rho as in orc_scattering_ex.
+ */
+typedef struct { long n; } cntctx_t;
+static void visit_count(void *c, int ll, int mm, int nn, int llp, int mmp, int nnp, double prod6) {
+    (void)ll; (void)mm; (void)nn; (void)llp; (void)mmp; (void)nnp; (void)prod6;
+    ((cntctx_t *)c)->n += 1;
+}
+
+int orc_count_te(int ngto, const double *ga, const int *l, const int *m, const int *n,
+                 const double *xx, const double *yy, const double *zz, const int *group,
+                 const double *mmod, int nmo, const int *mat, const double *total, int nmat,
+                 const double *rho, double cutoffz, double cutoffmd, double cutoffcentre,
+                 const int *quartets, long nquart, int nthreads, long *te, int *is_p0) {
+    double q1 = 1.0;
+    setup_t S;
+    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, &q1, 1, 1);
+    if (e != ORC_OK) { free_setup(&S); return e; }
+    dens_t D;
+    e = build_dens(&D, mmod, nmo, mat, total, nmat);
+    if (e != ORC_OK) { free_dens(&D); free_setup(&S); return e; }
+    D.rho = rho;
+    D.np = (long)ngto * (ngto + 1) / 2;
+    int mg = max_group(&S);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel
+    {
+        double *zblk = malloc(sizeof(double) * (size_t)mg * mg * mg * mg);
+        double *zbuf = rho ? NULL : malloc(sizeof(double) * (size_t)(nmat > 0 ? nmat : 1) * 4 * mg * mg);
+#pragma omp for schedule(dynamic, 64)
+        for (long c = 0; c < nquart; ++c) {
+            int i = quartets[5 * c], j = quartets[5 * c + 1], k = quartets[5 * c + 2], r = quartets[5 * c + 3];
+            int loop = quartets[5 * c + 4];
+            double hx = PX(&S, k, r) - PX(&S, i, j), hy = PY(&S, k, r) - PY(&S, i, j);
+            double hz = PZ(&S, k, r) - PZ(&S, i, j);
+            double h = loop == 1 ? pow(hx * hx + hy * hy + hz * hz, 0.5) : sqrt(hx * hx + hy * hy + hz * hz);
+            int p0 = loop == 5 || h < cutoffcentre;
+            build_total_block(&S, &D, i, j, k, r, zblk, zbuf);
+            zblock_t Z = {S.gc[i], S.gc[j], S.gc[k], S.gc[r], zblk};
+            cntctx_t cc = {0};
+            hermite_loop(&S, i, j, k, r, DDP(&S, S.ddx, j, i), DDP(&S, S.ddy, j, i), DDP(&S, S.ddz, j, i),
+                         DDP(&S, S.ddx, r, k), DDP(&S, S.ddy, r, k), DDP(&S, S.ddz, r, k), &Z,
+                         cutoffz, cutoffmd, p0 ? SKIP_PZERO : SKIP_KIJKR, 1, visit_count, &cc);
+            te[c] = cc.n;
+            is_p0[c] = p0;
+        }
+        free(zblk); free(zbuf);
+    }
+    free_dens(&D); free_setup(&S);
     return ORC_OK;
 }
 

@@ -325,6 +325,14 @@ def config5_fit(nq: int = 400) -> Problem:
     return _problem("fit6", atoms, shells, 30, 30, q_grid(14.0, nq), rng)
 
 
+def config5_aligned_grid(n: int = 64, qmax: float = 14.0) -> np.ndarray:
+    """The n^3 Cartesian q vectors of the ring's aligned intensity: every
+    component on linspace(-qmax, qmax, n) (bohr^-1), x fastest; shape (n^3, 3)."""
+    ax = np.linspace(-qmax, qmax, n)
+    qz, qy, qx = np.meshgrid(ax, ax, ax, indexing="ij")
+    return np.stack([qx.ravel(), qy.ravel(), qz.ravel()], axis=1)
+
+
 def config5_geometries(base: Problem, ngeom: int = 512, sigma: float = 0.1, seed: int = SEED0 + 55):
     rng = np.random.default_rng(seed)
     out = [base.atoms.copy()]

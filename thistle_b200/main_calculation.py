@@ -38,6 +38,26 @@ def read_twordm(filename):
     return mat, total
 
 
+def read_twordm_listing(filename):
+    """2-RDM rows as the reference's Python builder writes them
+    (src/twordm.py:300-316): ``[p s q r] value`` per line, the index list
+    printed by numpy with 0-based MO indices in the (m1, m2, m3, m4) order of
+    the Fortran rows.  Returns read_twordm's 1-based ``(mat, total)``."""
+    mat, total = [], []
+    with open(filename) as f:
+        for line in f:
+            line = line.strip()
+            if not line:
+                continue
+            head, _, val = line.rpartition("]")
+            idx = [int(t) for t in head.lstrip("[").split()]
+            if len(idx) != 4:
+                raise ValueError(f"{filename}: expected 4 indices in {line!r}")
+            mat.append([i + 1 for i in idx])
+            total.append(float(val))
+    return np.asarray(mat, dtype=np.int32).reshape(-1, 4), np.asarray(total, dtype=np.float64)
+
+
 def read_onerdm(filename):
     """Rows ``i j value``; the matrix size is the last row's i (src/one_rdm.f90:2072-2108)."""
     rows = np.loadtxt(filename, ndmin=2)
