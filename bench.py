@@ -486,6 +486,8 @@ def bench_extras(args, p, plan, stream, stage1_ms, peak_tf, fwd_ms):
                            "oracle under the same cutoffs (profiles/stage1_ab6_flops.json)",
             "rho_unique_half_bytes": 8 * npair * (npair + 1) // 2,
             "hbm_floor_ms": 8 * npair * (npair + 1) / 2 / 6524e9 * 1e3}
+    if args.extras != "all":
+        return out
     t0 = time.perf_counter()
     out["fit6"] = fit6_section(args.extra_fit_geometries, 16, 64)
     out["fit6"]["section_s"] = time.perf_counter() - t0
@@ -513,8 +515,9 @@ def main():
                     help="ab6_4atom: the first 4 atoms only, a profiling-size case of the same basis; "
                          "fit6: batched forward + adjoint over geometries (configuration 5); "
                          "batch4: uneven molecule batches (configuration 4)")
-    ap.add_argument("--no-extras", action="store_true",
-                    help="skip the AB6 adjoint, stage-1 roofline, fit6 and batch4 keys of the default line")
+    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "none"],
+                    help="keys of the default line beyond the forward step: all (AB6 adjoint, stage-1 "
+                         "roofline, fit6, batch4), adjoint (the first two only) or none")
     ap.add_argument("--extra-fit-geometries", type=int, default=128)
     ap.add_argument("--extra-batch-molecules", type=int, default=256)
     ap.add_argument("--fit-geometries", type=int, default=512)
@@ -612,7 +615,7 @@ def main():
                 "peak_source": "measured FP64 FMA rate of this GPU (thistle_probe_fp64_peak, in this run)"}
 
     extras = {}
-    if world == 1 and not args.no_extras:
+    if world == 1 and args.extras != "none":
         extras = bench_extras(args, p, plan, stream, st["stage1"] / n2, peak_tf, ms / args.steps)
 
     line = {

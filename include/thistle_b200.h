@@ -228,6 +228,17 @@ int thistle_plan_stage_totals(thistle_plan *plan, double *ms4, int64_t *nexec);
 int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32_t *ncls,
                          int64_t *cls_begin, int64_t *cls_end, int64_t *cls_recoff,
                          int32_t *cls_rs, const double **q_dev);
+/* The plan's density after the MO -> primitive transform, copied to host
+ * memory (no reference counterpart; for inspecting the transform).  Total
+ * and j2 plans: the pair density rho, np x np with np = ngto (ngto + 1) / 2,
+ * rho[P(a,b) np + P(c,d)] = ztot of functions a, b (electron 1) and c, d
+ * (electron 2) -- zcontrred + zcontrred2 of src/Integrals.f90:109-127 and
+ * 5163 -- with P(a,b) = max(a,b) (max(a,b) + 1) / 2 + min(a,b), 0-based.
+ * Elastic plans: the AO density Z (ngto x ngto, column-major) of
+ * variables_elastic (src/Variables.f90:1199-1217).  `count` is the capacity
+ * of out in doubles; *needed receives the size either way (out may then be
+ * NULL to query it). */
+int thistle_plan_density(const thistle_plan *plan, double *out, int64_t count, int64_t *needed);
 int thistle_plan_destroy(thistle_plan *plan);
 
 /*

@@ -75,7 +75,7 @@ def build(verbose: bool = False, force: bool = False, extra=None, out: str | Non
             print(pr.stdout + pr.stderr)
         if pr.returncode != 0:
             raise RuntimeError("nvcc failed: " + " ".join(cmd) + "\n" + pr.stdout + pr.stderr)
-    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIBOUT, *objs, "-lcublas"]
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIBOUT, *objs]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -7,9 +7,9 @@
 //                   accurate generator), warp per quartet, lanes over q,
 //                   accumulated per warp in shared memory
 //  tb_reduce        fixed-order sum of the per-block partial I(q)
-//  ghat_emit / ghat_runs / pack_pairs / sym_small: the density transform's
-//                   gathers (variables_total z11/z22 :1045-1065 re-expressed
-//                   as a 4-index transform)
+//  ghat_emit / ghat_runs / sym_small: the density transform's gathers
+//                   (variables_total z11/z22 :1045-1065 re-expressed as a
+//                   4-index transform, whose GEMM passes are in tb_transform.cu)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -336,148 +336,6 @@ __global__ void ghat_runs_kernel(const int *__restrict__ keys, const double *__r
   G[keys[i]] = s;
 }
 
-// out[b][fpair(c,d)] = in[b][c][d] for c <= d
-__global__ void pack_pairs_kernel(const double *__restrict__ in, int64_t nb, int ngto, double *__restrict__ out) {
-  int64_t np = (int64_t)ngto * (ngto + 1) / 2;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb * np) return;
-  int64_t b = i / np, p = i % np;
-  // invert fpair: d = largest with d(d+1)/2 <= p
-  int d = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
-  while ((int64_t)(d + 1) * (d + 2) / 2 <= p) ++d;
-  while ((int64_t)d * (d + 1) / 2 > p) --d;
-  int c = (int)(p - (int64_t)d * (d + 1) / 2);
-  out[i] = in[((size_t)b * ngto + c) * ngto + d];
-}
-
-// Last pass of the density transform: the pair-density columns of function
-// pairs (a <= b) for one b,
-//   rho[fpair(a, b)][r] = sum_i T3[i][b][r] C(i, a)   (C column-major, n x ngto),
-// a skinny product (k = n, the MO count).  A block owns 128 rows r of one b
-// (blocks of large b first).  It stages T3[i][b][r0..r0+127] and the columns
-// a <= b of Ct = C^T (n x cw, zero-padded, written by ct_kernel) in shared
-// memory -- all n MOs at once when they fit (ONESHOT), else RR_KC at a time
-// for each chunk of 64 columns -- and each warp
-// accumulates 8 columns x 128 rows at a time (a thread: rows 2 lane + {0, 1}
-// + {0, 64} x 8 columns in registers; the C values are warp broadcasts).
-// Sums run over i in order, so the result does not depend on the launch.
-constexpr int RR_R = 128, RR_AC = 64, RR_KC = 48;
-__host__ __device__ inline int rr_cw(int ngto) { return (ngto + 7) / 8 * 8; }
-
-// 8-byte global -> shared copy through the asynchronous copy unit; with
-// ok false nothing is read and the destination is zero-filled
-__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool ok) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-__device__ __forceinline__ void rr_block(const double *__restrict__ sA, const double *__restrict__ sC, int ldc,
-                                         int kc, int lane, double (&acc)[4][8]) {
-  for (int k = 0; k < kc; ++k) {
-    const double2 a0 = reinterpret_cast<const double2 *>(sA + k * RR_R)[lane];
-    const double2 a1 = reinterpret_cast<const double2 *>(sA + k * RR_R + 64)[lane];
-    const double av[4] = {a0.x, a0.y, a1.x, a1.y};
-    const double2 *c2 = reinterpret_cast<const double2 *>(sC + k * ldc);
-    double cv[8];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const double2 v = c2[c];
-      cv[2 * c] = v.x;
-      cv[2 * c + 1] = v.y;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) acc[j][c] = fma(av[j], cv[c], acc[j][c]);
-  }
-}
-
-__device__ __forceinline__ void rr_store(const double (&acc)[4][8], double *__restrict__ rho, int64_t col0, int ab,
-                                         int b, int64_t np, int64_t r0, int lane) {
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int a = ab + c;
-    if (a > b) break;
-    double *out = rho + (col0 + a) * np + r0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int r = 2 * lane + (j & 1) + 64 * (j >> 1);
-      if (r0 + r < np) out[r] = acc[j][c];
-    }
-  }
-}
-
-// Ct[k][a] = C(k, a) for a < ngto, 0 up to cw
-__global__ void ct_kernel(const double *__restrict__ C, int n, int ngto, int cw, double *__restrict__ Ct) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * cw) return;
-  const int k = e / cw, a = e % cw;
-  Ct[e] = a < ngto ? C[(int64_t)a * n + k] : 0.0;
-}
-
-template <bool ONESHOT>
-__global__ void __launch_bounds__(256, 2) rho_rows_kernel(const double *__restrict__ T3, const double *__restrict__ Ct,
-                                                          int n, int ngto, int64_t np, double *__restrict__ rho) {
-  extern __shared__ __align__(16) double sm[];
-  const int b = ngto - 1 - (int)blockIdx.x;
-  const int cwall = rr_cw(ngto);
-  // staged columns: 0 .. round8(b + 1) - 1 (ONESHOT) or one chunk of 64
-  const int cw = ONESHOT ? rr_cw(b + 1) : RR_AC;
-  const int kcap = ONESHOT ? n : RR_KC;
-  double *sA = sm;               // [k][RR_R]
-  double *sC = sm + kcap * RR_R;  // [k][cw]
-  const int64_t r0 = (int64_t)blockIdx.y * RR_R;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t istride = (int64_t)ngto * np;
-  const double *Ab = T3 + (int64_t)b * np + r0;
-  const int64_t col0 = fpair(0, b);
-  // asynchronous copies (zero-filled outside the matrices), all in flight
-  // before the block waits for them
-  auto stage = [&](int k0, int kc, int ac, int ncol) {
-    for (int e = threadIdx.x; e < kc * RR_R; e += blockDim.x) {
-      const int k = e / RR_R, r = e % RR_R;
-      const bool ok = r0 + r < np;
-      cp_async8(sA + e, ok ? Ab + (int64_t)(k0 + k) * istride + r : Ab, ok);
-    }
-    for (int e = threadIdx.x; e < kc * ncol; e += blockDim.x) {
-      const int k = e / ncol, a = ac + e % ncol;
-      const bool ok = a < cwall;
-      cp_async8(sC + e, ok ? Ct + (int64_t)(k0 + k) * cwall + a : Ct, ok);
-    }
-    cp_async_wait_all();
-  };
-  double acc[4][8];
-  if (ONESHOT) {
-    stage(0, n, 0, cw);
-    __syncthreads();
-    for (int ab = 8 * w; ab <= b; ab += RR_AC) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[j][c] = 0.0;
-      rr_block(sA, sC + ab, cw, n, lane, acc);
-      rr_store(acc, rho, col0, ab, b, np, r0, lane);
-    }
-    return;
-  }
-  for (int ac = 0; ac <= b; ac += RR_AC) {
-    const int ab = ac + 8 * w;  // this warp's first column
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) acc[j][c] = 0.0;
-    for (int k0 = 0; k0 < n; k0 += RR_KC) {
-      const int kc = min(RR_KC, n - k0);
-      __syncthreads();
-      stage(k0, kc, ac, RR_AC);
-      __syncthreads();
-      if (ab <= b) rr_block(sA, sC + 8 * w, RR_AC, kc, lane, acc);
-    }
-    if (ab <= b) rr_store(acc, rho, col0, ab, b, np, r0, lane);
-  }
-}
-
 // out = 0.5 (in + in^T) for a small n x n matrix
 __global__ void sym_small_kernel(const double *__restrict__ in, int n, double *__restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -641,38 +499,6 @@ cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, dou
   return cudaGetLastError();
 }
 
-size_t rho_rows_ct_doubles(int n, int ngto) { return (size_t)n * rr_cw(ngto); }
-
-cudaError_t launch_rho_rows(const double *T3, const double *C, double *Ct, int n, int ngto, int64_t np, double *rho,
-                            cudaStream_t st) {
-  if (ngto <= 0 || np <= 0 || n <= 0) return cudaSuccess;
-  const int64_t ry = (np + RR_R - 1) / RR_R;
-  if (ry > 65535) return cudaErrorInvalidValue;
-  const int nct = n * rr_cw(ngto);
-  ct_kernel<<<(nct + 255) / 256, 256, 0, st>>>(C, n, ngto, rr_cw(ngto), Ct);
-  const dim3 grid((unsigned)ngto, (unsigned)ry);
-  // all MOs at once while two blocks still fit an SM
-  const size_t one = sizeof(double) * (size_t)n * (RR_R + rr_cw(ngto));
-  cudaError_t e;
-  if (one <= 112 * 1024) {
-    e = cudaFuncSetAttribute(rho_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one);
-    if (e != cudaSuccess) return e;
-    rho_rows_kernel<true><<<grid, 256, one, st>>>(T3, Ct, n, ngto, np, rho);
-  } else {
-    const size_t smem = sizeof(double) * (size_t)RR_KC * (RR_R + RR_AC);
-    e = cudaFuncSetAttribute(rho_rows_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    rho_rows_kernel<false><<<grid, 256, smem, st>>>(T3, Ct, n, ngto, np, rho);
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st) {
-  int64_t tot = nb * ((int64_t)ngto * (ngto + 1) / 2);
-  if (tot <= 0) return cudaSuccess;
-  pack_pairs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, nb, ngto, out);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,
                                 uint64_t *quart, uint32_t *keys, cudaStream_t st) {

@@ -1,7 +1,6 @@
 // Internal launch interface between the plan code and the kernels.
 #pragma once
 
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -132,11 +131,9 @@ cudaError_t launch_pair_dtables(int ng, int maxa, const int *gstart, const doubl
 cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStream_t st);
 cudaError_t launch_adjoint_f(int L, const AdjointFArgs &a, int grid, int ngeom, bool split, cudaStream_t st);
 
-// Process-wide cache of device buffers and cuBLAS handles (tb_pool.cu).
+// Process-wide cache of device buffers (tb_pool.cu).
 cudaError_t pool_malloc(void **p, size_t bytes);
 void pool_free(void *p);
-cublasHandle_t pool_cublas();
-void pool_cublas_release(cublasHandle_t h);
 
 // Sets the calling thread's error string (thistle_last_error_string) and returns code.
 int set_error(int code, const std::string &msg);
@@ -191,12 +188,25 @@ cudaError_t launch_reduce_batch(const double *partial, int nblocks, int nq, int6
 cudaError_t launch_ghat_emit(const int *mat, const double *total, int nmat, int n, int *keys, double *vals,
                              cudaStream_t st);
 cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, double *G, cudaStream_t st);
-cudaError_t launch_pack_pairs(const double *in, int64_t nb, int ngto, double *out, cudaStream_t st);
-// last pass of the density transform: rho[fpair(a, b)][r] = sum_i T3[i][b][r] C(i, a);
-// Ct is scratch of rho_rows_ct_doubles(n, ngto) doubles
-size_t rho_rows_ct_doubles(int n, int ngto);
-cudaError_t launch_rho_rows(const double *T3, const double *C, double *Ct, int n, int ngto, int64_t np, double *rho,
-                            cudaStream_t st);
+// Density transform on the FP64 tensor cores (tb_transform.cu): D(m, j) =
+// sum_{k < K} A(m, k) B(k, j) with A(m, k) = A[m + k sak + batch a_batch]
+// (m contiguous) and B(k, j) = B[k sbk + j sbj], one of sbk, sbj equal to 1
+// (b_jcontig: sbj == 1).  mode 0 stores D[m sdm + j sdj + batch d_batch];
+// mode 1 the packed lower triangle j <= m at D[batch d_batch + m(m+1)/2 + j];
+// mode 2 the columns j <= batch at D[(batch(batch+1)/2 + j) sdj + m].
+struct DmmaGemmArgs {
+  const double *A;
+  int64_t sak, a_batch;
+  const double *B;
+  int64_t sbk, sbj;
+  int M, N, K;
+  double *D;
+  int64_t sdm, sdj, d_batch;
+};
+cudaError_t launch_dmma_gemm(const DmmaGemmArgs &g, int mode, bool b_jcontig, int nbatch, cudaStream_t st);
+// Ct[k][a] = C(k, a) (C column-major n x ngto), rows of transform_ct_width(ngto) doubles
+int transform_ct_width(int ngto);
+cudaError_t launch_transform_ct(const double *C, int n, int ngto, double *Ct, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
 // molecule batches: pair tables of every item (blocks pre[i] .. pre[i+1]-1 of 128 pairs)
 struct PairDesc {

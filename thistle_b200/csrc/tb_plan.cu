@@ -10,7 +10,6 @@
 //   the five quartet loops        src/Integrals.f90:79-468 (bra pair i<=j, ket pair k<=r)
 //   per-quartet kernels           src/Integrals.f90:4955-5226 and variants
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -57,12 +56,6 @@ int set_error(int code, const std::string &msg) { return fail(code, msg); }
   do {                                                                                      \
     cudaError_t e_ = (x);                                                                   \
     if (e_ != cudaSuccess) return fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-#define TB_CB(x)                                                                            \
-  do {                                                                                      \
-    cublasStatus_t s_ = (x);                                                                \
-    if (s_ != CUBLAS_STATUS_SUCCESS)                                                        \
-      return fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); \
   } while (0)
 
 // Device buffers come from the process-wide cache (tb_pool.cu).
@@ -117,7 +110,7 @@ struct thistle_plan {
   // device-resident density inputs and transform workspaces
   int *d_mat = nullptr;
   double *d_C = nullptr, *d_tot = nullptr, *d_D = nullptr, *d_Ds = nullptr, *d_Y = nullptr;
-  double *d_G = nullptr, *d_T1 = nullptr, *d_T2 = nullptr, *d_V = nullptr, *d_T3 = nullptr, *d_Ct = nullptr;
+  double *d_G = nullptr, *d_T1 = nullptr, *d_V = nullptr, *d_T3 = nullptr, *d_Ct = nullptr;
   // Ghat build: (index, value) per row placement, sorted by index
   int *d_gk0 = nullptr, *d_gk1 = nullptr;
   double *d_gv0 = nullptr, *d_gv1 = nullptr;
@@ -141,7 +134,6 @@ struct thistle_plan {
   int s2_bps[LMAXB + 1];             // resident stage-2 blocks per SM, per Bessel order
   cudaStream_t st = nullptr;
   bool own_stream = true;
-  cublasHandle_t cb = nullptr;
   cudaEvent_t ev[10];
   // per-execution stage events: slot = execution index mod NRING
   static const int NRING = 64;
@@ -339,14 +331,6 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
       goto done;                                                                                          \
     }                                                                                                     \
   } while (0)
-#define TB_TRYB(x)                                                                                        \
-  do {                                                                                                    \
-    cublasStatus_t s_ = (x);                                                                              \
-    if (s_ != CUBLAS_STATUS_SUCCESS) {                                                                    \
-      rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_));        \
-      goto done;                                                                                          \
-    }                                                                                                     \
-  } while (0)
 
 static int density_alloc(thistle_plan *P) {
   int rc = THISTLE_OK;
@@ -358,16 +342,16 @@ static int density_alloc(thistle_plan *P) {
     TB_TRY(dalloc(&P->d_D, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
     TB_TRY(dalloc(&P->d_Ds, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
     TB_TRY(dalloc(&P->d_Y, (size_t)P->nmo1 * ngto, "1-RDM x C"));
+    TB_TRY(dalloc(&P->d_Ct, (size_t)n * transform_ct_width(ngto), "transform C^T"));
   } else {
     TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
     TB_TRY(dalloc(&P->d_mat, (size_t)P->nmat * 4, "2-RDM indices"));
     TB_TRY(dalloc(&P->d_tot, (size_t)P->nmat, "2-RDM values"));
     TB_TRY(dalloc(&P->d_G, (size_t)n4, "Ghat"));
     TB_TRY(dalloc(&P->d_T1, (size_t)(n3 * ngto), "transform T1"));
-    TB_TRY(dalloc(&P->d_T2, (size_t)(n2 * ngto * ngto), "transform T2"));
     TB_TRY(dalloc(&P->d_V, (size_t)(n2 * np), "transform V"));
     TB_TRY(dalloc(&P->d_T3, (size_t)((int64_t)n * ngto * np), "transform T3"));
-    TB_TRY(dalloc(&P->d_Ct, rho_rows_ct_doubles(n, ngto), "transform C^T"));
+    TB_TRY(dalloc(&P->d_Ct, (size_t)n * transform_ct_width(ngto), "transform C^T"));
     const int64_t m = std::max<int64_t>(8 * (int64_t)P->nmat, 1);
     TB_TRY(dalloc(&P->d_gk0, (size_t)m, "Ghat keys"));
     TB_TRY(dalloc(&P->d_gk1, (size_t)m, "Ghat keys"));
@@ -396,20 +380,32 @@ static int density_upload(thistle_plan *P, const double *mmod, const int32_t *ma
   return THISTLE_OK;
 }
 
-// Pair density (total, j2) or AO density (elastic) from the device-resident inputs.
+// Pair density (total, j2) or AO density (elastic) from the device-resident
+// inputs, every GEMM pass on the FP64 tensor cores (tb_transform.cu).
 static int density_run(thistle_plan *P) {
   int rc = THISTLE_OK;
-  const int n = P->nmo, ngto = P->ngto;
+  const int n = P->nmo, ngto = P->ngto, cw = transform_ct_width(ngto);
   const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
-  const double one = 1.0, zero = 0.0;
+  TB_TRYC(launch_transform_ct(P->d_C, n, ngto, P->d_Ct, P->st));
+  P->launches += 1;
   if (P->kind == KIND_ELASTIC) {
-    // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217)
+    // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217),
+    // C1 the first nmo1 MOs: Y(i, a) = sum_j Ds(i, j) C(j, a), then
+    // Z(a, b) = sum_i C(i, a) Y(i, b)
     const int k = P->nmo1;
     TB_TRYC(launch_sym_small(P->d_D, k, P->d_Ds, P->st));
-    P->launches += 1;
-    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, k, ngto, k, &one, P->d_Ds, k, P->d_C, n, &zero, P->d_Y, k));
-    TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, ngto, k, &one, P->d_C, n, P->d_Y, k, &zero, P->d_zao,
-                        ngto));
+    DmmaGemmArgs g{};
+    g.A = P->d_Ds; g.sak = k; g.a_batch = 0;
+    g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
+    g.M = k; g.N = ngto; g.K = k;
+    g.D = P->d_Y; g.sdm = 1; g.sdj = k; g.d_batch = 0;
+    TB_TRYC(launch_dmma_gemm(g, 0, true, 1, P->st));
+    g.A = P->d_Ct; g.sak = cw;
+    g.B = P->d_Y; g.sbk = 1; g.sbj = k;
+    g.M = ngto; g.N = ngto; g.K = k;
+    g.D = P->d_zao; g.sdm = 1; g.sdj = ngto;
+    TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
+    P->launches += 3;
     goto done;
   }
   if (P->nmat == 0) {
@@ -427,22 +423,32 @@ static int density_run(thistle_plan *P) {
     TB_TRYC(launch_ghat_runs(P->d_gk1, P->d_gv1, m, P->d_G, P->st));
     P->launches += 3;
   }
-  // T1'(ngto x n^3) = C^T Ghat'   (C is (n, ngto) column-major, the mmod layout)
-  TB_TRYB(cublasDgemm(P->cb, CUBLAS_OP_T, CUBLAS_OP_N, ngto, (int)n3, n, &one, P->d_C, n, P->d_G, n, &zero, P->d_T1,
-                      ngto));
-  // T2[X] (ngto x ngto) = T1[X]' C, X over n^2
-  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, ngto, ngto, n, &one, P->d_T1, ngto,
-                                    (long long)n * ngto, P->d_C, n, 0, &zero, P->d_T2, ngto, (long long)ngto * ngto,
-                                    (int)n2));
-  TB_TRYC(launch_pack_pairs(P->d_T2, n2, ngto, P->d_V, P->st));
-  P->launches += 1;
-  // T3[m1] (np x ngto) = V[m1]' C
-  TB_TRYB(cublasDgemmStridedBatched(P->cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)np, ngto, n, &one, P->d_V, (int)np,
-                                    (long long)n * np, P->d_C, n, 0, &zero, P->d_T3, (int)np, (long long)ngto * np,
-                                    n));
-  // rho rows (a <= b, b fixed) = T3[:,b,:]' C[:,0..b] for every b (rho_rows_kernel)
-  TB_TRYC(launch_rho_rows(P->d_T3, P->d_C, P->d_Ct, n, ngto, np, P->d_rho, P->st));
-  P->launches += 2;  // C^T and the rows
+  {
+    DmmaGemmArgs g{};
+    // T1[xyz](a) = sum_w C(w, a) Ghat[x][y][z][w]: (ngto x n^3), leading dimension ngto
+    g.A = P->d_Ct; g.sak = cw; g.a_batch = 0;
+    g.B = P->d_G; g.sbk = 1; g.sbj = n;
+    g.M = ngto; g.N = (int)n3; g.K = n;
+    g.D = P->d_T1; g.sdm = 1; g.sdj = ngto; g.d_batch = 0;
+    TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
+    // V[xy](fpair(c, d)) = sum_z T1[xyz](d) C(z, c) for c <= d, one batch per xy
+    g.A = P->d_T1; g.sak = ngto; g.a_batch = (int64_t)n * ngto;
+    g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
+    g.M = ngto; g.N = ngto; g.K = n;
+    g.D = P->d_V; g.sdm = 0; g.sdj = 0; g.d_batch = np;
+    TB_TRYC(launch_dmma_gemm(g, 1, true, (int)n2, P->st));
+    // T3[x](p, b) = sum_y V[xy](p) C(y, b), one batch per x
+    g.A = P->d_V; g.sak = np; g.a_batch = (int64_t)n * np;
+    g.M = (int)np; g.N = ngto; g.K = n;
+    g.D = P->d_T3; g.sdm = 1; g.sdj = np; g.d_batch = (int64_t)ngto * np;
+    TB_TRYC(launch_dmma_gemm(g, 0, true, n, P->st));
+    // rho(p, fpair(a, b)) = sum_x T3[x](p, b) C(x, a) for a <= b, one batch per b
+    g.A = P->d_T3; g.sak = (int64_t)ngto * np; g.a_batch = np;
+    g.M = (int)np; g.N = ngto; g.K = n;
+    g.D = P->d_rho; g.sdm = 1; g.sdj = np; g.d_batch = 0;
+    TB_TRYC(launch_dmma_gemm(g, 2, true, ngto, P->st));
+    P->launches += 4;
+  }
 done:
   return rc;
 }
@@ -499,7 +505,7 @@ static void plan_free(thistle_plan *P) {
   dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
   dfree(P->d_partial); dfree(P->d_result); dfree(P->d_quart);
   dfree(P->d_mat); dfree(P->d_C); dfree(P->d_tot); dfree(P->d_D); dfree(P->d_Ds); dfree(P->d_Y);
-  dfree(P->d_G); dfree(P->d_T1); dfree(P->d_T2); dfree(P->d_V); dfree(P->d_T3); dfree(P->d_Ct);
+  dfree(P->d_G); dfree(P->d_T1); dfree(P->d_V); dfree(P->d_T3); dfree(P->d_Ct);
   dfree(P->d_gk0); dfree(P->d_gk1); dfree(P->d_gv0); dfree(P->d_gv1); dfree(P->d_gsort_tmp);
   dfree(P->d_xbuf);
   dfree(P->d_braoff); dfree(P->d_gL); dfree(P->d_k0); dfree(P->d_k1); dfree(P->d_v0); dfree(P->d_p0count);
@@ -509,7 +515,6 @@ static void plan_free(thistle_plan *P) {
   if (P->gx_vjp) cudaGraphExecDestroy(P->gx_vjp);
   dfree(P->d_s2sort_tmp);
   dfree(P->d_sort_tmp);
-  if (P->cb) pool_cublas_release(P->cb);
   if (P->have_ev) {
     for (int i = 0; i < 10; ++i) cudaEventDestroy(P->ev[i]);
     for (int r = 0; r < thistle_plan::NRING; ++r)
@@ -646,14 +651,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   for (int r = 0; r < thistle_plan::NRING; ++r)
     for (int i = 0; i < 5; ++i) TB_TRYC(cudaEventCreate(&P->rev[r][i]));
   P->have_ev = true;
-  P->cb = pool_cublas();
-  if (!P->cb) {
-    rc = fail(THISTLE_ERR_CUDA, "cublasCreate failed");
-    goto done;
-  }
-  TB_TRYB(cublasSetStream(P->cb, P->st));
-  TB_TRYB(cublasSetMathMode(P->cb, CUBLAS_PEDANTIC_MATH));
-  tr.mark("stream, events, cuBLAS");
+  tr.mark("stream, events");
   TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_flmn, (size_t)ngto, "functions"));
@@ -1807,7 +1805,6 @@ int thistle_plan_set_stream(thistle_plan *P, void *stream) {
   if (P->own_stream) cudaStreamDestroy(P->st);
   P->st = (cudaStream_t)stream;
   P->own_stream = false;
-  TB_CB(cublasSetStream(P->cb, P->st));
   return THISTLE_OK;
 }
 
@@ -1928,6 +1925,22 @@ int thistle_plan_records(const thistle_plan *P, const double **rec_dev, int32_t 
     cls_recoff[c] = P->cls_recoff[c];
     cls_rs[c] = P->cls_rs[c];
   }
+  return THISTLE_OK;
+}
+
+int thistle_plan_density(const thistle_plan *P, double *out, int64_t count, int64_t *needed) {
+  if (!P || !needed) return fail(THISTLE_ERR_ARG, "null argument");
+  if (P->kind == KIND_ALIGNED || P->kind == KIND_TOTAL || P->kind == KIND_J2) {
+    *needed = P->np * P->np;
+  } else {
+    *needed = (int64_t)P->ngto * P->ngto;
+  }
+  if (!out) return THISTLE_OK;
+  if (count < *needed) return fail(THISTLE_ERR_ARG, "output holds " + std::to_string(count) + " doubles, the density " +
+                                                       std::to_string(*needed));
+  const double *src = P->kind == KIND_ELASTIC ? P->d_zao : P->d_rho;
+  TB_CK(cudaStreamSynchronize(P->st));
+  TB_CK(cudaMemcpy(out, src, sizeof(double) * (size_t)*needed, cudaMemcpyDeviceToHost));
   return THISTLE_OK;
 }
 

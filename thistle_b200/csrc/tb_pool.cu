@@ -1,8 +1,8 @@
-// Device-memory and cuBLAS-handle cache shared by the plans of a process.
+// Device-memory cache shared by the plans of a process.
 //
 // A plan holds several GB (the pair density alone is Np^2 doubles) and the
 // drop-in entry point builds and drops a plan per call, so cudaMalloc,
-// cudaFree (which also synchronises the device) and cublasCreate would cost
+// and cudaFree (which also synchronises the device) would cost
 // tens of milliseconds per call.  Buffers a plan releases stay cached, per
 // device, and are handed to the next request of a similar size (at least the
 // requested bytes, at most twice them); a failed cudaMalloc first returns
@@ -10,7 +10,6 @@
 // synchronises its stream before it releases anything, so a reused buffer
 // has no work pending on it.  thistle_release_device_cache() empties the
 // cache of the current device.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,7 +32,6 @@ struct Block {
 std::mutex g_mu;
 std::vector<Block> g_free;                  // cached, unused
 std::unordered_map<void *, Block> g_live;   // handed out
-std::vector<std::pair<int, cublasHandle_t>> g_handles;
 
 size_t round_bytes(size_t n) {
   const size_t big = size_t(2) << 20, small = 512;
@@ -96,31 +94,6 @@ void pool_free(void *p) {
   g_live.erase(it);
 }
 
-cublasHandle_t pool_cublas() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_mu);
-    for (size_t i = 0; i < g_handles.size(); ++i)
-      if (g_handles[i].first == dev) {
-        cublasHandle_t h = g_handles[i].second;
-        g_handles.erase(g_handles.begin() + i);
-        return h;
-      }
-  }
-  cublasHandle_t h = nullptr;
-  if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
-  return h;
-}
-
-void pool_cublas_release(cublasHandle_t h) {
-  if (!h) return;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lock(g_mu);
-  g_handles.emplace_back(dev, h);
-}
-
 }  // namespace tb
 
 extern "C" {
@@ -132,12 +105,6 @@ int thistle_release_device_cache(void) {
     return tb::set_error(THISTLE_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(tb::g_mu);
   tb::drop_cached(dev);
-  std::vector<std::pair<int, cublasHandle_t>> keep;
-  for (auto &h : tb::g_handles) {
-    if (h.first == dev) cublasDestroy(h.second);
-    else keep.push_back(h);
-  }
-  tb::g_handles.swap(keep);
   return THISTLE_OK;
 }
 

@@ -145,17 +145,25 @@ struct BoolTag {
   static constexpr bool value = B;
 };
 
-// quartets per lane, and the resident blocks per SM the register allocation aims at
-#ifndef TB_S2_K_LO
-#define TB_S2_K_LO 2
-#endif
-#ifndef TB_S2_K_MID
-#define TB_S2_K_MID 2
-#endif
+// quartets per lane, and the resident blocks per SM the register allocation
+// aims at (4 blocks of 4 warps: 128 registers a thread).  Measured on the
+// AB6 step, two quartets per lane at 4 blocks per SM beat 1 (6 blocks), 3
+// (3 blocks) and 2 at 3 or 5 blocks by 1-8 %.
 #ifndef TB_S2_MINB
 #define TB_S2_MINB 4
 #endif
-TB_HD constexpr int stage2_k(int LB) { return LB <= 2 ? TB_S2_K_LO : (LB <= 8 ? TB_S2_K_MID : 1); }
+#ifndef TB_S2_K03
+#define TB_S2_K03 2
+#endif
+#ifndef TB_S2_K45
+#define TB_S2_K45 2
+#endif
+#ifndef TB_S2_K68
+#define TB_S2_K68 2
+#endif
+TB_HD constexpr int stage2_k(int LB) {
+  return LB <= 3 ? TB_S2_K03 : (LB <= 5 ? TB_S2_K45 : (LB <= 8 ? TB_S2_K68 : 1));
+}
 
 // Crossover of the polynomial form: the smallest x at which its float64 error
 // stays within ~2e-13 of the largest term |hhat_b g_b| -- the level the same

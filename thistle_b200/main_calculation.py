@@ -275,6 +275,16 @@ class ScatteringPlan:
         check(_abi.lib().thistle_plan_execute_quartets(self._p, iptr(qt), qt.shape[0], dptr(out)))
         return out
 
+    def density(self):
+        """The transformed density: the pair density (np, np) of total / j2 /
+        aligned plans, the AO density (ngto, ngto) of elastic plans."""
+        need = C.c_int64(0)
+        check(_abi.lib().thistle_plan_density(self._p, None, 0, C.byref(need)))
+        out = np.zeros(need.value)
+        check(_abi.lib().thistle_plan_density(self._p, dptr(out), need.value, C.byref(need)))
+        k = int(round(np.sqrt(need.value)))
+        return out.reshape(k, k) if self.type != ELASTIC_J0 else out.reshape(k, k, order="F")
+
     def info(self):
         a = np.zeros(6, dtype=np.int64)
         check(_abi.lib().thistle_plan_info(self._p, a.ctypes.data_as(_abi.I64)))
