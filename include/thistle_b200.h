@@ -37,7 +37,15 @@ int thistle_probe_fp64_peak(int32_t reps, double *tflops);
 #define THISTLE_TOTAL_J0 1
 #define THISTLE_ELASTIC_J0 2
 #define THISTLE_TOTAL_ALIGNED 3
+/* elastic aligned: |F(q)|^2 with F the Fourier transform of the electron
+ * density (elastic_integration_alig, src/Integrals.f90:2366-2490; CASE(4),
+ * src/main_calculation.f90:218-265); Entry 1 and thistle_plan_form_factor. */
+#define THISTLE_ELASTIC_ALIGNED 4
 #define THISTLE_TOTAL_J2 7
+/* elastic j2: the P2-weighted orientational average of the elastic
+ * intensity (elastic_integration_j2, src/Integrals.f90:1941-2365; dispatch
+ * CASE(8), src/main_calculation.f90:407-419); needs the 1-RDM like type 2. */
+#define THISTLE_ELASTIC_J2 8
 /* electron scattering: I_e - 2 Ine + Inn (src/main_calculation.f90:277-329,
  * 330-...), I_e the total (5) or elastic (6) j0 intensity, Ine the
  * nuclear-electron term, Inn the nuclear-nuclear sinc sum; Entry 1 only.
@@ -57,7 +65,8 @@ int thistle_version(void);
  * files: mat/total/nmat are read_twordm's rows (src/one_rdm.f90:2112-2147),
  * onerdm is read_onerdm's matrix (:2072-2108).
  *
- *   type          1 total j0, 2 elastic j0, 3 total aligned, 7 total j2
+ *   type          1 total j0, 2 elastic j0, 3 total aligned, 7 total j2,
+ *                 8 elastic j2
  *   Zn, geom      atomic numbers and (natoms,3) geometry; not used by these
  *                 types (kept for the reference's argument list), may be NULL
  *   maxl          maxval(l) as the reference passes it (checked, not trusted)
@@ -68,9 +77,13 @@ int thistle_version(void);
  *   cutoffz, cutoffmd, cutoffcentre  the reference's three cutoffs
  *   mat, total, nmat   (nmat,4) column-major 1-based MO indices and values
  *                      (types 1 and 7)
- *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (type 2)
+ *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (types 2 and 8)
  *   q_abs_out     nq doubles, set to q (the reference returns |q| here)
  *   result_out    nq doubles, I(q)
+ * Type 4 (CASE(4), src/main_calculation.f90:218-265) evaluates the elastic
+ * aligned intensity |F(q)|^2 on the reference's own grid of nq vectors
+ * (thistle_elastic_aligned_grid); q is not read, q_abs_out gets |q|, and the
+ * 1-RDM is needed as for type 2.
  * Type 3 (CASE(3), src/main_calculation.f90:156-217) evaluates the aligned
  * intensity on the reference's own QCOORD3 grid (k0 = 10.583544175): nq must
  * be 3131, q is not read, q_abs_out gets |q| of the grid vectors and
@@ -162,6 +175,19 @@ int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom
  */
 int thistle_plan_nuclear(thistle_plan *plan, const double *Zn, const double *geom, int32_t natoms,
                          double *ine_host);
+/*
+ * Elastic plans (types 2, 8): the Fourier transform of the electron density,
+ * F(q) = sum over ordered group pairs of e12(|q|) e^{i q.P} sum Z E E E (i q)^tuv
+ * (elastic_integration_alig with integral_k_ijkr_alig, src/Integrals.f90:
+ * 2366-2490, 6085-6190), for the plan's current centres on nq q vectors
+ * (qvec: (3, nq) column-major, host).  re/im get F, abs2 |F|^2 (the type 4
+ * intensity); any of the three may be NULL.
+ */
+int thistle_plan_form_factor(thistle_plan *plan, const double *qvec, int32_t nq, double *re_host,
+                             double *im_host, double *abs2_host);
+/* The nq q vectors of CASE(4) (src/main_calculation.f90:227-241), written as
+ * a (3, nq) column-major array.  Host-only. */
+int thistle_elastic_aligned_grid(int32_t nq, double *q_al);
 
 /*
  * Molecule batches (no reference counterpart).  Several plans -- any bases,

@@ -336,3 +336,40 @@ def count_te(prob, quartets=None, *, rho=None, nthreads: int = 0):
     if rc != 0:
         raise RuntimeError(f"oracle orc_count_te failed with code {rc}")
     return te, p0.astype(bool)
+
+
+def elastic_aligned_grid(nq: int) -> np.ndarray:
+    """The q vectors of CASE(4) (src/main_calculation.f90:227-241), shape (nq, 3)."""
+    out = np.zeros((nq, 3))
+    lib().orc_elastic_aligned_grid(C.c_int(nq), out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def elastic_aligned(prob, qal=None, nq: int = 100):
+    """Elastic aligned intensity |F(q)|^2 of CASE(4) (elastic_integration_alig,
+    src/Integrals.f90:2366-2490); q vectors default to the CASE(4) grid.
+    Returns (F_re, F_im, |F|^2)."""
+    keep = []
+
+    def d(x):
+        a, p = _d(x)
+        keep.append(a)
+        return p
+
+    def i(x):
+        a, p = _i(x)
+        keep.append(a)
+        return p
+
+    qal = elastic_aligned_grid(nq) if qal is None else np.ascontiguousarray(qal, dtype=np.float64).reshape(-1, 3)
+    n = qal.shape[0]
+    fr, fi, res = np.zeros(n), np.zeros(n), np.zeros(n)
+    rc = lib().orc_elastic_aligned(
+        C.c_int(prob.ngto), d(prob.ga), i(prob.l), i(prob.m), i(prob.n), d(prob.xx), d(prob.yy), d(prob.zz),
+        i(prob.group), d(np.asfortranarray(prob.mmod).ravel(order="F")), C.c_int(prob.nmo),
+        d(np.asfortranarray(prob.onerdm).ravel(order="F")), C.c_int(prob.onerdm.shape[0]), d(qal), C.c_int(n),
+        fr.ctypes.data_as(C.POINTER(C.c_double)), fi.ctypes.data_as(C.POINTER(C.c_double)),
+        res.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle orc_elastic_aligned failed with code {rc}")
+    return fr, fi, res

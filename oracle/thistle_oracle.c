@@ -408,7 +408,7 @@ typedef struct { int si, sj, sk, sr; const double *z; } zblock_t;
 #define ZAT(Z, a, b, c, d) ((Z)->z[(((size_t)(a) * (Z)->sj + (b)) * (Z)->sk + (c)) * (Z)->sr + (d)])
 
 typedef struct { int kind; int bessel_mode; double cutoff1, cutoff2, cutoffcentre; } kopts_t;
-enum { K_TOTAL = 0, K_ELASTIC = 1, K_J2 = 2 };
+enum { K_TOTAL = 0, K_ELASTIC = 1, K_J2 = 2, K_ELASTIC_J2 = 3 };
 
 /* |E|<1e-30 skips active per kernel (bit k = k-th of MDL MDM MDN MDLp MDMp MDNp) */
 #define SKIP_PZERO   0x1f   /* tot_integral_ijkr_pzero :5010-5031 */
@@ -507,7 +507,10 @@ static int llmax_of(const setup_t *S, int gi, int gj, int gk, int gr) {
 static size_t kernel_work_doubles(void) { return (size_t)DIM * 21 * 21 * 21 + 4096; }
 
 /* tot_integral_k_ijkr (K_TOTAL), integral_k_ijkr (K_ELASTIC),
- * tot_integral_k_ijkr_j2 (K_J2). */
+ * tot_integral_k_ijkr_j2 (K_J2), integral_k_ijkr_j2 (K_ELASTIC_J2,
+ * src/Integrals.f90:5903-6083: the j2 tables and Bessel order of
+ * tot_integral_k_ijkr_j2 with the elastic density and |E| < 1e-30 skips on
+ * MDL..MDMp, no zero-sum return). */
 static int kernel_k_ijkr(const setup_t *S, const kopts_t *o, int gi, int gj, int gk, int gr,
                          double hx, double hy, double hz, double h,
                          const double *dx1, const double *dy1, const double *dz1,
@@ -515,7 +518,7 @@ static int kernel_k_ijkr(const setup_t *S, const kopts_t *o, int gi, int gj, int
                          const zblock_t *Z, double *f, double *work) {
     int LLmax = llmax_of(S, gi, gj, gk, gr);
     if (LLmax + 1 > DIM) return ORC_ERR_L;
-    if (o->kind == K_J2 && LLmax + 3 > DIM) return ORC_ERR_L;
+    if ((o->kind == K_J2 || o->kind == K_ELASTIC_J2) && LLmax + 3 > DIM) return ORC_ERR_L;
     static const double zero20[DIM][DIM];
     double a[DIM][DIM], b[DIM][DIM], c[DIM][DIM], ap[DIM][DIM], bp[DIM][DIM], cp[DIM][DIM];
     memcpy(ap, zero20, sizeof ap); memcpy(bp, zero20, sizeof bp); memcpy(cp, zero20, sizeof cp);
@@ -553,7 +556,8 @@ static int kernel_k_ijkr(const setup_t *S, const kopts_t *o, int gi, int gj, int
     double h_saved[DIM];
     for (int t = 0; t < DIM; ++t) h_saved[t] = 0.0;
     hctx_t hc = {h_saved, h_pre2, Ld};
-    int skip = o->kind == K_TOTAL ? SKIP_KIJKR : (o->kind == K_ELASTIC ? SKIP_ELASTIC : SKIP_J2);
+    int skip = o->kind == K_TOTAL ? SKIP_KIJKR
+             : (o->kind == K_ELASTIC || o->kind == K_ELASTIC_J2) ? SKIP_ELASTIC : SKIP_J2;
     hermite_loop(S, gi, gj, gk, gr, dx1, dy1, dz1, dx2, dy2, dz2, Z, o->cutoff1, o->cutoff2,
                  skip, 1, visit_h, &hc);
     double *scratch = h_pre2 + (size_t)DIM * Ld * Ld * Ld;
@@ -562,7 +566,7 @@ static int kernel_k_ijkr(const setup_t *S, const kopts_t *o, int gi, int gj, int
         for (int t = 0; t < DIM; ++t) s += h_saved[t];
         if (s == 0.0) { for (int iq = 0; iq < S->nq; ++iq) f[iq] = 0.0; return ORC_OK; }
     }
-    if (o->kind == K_J2) {
+    if (o->kind == K_J2 || o->kind == K_ELASTIC_J2) {
         bessels0rr(f, LLmax + 2, S->q, S->nq, h, h_saved, o->bessel_mode, scratch);
         for (int iq = 0; iq < S->nq; ++iq) f[iq] = f[iq] / pow(S->q[iq], 2.0);
     } else {
@@ -579,7 +583,7 @@ static void kernel_pzero(const setup_t *S, const kopts_t *o, int gi, int gj, int
     for (int iq = 0; iq < S->nq; ++iq) f[iq] = 0.0;
     p0ctx_t pc = {f, S};
     hermite_loop(S, gi, gj, gk, gr, dx1, dy1, dz1, dx2, dy2, dz2, Z, o->cutoff1, o->cutoff2,
-                 o->kind == K_ELASTIC ? SKIP_ELASTIC : SKIP_PZERO, 1, visit_p0, &pc);
+                 (o->kind == K_ELASTIC || o->kind == K_ELASTIC_J2) ? SKIP_ELASTIC : SKIP_PZERO, 1, visit_p0, &pc);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -719,6 +723,27 @@ static long enum_quartets(int ng, quartet_t *out) {
     return c;
 }
 
+/* elastic_integration_j2 (src/Integrals.f90:1941-2365) splits loop 2: (i,j,i,r)
+ * for i < j < r with weight 8 (loop id 6), and (i,j,i,j) with weight 4;
+ * loops 1, 3, 4, 5 as above (fewer quartets than enum_quartets: loop 2 takes
+ * each unordered {j, r} once). */
+static long enum_quartets_elastic_j2(int ng, quartet_t *out) {
+    long c = 0;
+    for (int i = 0; i < ng; ++i) for (int j = i + 1; j < ng; ++j)          /* :2005-2074 */
+        for (int k = i + 1; k < ng; ++k) for (int r = k + 1; r < ng; ++r)
+            out[c++] = (quartet_t){i, j, k, r, 1};
+    for (int i = 0; i < ng; ++i) for (int j = i + 1; j < ng; ++j) {        /* :2080-2150 */
+        for (int r = j + 1; r < ng; ++r) out[c++] = (quartet_t){i, j, i, r, 6};
+        out[c++] = (quartet_t){i, j, i, j, 2};
+    }
+    for (int i = 0; i < ng; ++i) for (int k = 0; k < ng; ++k)
+        for (int r = k + 1; r < ng; ++r) out[c++] = (quartet_t){i, i, k, r, 3};
+    for (int i = 0; i < ng; ++i) for (int k = i + 1; k < ng; ++k)
+        out[c++] = (quartet_t){i, i, k, k, 4};
+    for (int i = 0; i < ng; ++i) out[c++] = (quartet_t){i, i, i, i, 5};
+    return c;
+}
+
 /* Fill 5 ints per quartet (i,j,k,r,loop), 0-based groups, in reference order. */
 long orc_enum_quartets(int ng, int *out) {
     long nq = orc_count_quartets(ng);
@@ -733,7 +758,7 @@ long orc_enum_quartets(int ng, int *out) {
     return nq;
 }
 
-static const double loop_weight[6] = {0.0, 8.0, 4.0, 4.0, 2.0, 1.0};
+static const double loop_weight[7] = {0.0, 8.0, 4.0, 4.0, 2.0, 1.0, 8.0};
 
 /* One group quartet: f (nq) before the weight and the e12 factors. */
 static int eval_quartet(const setup_t *S, const dens_t *D, const kopts_t *o, const quartet_t *Q,
@@ -744,7 +769,7 @@ static int eval_quartet(const setup_t *S, const dens_t *D, const kopts_t *o, con
     double hz = PZ(S, k, r) - PZ(S, i, j);
     double h = Q->loop == 1 ? pow(hx * hx + hy * hy + hz * hz, 0.5) : sqrt(hx * hx + hy * hy + hz * hz);
     zblock_t Z = {S->gc[i], S->gc[j], S->gc[k], S->gc[r], zblk};
-    if (o->kind == K_ELASTIC) build_elastic_block(S, D, i, j, k, r, zblk);
+    if (o->kind == K_ELASTIC || o->kind == K_ELASTIC_J2) build_elastic_block(S, D, i, j, k, r, zblk);
     else build_total_block(S, D, i, j, k, r, zblk, zbuf);
     const double *dx1 = DDP(S, S->ddx, j, i), *dy1 = DDP(S, S->ddy, j, i), *dz1 = DDP(S, S->ddz, j, i);
     const double *dx2 = DDP(S, S->ddx, r, k), *dy2 = DDP(S, S->ddy, r, k), *dz2 = DDP(S, S->ddz, r, k);
@@ -780,7 +805,8 @@ static int run_quartets(const setup_t *S, const dens_t *D, const kopts_t *o, con
 #pragma omp parallel
     {
         double *zblk = malloc(sizeof(double) * zbsz);
-        double *zbuf = (o->kind == K_ELASTIC || D->rho) ? NULL : malloc(sizeof(double) * zbuf_sz);
+        double *zbuf = (o->kind == K_ELASTIC || o->kind == K_ELASTIC_J2 || D->rho) ? NULL
+                                                                              : malloc(sizeof(double) * zbuf_sz);
         double *work = malloc(sizeof(double) * kernel_work_doubles());
         double *f = malloc(sizeof(double) * nq);
 #pragma omp for schedule(dynamic, 1)
@@ -865,13 +891,14 @@ int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const 
                       double cutoffz, double cutoffmd, double cutoffcentre, int bessel_mode, int nthreads,
                       const int *quartets, long nquart, const double *weights, const double *rho,
                       double *result) {
-    if (type != 1 && type != 2 && type != 7) return ORC_ERR_ARG;
+    if (type != 1 && type != 2 && type != 7 && type != 8) return ORC_ERR_ARG;
     setup_t S;
-    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, q, nq, type == 7 ? 2 : 1);
+    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, q, nq, (type == 7 || type == 8) ? 2 : 1);
     if (e != ORC_OK) { free_setup(&S); return e; }
     dens_t D;
-    kopts_t o = {type == 1 ? K_TOTAL : (type == 2 ? K_ELASTIC : K_J2), bessel_mode, cutoffz, cutoffmd, cutoffcentre};
-    if (type == 2) {
+    kopts_t o = {type == 1 ? K_TOTAL : type == 2 ? K_ELASTIC : type == 7 ? K_J2 : K_ELASTIC_J2, bessel_mode, cutoffz,
+                 cutoffmd, cutoffcentre};
+    if (type == 2 || type == 8) {
         memset(&D, 0, sizeof D);
         D.mmod = mmod; D.nmo = nmo;
         if (nmo1 > nmo) { free_setup(&S); return ORC_ERR_ARG; }
@@ -896,7 +923,8 @@ int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const 
     } else {
         nqt = orc_count_quartets(S.ng);
         Qs = malloc(sizeof(quartet_t) * (size_t)nqt);
-        enum_quartets(S.ng, Qs);
+        if (type == 8) nqt = enum_quartets_elastic_j2(S.ng, Qs);
+        else enum_quartets(S.ng, Qs);
     }
     if (e == ORC_OK) e = run_quartets(&S, &D, &o, Qs, nqt, weights, result, nthreads);
     free(Qs);
@@ -1194,6 +1222,106 @@ int orc_count_te(int ngto, const double *ga, const int *l, const int *m, const i
     }
     free_dens(&D); free_setup(&S);
     return ORC_OK;
+}
+
+/*
+ * Elastic aligned intensity, CASE(4) of total_scattering_calculation
+ * (src/main_calculation.f90:218-265): F(q) of elastic_integration_alig
+ * (src/Integrals.f90:2366-2490) with integral_k_ijkr_alig (:6085-6190) --
+ * every ordered group pair (i, j), H = P_ij, the pair's functions with
+ * ztot = Z(a, b), the three MD factors with their |E| < 1e-30 skips and the
+ * product kept when |prod3| > 1e-30, times (i qx)^ll (i qy)^mm (i qz)^nn,
+ * e^{i qx Hx} e^{i qy Hy} e^{i qz Hz} and e12(|q|, i, j) -- and the result
+ * |F|^2.  qal is (3, nq) column-major; Z comes from the 1-RDM as for type 2.
+ */
+int orc_elastic_aligned(int ngto, const double *ga, const int *l, const int *m, const int *n,
+                        const double *xx, const double *yy, const double *zz, const int *group,
+                        const double *mmod, int nmo, const double *onerdm, int nmo1, const double *qal, int nq,
+                        double *f_re, double *f_im, double *result) {
+    double *qabs = malloc(sizeof(double) * nq);
+    for (int iq = 0; iq < nq; ++iq)
+        qabs[iq] = sqrt(pow(qal[3 * iq], 2.0) + pow(qal[3 * iq + 1], 2.0) + pow(qal[3 * iq + 2], 2.0));
+    setup_t S;
+    int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, qabs, nq, 0);
+    if (e != ORC_OK) { free_setup(&S); free(qabs); return e; }
+    if (nmo1 > nmo) { free_setup(&S); free(qabs); return ORC_ERR_ARG; }
+    dens_t D;
+    memset(&D, 0, sizeof D);
+    D.mmod = mmod; D.nmo = nmo;
+    D.zao = malloc(sizeof(double) * (size_t)ngto * ngto);
+    build_zao(&S, &D, onerdm, nmo1);
+    int dt = S.dt, dl = S.dl;
+    for (int iq = 0; iq < nq; ++iq) { f_re[iq] = 0.0; f_im[iq] = 0.0; }
+    for (int gi = 0; gi < S.ng; ++gi)
+        for (int gj = 0; gj < S.ng; ++gj) {
+            const double Hx = PX(&S, gi, gj), Hy = PY(&S, gi, gj), Hz = PZ(&S, gi, gj);
+            const double *dx1 = DDP(&S, S.ddx, gj, gi), *dy1 = DDP(&S, S.ddy, gj, gi), *dz1 = DDP(&S, S.ddz, gj, gi);
+#define DXA(arr, t, a, b) (arr)[(t) + dt * ((a) + dl * (b))]
+            for (int iq = 0; iq < nq; ++iq) {
+                const double qx = qal[3 * iq], qy = qal[3 * iq + 1], qz = qal[3 * iq + 2];
+                double hr = 0.0, hi = 0.0;
+                for (int i = S.gs[gi] - 1; i < S.gs[gi] - 1 + S.gc[gi]; ++i)
+                    for (int j = S.gs[gj] - 1; j < S.gs[gj] - 1 + S.gc[gj]; ++j) {
+                        double ztot = D.zao[i + (size_t)ngto * j];
+                        for (int ll = 0; ll <= l[i] + l[j]; ++ll) {
+                            double MDL = DXA(dx1, ll, l[i], l[j]);
+                            if (fabs(MDL) < SKIP30) continue;
+                            double prod1 = MDL * ztot;
+                            for (int mm = 0; mm <= m[i] + m[j]; ++mm) {
+                                double MDM = DXA(dy1, mm, m[i], m[j]);
+                                if (fabs(MDM) < SKIP30) continue;
+                                double prod2 = MDM * prod1;
+                                for (int nn = 0; nn <= n[i] + n[j]; ++nn) {
+                                    double MDN = DXA(dz1, nn, n[i], n[j]);
+                                    if (fabs(MDN) < SKIP30) continue;
+                                    double prod3 = MDN * prod2;
+                                    if (!(fabs(prod3) > SKIP30)) continue;
+                                    /* exponent1 = (i qx)^ll (i qy)^mm (i qz)^nn */
+                                    double er = 1.0, ei = 0.0;
+                                    const double comp[3] = {qx, qy, qz};
+                                    const int pw[3] = {ll, mm, nn};
+                                    for (int ax = 0; ax < 3; ++ax)
+                                        for (int t = 0; t < pw[ax]; ++t) {
+                                            double a = -ei * comp[ax], b = er * comp[ax];
+                                            er = a; ei = b;
+                                        }
+                                    hr = hr + er * prod3;
+                                    hi = hi + ei * prod3;
+                                }
+                            }
+                        }
+                    }
+                double fr = hr, fi = hi;
+                const double ang[3] = {qx * Hx, qy * Hy, qz * Hz};
+                for (int ax = 0; ax < 3; ++ax) {
+                    double cr = cos(ang[ax]), ci = sin(ang[ax]);
+                    double a = fr * cr - fi * ci, b = fr * ci + fi * cr; fr = a; fi = b;
+                }
+                const double w = E12(&S, iq, gi, gj);
+                f_re[iq] += fr * w;
+                f_im[iq] += fi * w;
+            }
+#undef DXA
+        }
+    for (int iq = 0; iq < nq; ++iq) result[iq] = f_re[iq] * f_re[iq] + f_im[iq] * f_im[iq];
+    free_dens(&D); free_setup(&S); free(qabs);
+    return ORC_OK;
+}
+
+/* The q vectors of CASE(4) (src/main_calculation.f90:227-241) for nq points:
+ * ss = (linspace(0, pi/2, nq) - pi) / 2, k0 = 3.00 * 1.889726125 * 0.529,
+ * q = 2 k0 cos(ss) (sin ss, 0, cos ss); written (3, nq) column-major. */
+void orc_elastic_aligned_grid(int nq, double *qal) {
+    const double pi = acos(-1.0);
+    const double k0 = 3.00 * 1.889726125 * 0.529;
+    for (int mm = 0; mm < nq; ++mm) {
+        double ss = nq > 1 ? (pi / 2.0) * (double)mm / (double)(nq - 1) : 0.0;
+        ss = (ss - pi) / 2.0;
+        const double rr = 2.0 * k0 * cos(ss);
+        qal[3 * mm] = rr * sin(ss) * cos(0.0);
+        qal[3 * mm + 1] = rr * sin(ss) * sin(0.0);
+        qal[3 * mm + 2] = rr * cos(ss);
+    }
 }
 
 /* QCOORD3 (src/main_calculation.f90:864-929): the 3131-vector aligned grid. */

@@ -4,7 +4,8 @@
 
 Inputs are regenerated from the seeded generators in thistle_b200.inputs;
 outputs are the oracle's restatement of the reference integrators
-(bessel_mode 0: the reference's own 100-term dphrec start).
+(bessel_mode 0: the reference's own 100-term dphrec start) for types 1, 2,
+7 and 8, and the elastic aligned intensity of type 4 on the CASE(4) grid.
 """
 import os
 import sys
@@ -22,8 +23,10 @@ def main():
     for cfg in (1, 2):
         p = I.CONFIGS[cfg]()
         out = {"q": p.q}
-        for t in (1, 2, 7):
+        for t in (1, 2, 7, 8):
             out[f"type{t}"] = O.scattering(p, t, nthreads=8)
+        # type 4 on the reference's CASE(4) grid of nq vectors: |F(q)|^2
+        out["type4"] = O.elastic_aligned(p, nq=p.nq)[2]
         np.savez(os.path.join(HERE, f"golden_cfg{cfg}.npz"), **out)
         print(cfg, {k: v[:2] for k, v in out.items()})
 

@@ -33,7 +33,7 @@ EXPORTS = sorted([
     "thistle_plan_vjp_batch", "thistle_plan_vjp_batch_device", "thistle_plan_use_graph",
     "thistle_plan_autotune_batch", "thistle_batch_create", "thistle_batch_use_graph", "thistle_batch_execute",
     "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy", "thistle_plan_nuclear",
-    "thistle_plan_density",
+    "thistle_plan_density", "thistle_plan_form_factor", "thistle_elastic_aligned_grid",
 ])
 
 

@@ -415,6 +415,7 @@ cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args 
   if (kind == KIND_TOTAL) return launch_stage1_xk_k<KIND_TOTAL>(L, LK, XB, a, ngeom, st);
   if (kind == KIND_ELASTIC) return launch_stage1_xk_k<KIND_ELASTIC>(L, LK, XB, a, ngeom, st);
   if (kind == KIND_ALIGNED) return launch_stage1_xk_k<KIND_ALIGNED>(L, LK, XB, a, ngeom, st);
+  if (kind == KIND_ELASTIC_J2) return launch_stage1_xk_k<KIND_ELASTIC_J2>(L, LK, XB, a, ngeom, st);
   return launch_stage1_xk_k<KIND_J2>(L, LK, XB, a, ngeom, st);
 }
 
@@ -423,6 +424,7 @@ cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1A
   if (kind == KIND_TOTAL) return launch_stage1_xsplit_k<KIND_TOTAL>(L, LK, XB, a, xbuf, nout, st);
   if (kind == KIND_ELASTIC) return launch_stage1_xsplit_k<KIND_ELASTIC>(L, LK, XB, a, xbuf, nout, st);
   if (kind == KIND_ALIGNED) return launch_stage1_xsplit_k<KIND_ALIGNED>(L, LK, XB, a, xbuf, nout, st);
+  if (kind == KIND_ELASTIC_J2) return launch_stage1_xsplit_k<KIND_ELASTIC_J2>(L, LK, XB, a, xbuf, nout, st);
   return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, st);
 }
 
@@ -433,6 +435,7 @@ cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const St
   if (kind == KIND_TOTAL) TB_K(KIND_TOTAL);
   if (kind == KIND_ELASTIC) TB_K(KIND_ELASTIC);
   if (kind == KIND_ALIGNED) TB_K(KIND_ALIGNED);
+  if (kind == KIND_ELASTIC_J2) TB_K(KIND_ELASTIC_J2);
   TB_K(KIND_J2);
 #undef TB_K
 }
@@ -454,14 +457,16 @@ cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Arg
   if (kind == KIND_TOTAL) return launch_stage1_batch_k<KIND_TOTAL>(L, LK, XB, d, pre, n, blocks, st);
   if (kind == KIND_ELASTIC) return launch_stage1_batch_k<KIND_ELASTIC>(L, LK, XB, d, pre, n, blocks, st);
   if (kind == KIND_ALIGNED) return launch_stage1_batch_k<KIND_ALIGNED>(L, LK, XB, d, pre, n, blocks, st);
+  if (kind == KIND_ELASTIC_J2) return launch_stage1_batch_k<KIND_ELASTIC_J2>(L, LK, XB, d, pre, n, blocks, st);
   return launch_stage1_batch_k<KIND_J2>(L, LK, XB, d, pre, n, blocks, st);
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st) {
-  // instantiated in tb_stage1_{total,elastic,j2,aligned}.cu
+  // instantiated in tb_stage1_{total,elastic,j2,aligned,elastic_j2}.cu
   if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, ngeom, st);
   if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, ngeom, st);
   if (kind == KIND_ALIGNED) return launch_stage1_k<KIND_ALIGNED>(L, a, ngeom, st);
+  if (kind == KIND_ELASTIC_J2) return launch_stage1_k<KIND_ELASTIC_J2>(L, a, ngeom, st);
   return launch_stage1_k<KIND_J2>(L, a, ngeom, st);
 }
 

@@ -208,6 +208,12 @@ cudaError_t launch_dmma_gemm(const DmmaGemmArgs &g, int mode, bool b_jcontig, in
 int transform_ct_width(int ngto);
 cudaError_t launch_transform_ct(const double *C, int n, int ngto, double *Ct, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *v, int64_t n, cudaStream_t st);
+// elastic aligned intensity (tb_formfactor.cu): one record per unordered group
+// pair (form_factor_record_doubles(npair) doubles at rec), then F(q) on nq q
+// vectors (3 interleaved doubles each): real and imaginary part and |F|^2
+int64_t form_factor_record_doubles(int64_t npair);
+cudaError_t launch_form_factor(const Stage1Args &a, double *rec, const double *qv, int nq, double *out_re,
+                               double *out_im, double *out_abs2, cudaStream_t st);
 // molecule batches: pair tables of every item (blocks pre[i] .. pre[i+1]-1 of 128 pairs)
 struct PairDesc {
   int ng, maxa;

@@ -43,7 +43,12 @@ constexpr int SER_K = 24;
 #define TB_SKIP30 1.0000000031710769e-30
 #define TB_PI 3.141592653589793
 
-enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2, KIND_ALIGNED = 3 };
+// KIND_ELASTIC_J2: the j2 Bessel expansion of total j2 on the elastic density
+// product Z_ab Z_cd (integral_k_ijkr_j2, src/Integrals.f90:5903-6083)
+enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2, KIND_ALIGNED = 3, KIND_ELASTIC_J2 = 4 };
+// j2 Bessel expansion (order LLmax + 2, P2 weight) / density from the 1-RDM
+TB_HD constexpr bool kind_j2(int k) { return k == KIND_J2 || k == KIND_ELASTIC_J2; }
+TB_HD constexpr bool kind_elastic(int k) { return k == KIND_ELASTIC || k == KIND_ELASTIC_J2; }
 enum RecKind { REC_BESSEL = 0, REC_BESSEL_J2 = 1, REC_P0 = 2 };
 
 // number of (T,U,V) with T+U+V <= L

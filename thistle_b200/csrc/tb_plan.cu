@@ -337,7 +337,7 @@ static int density_alloc(thistle_plan *P) {
   const int n = P->nmo, ngto = P->ngto;
   const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
   TB_TRY(dalloc(&P->d_C, (size_t)n * ngto, "MO coefficients"));
-  if (P->kind == KIND_ELASTIC) {
+  if (kind_elastic(P->kind)) {
     TB_TRY(dalloc(&P->d_zao, (size_t)ngto * ngto, "AO density"));
     TB_TRY(dalloc(&P->d_D, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
     TB_TRY(dalloc(&P->d_Ds, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
@@ -370,7 +370,7 @@ done:
 static int density_upload(thistle_plan *P, const double *mmod, const int32_t *mat, const double *total,
                           const double *onerdm) {
   TB_CK(cudaMemcpyAsync(P->d_C, mmod, sizeof(double) * (size_t)P->nmo * P->ngto, cudaMemcpyHostToDevice, P->st));
-  if (P->kind == KIND_ELASTIC) {
+  if (kind_elastic(P->kind)) {
     TB_CK(cudaMemcpyAsync(P->d_D, onerdm, sizeof(double) * (size_t)P->nmo1 * P->nmo1, cudaMemcpyHostToDevice,
                           P->st));
   } else if (P->nmat > 0) {
@@ -388,7 +388,7 @@ static int density_run(thistle_plan *P) {
   const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
   TB_TRYC(launch_transform_ct(P->d_C, n, ngto, P->d_Ct, P->st));
   P->launches += 1;
-  if (P->kind == KIND_ELASTIC) {
+  if (kind_elastic(P->kind)) {
     // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217),
     // C1 the first nmo1 MOs: Y(i, a) = sum_j Ds(i, j) C(j, a), then
     // Z(a, b) = sum_i C(i, a) Y(i, b)
@@ -592,7 +592,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   if (!out) return fail(THISTLE_ERR_ARG, "null plan pointer");
   *out = nullptr;
   if (type != THISTLE_TOTAL_J0 && type != THISTLE_ELASTIC_J0 && type != THISTLE_TOTAL_J2 &&
-      type != THISTLE_TOTAL_ALIGNED)
+      type != THISTLE_TOTAL_ALIGNED && type != THISTLE_ELASTIC_J2)
     return fail(THISTLE_ERR_TYPE, "calculation type " + std::to_string(type) + " is not provided by this entry");
   thistle_plan *P = new thistle_plan();
   int rc = THISTLE_OK;
@@ -616,6 +616,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   P->type = type;
   P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL
             : type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC
+            : type == THISTLE_ELASTIC_J2 ? KIND_ELASTIC_J2
             : type == THISTLE_TOTAL_ALIGNED ? KIND_ALIGNED : KIND_J2;
   P->nq = nq;
   P->qdim = type == THISTLE_TOTAL_ALIGNED ? 3 : 1;
@@ -625,7 +626,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   P->cutoffmd = cutoffmd;
   P->cutoffcentre = cutoffcentre;
   P->np = (int64_t)ngto * (ngto + 1) / 2;
-  if (P->kind == KIND_ELASTIC) {
+  if (kind_elastic(P->kind)) {
     if (!onerdm || nmo1 <= 0 || nmo1 > norbs) { rc = fail(THISTLE_ERR_ARG, "1-RDM must be (nmo1,nmo1) with nmo1 <= norbs"); goto done; }
     if (!finite_all(onerdm, (int64_t)nmo1 * nmo1)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 1-RDM"); goto done; }
     P->nmo1 = nmo1;
@@ -681,8 +682,8 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     int maxbps = 1;
     for (int b = 0; b <= LMAXB; ++b) P->s2_bps[b] = 0;
     for (int c = 0; c < P->ncls && P->kind != KIND_ALIGNED; ++c) {
-      int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
-      P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, P->kind == KIND_J2, P->s2_qtile);
+      int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
+      P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, kind_j2(P->kind), P->s2_qtile);
       maxbps = std::max(maxbps, P->s2_bps[LB]);
     }
     // aligned: quartet slices of the q-vector kernel (one partial row each)
@@ -872,7 +873,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     double dq = 0.0;
     grid_info(P->hq.data() + q0, tn, uniform, first_on_grid, dq);
     for (int c = 0; c < ncls; ++c) {
-      const int LB = cL[c] + (P->kind == KIND_J2 ? 2 : 0);
+      const int LB = cL[c] + (kind_j2(P->kind) ? 2 : 0);
       Stage2ClassArgs s;
       s.rec = d_rec + recoff[c];
       s.rs = rs[c];
@@ -886,7 +887,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       s.uniform = uniform;
       s.first_on_grid = first_on_grid;
       s.dq = dq;
-      s.j2 = P->kind == KIND_J2;
+      s.j2 = kind_j2(P->kind);
       s.partial = P->d_partial + q0;
       s.pstride = P->nq;
       // a class too small to fill the GPU several times over is also split
@@ -1177,6 +1178,59 @@ done:
 
 // Inn(q) = sum_ij Zn_i Zn_j sinc(q R_ij), sinc(x) = 1 for |x| < 1e-10
 // (src/main_calculation.f90:302-311, 853-861)
+// ---------------------------------------------------------------------------
+// elastic aligned intensity (type 4): F(q) on q vectors from the AO density
+// ---------------------------------------------------------------------------
+// F(q) of elastic_integration_alig (src/Integrals.f90:2366-2490) for the
+// plan's current centres on nq q vectors (3 interleaved doubles each, host);
+// re / im / abs2 (host, any may be NULL) get F and |F|^2 (tb_formfactor.cu).
+static int form_factor(thistle_plan *P, const double *qvec, int nq, double *re, double *im, double *abs2) {
+  if (!kind_elastic(P->kind)) return fail(THISTLE_ERR_TYPE, "the form factor needs an elastic plan (the 1-RDM)");
+  if (!qvec || nq <= 0) return fail(THISTLE_ERR_ARG, "empty q-vector list");
+  if (!finite_all(qvec, 3 * (int64_t)nq)) return fail(THISTLE_ERR_NONFINITE, "non-finite q vector");
+  if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "the form factor is computed for single-geometry plans");
+  int rc = THISTLE_OK;
+  double *d_rec = nullptr, *d_qv = nullptr, *d_out = nullptr;
+  std::vector<double> h((size_t)3 * nq);
+  TB_TRY(dalloc(&d_rec, (size_t)form_factor_record_doubles(npairs(P->ng)), "form-factor records"));
+  TB_TRY(dalloc(&d_qv, (size_t)3 * nq, "q vectors"));
+  TB_TRY(dalloc(&d_out, (size_t)3 * nq, "form factor"));
+  TB_TRYC(cudaMemcpyAsync(d_qv, qvec, sizeof(double) * 3 * (size_t)nq, cudaMemcpyHostToDevice, P->st));
+  TB_TRYC(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa, 1,
+                             3 * (int64_t)P->ngto, gs_pair(P), gs_esoa(P), P->st));
+  {
+    const Stage1Args a = stage1_args(P, P->d_quart, 0, 0, nullptr, 0, 0);
+    TB_TRYC(launch_form_factor(a, d_rec, d_qv, nq, d_out, d_out + nq, d_out + 2 * (size_t)nq, P->st));
+  }
+  P->launches = 3;
+  TB_TRYC(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * 3 * (size_t)nq, cudaMemcpyDeviceToHost, P->st));
+  TB_TRYC(cudaStreamSynchronize(P->st));
+  P->fwd_valid = false;  // the pair tables were rebuilt
+  if (re) std::copy(h.begin(), h.begin() + nq, re);
+  if (im) std::copy(h.begin() + nq, h.begin() + 2 * (size_t)nq, im);
+  if (abs2) std::copy(h.begin() + 2 * (size_t)nq, h.end(), abs2);
+done:
+  dfree(d_rec);
+  dfree(d_qv);
+  dfree(d_out);
+  return rc;
+}
+
+// The q vectors of CASE(4) (src/main_calculation.f90:227-241) for nq points:
+// ss = (linspace(0, pi/2, nq) - pi) / 2, k0 = 3.00 * 1.889726125 * 0.529,
+// q = 2 k0 cos(ss) (sin ss, 0, cos ss), written (3, nq) column-major.
+static void elastic_aligned_grid(int nq, double *qal) {
+  const double pi = std::acos(-1.0), k0 = 3.00 * 1.889726125 * 0.529;
+  for (int mm = 0; mm < nq; ++mm) {
+    double ss = nq > 1 ? (pi / 2.0) * (double)mm / (double)(nq - 1) : 0.0;
+    ss = (ss - pi) / 2.0;
+    const double rr = 2.0 * k0 * std::cos(ss);
+    qal[3 * mm] = rr * std::sin(ss) * std::cos(0.0);
+    qal[3 * mm + 1] = rr * std::sin(ss) * std::sin(0.0);
+    qal[3 * mm + 2] = rr * std::cos(ss);
+  }
+}
+
 static void nuclear_nuclear(const double *Zn, const double *geom, int natoms, const double *q, int nq, double *out) {
   for (int k = 0; k < nq; ++k) out[k] = 0.0;
   for (int i = 0; i < natoms; ++i)
@@ -1262,7 +1316,7 @@ static int batch_run(thistle_batch *B) {
   }
   TB_CK(cudaMemsetAsync(B->d_partial, 0, sizeof(double) * B->partial_len, st));
   for (auto &x : B->s2) {
-    TB_CK(launch_stage2_class_batch(x.LB, B->kind == KIND_J2, x.d, x.pre, x.n, x.blocks, B->nqmax, st));
+    TB_CK(launch_stage2_class_batch(x.LB, kind_j2(B->kind), x.d, x.pre, x.n, x.blocks, B->nqmax, st));
     B->launches += 1;
   }
   TB_CK(launch_reduce_desc(B->d_red, (int)B->plans.size(), B->nqmax, st));
@@ -1428,7 +1482,7 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
       double dq = 0.0;
       grid_info(P->hq.data(), P->nq, uniform, first_on_grid, dq);
       for (int c = 0; c < P->ncls; ++c) {
-        const int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
+        const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
         Stage2ClassArgs s;
         s.rec = P->d_rec + P->cls_recoff[c];
         s.rs = P->cls_rs[c];
@@ -1441,7 +1495,7 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
         s.first_on_grid = first_on_grid;
         s.dq = dq;
         s.chunk = 0;
-        s.j2 = P->kind == KIND_J2;
+        s.j2 = kind_j2(P->kind);
         s.partial = part[i];
         s.pstride = P->nq;
         s.gs_rec = 0;
@@ -1682,8 +1736,8 @@ static int set_qtile(thistle_plan *P, int qt) {
   P->s2_qtile = std::max(1, std::min(qt, std::min(P->nq, STAGE2_QTILE)));
   int maxbps = 1;
   for (int c = 0; c < P->ncls; ++c) {
-    const int LB = P->cls_L[c] + (P->kind == KIND_J2 ? 2 : 0);
-    P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, P->kind == KIND_J2, P->s2_qtile);
+    const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
+    P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, kind_j2(P->kind), P->s2_qtile);
     maxbps = std::max(maxbps, P->s2_bps[LB]);
   }
   P->s2_rows = P->nsm * maxbps;
@@ -1938,7 +1992,7 @@ int thistle_plan_density(const thistle_plan *P, double *out, int64_t count, int6
   if (!out) return THISTLE_OK;
   if (count < *needed) return fail(THISTLE_ERR_ARG, "output holds " + std::to_string(count) + " doubles, the density " +
                                                        std::to_string(*needed));
-  const double *src = P->kind == KIND_ELASTIC ? P->d_zao : P->d_rho;
+  const double *src = kind_elastic(P->kind) ? P->d_zao : P->d_rho;
   TB_CK(cudaStreamSynchronize(P->st));
   TB_CK(cudaMemcpy(out, src, sizeof(double) * (size_t)*needed, cudaMemcpyDeviceToHost));
   return THISTLE_OK;
@@ -2002,6 +2056,18 @@ int thistle_plan_destroy(thistle_plan *P) {
   return THISTLE_OK;
 }
 
+int thistle_plan_form_factor(thistle_plan *P, const double *qvec, int32_t nq, double *re_host, double *im_host,
+                             double *abs2_host) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  return form_factor(P, qvec, nq, re_host, im_host, abs2_host);
+}
+
+int thistle_elastic_aligned_grid(int32_t nq, double *q_al) {
+  if (nq <= 0 || !q_al) return fail(THISTLE_ERR_ARG, "nq must be positive and q_al non-null");
+  elastic_aligned_grid(nq, q_al);
+  return THISTLE_OK;
+}
+
 int thistle_plan_nuclear(thistle_plan *P, const double *Zn, const double *geom, int32_t natoms, double *ine_host) {
   if (!P || !ine_host) return fail(THISTLE_ERR_ARG, "null argument");
   return nuclear_term(P, Zn, geom, natoms, ine_host);
@@ -2042,6 +2108,25 @@ int thistle_total_scattering(int32_t type, const double *Zn, const double *geom,
         for (int k = 0; k < nq; ++k) q_abs_out[k] = q[k];
     }
     if (T) thistle_plan_destroy(T);
+    thistle_plan_destroy(E);
+    return rc;
+  }
+  if (type == THISTLE_ELASTIC_ALIGNED) {
+    // CASE(4): |F(q)|^2 on the reference's own grid of nq vectors, whatever q
+    // holds; q_abs_out gets |q| (src/main_calculation.f90:218-265)
+    if (!onerdm || nmo1 <= 0) return fail(THISTLE_ERR_ARG, "the elastic aligned intensity needs the 1-RDM");
+    if (nq <= 0) return fail(THISTLE_ERR_ARG, "nq must be positive");
+    std::vector<double> qal((size_t)3 * nq), qabs((size_t)nq);
+    elastic_aligned_grid(nq, qal.data());
+    for (int i = 0; i < nq; ++i)
+      qabs[i] = std::sqrt(qal[3 * i] * qal[3 * i] + qal[3 * i + 1] * qal[3 * i + 1] + qal[3 * i + 2] * qal[3 * i + 2]);
+    thistle_plan *E = nullptr;
+    int rc = plan_create(&E, THISTLE_ELASTIC_J0, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, nullptr, nullptr,
+                         0, onerdm, nmo1, qabs.data(), nq, cutoffz, cutoffmd, cutoffcentre);
+    if (rc != THISTLE_OK) return rc;
+    if (ng != E->ng) rc = fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
+    if (rc == THISTLE_OK) rc = form_factor(E, qal.data(), nq, nullptr, nullptr, result_out);
+    if (rc == THISTLE_OK && q_abs_out) std::copy(qabs.begin(), qabs.end(), q_abs_out);
     thistle_plan_destroy(E);
     return rc;
   }

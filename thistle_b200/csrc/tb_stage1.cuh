@@ -122,7 +122,7 @@ __device__ __forceinline__ QuartetHead quartet_head(const Stage1Args &A, int64_t
   Q.p0 = KIND == KIND_ALIGNED ? false : (Q.loop == 5 || Q.h < A.cutoffcentre);
   // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
   // a skipped factor removes every term it multiplies, i.e. it is a zero.
-  Q.skip = (Q.p0 || KIND == KIND_ALIGNED || KIND == KIND_ELASTIC) ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : 0x0f);
+  Q.skip = (Q.p0 || KIND == KIND_ALIGNED || kind_elastic(KIND)) ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : 0x0f);
   return Q;
 }
 
@@ -167,8 +167,8 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
         for (int U = 0; U <= 2 * k - T; U += 2) {
           if ((cnt++ % S) != sub) continue;
           int V = 2 * k - T - U;
-          double f = p0_factor(T, U, V, KIND == KIND_J2);
-          if (KIND == KIND_J2) f = (T + U - 2 * V) / 4.0 * f;
+          double f = p0_factor(T, U, V, kind_j2(KIND));
+          if (kind_j2(KIND)) f = (T + U - 2 * V) / 4.0 * f;
           cs[k] += D[dindex<L>(T, U, V) * dstride] * f;
         }
 #pragma unroll
@@ -182,7 +182,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
     r[3] = (double)(NS - 1);
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      double acc = KIND == KIND_J2 ? cs[k] * fj2 : cs[k];
+      double acc = kind_j2(KIND) ? cs[k] * fj2 : cs[k];
       r[4 + k] = pre * ((k & 1) ? -acc : acc);
     }
     return;
@@ -191,7 +191,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
   // Bessel expansion: h[b] = sum_TUV D[TUV] sum_{p} a(T,px) b(U,py) c(V,pz),
   // b = (T+px)/2 + (U+py)/2 + (V+pz)/2 (BesselDeriv); for j2 the four-term
   // BesselDeriv2j form with two extra orders (src/Integrals.f90:6370-6434).
-  constexpr int LB = KIND == KIND_J2 ? L + 2 : L;
+  constexpr int LB = kind_j2(KIND) ? L + 2 : L;
   constexpr int TP = tp_size(L);
   double ax[TP], ay[TP], az[TP];
   hermite_table(L, Q.Hx, ax);
@@ -217,7 +217,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
             for (int k3 = 0; 2 * k3 <= V; ++k3) {
               double cz = az[tp_off(V) + k3];
               int s3 = (T - k1) + (U - k2) + (V - k3);
-              if (KIND != KIND_J2) {
+              if (!kind_j2(KIND)) {
                 hh[s3] += d * (cx * cy * cz);
               } else {
                 double cz1 = (double)(2 * (V - k3)) * cz;
@@ -231,7 +231,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
 #pragma unroll
   for (int b = 0; b <= LB; ++b) hh[b] = group_sum<S>(hh[b], gmask);
   if (!leader) return;
-  if (KIND == KIND_J2) {
+  if (kind_j2(KIND)) {
     const double f = 0.25 * sqrt(5.0 / TB_PI);
 #pragma unroll
     for (int b = 0; b <= LB; ++b) hh[b] *= f;
@@ -248,7 +248,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
   }
   r[0] = Q.h;
   r[1] = Q.tb[5] + Q.tk[5];
-  r[2] = (double)(KIND == KIND_J2 ? REC_BESSEL_J2 : REC_BESSEL);
+  r[2] = (double)(kind_j2(KIND) ? REC_BESSEL_J2 : REC_BESSEL);
   r[3] = (double)LB;
   // hhat_b = h_b / H^{2b}: F = sum_b hhat_b j_b(x) x^b, x = qH
   const double invH2 = 1.0 / (Q.h * Q.h);
@@ -329,8 +329,8 @@ __device__ __forceinline__ void stage1_reg_body(Stage1Args &A, int64_t vb) {
       const int ia = ab / nj, ib = ab - ia * nj;
       const int fa = si + ia, fb = sj + ib;
       const int la = A.flmn[fa], lb = A.flmn[fb];
-      const int64_t rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-      const double zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      const int64_t rowp = kind_elastic(KIND) ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      const double zab = kind_elastic(KIND) ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
       // bra coefficients with the (-1)^t sign of src/Integrals.f90:5181
       double bx[L + 1], by[L + 1], bz[L + 1];
       {
@@ -352,7 +352,7 @@ __device__ __forceinline__ void stage1_reg_body(Stage1Args &A, int64_t vb) {
       const int ncd = nk * nr;
       auto fetch = [&](int ic, int id, double &zo, double *kxo, double *kyo, double *kzo) {
         const int fc = sk + ic, fd = sr + id;
-        if (KIND == KIND_ELASTIC) zo = A.zao[(size_t)fc * A.ngto + fd] * zab;
+        if (kind_elastic(KIND)) zo = A.zao[(size_t)fc * A.ngto + fd] * zab;
         else zo = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
         const int lc = A.flmn[fc], ld = A.flmn[fd];
         const double *ex = esoa_slot(A, Q.skip & 8, 0, lc & 0xff, ld & 0xff, pk);
@@ -512,8 +512,8 @@ __device__ __forceinline__ void stage1_smem_body(Stage1Args &A, int64_t vb) {
       cur_ab = ab;
       const int fa = si + ab / nj, fb = sj + ab % nj;
       const int la = A.flmn[fa], lb = A.flmn[fb];
-      rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-      zab = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+      rowp = kind_elastic(KIND) ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+      zab = kind_elastic(KIND) ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
       const int lx1 = la & 0xff, ly1 = (la >> 8) & 0xff, lz1 = (la >> 16) & 0xff;
       const int lx2 = lb & 0xff, ly2 = (lb >> 8) & 0xff, lz2 = (lb >> 16) & 0xff;
       nx1 = lx1 + lx2;
@@ -535,7 +535,7 @@ __device__ __forceinline__ void stage1_smem_body(Stage1Args &A, int64_t vb) {
     }
     const int fc = sk + cd / nr, fd = sr + cd % nr;
     double ztot;
-    if (KIND == KIND_ELASTIC) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
+    if (kind_elastic(KIND)) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
     else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
     if (fabs(ztot) < A.cutoffz) continue;
     const int lc = A.flmn[fc], ld = A.flmn[fd];
@@ -672,17 +672,17 @@ __device__ __forceinline__ void xk_contract(const Stage1Args &A, const QuartetHe
   int64_t rowp = 0;
   double zo = 0.0;
   if (!XB) {
-    rowp = KIND == KIND_ELASTIC ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
-    zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+    rowp = kind_elastic(KIND) ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+    zo = kind_elastic(KIND) ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
   } else {
-    zo = KIND == KIND_ELASTIC ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
+    zo = kind_elastic(KIND) ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
   }
   for (int c = 0; c < S.nin; ++c) {
     int ga, gb2, gc, gd;
     if (XB) { ga = S.si + c / S.nj; gb2 = S.sj + c % S.nj; gc = fc; gd = fd; }
     else { gc = S.sk + c / S.nr; gd = S.sr + c % S.nr; ga = fa; gb2 = fb; }
     double z;
-    if (KIND == KIND_ELASTIC) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
+    if (kind_elastic(KIND)) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
     else {
       const int64_t rp = XB ? fpair(min(ga, gb2), max(ga, gb2)) * A.np : rowp;
       z = A.rho[rp + fpair(min(gc, gd), max(gc, gd))];

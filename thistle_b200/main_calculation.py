@@ -25,7 +25,9 @@ from ._abi import ThistleError, check, colmajor_f64, colmajor_i32, dptr, iptr
 TOTAL_J0 = 1
 ELASTIC_J0 = 2
 TOTAL_ALIGNED = 3
+ELASTIC_ALIGNED = 4
 TOTAL_J2 = 7
+ELASTIC_J2 = 8
 TOTAL_ELECTRON = 5
 ELASTIC_ELECTRON = 6
 
@@ -71,8 +73,8 @@ def read_onerdm(filename):
 def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
                                  mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=None, total=None,
                                  onerdm=None):
-    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 5 total electron,
-    6 elastic electron, 7 total j2).
+    """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 4 elastic aligned,
+    5 total electron, 6 elastic electron, 7 total j2, 8 elastic j2).
 
     Types 5 and 6 return I_e - 2 Ine + Inn (I_e the total or elastic j0
     intensity, Ine the nuclear-electron term, Inn the nuclear-nuclear sinc
@@ -81,10 +83,12 @@ def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng,
 
     Type 3 runs on the reference's QCOORD3 grid (``nq`` must be 3131; ``q``
     is not read): ``q_abs`` is |q| of the grid vectors and ``result`` the real
-    part of the aligned intensity.
+    part of the aligned intensity.  Type 4 runs on the reference's CASE(4) grid
+    of ``nq`` vectors (``elastic_aligned_grid``; ``q`` is not read) and
+    returns |q| and the elastic aligned intensity |F(q)|^2.
 
     ``mmod`` is (norbs, ngto) as the reference passes it; ``mat``/``total``
-    are the 2-RDM rows (types 1 and 7), ``onerdm`` the 1-RDM (type 2).
+    are the 2-RDM rows (types 1 and 7), ``onerdm`` the 1-RDM (types 2 and 8).
     ``state1``/``state2`` select CI states in the reference and are unused
     here, where the RDMs are inputs.  Returns ``(q_abs, result)``.
     """
@@ -123,13 +127,13 @@ def total_scattering_calculation_2(type, Zn, geom, state1, state2, maxl, ngto, n
                                    mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, fileJ, fileJ_2,
                                    readrdm=True):
     """The ``readrdm`` branch of total_scattering_calculation_2: type 1 and 7
-    read the 2-RDM from ``fileJ_2``, type 2 the 1-RDM from ``fileJ``."""
+    read the 2-RDM from ``fileJ_2``, types 2 and 8 the 1-RDM from ``fileJ``."""
     if not readrdm:
         raise ThistleError(-7, "only the readrdm path is provided; CI-vector RDM construction is upstream")
     mat = total = onerdm = None
     if type in (TOTAL_J0, TOTAL_J2):
         mat, total = read_twordm(fileJ_2)
-    elif type == ELASTIC_J0:
+    elif type in (ELASTIC_J0, ELASTIC_J2):
         onerdm = read_onerdm(fileJ)
     return total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy,
                                         zz, mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=mat,
@@ -175,8 +179,9 @@ class ScatteringPlan:
     def from_problem(cls, prob, type=TOTAL_J0, q=None):
         return cls(type, prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.group, prob.mmod,
                    prob.q if q is None else q, prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
-                   mat=prob.mat if type != ELASTIC_J0 else None, total=prob.total if type != ELASTIC_J0 else None,
-                   onerdm=prob.onerdm if type == ELASTIC_J0 else None)
+                   mat=prob.mat if type not in (ELASTIC_J0, ELASTIC_J2) else None,
+                   total=prob.total if type not in (ELASTIC_J0, ELASTIC_J2) else None,
+                   onerdm=prob.onerdm if type in (ELASTIC_J0, ELASTIC_J2) else None)
 
     def set_centres(self, xx, yy, zz):
         xx, yy, zz = (_abi.as_f64(a) for a in (xx, yy, zz))
@@ -201,6 +206,15 @@ class ScatteringPlan:
         g = np.zeros((self.ng, 3))
         check(_abi.lib().thistle_plan_vjp(self._p, dptr(v), dptr(g)))
         return g
+
+    def form_factor(self, qvec):
+        """Elastic plans: F(q) of the electron density on q vectors (nq, 3)
+        and the elastic aligned intensity |F|^2 (type 4): (re, im, abs2)."""
+        qv = np.ascontiguousarray(np.asarray(qvec, dtype=np.float64).reshape(-1, 3))
+        n = qv.shape[0]
+        re, im, a2 = np.zeros(n), np.zeros(n), np.zeros(n)
+        check(_abi.lib().thistle_plan_form_factor(self._p, dptr(qv), n, dptr(re), dptr(im), dptr(a2)))
+        return re, im, a2
 
     def nuclear(self, Zn, geom):
         """Elastic plans: the nuclear-electron term Ine(q) for nuclei at geom
@@ -283,7 +297,7 @@ class ScatteringPlan:
         out = np.zeros(need.value)
         check(_abi.lib().thistle_plan_density(self._p, dptr(out), need.value, C.byref(need)))
         k = int(round(np.sqrt(need.value)))
-        return out.reshape(k, k) if self.type != ELASTIC_J0 else out.reshape(k, k, order="F")
+        return out.reshape(k, k) if self.type not in (ELASTIC_J0, ELASTIC_J2) else out.reshape(k, k, order="F")
 
     def info(self):
         a = np.zeros(6, dtype=np.int64)
@@ -395,6 +409,14 @@ def atom_gradient(prob, group_grad):
     return out
 
 
+def elastic_aligned_grid(nq: int) -> np.ndarray:
+    """The reference's q vectors of the elastic aligned intensity (CASE(4),
+    src/main_calculation.f90:227-241), shape (nq, 3)."""
+    out = np.zeros((int(nq), 3))
+    check(_abi.lib().thistle_elastic_aligned_grid(int(nq), dptr(out)))
+    return out
+
+
 def qcoord3(k0: float = 10.583544175) -> np.ndarray:
     """The reference's 3131 aligned q vectors (QCOORD3), shape (3131, 3)."""
     out = np.zeros((3131, 3))
@@ -414,7 +436,7 @@ def scattering(prob, type=TOTAL_J0, q=None, Zn=None):
     (types 5 and 6: nuclei at ``prob.atoms`` with charges ``Zn``)."""
     qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
     two = type in (TOTAL_J0, TOTAL_J2, TOTAL_ELECTRON)
-    one = type in (ELASTIC_J0, TOTAL_ELECTRON, ELASTIC_ELECTRON)
+    one = type in (ELASTIC_J0, ELASTIC_J2, ELASTIC_ALIGNED, TOTAL_ELECTRON, ELASTIC_ELECTRON)
     _, res = total_scattering_calculation(
         type, Zn, prob.atoms, 0, 0, int(max(prob.l.max(), prob.m.max(), prob.n.max())), prob.ngto, prob.ng,
         prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.mmod, qv, qv.size, prob.group,
