@@ -159,6 +159,11 @@ int thistle_plan_set_batch(thistle_plan *plan, int32_t ngeom);
 int thistle_plan_set_centres_batch(thistle_plan *plan, const double *xyz);
 int thistle_plan_execute_batch(thistle_plan *plan, double *result_host);
 int thistle_plan_execute_batch_device(thistle_plan *plan, double *result_dev);
+/* Centres of every geometry from device memory (ngeom x ngto x 3,
+ * interleaved), copied on the plan's stream without synchronising; the
+ * functions of a group must share their centre (not checked here, unlike
+ * set_centres_batch). */
+int thistle_plan_set_centres_batch_device(thistle_plan *plan, const double *xyz_dev);
 int thistle_plan_vjp_batch(thistle_plan *plan, const double *v_host, double *grad_host);
 int thistle_plan_vjp_batch_device(thistle_plan *plan, const double *v_dev, double *grad_dev);
 int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);

@@ -98,9 +98,44 @@ def test_autograd_function():
     p = I.config2_diatomic()
     v = np.random.default_rng(11).normal(size=p.nq)
     with MC.ScatteringPlan.from_problem(p, 1) as pl:
-        R = torch.tensor(p.atoms, dtype=torch.float64, requires_grad=True)
+        R = torch.tensor(p.atoms, dtype=torch.float64, device="cuda", requires_grad=True)
         Iq = intensity(R, pl, p.atom_of)
-        assert np.allclose(Iq.detach().numpy(), pl.execute(), rtol=0, atol=0)
-        (Iq * torch.as_tensor(v)).sum().backward()
+        assert Iq.is_cuda
+        assert np.allclose(Iq.detach().cpu().numpy(), pl.execute(), rtol=0, atol=0)
+        (Iq * torch.as_tensor(v, device="cuda")).sum().backward()
         ref = _vjp_atoms(p, pl, v)
-    assert np.allclose(R.grad.numpy(), ref, rtol=1e-14, atol=0)
+    assert R.grad.is_cuda
+    assert np.allclose(R.grad.cpu().numpy(), ref, rtol=1e-14, atol=0)
+
+
+def test_batched_autograd_on_device_matches_per_geometry_and_oracle_differences():
+    """Configuration 5: a batch of displaced ring geometries through the
+    device-resident batched binding, against the per-geometry plan path (the
+    same numbers to rounding) and against central differences of the oracle
+    at six coordinates of two geometries (committed fixture, h = 1e-4)."""
+    import os
+    import torch
+    from thistle_b200.autograd import intensity_batch
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_cfg5_adjoint.npz"))
+    base = I.config5_fit()
+    geoms = np.concatenate([g["geoms"], I.config5_geometries(base, 4)[3:]])  # 3 geometries
+    v = np.concatenate([g["v"], np.random.default_rng(4).normal(size=(1, base.nq))])
+    with MC.ScatteringPlan.from_problem(base, 1) as pl:
+        R = torch.tensor(geoms, dtype=torch.float64, device="cuda", requires_grad=True)
+        Iq = intensity_batch(R, pl, base.atom_of)
+        assert Iq.shape == (3, base.nq) and Iq.is_cuda
+        (Iq * torch.as_tensor(v, device="cuda")).sum().backward()
+        got_I = Iq.detach().cpu().numpy()
+        got_g = R.grad.cpu().numpy()
+    with MC.ScatteringPlan.from_problem(base, 1) as single:
+        for k in range(3):
+            pk = base.with_geometry(geoms[k])
+            single.set_centres(pk.xx, pk.yy, pk.zz)
+            ref_I = single.execute()
+            ref_g = MC.atom_gradient(pk, single.vjp(v[k]))
+            assert np.max(np.abs(got_I[k] - ref_I)) < 1e-12 * np.max(np.abs(ref_I))
+            assert np.max(np.abs(got_g[k] - ref_g)) < 1e-10 * np.max(np.abs(ref_g))
+    for k in range(2):
+        fd = g["fd"][k]
+        got = np.array([got_g[k, a, ax] for a, ax in g["coords"]])
+        assert np.max(np.abs(got - fd)) < 2e-6 * np.max(np.abs(fd)), (got, fd)

@@ -12,11 +12,13 @@ batch, and the reference's own 2-RDM files.  Inputs are regenerated from the
 seeded generators.
 
 Tolerance: 1e-10 relative per q point (floor 1e-12 of max |I| where I
-crosses zero).  Total j2 is a P2-weighted orientational average that changes
-sign several times over the grid; its points below 1e-5 of max |I| are held
-to an absolute 1e-15 max |I| instead (a few rounding units of the largest
-value).  The adjoint: 2e-6 of the largest difference quotient (the central
-difference's own truncation error at h = 1e-4 bohr).
+crosses zero).  Total j2 is a P2-weighted orientational average, a signed
+sum whose terms are bounded by those of total j0 and which is only 1e-3 to
+1e-2 of it on these molecules (it changes sign, and on the octahedral AB6
+cubic symmetry cancels most of it); its rounding error scales with the j0
+intensity, so a j2 point is held to 1e-10 |I_j2(q)| + 1e-12 |I_j0(q)|.  The
+adjoint: 2e-6 of the largest difference quotient (the central difference's
+own truncation error at h = 1e-4 bohr).
 """
 import os
 import sys
@@ -32,7 +34,7 @@ from conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
-J2_FLOOR = 1e-5  # j2 near its zero crossings: |error| <= TOL * 1e-5 max|I|
+J0_SCALE = 1e-12  # j2: |error| <= TOL |I_j2| + J0_SCALE |I_j0| at each q
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
 SP = (float(np.float32(np.pi)) / np.pi) ** 3
@@ -44,9 +46,13 @@ def gold(name):
     return np.load(os.path.join(GOLD, name))
 
 
-def check(got, ref, tol=TOL, floor=1e-12):
-    err = float(np.max(rel_err(got, ref, floor=floor)))
+def check(got, ref, tol=TOL, floor=1e-12, j0=None):
     assert np.all(np.isfinite(got))
+    if j0 is not None:
+        excess = np.abs(got - ref) - (tol * np.abs(ref) + J0_SCALE * np.abs(j0))
+        assert np.max(excess) <= 0.0, float(np.max(np.abs(got - ref) / (np.abs(ref) + 1e-300)))
+        return
+    err = float(np.max(rel_err(got, ref, floor=floor)))
     assert err < tol, err
 
 
@@ -64,7 +70,7 @@ def test_ab6_full_intensity_vs_oracle(ab6, type_):
     np.testing.assert_array_equal(ab6.q, g["q"])
     with MC.ScatteringPlan.from_problem(ab6, type_) as pl:
         got = pl.execute()
-    check(got, g[f"type{type_}"], floor=J2_FLOOR if type_ == 7 else 1e-12)
+    check(got, g[f"type{type_}"], j0=g["type1"] if type_ == 7 else None)
     if type_ == 1:
         # the reference's own Bessel start where it has converged (qH <= 70)
         check(got[g["ref_mask"]], g["type1_ref"])
@@ -80,7 +86,7 @@ def test_ab6_stratified_sample_vs_oracle(ab6, type_):
     assert qs.shape[0] >= 0.01 * 11_920_622
     with MC.ScatteringPlan.from_problem(ab6, type_) as pl:
         got = pl.execute_quartets(qs[:, :4])
-    check(got, g[f"type{type_}"], floor=J2_FLOOR if type_ == 7 else 1e-12)
+    check(got, g[f"type{type_}"], j0=g["type1"] if type_ == 7 else None)
 
 
 # ------------------------------------------------------- configuration 5 ---
@@ -95,7 +101,7 @@ def test_ring_full_intensity_vs_oracle(ring, type_):
     np.testing.assert_array_equal(ring.q, g["q"])
     with MC.ScatteringPlan.from_problem(ring, type_) as pl:
         got = pl.execute()
-    check(got, g[f"type{type_}"], floor=J2_FLOOR if type_ == 7 else 1e-12)
+    check(got, g[f"type{type_}"], j0=g["type1"] if type_ == 7 else None)
     if type_ == 1:
         check(got[g["ref_mask"]], g["type1_ref"])
 
@@ -145,7 +151,7 @@ def test_uneven_molecule_batch_vs_oracle(type_):
         for pl in plans:
             pl.close()
     for k, row in enumerate(out):
-        check(row, g[f"type{type_}"][k], floor=J2_FLOOR if type_ == 7 else 1e-12)
+        check(row, g[f"type{type_}"][k], j0=g["type1"][k] if type_ == 7 else None)
 
 
 # ------------------------------------------- the reference's own 2-RDMs ----
@@ -156,7 +162,7 @@ def test_reference_2rdm_files_vs_oracle(key):
     p = MG.refrdm_problem(key, g[f"{key}_mat"], g[f"{key}_total"], spec[3], spec[4])
     for type_ in (1, 7):
         got = MC.scattering(p, type_)
-        check(got, g[f"{key}_type{type_}"], floor=J2_FLOOR if type_ == 7 else 1e-12)
+        check(got, g[f"{key}_type{type_}"], j0=g[f"{key}_type1"] if type_ == 7 else None)
         if type_ == 1:
             # trace of the file's 2-RDM at q -> 0: N(N-1) (182 for the HF file)
             m = g[f"{key}_mat"]

@@ -10,8 +10,9 @@ loop order (loop 2 split into j < r at weight 8 and j = r at weight 4) is
 also checked against the shared five-loop list.
 
 GPU: both types through Entry 1 and the plan API against the golden vectors
-and the live oracle (1e-10 relative per point; j2 near its zero crossings
-held to 1e-15 of max |I| absolute, as in the other j2 tests).
+and the live oracle (1e-10 relative per point; elastic j2, a small signed
+residual of the elastic j0 terms, held to 1e-10 |I_j2(q)| + 1e-12 |I_j0(q)|
+as total j2 is in the other tests).
 """
 import os
 
@@ -72,6 +73,10 @@ def test_oracle_elastic_j2_reference_loops_match_shared_list(oracle):
     assert np.max(rel_err(b, a, floor=1e-5)) < 1e-12
 
 
+def _j2_ok(got, ref, j0):
+    return np.all(np.abs(got - ref) <= TOL * np.abs(ref) + 1e-12 * np.abs(j0))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("cfg", [1, 2])
 def test_elastic_j2_golden(cfg):
@@ -79,9 +84,9 @@ def test_elastic_j2_golden(cfg):
     g = np.load(os.path.join(HERE, "golden", f"golden_cfg{cfg}.npz"))
     p = I.CONFIGS[cfg]()
     got = MC.scattering(p, MC.ELASTIC_J2)
-    assert np.max(rel_err(got, g["type8"], floor=1e-5)) < TOL
+    assert _j2_ok(got, g["type8"], g["type2"])
     with MC.ScatteringPlan.from_problem(p, MC.ELASTIC_J2) as pl:
-        assert np.max(rel_err(pl.execute(), g["type8"], floor=1e-5)) < TOL
+        assert _j2_ok(pl.execute(), g["type8"], g["type2"])
 
 
 @pytest.mark.gpu
@@ -89,7 +94,8 @@ def test_elastic_j2_live_oracle_accurate_bessel(oracle):
     from thistle_b200 import main_calculation as MC
     p = I.config2_diatomic()
     ref = oracle.scattering(p, 8, bessel_mode=1, nthreads=4)
-    assert np.max(rel_err(MC.scattering(p, MC.ELASTIC_J2), ref, floor=1e-5)) < TOL
+    el = oracle.scattering(p, 2, bessel_mode=1, nthreads=4)
+    assert _j2_ok(MC.scattering(p, MC.ELASTIC_J2), ref, el)
 
 
 @pytest.mark.gpu

@@ -34,6 +34,7 @@ EXPORTS = sorted([
     "thistle_plan_autotune_batch", "thistle_batch_create", "thistle_batch_use_graph", "thistle_batch_execute",
     "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy", "thistle_plan_nuclear",
     "thistle_plan_density", "thistle_plan_form_factor", "thistle_elastic_aligned_grid",
+    "thistle_plan_set_centres_batch_device",
 ])
 
 

@@ -1679,6 +1679,14 @@ int thistle_plan_set_centres_batch(thistle_plan *P, const double *xyz) {
   return upload_centres_batch(P, xyz);
 }
 
+int thistle_plan_set_centres_batch_device(thistle_plan *P, const double *xyz_dev) {
+  if (!P || !xyz_dev) return fail(THISTLE_ERR_ARG, "null argument");
+  TB_CK(cudaMemcpyAsync(P->d_xyz, xyz_dev, sizeof(double) * (size_t)P->ngeom * 3 * P->ngto,
+                        cudaMemcpyDeviceToDevice, P->st));
+  P->hxyz.clear();  // the host copy no longer describes the device centres
+  P->fwd_valid = false;
+  return THISTLE_OK;
+}
 int thistle_plan_execute_batch_device(thistle_plan *P, double *result_dev) {
   if (!P || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
   P->launches = 0;

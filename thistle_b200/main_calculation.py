@@ -264,6 +264,19 @@ class ScatteringPlan:
         self.ngeom = g.value
         return g.value, qt.value, gps.value
 
+    def set_centres_batch_device(self, ptr: int):
+        """Centres of every geometry from device memory ((ngeom, ngto, 3)
+        doubles at ``ptr``), stream-ordered on the plan's stream."""
+        check(_abi.lib().thistle_plan_set_centres_batch_device(self._p, C.c_void_p(ptr)))
+
+    def execute_batch_device(self, ptr: int):
+        """I(q) of every geometry, (ngeom, nq) doubles to the device address ``ptr``."""
+        check(_abi.lib().thistle_plan_execute_batch_device(self._p, C.c_void_p(ptr)))
+
+    def vjp_batch_device(self, v_ptr: int, grad_ptr: int):
+        """Device cotangents (ngeom, nq) -> group-centre gradients (ngeom, ng, 3)."""
+        check(_abi.lib().thistle_plan_vjp_batch_device(self._p, C.c_void_p(v_ptr), C.c_void_p(grad_ptr)))
+
     def execute_device(self, ptr: int):
         """Integrator only, I(q) to the device address ``ptr`` (stream-ordered)."""
         check(_abi.lib().thistle_plan_execute_device(self._p, C.c_void_p(ptr)))
@@ -372,6 +385,19 @@ class MoleculeBatch:
         out = np.zeros(self._nq)
         check(_abi.lib().thistle_batch_execute(self._b, dptr(out)))
         return np.split(out, self._split)
+
+    def set_centres_batch_device(self, ptr: int):
+        """Centres of every geometry from device memory ((ngeom, ngto, 3)
+        doubles at ``ptr``), stream-ordered on the plan's stream."""
+        check(_abi.lib().thistle_plan_set_centres_batch_device(self._p, C.c_void_p(ptr)))
+
+    def execute_batch_device(self, ptr: int):
+        """I(q) of every geometry, (ngeom, nq) doubles to the device address ``ptr``."""
+        check(_abi.lib().thistle_plan_execute_batch_device(self._p, C.c_void_p(ptr)))
+
+    def vjp_batch_device(self, v_ptr: int, grad_ptr: int):
+        """Device cotangents (ngeom, nq) -> group-centre gradients (ngeom, ng, 3)."""
+        check(_abi.lib().thistle_plan_vjp_batch_device(self._p, C.c_void_p(v_ptr), C.c_void_p(grad_ptr)))
 
     def execute_device(self, ptr: int):
         """All plans' I(q), one after the other, to the device address ``ptr``
