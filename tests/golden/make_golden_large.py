@@ -3,7 +3,7 @@
     python tests/golden/make_golden_large.py [section ...]
 
 Sections (default: all): ab6, ab6_sample, cfg5, cfg5_adjoint, cfg5_aligned,
-cfg4, refrdm.  Inputs are regenerated from the seeded generators in
+cfg4, refrdm, co.  Inputs are regenerated from the seeded generators in
 thistle_b200.inputs (the tests regenerate the same inputs); only the
 oracle's outputs, the sample selections and small derived inputs are stored.
 
@@ -15,9 +15,11 @@ functions: bessel_mode 1 (accurate start of dphrec) for the full grids,
 plus bessel_mode 0 (the reference's own 100-term start) where stated.
 
 The refrdm section reads the reference's own 2-RDM files
-(src/HF_NonZero2RM_MO_Coeffs, src/NonZero2RDM_MO_Coeffs, src/twordm.dat) from
-a reference checkout (THISTLE_REFERENCE, default /root/reference) and stores
-their rows, so that the GPU tests need no checkout.
+(src/HF_NonZero2RM_MO_Coeffs, src/NonZero2RDM_MO_Coeffs, src/twordm.dat) and
+the co section its CO molden file (src/UCCSD_CO_4Bohr_Molden_631star.txt,
+through thistle_b200.molden) from a reference checkout (THISTLE_REFERENCE,
+default /root/reference), and store the parsed arrays, so that the GPU tests
+need no checkout.
 """
 import os
 import sys
@@ -213,7 +215,44 @@ def sec_refrdm():
     _save("golden_refrdm.npz", **out)
 
 
-SECTIONS = {"ab6": sec_ab6, "ab6_sample": sec_ab6_sample, "cfg5": sec_cfg5, "cfg5_adjoint": sec_cfg5_adjoint,
+CO_MOLDEN = "src/UCCSD_CO_4Bohr_Molden_631star.txt"
+
+
+def co_problem(g, rdm):
+    """The CO basis of the reference's molden fixture (parsed arrays in g)
+    carrying the reference's HF 2-RDM file and its 1-RDM, 60 q on 0..8
+    (q[0] = 1e-10)."""
+    q = np.linspace(0.0, 8.0, 60)
+    q[0] = 1e-10
+    atoms = np.array(g["atoms"]).reshape(-1, 3)
+    mat, total = rdm["hf_mat"], rdm["hf_total"]
+    p = I.Problem(name="co", atoms=atoms, ga=g["ga"], l=g["l"], m=g["m"], n=g["n"], xx=g["x"], yy=g["y"],
+                  zz=g["z"], group=g["group"], atom_of=g["atom_of"], mmod=g["mmod"], mat=mat, total=total,
+                  onerdm=np.zeros((1, 1)), q=q, nelec=14)
+    nmo = int(mat.max())
+    G = np.zeros((nmo,) * 4)
+    G[tuple((mat - 1).T)] = total
+    p.onerdm = I.onerdm_from_2rdm(G, 14)
+    return p
+
+
+def sec_co():
+    """The reference's CO molden file through the molden reader (decontracted,
+    the reference's unit handling), with the HF 2-RDM file."""
+    from thistle_b200 import molden
+    gt, at = molden.read_orbitals(os.path.join(REF, CO_MOLDEN), N=100, decontract=True)
+    atom_of = np.array([int(np.argmin(np.sum((at.xyz - np.array([x, y, z])) ** 2, axis=1)))
+                        for x, y, z in zip(gt.x, gt.y, gt.z)], dtype=np.int32)
+    g = dict(ga=gt.ga, l=gt.l, m=gt.m, n=gt.n, x=gt.x, y=gt.y, z=gt.z, group=gt.group, mmod=gt.mo.T.copy(),
+             atoms=at.xyz, numbers=at.numbers, atom_of=atom_of)
+    p = co_problem(g, np.load(os.path.join(HERE, "golden_refrdm.npz")))
+    for ty in (1, 2, 7):
+        g[f"type{ty}"] = O.scattering(p, ty, bessel_mode=1, nthreads=NT)
+    g["q"] = p.q
+    _save("golden_co.npz", **g)
+
+
+SECTIONS = {"co": sec_co, "ab6": sec_ab6, "ab6_sample": sec_ab6_sample, "cfg5": sec_cfg5, "cfg5_adjoint": sec_cfg5_adjoint,
             "cfg5_aligned": sec_cfg5_aligned, "cfg4": sec_cfg4, "refrdm": sec_refrdm}
 
 
