@@ -13,9 +13,9 @@
 // D; the pair density rho is fixed.
 //
 // Stage A (q side, per quartet): Jbar_b = H^{-2b} sum_q v(q) exp(-q^2 s)
-//   g_b(qH) for b <= LLmax + 1 (g_b = j_b x^b from the same generator as the
-//   forward stage 2), or the moments M_s = sum_q v exp(-q^2 s) q^{2s} for
-//   P = Q quartets.  Lanes over quartets, no cross-lane sums.
+//   g_b(qH) for b <= LLmax + 1 (g_b = j_b x^b: upward recurrence above the
+//   crossover, series below it), or the moments M_s = sum_q v exp(-q^2 s)
+//   q^{2s} for P = Q quartets.  A thread per quartet, no cross-lane sums.
 // Stage B (function-quartet side, thread per quartet):
 //   Abar_TUV = w K K' sum_k a a a Jbar_b   (T+U+V <= LLmax + 1), then over the
 //   function quartets, with the convolutions C of the forward stage 1 and
@@ -28,6 +28,8 @@
 //   in a fixed order (deterministic), then into per-block partial rows.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "tb_kernels.h"
 #include "tb_math.cuh"
@@ -117,18 +119,26 @@ __device__ __noinline__ void gb_small(double y, double *g) {
   }
 }
 
+// The q grid is staged through shared memory in chunks of AQ_CHUNK points as
+// (q, 1/q, v(q)), so a point costs no division and no global load.  On an
+// ascending grid the points below the crossover x = qH < XC form a prefix
+// of each quartet's points; the warp walks the longest such prefix of its
+// lanes with the per-point branch (series or recurrence) and the rest
+// without it.
+constexpr int AQ_CHUNK = 2048;
+
 template <int LB1>
 __global__ void __launch_bounds__(128) adjoint_q_kernel(AdjointQArgs A) {
+  extern __shared__ double aq[];  // [AQ_CHUNK][3]: q, 1/q, v
   A.rec += blockIdx.y * A.gs_rec;
   A.adj += blockIdx.y * A.gs_rec;
   A.v += (int64_t)blockIdx.y * A.nq;
   const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= A.nquart) return;
-  const int64_t idx = A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot;
+  const bool act = slot < A.nquart;
+  const int64_t idx = !act ? 0 : (A.perm ? (int64_t)A.perm[A.pbase + slot] - A.pbase : slot);
   const double *rec = A.rec + idx * A.rs;
-  double *out = A.adj + idx * A.rs;
-  const bool p0 = (int)rec[2] == REC_P0;
-  const double H = p0 ? 1.0 : rec[0], s = rec[1], invH = 1.0 / H;
+  const bool p0 = act && (int)rec[2] == REC_P0;
+  const double H = (act && !p0) ? rec[0] : 1.0, s = act ? rec[1] : 0.0, invH = 1.0 / H;
   constexpr double XC = bessel_crossover(LB1);
   double acc[LB1 + 1];
 #pragma unroll
@@ -138,46 +148,93 @@ __global__ void __launch_bounds__(128) adjoint_q_kernel(AdjointQArgs A) {
   sincos(dq * H, &sd, &cd);
   const double kk = exp(-2.0 * dq * dq * s);
   double sn = 0.0, cs = 0.0, g = 0.0, r = 0.0;
-  int next_seed = 0;
-  for (int m = 0; m < A.nq; ++m) {
-    const double q = A.q[m], vq = A.v[m];
-    if (m == next_seed) {
+  // series points of this lane: q H < XC (an ascending prefix on uniform grids)
+  const double qc = XC * invH;
+  for (int c0 = 0; c0 < A.nq; c0 += AQ_CHUNK) {
+    const int cn = min(AQ_CHUNK, A.nq - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) {
+      const double q = A.q[c0 + i];
+      aq[3 * i] = q;
+      aq[3 * i + 1] = 1.0 / q;
+      aq[3 * i + 2] = A.v[c0 + i];
+    }
+    __syncthreads();
+    int pe = 0;  // this lane's points (in the chunk) that may need the series
+    if (act && !p0) {
+      if (!A.uniform) pe = cn;
+      else {
+        while (pe < cn && aq[3 * pe] < qc) ++pe;
+      }
+    }
+    const int mse = (int)__reduce_max_sync(0xffffffffu, (unsigned)pe);
+    if (!act) continue;
+    auto seed = [&](int m) {
+      const double q = aq[3 * m];
       sincos(q * H, &sn, &cs);
       g = exp(-(q * q) * s);
       r = exp(-(2.0 * q * dq + dq * dq) * s);
-      next_seed = !A.uniform ? m + 1 : ((m == 0 && !A.first_on_grid) ? 1 : m + 64);
-    }
-    const double w = vq * g;
+    };
+    auto advance = [&]() {
+      const double s2 = fma(sn, cd, cs * sd);
+      cs = fma(cs, cd, -sn * sd);
+      sn = s2;
+      g *= r;
+      r *= kk;
+    };
+    // seeds at the chunk start, every 64 points, at every point of a
+    // non-uniform grid, and at point 1 when q[0] lies off the grid
+    auto reseed_at = [&](int m) {
+      const int gm = c0 + m;
+      return m == 0 || !A.uniform || (gm & 63) == 0 || (gm == 1 && !A.first_on_grid);
+    };
     if (p0) {
       // moments sum_q v exp(-q^2 s) q^{2s}
-      const double q2 = q * q;
-      double t = w;
+      for (int m = 0; m < cn; ++m) {
+        if (reseed_at(m)) seed(m);
+        const double q = aq[3 * m], w = aq[3 * m + 2] * g, q2 = q * q;
+        double t = w;
 #pragma unroll
-      for (int b = 0; b <= LB1; ++b) {
-        acc[b] += t;
-        t *= q2;
+        for (int b = 0; b <= LB1; ++b) {
+          acc[b] += t;
+          t *= q2;
+        }
+        advance();
       }
-    } else {
-      const double x = q * H;
+      continue;
+    }
+    auto up = [&](int m) {
+      const double q = aq[3 * m], w = aq[3 * m + 2] * g, x = q * H;
       double gb[LB1 + 1];
-      if (x >= XC) {
-        gb[0] = sn * ((1.0 / q) * invH);
-        gb[1] = gb[0] - cs;
-        const double y = x * x;
+      gb[0] = sn * (aq[3 * m + 1] * invH);
+      gb[1] = gb[0] - cs;
+      const double y = x * x;
 #pragma unroll
-        for (int b = 1; b < LB1; ++b) gb[b + 1] = fma((double)(2 * b + 1), gb[b], -y * gb[b - 1]);
-      } else {
-        gb_small<LB1>(x * x, gb);
-      }
+      for (int b = 1; b < LB1; ++b) gb[b + 1] = fma((double)(2 * b + 1), gb[b], -y * gb[b - 1]);
 #pragma unroll
       for (int b = 0; b <= LB1; ++b) acc[b] = fma(w, gb[b], acc[b]);
+    };
+    int m = 0;
+    for (; m < mse; ++m) {
+      if (reseed_at(m)) seed(m);
+      if (aq[3 * m] * H >= XC) up(m);
+      else {
+        const double q = aq[3 * m], w = aq[3 * m + 2] * g, x = q * H;
+        double gb[LB1 + 1];
+        gb_small<LB1>(x * x, gb);
+#pragma unroll
+        for (int b = 0; b <= LB1; ++b) acc[b] = fma(w, gb[b], acc[b]);
+      }
+      advance();
     }
-    const double s2 = fma(sn, cd, cs * sd);
-    cs = fma(cs, cd, -sn * sd);
-    sn = s2;
-    g *= r;
-    r *= kk;
+    for (; m < cn; ++m) {
+      if (reseed_at(m)) seed(m);
+      up(m);
+      advance();
+    }
   }
+  if (!act) return;
+  double *out = A.adj + idx * A.rs;
   if (p0) {
 #pragma unroll
     for (int b = 0; b <= LB1; ++b) out[b] = acc[b];
@@ -464,8 +521,17 @@ int64_t dsoa_doubles(int ng, int maxa) { return (int64_t)3 * (maxa + 1) * (maxa 
 cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStream_t st) {
   if (a.nquart <= 0) return cudaSuccess;
   const dim3 grid((unsigned)((a.nquart + 127) / 128), ngeom);
+  const size_t smem = sizeof(double) * 3 * (size_t)std::min(a.nq, AQ_CHUNK);
   switch (LB1) {
-#define TB_Q(n) case n: adjoint_q_kernel<n><<<grid, 128, 0, st>>>(a); break;
+#define TB_Q(n)                                                                                              \
+  case n:                                                                                                    \
+    if (smem > 48 * 1024) {                                                                                  \
+      cudaError_t e = cudaFuncSetAttribute(adjoint_q_kernel<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                           (int)smem);                                                       \
+      if (e != cudaSuccess) return e;                                                                        \
+    }                                                                                                        \
+    adjoint_q_kernel<n><<<grid, 128, smem, st>>>(a);                                                         \
+    break;
     TB_Q(1) TB_Q(2) TB_Q(3) TB_Q(4) TB_Q(5) TB_Q(6) TB_Q(7) TB_Q(8) TB_Q(9)
 #undef TB_Q
     default: return cudaErrorInvalidValue;

@@ -947,7 +947,9 @@ static int adjoint_alloc(thistle_plan *P) {
   if (!P->d_dsoa) {
     TB_TRY(dalloc(&P->d_dsoa, (size_t)G * dsoa_doubles(P->ng, P->maxa), "dE tables"));
     TB_TRY(dalloc(&P->d_adj, (size_t)G * gs_rec(P), "adjoint records"));
-    P->adj_rows = 2 * P->nsm;
+    // partial gradient rows = the most stage-B blocks of a launch (8 per SM;
+    // at their register count about 4 are resident)
+    P->adj_rows = 8 * P->nsm;
     TB_TRY(dalloc(&P->d_gpart, (size_t)G * P->adj_rows * 3 * P->ng, "gradient rows"));
   }
   if (!P->d_v) {
