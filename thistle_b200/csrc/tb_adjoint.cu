@@ -268,8 +268,26 @@ __device__ __forceinline__ const double *dsoa_slot(const AdjointFArgs &A, int ax
   return A.dsoa + (int64_t)((axis * m1 + la) * m1 + lb) * DE_T * A.s1.npair + pair;
 }
 
+// A read-only load the compiler may not merge with an earlier load of the
+// same address: the ket E tables are read twice per function quartet rather
+// than held in registers across the Abar contraction.
+__device__ __forceinline__ double ld_nc(const double *p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+#ifndef TB_ADJ_MINB_LO
+#define TB_ADJ_MINB_LO 1
+#endif
+#ifndef TB_ADJ_MINB_HI
+#define TB_ADJ_MINB_HI 1
+#endif
+// resident blocks per SM the register allocation is sized for (L <= 3, L >= 4)
+TB_HD constexpr int adj_minb(int L) { return L <= 3 ? TB_ADJ_MINB_LO : TB_ADJ_MINB_HI; }
+
 template <int L, bool SPLIT>
-__global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) {
+__global__ void __launch_bounds__(ADJ_THREADS, adj_minb(L)) adjoint_f_kernel(AdjointFArgs A) {
   {
     const int64_t g = blockIdx.y;  // geometry of a batch
     A.s1.pairtab += g * A.s1.gs_pair;
@@ -297,6 +315,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
   const int gsub = threadIdx.x % P, grp = threadIdx.x / P, pa = gsub % PA, pc = gsub / PA;
   const unsigned gmask = P == 32 ? 0xffffffffu : (((1u << P) - 1u) << (lane - gsub));
   double *Ab = sm + grp;  // the group's Abar_TUV at Ab[adx * QPB]
+  // this thread's bra tables: be[ax][t] at sbe[(ax (L+1) + t) ADJ_THREADS], bd likewise
+  double *sbe = sm + (size_t)QPB0 * NA + (ADJ_THREADS / 32) * 3 * ng + threadIdx.x;
+  double *sbd = sbe + 3 * (L + 1) * ADJ_THREADS;
+#define BE(ax, t) sbe[((ax) * (L + 1) + (t)) * ADJ_THREADS]
+#define BD(ax, t) sbd[((ax) * (L1 + 1) + (t)) * ADJ_THREADS]
   for (int64_t base = (int64_t)blockIdx.x * QPB; base < n; base += (int64_t)gridDim.x * QPB) {
     const int64_t qi = S.qbegin + base + grp;
     const bool act = base + grp < n;  // whole groups
@@ -354,8 +377,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
         const int64_t rowp = fpair(min(fa, fb), max(fa, fb)) * S.np;
         const int lab[3][2] = {{la & 0xff, lb & 0xff}, {(la >> 8) & 0xff, (lb >> 8) & 0xff},
                                {(la >> 16) & 0xff, (lb >> 16) & 0xff}};
-        // bra E (signed, skips as forward) and bra dE/dA_i (signed)
-        double be[3][L + 1], bd[3][L1 + 1];
+        // bra E (signed, skips as forward) and bra dE/dA_i (signed), in this
+        // thread's shared-memory slots: they stay fixed over the ket loop
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
           const double *e = esoa_slot(S, Q.skip & (1 << ax), ax, lab[ax][0], lab[ax][1], pb);
@@ -363,51 +386,48 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
 #pragma unroll
           for (int t = 0; t <= L; ++t) {
             const double v = t <= TM ? e[t * np] : 0.0;
-            be[ax][t] = (t & 1) ? -v : v;
+            BE(ax, t) = (t & 1) ? -v : v;
           }
 #pragma unroll
           for (int t = 0; t <= L1; ++t) {
             const double v = t <= TD ? d[t * np] : 0.0;
-            bd[ax][t] = (t & 1) ? -v : v;
+            BD(ax, t) = (t & 1) ? -v : v;
           }
         }
         for (int cd = pc; cd < nk * nr; cd += PC) {
           const int fc = sk + cd / nr, fd = sr + cd % nr;
           double z = S.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
-          z = fabs(z) < S.cutoffz ? 0.0 : z;
+          if (!(fabs(z) >= S.cutoffz)) continue;  // below cutoffz: the quartet adds exactly zero
           const int lc = S.flmn[fc], ld = S.flmn[fd];
           const int lcd[3][2] = {{lc & 0xff, ld & 0xff}, {(lc >> 8) & 0xff, (ld >> 8) & 0xff},
                                  {(lc >> 16) & 0xff, (ld >> 16) & 0xff}};
-          // per axis: C (forward), dCi (bra centre), dCk (ket centre), orders 0..L+1
-          double C[3][L1 + 1], Ci[3][L1 + 1], Ck[3][L1 + 1];
+          const double *ke_p[3], *kd_p[3];
 #pragma unroll
           for (int ax = 0; ax < 3; ++ax) {
             const bool sk2 = ax == 0 ? (Q.skip & 8) : (ax == 1 ? (Q.skip & 16) : false);
-            const double *e = esoa_slot(S, sk2, ax, lcd[ax][0], lcd[ax][1], pk);
-            const double *d = dsoa_slot(A, ax, lcd[ax][0], lcd[ax][1], pk);
-            double ke[L + 1], kd[L1 + 1];
+            ke_p[ax] = esoa_slot(S, sk2, ax, lcd[ax][0], lcd[ax][1], pk);
+            kd_p[ax] = dsoa_slot(A, ax, lcd[ax][0], lcd[ax][1], pk);
+          }
+          // per axis the forward convolution C[T] = sum_t be[t] ke[T - t], T <= L+1
+          double C[3][L1 + 1];
 #pragma unroll
-            for (int t = 0; t <= L; ++t) ke[t] = t <= TM ? e[t * np] : 0.0;
+          for (int ax = 0; ax < 3; ++ax) {
+            double ke[L + 1];
 #pragma unroll
-            for (int t = 0; t <= L1; ++t) kd[t] = t <= TD ? d[t * np] : 0.0;
+            for (int t = 0; t <= L; ++t) ke[t] = t <= TM ? ke_p[ax][t * np] : 0.0;
 #pragma unroll
             for (int T = 0; T <= L1; ++T) {
-              double c = 0.0, c1 = 0.0, c2 = 0.0;
+              double c = 0.0;
 #pragma unroll
-              for (int t = 0; t <= T; ++t) {
-                if (t <= L && T - t <= L) c = fma(be[ax][t], ke[T - t], c);
-                c1 = fma(bd[ax][t], T - t <= L ? ke[T - t] : 0.0, c1);
-                if (t <= L) c2 = fma(be[ax][t], kd[T - t], c2);
-              }
+              for (int t = 0; t <= T; ++t)
+                if (t <= L && T - t <= L) c = fma(BE(ax, t), ke[T - t], c);
               C[ax][T] = c;
-              Ci[ax][T] = c1;
-              Ck[ax][T] = c2;
             }
           }
           // contractions of Abar with two of the three convolutions
-          double Yx[L1 + 1], Yy[L1 + 1], Yz[L1 + 1];
+          double Y[3][L1 + 1];
 #pragma unroll
-          for (int i = 0; i <= L1; ++i) Yx[i] = Yy[i] = Yz[i] = 0.0;
+          for (int i = 0; i <= L1; ++i) Y[0][i] = Y[1][i] = Y[2][i] = 0.0;
 #pragma unroll
           for (int T = 0; T <= L1; ++T)
 #pragma unroll
@@ -418,39 +438,48 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
               for (int V = 0; V <= L1 - T - U; ++V) {
                 const double a = Ab[adx<L>(T, U, V) * QPB];
                 w = fma(a, C[2][V], w);
-                Yz[V] = fma(a, cxy, Yz[V]);
+                Y[2][V] = fma(a, cxy, Y[2][V]);
               }
-              Yx[T] = fma(w, C[1][U], Yx[T]);
-              Yy[U] = fma(w, C[0][T], Yy[U]);
+              Y[0][T] = fma(w, C[1][U], Y[0][T]);
+              Y[1][U] = fma(w, C[0][T], Y[1][U]);
             }
           double s0 = 0.0, h0 = 0.0, h1 = 0.0, h2 = 0.0;
 #pragma unroll
           for (int T = 0; T <= L; ++T) {
-            s0 = fma(C[0][T], Yx[T], s0);
-            h0 = fma(C[0][T], Yx[T + 1], h0);
-            h1 = fma(C[1][T], Yy[T + 1], h1);
-            h2 = fma(C[2][T], Yz[T + 1], h2);
-          }
-          double e0 = 0.0, e1 = 0.0, e2 = 0.0, k0 = 0.0, k1 = 0.0, k2 = 0.0;
-#pragma unroll
-          for (int T = 0; T <= L1; ++T) {
-            e0 = fma(Ci[0][T], Yx[T], e0);
-            e1 = fma(Ci[1][T], Yy[T], e1);
-            e2 = fma(Ci[2][T], Yz[T], e2);
-            k0 = fma(Ck[0][T], Yx[T], k0);
-            k1 = fma(Ck[1][T], Yy[T], k1);
-            k2 = fma(Ck[2][T], Yz[T], k2);
+            s0 = fma(C[0][T], Y[0][T], s0);
+            h0 = fma(C[0][T], Y[0][T + 1], h0);
+            h1 = fma(C[1][T], Y[1][T + 1], h1);
+            h2 = fma(C[2][T], Y[2][T + 1], h2);
           }
           S0 = fma(z, s0, S0);
           gH[0] = fma(z, h0, gH[0]);
           gH[1] = fma(z, h1, gH[1]);
           gH[2] = fma(z, h2, gH[2]);
-          gEi[0] = fma(z, e0, gEi[0]);
-          gEi[1] = fma(z, e1, gEi[1]);
-          gEi[2] = fma(z, e2, gEi[2]);
-          gEk[0] = fma(z, k0, gEk[0]);
-          gEk[1] = fma(z, k1, gEk[1]);
-          gEk[2] = fma(z, k2, gEk[2]);
+          // centre derivatives of the convolutions, as correlations with Y:
+          //   sum_T (bd * ke)[T] Y[T] = sum_t bd[t] sum_s ke[s] Y[t + s]
+          //   sum_T (be * kd)[T] Y[T] = sum_t be[t] sum_s kd[s] Y[t + s]
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax) {
+            double ke[L + 1], kd[L1 + 1];
+#pragma unroll
+            for (int t = 0; t <= L; ++t) ke[t] = t <= TM ? ld_nc(ke_p[ax] + t * np) : 0.0;
+#pragma unroll
+            for (int t = 0; t <= L1; ++t) kd[t] = t <= TD ? ld_nc(kd_p[ax] + t * np) : 0.0;
+            double e = 0.0, k = 0.0;
+#pragma unroll
+            for (int t = 0; t <= L1; ++t) {
+              double zi = 0.0, zk = 0.0;
+#pragma unroll
+              for (int s2 = 0; s2 <= L1 - t; ++s2) {
+                if (s2 <= L) zi = fma(ke[s2], Y[ax][t + s2], zi);
+                if (t <= L) zk = fma(kd[s2], Y[ax][t + s2], zk);
+              }
+              e = fma(BD(ax, t), zi, e);
+              if (t <= L) k = fma(BE(ax, t), zk, k);
+            }
+            gEi[ax] = fma(z, e, gEi[ax]);
+            gEk[ax] = fma(z, k, gEk[ax]);
+          }
         }
       }
       if (P > 1) {
@@ -504,6 +533,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_f_kernel(AdjointFArgs A) 
     for (int w = 0; w < ADJ_THREADS / 32; ++w) t += sm[(size_t)QPB0 * NA + w * 3 * ng + i];
     A.gpart[(size_t)blockIdx.x * A.gstride + i] += t;
   }
+#undef BE
+#undef BD
 }
 
 }  // namespace
@@ -542,7 +573,8 @@ cudaError_t launch_adjoint_q(int LB1, const AdjointQArgs &a, int ngeom, cudaStre
 template <int L, bool SPLIT>
 static cudaError_t launch_adjoint_f_l(const AdjointFArgs &a, int grid, int ngeom, cudaStream_t st) {
   const int qpb = SPLIT ? ADJ_THREADS / (adj_pa(L) * adj_pc(L)) : ADJ_THREADS;
-  const size_t smem = sizeof(double) * ((size_t)qpb * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng);
+  const size_t smem = sizeof(double) * ((size_t)qpb * ntuv(L + 1) + (ADJ_THREADS / 32) * 3 * (size_t)a.s1.ng +
+                                        (size_t)ADJ_THREADS * 3 * (2 * L + 3));
   cudaError_t e =
       cudaFuncSetAttribute(adjoint_f_kernel<L, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
