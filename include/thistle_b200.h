@@ -46,6 +46,19 @@ int thistle_probe_fp64_peak(int32_t reps, double *tflops);
  * intensity (elastic_integration_j2, src/Integrals.f90:1941-2365; dispatch
  * CASE(8), src/main_calculation.f90:407-419); needs the 1-RDM like type 2. */
 #define THISTLE_ELASTIC_J2 8
+/* energy-resolved CMS: the elastic j0 kernel on zi_ab zj_cd, zi and zj the
+ * AO densities of two (transition) 1-RDMs, summed over every ordered pair of
+ * group pairs with weights 4, 2, 2, 1 (resolved_cms_integration,
+ * src/Integrals.f90:2598-2930; variables_resolved_cms, src/Variables.f90:
+ * 1283-1410; CASE(9), src/main_calculation.f90:438-471 and :820-846).  onerdm
+ * holds the two (nmo1, nmo1) matrices back to back: the bra's, then the
+ * ket's.  Plans of this type have no batch or adjoint form. */
+#define THISTLE_RESOLVED_CMS 9
+/* total j1 (CASE(10), src/main_calculation.f90:473-497): the reference's
+ * tot_integration_j1 prints and stops before integrating
+ * (src/Integrals.f90:526-527), so no result exists to reproduce; Entry 1 and
+ * thistle_plan_create return THISTLE_ERR_TYPE with that reason. */
+#define THISTLE_TOTAL_J1 10
 /* electron scattering: I_e - 2 Ine + Inn (src/main_calculation.f90:277-329,
  * 330-...), I_e the total (5) or elastic (6) j0 intensity, Ine the
  * nuclear-electron term, Inn the nuclear-nuclear sinc sum; Entry 1 only.
@@ -65,8 +78,10 @@ int thistle_version(void);
  * files: mat/total/nmat are read_twordm's rows (src/one_rdm.f90:2112-2147),
  * onerdm is read_onerdm's matrix (:2072-2108).
  *
- *   type          1 total j0, 2 elastic j0, 3 total aligned, 7 total j2,
- *                 8 elastic j2
+ *   type          1 total j0, 2 elastic j0, 3 total aligned, 4 elastic
+ *                 aligned, 5 / 6 electron, 7 total j2, 8 elastic j2,
+ *                 9 resolved CMS (10, total j1, is refused as the reference
+ *                 stops there)
  *   Zn, geom      atomic numbers and (natoms,3) geometry; not used by these
  *                 types (kept for the reference's argument list), may be NULL
  *   maxl          maxval(l) as the reference passes it (checked, not trusted)
@@ -77,7 +92,8 @@ int thistle_version(void);
  *   cutoffz, cutoffmd, cutoffcentre  the reference's three cutoffs
  *   mat, total, nmat   (nmat,4) column-major 1-based MO indices and values
  *                      (types 1 and 7)
- *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (types 2 and 8)
+ *   onerdm, nmo1  (nmo1,nmo1) column-major 1-RDM (types 2, 4, 6 and 8); two
+ *                 of them back to back for type 9
  *   q_abs_out     nq doubles, set to q (the reference returns |q| here)
  *   result_out    nq doubles, I(q)
  * Type 4 (CASE(4), src/main_calculation.f90:218-265) evaluates the elastic
@@ -266,7 +282,8 @@ int thistle_plan_records(const thistle_plan *plan, const double **rec_dev, int32
  * (electron 2) -- zcontrred + zcontrred2 of src/Integrals.f90:109-127 and
  * 5163 -- with P(a,b) = max(a,b) (max(a,b) + 1) / 2 + min(a,b), 0-based.
  * Elastic plans: the AO density Z (ngto x ngto, column-major) of
- * variables_elastic (src/Variables.f90:1199-1217).  `count` is the capacity
+ * variables_elastic (src/Variables.f90:1199-1217); resolved CMS plans: zi
+ * then zj (2 ngto^2 doubles).  `count` is the capacity
  * of out in doubles; *needed receives the size either way (out may then be
  * NULL to query it). */
 int thistle_plan_density(const thistle_plan *plan, double *out, int64_t count, int64_t *needed);

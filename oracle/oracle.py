@@ -89,12 +89,14 @@ def pair_density(prob) -> np.ndarray:
 
 
 def scattering(prob, type_: int = 1, *, bessel_mode: int = 0, nthreads: int = 0,
-               quartets=None, weights=None, q=None, rho=None) -> np.ndarray:
-    """Reference restatement of total_scattering_calculation_2 (types 1, 2, 7).
+               quartets=None, weights=None, q=None, rho=None, onerdm2=None) -> np.ndarray:
+    """Reference restatement of total_scattering_calculation_2 (types 1, 2,
+    7, 8 and 9).
 
     rho: optional ``pair_density(prob)`` for types 1 and 7; the per-quartet
     contraction of the 2-RDM rows is then read from it (the rest of the
-    evaluation is unchanged)."""
+    evaluation is unchanged).  onerdm2: type 9 (resolved CMS) only, the ket's
+    1-RDM (zj); the bra's (zi) is ``prob.onerdm``."""
     keep = []
 
     def d(x):
@@ -113,6 +115,10 @@ def scattering(prob, type_: int = 1, *, bessel_mode: int = 0, nthreads: int = 0,
     mat_cm = np.asfortranarray(prob.mat.astype(np.int32)).ravel(order="F")
     mmod_cm = np.asfortranarray(prob.mmod).ravel(order="F")
     one_cm = np.asfortranarray(prob.onerdm).ravel(order="F")
+    if type_ == 9:
+        if onerdm2 is None or np.shape(onerdm2) != prob.onerdm.shape:
+            raise ValueError("type 9 needs onerdm2 with the shape of prob.onerdm")
+        one_cm = np.concatenate([one_cm, np.asfortranarray(onerdm2, dtype=np.float64).ravel(order="F")])
     if quartets is not None:
         qt = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 5)
         qptr, nqt = i(qt), qt.shape[0]

@@ -596,6 +596,7 @@ typedef struct {
     const double *total;
     const double *mmod;            /* (nmo, ngto) column-major */
     double *zao;                   /* elastic Z (ngto, ngto) column-major */
+    double *zao2;                  /* resolved CMS: the ket's Z (zj); NULL otherwise */
     /* optional: the contracted density already summed over the rows,
      * rho[P(x,y) * np + P(u,v)] = ztot for functions x,y (electron 1) and
      * u,v (electron 2), P(x,y) = max(x,y)(max(x,y)+1)/2 + min(x,y) */
@@ -660,24 +661,28 @@ static void build_total_block(const setup_t *S, const dens_t *D, int gi, int gj,
                 }
 }
 
-/* elastic: ztot = Zb(K,R) * Za(I,J) (src/Integrals.f90:5821-5825) */
+/* elastic: ztot = Zb(K,R) * Za(I,J) (src/Integrals.f90:5821-5825); the
+ * resolved CMS passes za = zi(I,J), zb = zj(K,R) (src/Integrals.f90:2687-2688),
+ * zi and zj from two 1-RDMs */
 static void build_elastic_block(const setup_t *S, const dens_t *D, int gi, int gj, int gk, int gr,
                                 double *zblk) {
     int si = S->gc[gi], sj = S->gc[gj], sk = S->gc[gk], sr = S->gc[gr];
     size_t N = S->ngto;
+    const double *zk = D->zao2 ? D->zao2 : D->zao;
     for (int a = 0; a < si; ++a)
         for (int b = 0; b < sj; ++b) {
             double z1 = D->zao[(S->gs[gi] - 1 + a) + N * (S->gs[gj] - 1 + b)];
             for (int c = 0; c < sk; ++c)
                 for (int d = 0; d < sr; ++d) {
-                    double zb = D->zao[(S->gs[gk] - 1 + c) + N * (S->gs[gr] - 1 + d)];
+                    double zb = zk[(S->gs[gk] - 1 + c) + N * (S->gs[gr] - 1 + d)];
                     zblk[(((size_t)a * sj + b) * sk + c) * sr + d] = zb * z1;
                 }
         }
 }
 
-/* variables_elastic Z (src/Variables.f90:1199-1217) */
-static void build_zao(const setup_t *S, dens_t *D, const double *onerdm, int nmo1) {
+/* variables_elastic Z (src/Variables.f90:1199-1217); variables_resolved_cms
+ * forms zi and zj the same way from its two 1-RDMs (src/Variables.f90:1322-1345) */
+static void build_zao_into(const setup_t *S, dens_t *D, const double *onerdm, int nmo1, double *zout) {
     int N = S->ngto;
     for (int ii = 0; ii < N; ++ii)
         for (int jj = 0; jj < N; ++jj) {
@@ -688,8 +693,12 @@ static void build_zao(const setup_t *S, dens_t *D, const double *onerdm, int nmo
                     temp = temp + o1 * MMOD(D, cc, ii) * MMOD(D, cc2, jj);
                     temp = temp + o1 * MMOD(D, cc, jj) * MMOD(D, cc2, ii);
                 }
-            D->zao[ii + (size_t)N * jj] = temp / 2.0;
+            zout[ii + (size_t)N * jj] = temp / 2.0;
         }
+}
+
+static void build_zao(const setup_t *S, dens_t *D, const double *onerdm, int nmo1) {
+    build_zao_into(S, D, onerdm, nmo1, D->zao);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -744,6 +753,31 @@ static long enum_quartets_elastic_j2(int ng, quartet_t *out) {
     return c;
 }
 
+/* resolved_cms_integration (src/Integrals.f90:2598-2930): no bra-ket symmetry
+ * (zi on the bra, zj on the ket), so every bra pair meets every ket pair:
+ *   loop 7:  i < j, k < r  weight 4   (:2657-2727)
+ *   loop 8:  i = j, k < r  weight 2   (:2734-2794)
+ *   loop 9:  i < j, k = r  weight 2   (:2799-2859)
+ *   loop 10: i = j, k = r  weight 1   (:2864-2926)
+ * each with P = Q only for h < cutoffcentre. */
+static long count_quartets_cms(int ng) {
+    long np = (long)ng * (ng + 1) / 2;
+    return np * np;
+}
+
+static long enum_quartets_cms(int ng, quartet_t *out) {
+    long c = 0;
+    for (int i = 0; i < ng; ++i) for (int j = i + 1; j < ng; ++j)
+        for (int k = 0; k < ng; ++k) for (int r = k + 1; r < ng; ++r)
+            out[c++] = (quartet_t){i, j, k, r, 7};
+    for (int i = 0; i < ng; ++i) for (int k = 0; k < ng; ++k)
+        for (int r = k + 1; r < ng; ++r) out[c++] = (quartet_t){i, i, k, r, 8};
+    for (int i = 0; i < ng; ++i) for (int j = i + 1; j < ng; ++j)
+        for (int k = 0; k < ng; ++k) out[c++] = (quartet_t){i, j, k, k, 9};
+    for (int i = 0; i < ng; ++i) for (int k = 0; k < ng; ++k) out[c++] = (quartet_t){i, i, k, k, 10};
+    return c;
+}
+
 /* Fill 5 ints per quartet (i,j,k,r,loop), 0-based groups, in reference order. */
 long orc_enum_quartets(int ng, int *out) {
     long nq = orc_count_quartets(ng);
@@ -758,7 +792,7 @@ long orc_enum_quartets(int ng, int *out) {
     return nq;
 }
 
-static const double loop_weight[7] = {0.0, 8.0, 4.0, 4.0, 2.0, 1.0, 8.0};
+static const double loop_weight[11] = {0.0, 8.0, 4.0, 4.0, 2.0, 1.0, 8.0, 4.0, 2.0, 2.0, 1.0};
 
 /* One group quartet: f (nq) before the weight and the e12 factors. */
 static int eval_quartet(const setup_t *S, const dens_t *D, const kopts_t *o, const quartet_t *Q,
@@ -767,7 +801,8 @@ static int eval_quartet(const setup_t *S, const dens_t *D, const kopts_t *o, con
     double hx = PX(S, k, r) - PX(S, i, j);
     double hy = PY(S, k, r) - PY(S, i, j);
     double hz = PZ(S, k, r) - PZ(S, i, j);
-    double h = Q->loop == 1 ? pow(hx * hx + hy * hy + hz * hz, 0.5) : sqrt(hx * hx + hy * hy + hz * hz);
+    double h = (Q->loop == 1 || Q->loop == 7) ? pow(hx * hx + hy * hy + hz * hz, 0.5)
+                                              : sqrt(hx * hx + hy * hy + hz * hz);
     zblock_t Z = {S->gc[i], S->gc[j], S->gc[k], S->gc[r], zblk};
     if (o->kind == K_ELASTIC || o->kind == K_ELASTIC_J2) build_elastic_block(S, D, i, j, k, r, zblk);
     else build_total_block(S, D, i, j, k, r, zblk, zbuf);
@@ -846,7 +881,9 @@ static int build_dens(dens_t *D, const double *mmod, int nmo, const int *mat, co
     return ORC_OK;
 }
 
-static void free_dens(dens_t *D) { free(D->m1); free(D->m2); free(D->m3); free(D->m4); free(D->zao); }
+static void free_dens(dens_t *D) {
+    free(D->m1); free(D->m2); free(D->m3); free(D->m4); free(D->zao); free(D->zao2);
+}
 
 /*
  * Full driver in the shape of total_scattering_calculation_2 with readrdm
@@ -854,6 +891,10 @@ static void free_dens(dens_t *D) { free(D->m1); free(D->m2); free(D->m3); free(D
  *   type 1: total j0 (set_P0, variables_total, tot_integration)
  *   type 2: elastic j0 (set_P0, variables_elastic, elastic_integration)
  *   type 7: total j2 (set_P0_j2, variables_total, tot_integration_j2)
+ *   type 8: elastic j2 (set_P0_j2, variables_elastic, elastic_integration_j2)
+ *   type 9: resolved CMS (set_P0, variables_resolved_cms, resolved_cms_integration):
+ *           onerdm holds two (nmo1,nmo1) matrices back to back, the bra's
+ *           (zi) then the ket's (zj)
  * mmod is (nmo, ngto) column-major; mat is (nmat,4) column-major, 1-based;
  * onerdm is (nmo1,nmo1) column-major.  quartets: optional 5 ints per quartet
  * (i,j,k,r,loop) with 0-based groups, evaluated with the loop's weight, or with
@@ -891,19 +932,23 @@ int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const 
                       double cutoffz, double cutoffmd, double cutoffcentre, int bessel_mode, int nthreads,
                       const int *quartets, long nquart, const double *weights, const double *rho,
                       double *result) {
-    if (type != 1 && type != 2 && type != 7 && type != 8) return ORC_ERR_ARG;
+    if (type != 1 && type != 2 && type != 7 && type != 8 && type != 9) return ORC_ERR_ARG;
     setup_t S;
     int e = build_setup(&S, ngto, ga, l, m, n, xx, yy, zz, group, q, nq, (type == 7 || type == 8) ? 2 : 1);
     if (e != ORC_OK) { free_setup(&S); return e; }
     dens_t D;
-    kopts_t o = {type == 1 ? K_TOTAL : type == 2 ? K_ELASTIC : type == 7 ? K_J2 : K_ELASTIC_J2, bessel_mode, cutoffz,
-                 cutoffmd, cutoffcentre};
-    if (type == 2 || type == 8) {
+    kopts_t o = {type == 1 ? K_TOTAL : (type == 2 || type == 9) ? K_ELASTIC : type == 7 ? K_J2 : K_ELASTIC_J2,
+                 bessel_mode, cutoffz, cutoffmd, cutoffcentre};
+    if (type == 2 || type == 8 || type == 9) {
         memset(&D, 0, sizeof D);
         D.mmod = mmod; D.nmo = nmo;
         if (nmo1 > nmo) { free_setup(&S); return ORC_ERR_ARG; }
         D.zao = malloc(sizeof(double) * (size_t)ngto * ngto);
         build_zao(&S, &D, onerdm, nmo1);
+        if (type == 9) {
+            D.zao2 = malloc(sizeof(double) * (size_t)ngto * ngto);
+            build_zao_into(&S, &D, onerdm + (size_t)nmo1 * nmo1, nmo1, D.zao2);
+        }
     } else {
         e = build_dens(&D, mmod, nmo, mat, total, nmat);
         if (e != ORC_OK) { free_dens(&D); free_setup(&S); return e; }
@@ -918,12 +963,13 @@ int orc_scattering_ex(int type, int ngto, const double *ga, const int *l, const 
         for (long c = 0; c < nqt; ++c) {
             Qs[c] = (quartet_t){quartets[5 * c], quartets[5 * c + 1], quartets[5 * c + 2],
                                 quartets[5 * c + 3], quartets[5 * c + 4]};
-            if (Qs[c].loop < 1 || Qs[c].loop > 5) { e = ORC_ERR_ARG; }
+            if (Qs[c].loop < 1 || Qs[c].loop > 10) { e = ORC_ERR_ARG; }
         }
     } else {
-        nqt = orc_count_quartets(S.ng);
+        nqt = type == 9 ? count_quartets_cms(S.ng) : orc_count_quartets(S.ng);
         Qs = malloc(sizeof(quartet_t) * (size_t)nqt);
         if (type == 8) nqt = enum_quartets_elastic_j2(S.ng, Qs);
+        else if (type == 9) nqt = enum_quartets_cms(S.ng, Qs);
         else enum_quartets(S.ng, Qs);
     }
     if (e == ORC_OK) e = run_quartets(&S, &D, &o, Qs, nqt, weights, result, nthreads);

@@ -5,7 +5,9 @@
 Inputs are regenerated from the seeded generators in thistle_b200.inputs;
 outputs are the oracle's restatement of the reference integrators
 (bessel_mode 0: the reference's own 100-term dphrec start) for types 1, 2,
-7 and 8, and the elastic aligned intensity of type 4 on the CASE(4) grid.
+7 and 8, the resolved CMS (type 9) on the seeded 1-RDM pair of
+``inputs.cms_onerdms``, and the elastic aligned intensity of type 4 on the
+CASE(4) grid.
 """
 import os
 import sys
@@ -25,6 +27,9 @@ def main():
         out = {"q": p.q}
         for t in (1, 2, 7, 8):
             out[f"type{t}"] = O.scattering(p, t, nthreads=8)
+        d1, d2 = I.cms_onerdms(p)
+        pc = I.Problem(**{**p.__dict__, "onerdm": d1})
+        out["type9"] = O.scattering(pc, 9, onerdm2=d2, nthreads=8)
         # type 4 on the reference's CASE(4) grid of nq vectors: |F(q)|^2
         out["type4"] = O.elastic_aligned(p, nq=p.nq)[2]
         np.savez(os.path.join(HERE, f"golden_cfg{cfg}.npz"), **out)

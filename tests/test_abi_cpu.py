@@ -75,7 +75,15 @@ def test_nonfinite_rejected(h2):
 
 
 def test_bad_type_rejected(h2):
-    assert code_of(lambda: _call(h2, type=9)) == -7
+    assert code_of(lambda: _call(h2, type=11)) == -7
+
+
+def test_total_j1_refused_with_the_references_reason(h2):
+    """Type 10: the reference's tot_integration_j1 stops before it integrates
+    (src/Integrals.f90:526-527), so the library refuses it by name."""
+    with pytest.raises(ThistleError) as e:
+        _call(h2, type=10)
+    assert e.value.code == -7 and "stops before integrating" in str(e.value)
 
 
 def test_noncontiguous_group_rejected(h2):

@@ -125,3 +125,38 @@ def test_command_line_co_molden_vs_oracle(tmp_path, type_):
         assert np.all(np.abs(out[:, 1] - ref) <= 1e-10 * np.abs(ref) + 1e-12 * np.abs(g["type1"]))
     else:
         assert np.max(rel_err(out[:, 1], ref)) < 1e-10
+
+
+def _write_onerdm(path, D):
+    with open(path, "w") as f:
+        for i in range(D.shape[0]):
+            for j in range(D.shape[1]):
+                f.write(f"{i + 1} {j + 1} {float(D[i, j])!r}\n")
+
+
+def test_command_line_refuses_total_j1(tmp_path):
+    """Type 10 stops as the reference's does (tot_integration_j1 stops before
+    integrating, src/Integrals.f90:526-527), before any device work."""
+    p = I.config1_h2()
+    write_inputs(str(tmp_path), p, 10, 0.0, 4.0, 20)
+    with pytest.raises(SystemExit) as e:
+        M.run(str(tmp_path))
+    assert "stops before integrating" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_command_line_resolved_cms_vs_golden(tmp_path):
+    """Type 9 reads its two 1-RDM files (the bra's, then the ket's) from the
+    two RDM names of the readrdm branch."""
+    p = I.config2_diatomic()
+    d1, d2 = I.cms_onerdms(p)
+    p = I.Problem(**{**p.__dict__, "onerdm": d1})
+    write_inputs(str(tmp_path), p, 9, 0.0, float(p.q[-1]), p.nq)
+    _write_onerdm(str(tmp_path / "twordm.txt"), d2)
+    r = subprocess.run([sys.executable, "-m", "thistle_b200.main", str(tmp_path)], cwd=ROOT,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = np.loadtxt(str(tmp_path / "result.dat"))
+    g = np.load(os.path.join(GOLD, "golden_cfg2.npz"))
+    np.testing.assert_allclose(out[1:, 0], g["q"][1:], rtol=1e-14)
+    assert np.max(rel_err(out[:, 1], g["type9"])) < 1e-10

@@ -1,4 +1,5 @@
-"""Calculation types 4 (elastic aligned, CASE(4)) and 8 (elastic j2, CASE(8)).
+"""Calculation types 4 (elastic aligned, CASE(4)), 8 (elastic j2, CASE(8)) and
+9 (resolved CMS, CASE(9)).
 
 CPU: the oracle's restatements are pinned to each other and to elastic j0 by
 two identities of the rotational average -- the average over directions of
@@ -124,3 +125,74 @@ def test_form_factor_random_vectors_vs_oracle(oracle):
     assert np.max(np.abs(re - fr)) < 1e-12 * scale
     assert np.max(np.abs(im - fi)) < 1e-12 * scale
     assert np.max(rel_err(ab, a2)) < TOL
+
+
+# ---------------------------------------------------------------------------
+# type 9: energy-resolved CMS (resolved_cms_integration, src/Integrals.f90:2598-2930)
+# ---------------------------------------------------------------------------
+def _cms_problem(cfg):
+    p = I.CONFIGS[cfg]()
+    d1, d2 = I.cms_onerdms(p)
+    return I.Problem(**{**p.__dict__, "onerdm": d1}), d2
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_oracle_cms_with_equal_densities_is_elastic_j0(oracle, cfg):
+    """With zi = zj the ordered sum over every (bra pair, ket pair) at weights
+    4, 2, 2, 1 is the elastic five-loop sum (weights 8, 4, 4, 2, 1 over the
+    bra-ket symmetric list)."""
+    p = I.CONFIGS[cfg]()
+    el = oracle.scattering(p, 2, nthreads=4)
+    cms = oracle.scattering(p, 9, onerdm2=p.onerdm, nthreads=4)
+    assert np.max(rel_err(cms, el)) < 1e-13
+
+
+def test_oracle_cms_is_symmetric_in_its_two_densities(oracle):
+    p, d2 = _cms_problem(2)
+    a = oracle.scattering(p, 9, onerdm2=d2, nthreads=4)
+    b = oracle.scattering(I.Problem(**{**p.__dict__, "onerdm": d2}), 9, onerdm2=p.onerdm, nthreads=4)
+    assert np.max(rel_err(a, b)) < 1e-13
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_oracle_cms_golden(oracle, cfg):
+    g = np.load(os.path.join(HERE, "golden", f"golden_cfg{cfg}.npz"))
+    p, d2 = _cms_problem(cfg)
+    got = oracle.scattering(p, 9, onerdm2=d2, nthreads=8)
+    np.testing.assert_allclose(got, g["type9"], rtol=1e-13, atol=1e-13 * np.max(np.abs(got)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_cms_golden(cfg):
+    from thistle_b200 import main_calculation as MC
+    g = np.load(os.path.join(HERE, "golden", f"golden_cfg{cfg}.npz"))
+    p, d2 = _cms_problem(cfg)
+    assert np.max(rel_err(MC.scattering(p, MC.RESOLVED_CMS, onerdm2=d2), g["type9"])) < TOL
+    with MC.ScatteringPlan.from_problem(p, MC.RESOLVED_CMS, onerdm2=d2) as pl:
+        assert np.max(rel_err(pl.execute(), g["type9"])) < TOL
+        z = pl.density()
+        assert z.shape == (2, p.ngto, p.ngto)
+        np.testing.assert_allclose(z[0], z[0].T, rtol=0, atol=1e-14 * np.max(np.abs(z[0])))
+
+
+@pytest.mark.gpu
+def test_cms_live_oracle_p0_threshold(oracle):
+    """A cutoffcentre large enough to send whole quartets with distinct
+    centres to the P = Q branch, on both sides' densities."""
+    from thistle_b200 import main_calculation as MC
+    p, d2 = _cms_problem(2)
+    p.cutoffcentre = 0.5
+    ref = oracle.scattering(p, 9, onerdm2=d2, nthreads=4)
+    assert np.max(rel_err(MC.scattering(p, MC.RESOLVED_CMS, onerdm2=d2), ref)) < TOL
+
+
+@pytest.mark.gpu
+def test_cms_plans_do_not_batch():
+    from thistle_b200 import main_calculation as MC
+    from thistle_b200._abi import ThistleError
+    p, d2 = _cms_problem(1)
+    with MC.ScatteringPlan.from_problem(p, MC.RESOLVED_CMS, onerdm2=d2) as pl:
+        with pytest.raises(ThistleError) as e:
+            pl.set_batch(2)
+        assert e.value.code == -7

@@ -352,9 +352,10 @@ __global__ void sym_small_kernel(const double *__restrict__ in, int n, double *_
 //   i == j : every ket (k,r) with k < r                 (loop 3)
 //            and (k,k) with k >= i                      (loops 4 and 5)
 // bra_off[b] is the first quartet of bra pair b (pair_index order).
+// all_pairs (the resolved CMS): every ket (k <= r) for every bra, in pair order.
 __global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off, int nbra, int64_t nquart,
                                     const int *__restrict__ gL, uint64_t *__restrict__ quart,
-                                    uint32_t *__restrict__ keys) {
+                                    uint32_t *__restrict__ keys, int all_pairs) {
   int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (qi >= nquart) return;
   int lo = 0, hi = nbra - 1;
@@ -369,7 +370,11 @@ __global__ void quartet_fill_kernel(int ng, const int64_t *__restrict__ bra_off,
   int64_t m = qi - bra_off[b];
   int k, r;
   int64_t noff_all = (int64_t)ng * (ng - 1) / 2;
-  if (i < j || m < noff_all) {
+  if (all_pairs) {
+    k = 0;
+    while (m >= ng - k) { m -= ng - k; ++k; }
+    r = k + (int)m;
+  } else if (i < j || m < noff_all) {
     // m-th off-diagonal pair (k < r) starting at k = (i < j ? i : 0)
     k = i < j ? i : 0;
     while (m >= ng - 1 - k) { m -= ng - 1 - k; ++k; }
@@ -416,6 +421,7 @@ cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args 
   if (kind == KIND_ELASTIC) return launch_stage1_xk_k<KIND_ELASTIC>(L, LK, XB, a, ngeom, st);
   if (kind == KIND_ALIGNED) return launch_stage1_xk_k<KIND_ALIGNED>(L, LK, XB, a, ngeom, st);
   if (kind == KIND_ELASTIC_J2) return launch_stage1_xk_k<KIND_ELASTIC_J2>(L, LK, XB, a, ngeom, st);
+  if (kind == KIND_CMS) return launch_stage1_xk_k<KIND_CMS>(L, LK, XB, a, ngeom, st);
   return launch_stage1_xk_k<KIND_J2>(L, LK, XB, a, ngeom, st);
 }
 
@@ -425,6 +431,7 @@ cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1A
   if (kind == KIND_ELASTIC) return launch_stage1_xsplit_k<KIND_ELASTIC>(L, LK, XB, a, xbuf, nout, st);
   if (kind == KIND_ALIGNED) return launch_stage1_xsplit_k<KIND_ALIGNED>(L, LK, XB, a, xbuf, nout, st);
   if (kind == KIND_ELASTIC_J2) return launch_stage1_xsplit_k<KIND_ELASTIC_J2>(L, LK, XB, a, xbuf, nout, st);
+  if (kind == KIND_CMS) return launch_stage1_xsplit_k<KIND_CMS>(L, LK, XB, a, xbuf, nout, st);
   return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, st);
 }
 
@@ -436,6 +443,7 @@ cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const St
   if (kind == KIND_ELASTIC) TB_K(KIND_ELASTIC);
   if (kind == KIND_ALIGNED) TB_K(KIND_ALIGNED);
   if (kind == KIND_ELASTIC_J2) TB_K(KIND_ELASTIC_J2);
+  if (kind == KIND_CMS) TB_K(KIND_CMS);
   TB_K(KIND_J2);
 #undef TB_K
 }
@@ -458,15 +466,17 @@ cudaError_t launch_stage1_batch(int kind, int L, int LK, int XB, const Stage1Arg
   if (kind == KIND_ELASTIC) return launch_stage1_batch_k<KIND_ELASTIC>(L, LK, XB, d, pre, n, blocks, st);
   if (kind == KIND_ALIGNED) return launch_stage1_batch_k<KIND_ALIGNED>(L, LK, XB, d, pre, n, blocks, st);
   if (kind == KIND_ELASTIC_J2) return launch_stage1_batch_k<KIND_ELASTIC_J2>(L, LK, XB, d, pre, n, blocks, st);
+  if (kind == KIND_CMS) return launch_stage1_batch_k<KIND_CMS>(L, LK, XB, d, pre, n, blocks, st);
   return launch_stage1_batch_k<KIND_J2>(L, LK, XB, d, pre, n, blocks, st);
 }
 
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st) {
-  // instantiated in tb_stage1_{total,elastic,j2,aligned,elastic_j2}.cu
+  // instantiated in tb_stage1_{total,elastic,j2,aligned,elastic_j2,cms}.cu
   if (kind == KIND_TOTAL) return launch_stage1_k<KIND_TOTAL>(L, a, ngeom, st);
   if (kind == KIND_ELASTIC) return launch_stage1_k<KIND_ELASTIC>(L, a, ngeom, st);
   if (kind == KIND_ALIGNED) return launch_stage1_k<KIND_ALIGNED>(L, a, ngeom, st);
   if (kind == KIND_ELASTIC_J2) return launch_stage1_k<KIND_ELASTIC_J2>(L, a, ngeom, st);
+  if (kind == KIND_CMS) return launch_stage1_k<KIND_CMS>(L, a, ngeom, st);
   return launch_stage1_k<KIND_J2>(L, a, ngeom, st);
 }
 
@@ -506,10 +516,10 @@ cudaError_t launch_ghat_runs(const int *keys, const double *vals, int64_t m, dou
 
 
 cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,
-                                uint64_t *quart, uint32_t *keys, cudaStream_t st) {
+                                uint64_t *quart, uint32_t *keys, bool all_pairs, cudaStream_t st) {
   if (nquart <= 0) return cudaSuccess;
   quartet_fill_kernel<<<(unsigned)((nquart + 255) / 256), 256, 0, st>>>(ng, bra_off, npairs(ng), nquart, gL,
-                                                                        quart, keys);
+                                                                        quart, keys, all_pairs ? 1 : 0);
   return cudaGetLastError();
 }
 

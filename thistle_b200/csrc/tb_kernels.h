@@ -18,7 +18,8 @@ struct Stage1Args {
   const int *flmn;            // l | m<<8 | n<<16 per function
   const double *rho;          // pair density (np x np), total / j2
   int64_t np;
-  const double *zao;          // AO density (ngto x ngto), elastic
+  const double *zao;          // AO density (ngto x ngto), elastic; the bra's for KIND_CMS
+  const double *zket;         // the ket's AO density: zao, or the second one for KIND_CMS
   int ngto;
   double cutoffz, cutoffmd, cutoffcentre;
   const double *esoa;         // E^{la,lb}_t transposed: [variant][axis][la][lb][t][pair]
@@ -231,7 +232,8 @@ struct ReduceDesc {
 cudaError_t launch_reduce_desc(const ReduceDesc *d, int n, int nqmax, cudaStream_t st);
 cudaError_t launch_sym_small(const double *in, int n, double *out, cudaStream_t st);
 int stage2_blocks_per_sm(int nqp, int nwarps);
+// all_pairs: every ket pair for every bra pair (the resolved CMS) instead of the five loops
 cudaError_t launch_quartet_fill(int ng, const int64_t *bra_off, int64_t nquart, const int *gL,
-                                uint64_t *quart, uint32_t *keys, cudaStream_t st);
+                                uint64_t *quart, uint32_t *keys, bool all_pairs, cudaStream_t st);
 
 }  // namespace tb

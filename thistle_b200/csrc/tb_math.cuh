@@ -45,10 +45,13 @@ constexpr int SER_K = 24;
 
 // KIND_ELASTIC_J2: the j2 Bessel expansion of total j2 on the elastic density
 // product Z_ab Z_cd (integral_k_ijkr_j2, src/Integrals.f90:5903-6083)
-enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2, KIND_ALIGNED = 3, KIND_ELASTIC_J2 = 4 };
-// j2 Bessel expansion (order LLmax + 2, P2 weight) / density from the 1-RDM
+// KIND_CMS: the elastic j0 kernel on zi_ab zj_cd, two AO densities from two
+// 1-RDMs, over every ordered (bra pair, ket pair) (resolved_cms_integration,
+// src/Integrals.f90:2598-2930)
+enum Kind { KIND_TOTAL = 0, KIND_ELASTIC = 1, KIND_J2 = 2, KIND_ALIGNED = 3, KIND_ELASTIC_J2 = 4, KIND_CMS = 5 };
+// j2 Bessel expansion (order LLmax + 2, P2 weight) / density from 1-RDMs
 TB_HD constexpr bool kind_j2(int k) { return k == KIND_J2 || k == KIND_ELASTIC_J2; }
-TB_HD constexpr bool kind_elastic(int k) { return k == KIND_ELASTIC || k == KIND_ELASTIC_J2; }
+TB_HD constexpr bool kind_elastic(int k) { return k == KIND_ELASTIC || k == KIND_ELASTIC_J2 || k == KIND_CMS; }
 enum RecKind { REC_BESSEL = 0, REC_BESSEL_J2 = 1, REC_P0 = 2 };
 
 // number of (T,U,V) with T+U+V <= L

@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(128) nuclear_kernel(Stage1Args A, const uint64
   QuartetHead Q;
   Q.gi = gi; Q.gj = gk; Q.gk = 0; Q.gr = 0;
   Q.loop = 5;  // weight 1
+  Q.w = 1.0;
   Q.tb = A.pairtab + (size_t)pr * PAIR_STRIDE;
   Q.tk = nucrec + (size_t)a * 8;  // [R_a, 0, Zn_a, 0, ...]: ket prefactor Zn_a, no Gaussian
   Q.Hx = Q.tk[0] - Q.tb[0];

@@ -89,7 +89,7 @@ struct SubRange {
 
 struct thistle_plan {
   int type = 0, kind = 0;
-  int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nq = 0, maxa = 0, nmat = 0;
+  int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nzao = 1, nq = 0, maxa = 0, nmat = 0;
   double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
   std::vector<int> gstart, gcount, gL, flmn;
   std::vector<double> hq;            // host copy of the q grid (aligned: interleaved q vectors)
@@ -225,7 +225,8 @@ static int check_q(const double *q, int32_t nq) {
 // ---------------------------------------------------------------------------
 // quartet classes
 // ---------------------------------------------------------------------------
-static int64_t bra_count(int i, int j, int ng) {
+static int64_t bra_count(int i, int j, int ng, bool all_pairs) {
+  if (all_pairs) return npairs(ng);  // resolved CMS: every ket pair
   if (i < j) return (int64_t)(ng - i) * (ng - i - 1) / 2;
   return (int64_t)ng * (ng - 1) / 2 + (ng - i);
 }
@@ -235,9 +236,20 @@ static inline int class_key(int Li, int Lj, int Lk, int Lr) {
 }
 
 // Quartet counts per class key, without enumerating quartets.
-static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt) {
+static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt, bool all_pairs) {
   int ng = (int)gL.size();
   cnt.assign(17 * 625, 0);
+  if (all_pairs) {
+    // every (bra pair, ket pair): products of the pair counts per (La, Lb)
+    int64_t pc[5][5] = {};
+    for (int i = 0; i < ng; ++i)
+      for (int j = i; j < ng; ++j) ++pc[gL[i]][gL[j]];
+    for (int a = 0; a < 25; ++a)
+      for (int b = 0; b < 25; ++b)
+        if (pc[a / 5][a % 5] && pc[b / 5][b % 5])
+          cnt[class_key(a / 5, a % 5, b / 5, b % 5)] += pc[a / 5][a % 5] * pc[b / 5][b % 5];
+    return;
+  }
   // off[k][a][b]: #{(k',r): k <= k' < r, gL[k']=a, gL[r]=b}; diag[k][a]: #{k' >= k: gL[k'] = a}
   std::vector<int64_t> off((size_t)(ng + 1) * 25, 0), after(5, 0), diag((size_t)(ng + 1) * 5, 0);
   for (int k = ng - 1; k >= 0; --k) {
@@ -338,10 +350,11 @@ static int density_alloc(thistle_plan *P) {
   const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
   TB_TRY(dalloc(&P->d_C, (size_t)n * ngto, "MO coefficients"));
   if (kind_elastic(P->kind)) {
-    TB_TRY(dalloc(&P->d_zao, (size_t)ngto * ngto, "AO density"));
-    TB_TRY(dalloc(&P->d_D, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
-    TB_TRY(dalloc(&P->d_Ds, (size_t)P->nmo1 * P->nmo1, "1-RDM"));
-    TB_TRY(dalloc(&P->d_Y, (size_t)P->nmo1 * ngto, "1-RDM x C"));
+    const size_t nz = (size_t)P->nzao;
+    TB_TRY(dalloc(&P->d_zao, nz * ngto * ngto, "AO density"));
+    TB_TRY(dalloc(&P->d_D, nz * P->nmo1 * P->nmo1, "1-RDM"));
+    TB_TRY(dalloc(&P->d_Ds, nz * P->nmo1 * P->nmo1, "1-RDM"));
+    TB_TRY(dalloc(&P->d_Y, nz * P->nmo1 * ngto, "1-RDM x C"));
     TB_TRY(dalloc(&P->d_Ct, (size_t)n * transform_ct_width(ngto), "transform C^T"));
   } else {
     TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
@@ -371,8 +384,8 @@ static int density_upload(thistle_plan *P, const double *mmod, const int32_t *ma
                           const double *onerdm) {
   TB_CK(cudaMemcpyAsync(P->d_C, mmod, sizeof(double) * (size_t)P->nmo * P->ngto, cudaMemcpyHostToDevice, P->st));
   if (kind_elastic(P->kind)) {
-    TB_CK(cudaMemcpyAsync(P->d_D, onerdm, sizeof(double) * (size_t)P->nmo1 * P->nmo1, cudaMemcpyHostToDevice,
-                          P->st));
+    TB_CK(cudaMemcpyAsync(P->d_D, onerdm, sizeof(double) * (size_t)P->nzao * P->nmo1 * P->nmo1,
+                          cudaMemcpyHostToDevice, P->st));
   } else if (P->nmat > 0) {
     TB_CK(cudaMemcpyAsync(P->d_mat, mat, sizeof(int) * (size_t)P->nmat * 4, cudaMemcpyHostToDevice, P->st));
     TB_CK(cudaMemcpyAsync(P->d_tot, total, sizeof(double) * (size_t)P->nmat, cudaMemcpyHostToDevice, P->st));
@@ -392,20 +405,24 @@ static int density_run(thistle_plan *P) {
     // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217),
     // C1 the first nmo1 MOs: Y(i, a) = sum_j Ds(i, j) C(j, a), then
     // Z(a, b) = sum_i C(i, a) Y(i, b)
+    // (the resolved CMS: the same for each of its two 1-RDMs)
     const int k = P->nmo1;
-    TB_TRYC(launch_sym_small(P->d_D, k, P->d_Ds, P->st));
-    DmmaGemmArgs g{};
-    g.A = P->d_Ds; g.sak = k; g.a_batch = 0;
-    g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
-    g.M = k; g.N = ngto; g.K = k;
-    g.D = P->d_Y; g.sdm = 1; g.sdj = k; g.d_batch = 0;
-    TB_TRYC(launch_dmma_gemm(g, 0, true, 1, P->st));
-    g.A = P->d_Ct; g.sak = cw;
-    g.B = P->d_Y; g.sbk = 1; g.sbj = k;
-    g.M = ngto; g.N = ngto; g.K = k;
-    g.D = P->d_zao; g.sdm = 1; g.sdj = ngto;
-    TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
-    P->launches += 3;
+    for (int z = 0; z < P->nzao; ++z) {
+      const int64_t dk = (int64_t)z * k * k;
+      TB_TRYC(launch_sym_small(P->d_D + dk, k, P->d_Ds + dk, P->st));
+      DmmaGemmArgs g{};
+      g.A = P->d_Ds + dk; g.sak = k; g.a_batch = 0;
+      g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
+      g.M = k; g.N = ngto; g.K = k;
+      g.D = P->d_Y + (int64_t)z * k * ngto; g.sdm = 1; g.sdj = k; g.d_batch = 0;
+      TB_TRYC(launch_dmma_gemm(g, 0, true, 1, P->st));
+      g.A = P->d_Ct; g.sak = cw;
+      g.B = P->d_Y + (int64_t)z * k * ngto; g.sbk = 1; g.sbj = k;
+      g.M = ngto; g.N = ngto; g.K = k;
+      g.D = P->d_zao + (int64_t)z * ngto * ngto; g.sdm = 1; g.sdj = ngto;
+      TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
+      P->launches += 3;
+    }
     goto done;
   }
   if (P->nmat == 0) {
@@ -465,7 +482,7 @@ static int quartets_alloc(thistle_plan *P) {
   for (int i = 0, b = 0; i < ng; ++i)
     for (int j = i; j < ng; ++j, ++b) {
       off[b] = acc;
-      acc += bra_count(i, j, ng);
+      acc += bra_count(i, j, ng, P->kind == KIND_CMS);
     }
   off[nb] = acc;
   if (acc != P->nquart) return fail(THISTLE_ERR_ARG, "internal: quartet count mismatch");
@@ -488,7 +505,8 @@ done:
 
 static int quartets_run(thistle_plan *P) {
   int rc = THISTLE_OK;
-  TB_TRYC(launch_quartet_fill(P->ng, P->d_braoff, P->nquart, P->d_gL, P->d_v0, P->d_k0, P->st));
+  TB_TRYC(launch_quartet_fill(P->ng, P->d_braoff, P->nquart, P->d_gL, P->d_v0, P->d_k0, P->kind == KIND_CMS,
+                              P->st));
   P->launches += 1;
   TB_TRYC(cub::DeviceRadixSort::SortPairs(P->d_sort_tmp, P->sort_tmp_bytes, P->d_k0, P->d_k1, P->d_v0, P->d_quart,
                                           (int)P->nquart, 0, KEY_BITS, P->st));
@@ -591,8 +609,12 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
                        int32_t nq, double cutoffz, double cutoffmd, double cutoffcentre) {
   if (!out) return fail(THISTLE_ERR_ARG, "null plan pointer");
   *out = nullptr;
+  if (type == THISTLE_TOTAL_J1)
+    return fail(THISTLE_ERR_TYPE,
+                "type 10 (total j1): the reference's tot_integration_j1 stops before integrating "
+                "(src/Integrals.f90:526-527), so there is no result to reproduce");
   if (type != THISTLE_TOTAL_J0 && type != THISTLE_ELASTIC_J0 && type != THISTLE_TOTAL_J2 &&
-      type != THISTLE_TOTAL_ALIGNED && type != THISTLE_ELASTIC_J2)
+      type != THISTLE_TOTAL_ALIGNED && type != THISTLE_ELASTIC_J2 && type != THISTLE_RESOLVED_CMS)
     return fail(THISTLE_ERR_TYPE, "calculation type " + std::to_string(type) + " is not provided by this entry");
   thistle_plan *P = new thistle_plan();
   int rc = THISTLE_OK;
@@ -617,6 +639,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   P->kind = type == THISTLE_TOTAL_J0 ? KIND_TOTAL
             : type == THISTLE_ELASTIC_J0 ? KIND_ELASTIC
             : type == THISTLE_ELASTIC_J2 ? KIND_ELASTIC_J2
+            : type == THISTLE_RESOLVED_CMS ? KIND_CMS
             : type == THISTLE_TOTAL_ALIGNED ? KIND_ALIGNED : KIND_J2;
   P->nq = nq;
   P->qdim = type == THISTLE_TOTAL_ALIGNED ? 3 : 1;
@@ -628,7 +651,11 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
   P->np = (int64_t)ngto * (ngto + 1) / 2;
   if (kind_elastic(P->kind)) {
     if (!onerdm || nmo1 <= 0 || nmo1 > norbs) { rc = fail(THISTLE_ERR_ARG, "1-RDM must be (nmo1,nmo1) with nmo1 <= norbs"); goto done; }
-    if (!finite_all(onerdm, (int64_t)nmo1 * nmo1)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 1-RDM"); goto done; }
+    P->nzao = P->kind == KIND_CMS ? 2 : 1;  // the resolved CMS takes two 1-RDMs, back to back
+    if (!finite_all(onerdm, (int64_t)P->nzao * nmo1 * nmo1)) {
+      rc = fail(THISTLE_ERR_NONFINITE, "non-finite 1-RDM");
+      goto done;
+    }
     P->nmo1 = nmo1;
   } else {
     if (nmat < 0 || (nmat > 0 && (!mat || !total))) { rc = fail(THISTLE_ERR_ARG, "missing 2-RDM rows"); goto done; }
@@ -644,7 +671,7 @@ static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const dou
     if (nmat > 0 && !finite_all(total, nmat)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 2-RDM value"); goto done; }
     P->nmat = nmat;
   }
-  class_counts(P->gL, cnt);
+  class_counts(P->gL, cnt, P->kind == KIND_CMS);
   TB_TRY(setup_classes(P, cnt, P->kind));
   tr.mark("validation, classes");
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
@@ -776,6 +803,7 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
   a.rho = P->d_rho;
   a.np = P->np;
   a.zao = P->d_zao;
+  a.zket = P->kind == KIND_CMS ? P->d_zao + (int64_t)P->ngto * P->ngto : P->d_zao;
   a.ngto = P->ngto;
   a.cutoffz = P->cutoffz;
   a.cutoffmd = P->cutoffmd;
@@ -1363,6 +1391,7 @@ static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t
     if (!P) return fail(THISTLE_ERR_ARG, "null plan in the batch");
     if (P->kind != plans[0]->kind) return fail(THISTLE_ERR_TYPE, "plans of one batch must share the calculation type");
     if (P->kind == KIND_ALIGNED) return fail(THISTLE_ERR_TYPE, "aligned plans cannot be batched");
+    if (P->kind == KIND_CMS) return fail(THISTLE_ERR_TYPE, "resolved CMS plans cannot be batched");
     if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "batched plans hold one geometry each");
     if (P->nq > STAGE2_QTILE) return fail(THISTLE_ERR_SHAPE, "batched plans need nq <= 1024");
   }
@@ -1654,6 +1683,7 @@ int thistle_plan_set_batch(thistle_plan *P, int32_t ngeom) {
   if (!P) return fail(THISTLE_ERR_ARG, "null plan");
   if (ngeom < 1 || ngeom > 65535) return fail(THISTLE_ERR_ARG, "ngeom must be 1..65535");
   if (P->kind == KIND_ALIGNED && ngeom != 1) return fail(THISTLE_ERR_TYPE, "aligned plans hold one geometry");
+  if (P->kind == KIND_CMS && ngeom != 1) return fail(THISTLE_ERR_TYPE, "resolved CMS plans hold one geometry");
   if (ngeom == P->ngeom) return THISTLE_OK;
   TB_CK(cudaStreamSynchronize(P->st));
   // every geometry starts at geometry 0's centres
@@ -1997,7 +2027,7 @@ int thistle_plan_density(const thistle_plan *P, double *out, int64_t count, int6
   if (P->kind == KIND_ALIGNED || P->kind == KIND_TOTAL || P->kind == KIND_J2) {
     *needed = P->np * P->np;
   } else {
-    *needed = (int64_t)P->ngto * P->ngto;
+    *needed = (int64_t)P->nzao * P->ngto * P->ngto;  // type 9: zi then zj
   }
   if (!out) return THISTLE_OK;
   if (count < *needed) return fail(THISTLE_ERR_ARG, "output holds " + std::to_string(count) + " doubles, the density " +

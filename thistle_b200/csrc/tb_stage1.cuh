@@ -100,6 +100,7 @@ TB_HD constexpr int reg_entries(int L, int S) {
 
 struct QuartetHead {
   int gi, gj, gk, gr, loop;
+  double w;  // loop weight
   bool p0;
   int skip;
   double Hx, Hy, Hz, h;
@@ -118,8 +119,16 @@ __device__ __forceinline__ QuartetHead quartet_head(const Stage1Args &A, int64_t
   Q.Hz = Q.tk[2] - Q.tb[2];
   Q.h = sqrt(Q.Hx * Q.Hx + Q.Hy * Q.Hy + Q.Hz * Q.Hz);
   Q.loop = quartet_loop(Q.gi, Q.gj, Q.gk, Q.gr);
+  Q.w = loop_weight(Q.loop);
   // the aligned kernel has no P = Q branch (tot_integral_k_ijkr_alig, src/Integrals.f90:5588-5727)
   Q.p0 = KIND == KIND_ALIGNED ? false : (Q.loop == 5 || Q.h < A.cutoffcentre);
+  if (KIND == KIND_CMS) {
+    // resolved_cms_integration: weight 2 for each off-diagonal side (4, 2, 2,
+    // 1), and the P = Q branch only where h < cutoffcentre, loop 4 included
+    // (src/Integrals.f90:2698-2716, 2908-2919)
+    Q.w = (Q.gi < Q.gj ? 2.0 : 1.0) * (Q.gk < Q.gr ? 2.0 : 1.0);
+    Q.p0 = Q.h < A.cutoffcentre;
+  }
   // |E| < 1e-30 skips that the reference keeps (bit: MDL MDM MDN MDLp MDMp):
   // a skipped factor removes every term it multiplies, i.e. it is a zero.
   Q.skip = (Q.p0 || KIND == KIND_ALIGNED || kind_elastic(KIND)) ? 0x1f : (KIND == KIND_TOTAL ? 0x00 : 0x0f);
@@ -140,7 +149,7 @@ template <int L, int KIND, int S>
 __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const QuartetHead &Q, const double *D, int dstride,
                                               int64_t qi, int sub, unsigned gmask) {
   if (A.s2key && sub == 0) A.s2key[qi] = ((uint32_t)A.cls << 6) | (Q.p0 ? 0u : h_bucket(Q.h));
-  const double pre = loop_weight(Q.loop) * Q.tb[4] * Q.tk[4];
+  const double pre = Q.w * Q.tb[4] * Q.tk[4];
   double *r = A.rec + A.recbase + (qi - A.qbegin) * (int64_t)A.rs;
   const bool leader = sub == 0;
   if (KIND == KIND_ALIGNED) {
@@ -236,7 +245,7 @@ __device__ __forceinline__ void stage1_finish(const Stage1Args &A, const Quartet
 #pragma unroll
     for (int b = 0; b <= LB; ++b) hh[b] *= f;
   }
-  if (KIND == KIND_ELASTIC) {
+  if (KIND == KIND_ELASTIC || KIND == KIND_CMS) {
     // integral_k_ijkr returns F = 0 when sum(h_saved) == 0 (src/Integrals.f90:5883-5886)
     double sum = 0.0;
 #pragma unroll
@@ -352,7 +361,7 @@ __device__ __forceinline__ void stage1_reg_body(Stage1Args &A, int64_t vb) {
       const int ncd = nk * nr;
       auto fetch = [&](int ic, int id, double &zo, double *kxo, double *kyo, double *kzo) {
         const int fc = sk + ic, fd = sr + id;
-        if (kind_elastic(KIND)) zo = A.zao[(size_t)fc * A.ngto + fd] * zab;
+        if (kind_elastic(KIND)) zo = A.zket[(size_t)fc * A.ngto + fd] * zab;
         else zo = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
         const int lc = A.flmn[fc], ld = A.flmn[fd];
         const double *ex = esoa_slot(A, Q.skip & 8, 0, lc & 0xff, ld & 0xff, pk);
@@ -535,7 +544,7 @@ __device__ __forceinline__ void stage1_smem_body(Stage1Args &A, int64_t vb) {
     }
     const int fc = sk + cd / nr, fd = sr + cd % nr;
     double ztot;
-    if (kind_elastic(KIND)) ztot = A.zao[(size_t)fc * A.ngto + fd] * zab;
+    if (kind_elastic(KIND)) ztot = A.zket[(size_t)fc * A.ngto + fd] * zab;
     else ztot = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
     if (fabs(ztot) < A.cutoffz) continue;
     const int lc = A.flmn[fc], ld = A.flmn[fd];
@@ -675,14 +684,14 @@ __device__ __forceinline__ void xk_contract(const Stage1Args &A, const QuartetHe
     rowp = kind_elastic(KIND) ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
     zo = kind_elastic(KIND) ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
   } else {
-    zo = kind_elastic(KIND) ? A.zao[(size_t)fc * A.ngto + fd] : 0.0;
+    zo = kind_elastic(KIND) ? A.zket[(size_t)fc * A.ngto + fd] : 0.0;
   }
   for (int c = 0; c < S.nin; ++c) {
     int ga, gb2, gc, gd;
     if (XB) { ga = S.si + c / S.nj; gb2 = S.sj + c % S.nj; gc = fc; gd = fd; }
     else { gc = S.sk + c / S.nr; gd = S.sr + c % S.nr; ga = fa; gb2 = fb; }
     double z;
-    if (kind_elastic(KIND)) z = A.zao[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
+    if (kind_elastic(KIND)) z = (XB ? A.zao : A.zket)[(size_t)(XB ? ga : gc) * A.ngto + (XB ? gb2 : gd)] * zo;
     else {
       const int64_t rp = XB ? fpair(min(ga, gb2), max(ga, gb2)) * A.np : rowp;
       z = A.rho[rp + fpair(min(gc, gd), max(gc, gd))];

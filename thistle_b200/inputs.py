@@ -311,6 +311,18 @@ def config3_ab6(nq: int = 500, natoms: int = 7) -> Problem:
     return _problem(name, atoms, shells, 40, 70, q_grid(15.0, nq), rng, density=0.05)
 
 
+def cms_onerdms(prob: Problem, seed: int = SEED0 + 9):
+    """Two seeded transition-like 1-RDMs for the resolved CMS (type 9): the
+    bra's (states 1-3) and the ket's (states 2-3), nonsymmetric, on the scale
+    of ``prob.onerdm``."""
+    rng = np.random.default_rng(seed)
+    n = prob.onerdm.shape[0]
+    s = float(np.max(np.abs(prob.onerdm)))
+    a = prob.onerdm + 0.3 * s * rng.standard_normal((n, n))
+    b = 0.5 * prob.onerdm + 0.3 * s * rng.standard_normal((n, n))
+    return a, b
+
+
 def hexagon(radius: float = 2.64) -> np.ndarray:
     ang = np.arange(6) * np.pi / 3.0
     return np.stack([radius * np.cos(ang), radius * np.sin(ang), np.zeros(6)], axis=1)

@@ -19,7 +19,10 @@ Input formats (written by src/File_creator_pyscf.py:109-255):
   mcci, hf); ``qmin qmax npoints``; the type; ``state1 state2 state3``; the
   output file name; three logicals (molpro, molcas, bagel); then for the
   RDM branch the word ``readrdm`` and the 1-RDM and 2-RDM file names
-  (read_onerdm / read_twordm formats, src/one_rdm.f90:2072-2147).
+  (read_onerdm / read_twordm formats, src/one_rdm.f90:2072-2147).  Type 9
+  (resolved CMS) reads both names as 1-RDM files: the bra's (states 1-3)
+  and the ket's (states 2-3).  Type 10 stops with the reference's reason:
+  its tot_integration_j1 stops before integrating (src/Integrals.f90:526-527).
 
 The q grid is linspace_1(qmin, qmax, npoints) (src/linspace.f90).  A q of 0
 makes the reference divide by zero (NaN in its output); here it is replaced
@@ -138,16 +141,22 @@ def run(directory: str = ".") -> str:
         print("thistle_b200.main: q <= 0 replaced by 1e-10 (the reference divides by q there)", file=sys.stderr)
         q = np.where(q <= 0.0, 1e-10, q)
     t = o["type"]
-    mat = total = onerdm = None
+    mat = total = onerdm = onerdm2 = None
+    if t == MC.TOTAL_J1:
+        raise SystemExit("thistle_b200.main: type 10 (total j1) is not computed by the reference either: "
+                         "tot_integration_j1 stops before integrating (src/Integrals.f90:526-527)")
     if t in (MC.TOTAL_J0, MC.TOTAL_J2, MC.TOTAL_ELECTRON):
         mat, total = MC.read_twordm(path(o["file_twordm"]))
     if t in (MC.ELASTIC_J0, MC.ELASTIC_J2, MC.ELASTIC_ALIGNED, MC.TOTAL_ELECTRON, MC.ELASTIC_ELECTRON):
         onerdm = MC.read_onerdm(path(o["file_onerdm"]))
+    if t == MC.RESOLVED_CMS:
+        onerdm = MC.read_onerdm(path(o["file_onerdm"]))
+        onerdm2 = MC.read_onerdm(path(o["file_twordm"]))
     nq = o["npoints"] if t not in (MC.TOTAL_ALIGNED,) else 3131
     qabs, result = MC.total_scattering_calculation(
         t, o["atoms"], o["geom"], o["state1"], o["state2"], int(l.max()), l.size, int(group.max()), ga, l, m, n,
         xx, yy, zz, mmod, q if t != MC.TOTAL_ALIGNED else np.zeros(3131), nq, group, o["cutoffz"],
-        o["cutoffmd"], o["cutoffcentre"], mat=mat, total=total, onerdm=onerdm)
+        o["cutoffmd"], o["cutoffcentre"], mat=mat, total=total, onerdm=onerdm, onerdm2=onerdm2)
     qout = q if t not in (MC.TOTAL_ALIGNED, MC.ELASTIC_ALIGNED) else qabs
     out = path(o["file_out"])
     with open(out, "w") as f:

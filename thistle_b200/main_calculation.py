@@ -30,6 +30,8 @@ TOTAL_J2 = 7
 ELASTIC_J2 = 8
 TOTAL_ELECTRON = 5
 ELASTIC_ELECTRON = 6
+RESOLVED_CMS = 9
+TOTAL_J1 = 10  # refused: the reference's tot_integration_j1 stops before integrating
 
 
 def read_twordm(filename):
@@ -70,11 +72,31 @@ def read_onerdm(filename):
     return D
 
 
+def _onerdms(onerdm, onerdm2):
+    """Column-major 1-RDM argument of the C-ABI: one matrix, or for the
+    resolved CMS the bra's and the ket's back to back."""
+    if onerdm is None:
+        return None, 0
+    one = colmajor_f64(onerdm)
+    nmo1 = int(np.asarray(onerdm).shape[0])
+    if onerdm2 is not None:
+        if np.shape(onerdm2) != np.shape(onerdm):
+            raise ValueError("the two 1-RDMs of the resolved CMS must have one shape")
+        one = np.concatenate([one, colmajor_f64(onerdm2)])
+    return one, nmo1
+
+
 def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy, zz,
                                  mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=None, total=None,
-                                 onerdm=None):
+                                 onerdm=None, onerdm2=None):
     """I(q) for calculation ``type`` (1 total j0, 2 elastic j0, 3 total aligned, 4 elastic aligned,
-    5 total electron, 6 elastic electron, 7 total j2, 8 elastic j2).
+    5 total electron, 6 elastic electron, 7 total j2, 8 elastic j2, 9 resolved CMS).
+
+    Type 9 (CASE(9), src/main_calculation.f90:438-471) takes two 1-RDMs:
+    ``onerdm`` for the bra's density zi and ``onerdm2`` for the ket's zj (the
+    reference's transition 1-RDMs of states 1-3 and 2-3).  Type 10 raises
+    :class:`ThistleError`: the reference's tot_integration_j1 stops before it
+    integrates (src/Integrals.f90:526-527).
 
     Types 5 and 6 return I_e - 2 Ine + Inn (I_e the total or elastic j0
     intensity, Ine the nuclear-electron term, Inn the nuclear-nuclear sinc
@@ -102,8 +124,9 @@ def total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng,
     matcm = colmajor_i32(mat) if mat is not None else None
     tot = _abi.as_f64(total) if total is not None else None
     nmat = 0 if mat is None else int(np.asarray(mat).shape[0])
-    one = colmajor_f64(onerdm) if onerdm is not None else None
-    nmo1 = 0 if onerdm is None else int(np.asarray(onerdm).shape[0])
+    if type == RESOLVED_CMS and (onerdm is None or onerdm2 is None):
+        raise ValueError("type 9 needs onerdm and onerdm2")
+    one, nmo1 = _onerdms(onerdm, onerdm2 if type == RESOLVED_CMS else None)
     Zn = _abi.as_f64(Zn) if Zn is not None else None
     natoms = 0
     if geom is not None:
@@ -127,24 +150,29 @@ def total_scattering_calculation_2(type, Zn, geom, state1, state2, maxl, ngto, n
                                    mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, fileJ, fileJ_2,
                                    readrdm=True):
     """The ``readrdm`` branch of total_scattering_calculation_2: type 1 and 7
-    read the 2-RDM from ``fileJ_2``, types 2 and 8 the 1-RDM from ``fileJ``."""
+    read the 2-RDM from ``fileJ_2``, types 2 and 8 the 1-RDM from ``fileJ``;
+    type 9 reads its two 1-RDMs (bra, then ket) from ``fileJ`` and
+    ``fileJ_2`` (the reference builds them from CI files there,
+    src/main_calculation.f90:820-846, which is upstream of this path)."""
     if not readrdm:
         raise ThistleError(-7, "only the readrdm path is provided; CI-vector RDM construction is upstream")
-    mat = total = onerdm = None
+    mat = total = onerdm = onerdm2 = None
     if type in (TOTAL_J0, TOTAL_J2):
         mat, total = read_twordm(fileJ_2)
     elif type in (ELASTIC_J0, ELASTIC_J2):
         onerdm = read_onerdm(fileJ)
+    elif type == RESOLVED_CMS:
+        onerdm, onerdm2 = read_onerdm(fileJ), read_onerdm(fileJ_2)
     return total_scattering_calculation(type, Zn, geom, state1, state2, maxl, ngto, ng, ga, l, m, n, xx, yy,
                                         zz, mmod, q, nq, group, cutoffz, cutoffmd, cutoffcentre, mat=mat,
-                                        total=total, onerdm=onerdm)
+                                        total=total, onerdm=onerdm, onerdm2=onerdm2)
 
 
 class ScatteringPlan:
     """One basis + density + q grid on the device, executed per geometry."""
 
     def __init__(self, type, ga, l, m, n, xx, yy, zz, group, mmod, q, cutoffz, cutoffmd, cutoffcentre,
-                 mat=None, total=None, onerdm=None):
+                 mat=None, total=None, onerdm=None, onerdm2=None):
         self._p = C.c_void_p()
         self.type = int(type)
         self._keep = [_abi.as_f64(ga), _abi.as_i32(l), _abi.as_i32(m), _abi.as_i32(n), _abi.as_f64(xx),
@@ -166,22 +194,24 @@ class ScatteringPlan:
         mcm = colmajor_f64(mmod)
         matcm = colmajor_i32(mat) if mat is not None else None
         tot = _abi.as_f64(total) if total is not None else None
-        one = colmajor_f64(onerdm) if onerdm is not None else None
+        one, nmo1 = _onerdms(onerdm, onerdm2 if self.type == RESOLVED_CMS else None)
         rc = _abi.lib().thistle_plan_create(
             C.byref(self._p), self.type, self.ngto, dptr(ga), iptr(l), iptr(m), iptr(n), dptr(xx), dptr(yy),
             dptr(zz), iptr(group), dptr(mcm), int(mmod.shape[0]), iptr(matcm), dptr(tot),
             0 if mat is None else int(np.asarray(mat).shape[0]), dptr(one),
-            0 if onerdm is None else int(np.asarray(onerdm).shape[0]), dptr(self.q), self.nq, float(cutoffz),
+            nmo1, dptr(self.q), self.nq, float(cutoffz),
             float(cutoffmd), float(cutoffcentre))
         check(rc)
 
     @classmethod
-    def from_problem(cls, prob, type=TOTAL_J0, q=None):
+    def from_problem(cls, prob, type=TOTAL_J0, q=None, onerdm2=None):
+        """Plan of a Problem; type 9 takes ``prob.onerdm`` for the bra and
+        ``onerdm2`` for the ket."""
+        one = type in (ELASTIC_J0, ELASTIC_J2, RESOLVED_CMS)
         return cls(type, prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.group, prob.mmod,
                    prob.q if q is None else q, prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
-                   mat=prob.mat if type not in (ELASTIC_J0, ELASTIC_J2) else None,
-                   total=prob.total if type not in (ELASTIC_J0, ELASTIC_J2) else None,
-                   onerdm=prob.onerdm if type in (ELASTIC_J0, ELASTIC_J2) else None)
+                   mat=prob.mat if not one else None, total=prob.total if not one else None,
+                   onerdm=prob.onerdm if one else None, onerdm2=onerdm2)
 
     def set_centres(self, xx, yy, zz):
         xx, yy, zz = (_abi.as_f64(a) for a in (xx, yy, zz))
@@ -304,11 +334,14 @@ class ScatteringPlan:
 
     def density(self):
         """The transformed density: the pair density (np, np) of total / j2 /
-        aligned plans, the AO density (ngto, ngto) of elastic plans."""
+        aligned plans, the AO density (ngto, ngto) of elastic plans, and the
+        two (zi, zj) of a resolved CMS plan as (2, ngto, ngto)."""
         need = C.c_int64(0)
         check(_abi.lib().thistle_plan_density(self._p, None, 0, C.byref(need)))
         out = np.zeros(need.value)
         check(_abi.lib().thistle_plan_density(self._p, dptr(out), need.value, C.byref(need)))
+        if self.type == RESOLVED_CMS:
+            return np.stack([z.reshape(self.ngto, self.ngto, order="F") for z in out.reshape(2, -1)])
         k = int(round(np.sqrt(need.value)))
         return out.reshape(k, k) if self.type not in (ELASTIC_J0, ELASTIC_J2) else out.reshape(k, k, order="F")
 
@@ -457,16 +490,17 @@ def aligned(prob, qvec=None):
         return pl.execute_aligned()
 
 
-def scattering(prob, type=TOTAL_J0, q=None, Zn=None):
+def scattering(prob, type=TOTAL_J0, q=None, Zn=None, onerdm2=None):
     """I(q) of an :class:`thistle_b200.inputs.Problem` through Entry 1
-    (types 5 and 6: nuclei at ``prob.atoms`` with charges ``Zn``)."""
+    (types 5 and 6: nuclei at ``prob.atoms`` with charges ``Zn``; type 9:
+    ``prob.onerdm`` on the bra, ``onerdm2`` on the ket)."""
     qv = prob.q if q is None else np.asarray(q, dtype=np.float64)
     two = type in (TOTAL_J0, TOTAL_J2, TOTAL_ELECTRON)
-    one = type in (ELASTIC_J0, ELASTIC_J2, ELASTIC_ALIGNED, TOTAL_ELECTRON, ELASTIC_ELECTRON)
+    one = type in (ELASTIC_J0, ELASTIC_J2, ELASTIC_ALIGNED, TOTAL_ELECTRON, ELASTIC_ELECTRON, RESOLVED_CMS)
     _, res = total_scattering_calculation(
         type, Zn, prob.atoms, 0, 0, int(max(prob.l.max(), prob.m.max(), prob.n.max())), prob.ngto, prob.ng,
         prob.ga, prob.l, prob.m, prob.n, prob.xx, prob.yy, prob.zz, prob.mmod, qv, qv.size, prob.group,
         prob.cutoffz, prob.cutoffmd, prob.cutoffcentre,
         mat=prob.mat if two else None, total=prob.total if two else None,
-        onerdm=prob.onerdm if one else None)
+        onerdm=prob.onerdm if one else None, onerdm2=onerdm2)
     return res
