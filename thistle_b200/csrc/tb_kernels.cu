@@ -403,13 +403,27 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
 #ifndef TB_S1_XK_MIN
 #define TB_S1_XK_MIN 4
 #endif
-// LLmax 4-6 always; 7-8 (a thread per quartet holding 120 / 165 density
-// entries, one block of 128 per SM) only with at least this many quartets
-// per SM, below which the register kernel's 32 threads per quartet fill the
-// GPU better
+// LLmax 4-6 always; 7-8 with at least this many quartets per SM.  On the
+// 7-atom AB6 step the split contracted-side kernels take class 7 (7315
+// quartets, 49 per SM) in 0.52 ms where the register kernel's 32 threads per
+// quartet took 1.10; class 8 (441 quartets, 3 per SM: a thread per quartet
+// leaves the convolution kernel on a few SMs) stays on the register kernel
+// (0.33 ms against 0.76).
 #ifndef TB_S1_XK_HIGH_PER_SM
-#define TB_S1_XK_HIGH_PER_SM 512
+#define TB_S1_XK_HIGH_PER_SM 16
 #endif
+#ifndef TB_S1_TPL_MAXL
+#define TB_S1_TPL_MAXL 3
+#endif
+bool stage1_tpl(int kind, int L, int shells_canonical) {
+  return kind == KIND_TOTAL && shells_canonical && L <= TB_S1_TPL_MAXL;
+}
+
+cudaError_t launch_stage1_tpl(int kind, int tuple, const Stage1Args &a, int ngeom, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_tpl_k<KIND_TOTAL>(tuple, a, ngeom, st);
+  return cudaErrorInvalidValue;
+}
+
 bool stage1_xk(int L, int64_t nquart, int nsm) {
   if (L < TB_S1_XK_MIN) return false;
   if (L <= 6) return true;

@@ -40,6 +40,10 @@ struct Stage1Args {
   // contraction threads per quartet
   int64_t xoff;
   int xstride, xg;
+  // every group of an s, p, d or f shell holds its (L+1)(L+2)/2 Cartesian
+  // components in the order cart_component gives (the shell-templated
+  // stage-1 kernels rely on it)
+  int shells_canonical;
 };
 
 constexpr int MAXCLS = 20;
@@ -146,6 +150,12 @@ cudaError_t launch_pair_tables(int ng, int maxa, const int *gstart, const int *f
                                int64_t gs_tab, int64_t gs_esoa, cudaStream_t st);
 template <int K>
 cudaError_t launch_stage1_k(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
+// Shell-templated stage 1 (one shell tuple ((Li 5 + Lj) 5 + Lk) 5 + Lr per
+// launch): whether a class of this kind and LLmax takes it, and its launcher.
+bool stage1_tpl(int kind, int L, int shells_canonical);
+template <int K>
+cudaError_t launch_stage1_tpl_k(int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
+cudaError_t launch_stage1_tpl(int kind, int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 template <int K>
 cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);

@@ -54,6 +54,18 @@ TB_HD constexpr bool kind_j2(int k) { return k == KIND_J2 || k == KIND_ELASTIC_J
 TB_HD constexpr bool kind_elastic(int k) { return k == KIND_ELASTIC || k == KIND_ELASTIC_J2 || k == KIND_CMS; }
 enum RecKind { REC_BESSEL = 0, REC_BESSEL_J2 = 1, REC_P0 = 2 };
 
+// Cartesian component i (axis 0, 1, 2 exponent) of an s, p, d or f shell, in
+// the order of the molden convention the reference reads
+// (src/molden_reader_nikola.py:196-240): p x y z; d xx yy zz xy xz yz;
+// f xxx yyy zzz xyy xxy xxz xzz yzz yyz xyz.
+TB_HD constexpr int cart_component(int L, int i, int axis) {
+  constexpr int t1[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  constexpr int t2[6][3] = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+  constexpr int t3[10][3] = {{3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {1, 2, 0}, {2, 1, 0},
+                             {2, 0, 1}, {1, 0, 2}, {0, 1, 2}, {0, 2, 1}, {1, 1, 1}};
+  return L == 0 ? 0 : L == 1 ? t1[i][axis] : L == 2 ? t2[i][axis] : t3[i][axis];
+}
+
 // number of (T,U,V) with T+U+V <= L
 TB_HD constexpr int ntuv(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
 // simplex index of (T,U,V)

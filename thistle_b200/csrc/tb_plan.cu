@@ -87,9 +87,16 @@ struct SubRange {
   int nout = 0;  // most function pairs of an outer (convolved) side; 0: unknown
 };
 
+// quartets of one shell tuple ((Li 5 + Lj) 5 + Lk) 5 + Lr within a class
+struct TupleRange {
+  int tuple;
+  int64_t begin, end;
+};
+
 struct thistle_plan {
   int type = 0, kind = 0;
   int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nzao = 1, nq = 0, maxa = 0, nmat = 0;
+  int shells_canonical = 1;  // s, p, d, f groups: complete shells in cart_component order
   double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
   std::vector<int> gstart, gcount, gL, flmn;
   std::vector<double> hq;            // host copy of the q grid (aligned: interleaved q vectors)
@@ -100,6 +107,7 @@ struct thistle_plan {
   int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
   int cls_rs[MAXCLS];
   std::vector<SubRange> cls_sub[MAXCLS];
+  std::vector<TupleRange> cls_tup[MAXCLS];
   double *d_xbuf = nullptr;  // contraction output of the split contracted-side stage 1
   int64_t xbuf_len = 0;
   int64_t rec_total = 0;
@@ -202,6 +210,13 @@ static int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const in
     if (P->gstart[g] < 0) return fail(THISTLE_ERR_SHAPE, "group " + std::to_string(g + 1) + " has no function");
     int h = P->gstart[g];
     P->gL[g] = l[h] + m[h] + n[h];
+    if (P->gL[g] <= 3) {
+      bool ok = P->gcount[g] == (P->gL[g] + 1) * (P->gL[g] + 2) / 2;
+      for (int i = 0; ok && i < P->gcount[g]; ++i)
+        ok = l[h + i] == cart_component(P->gL[g], i, 0) && m[h + i] == cart_component(P->gL[g], i, 1) &&
+             n[h + i] == cart_component(P->gL[g], i, 2);
+      if (!ok) P->shells_canonical = 0;
+    }
     for (int i = h; i < h + P->gcount[g]; ++i) {
       if (ga[i] != ga[h] || xx[i] != xx[h] || yy[i] != yy[h] || zz[i] != zz[h] ||
           l[i] + m[i] + n[i] != P->gL[g])
@@ -295,6 +310,7 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
     P->cls_recoff[k] = recoff;
     // sub-ranges in key order: (LK, XB) ascending
     P->cls_sub[k].clear();
+    P->cls_tup[k].clear();
     int64_t sp = pos;
     for (int LK = 0; LK <= 8; ++LK)
       for (int XB = 0; XB <= 1; ++XB) {
@@ -305,6 +321,7 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
           const uint32_t key = quartet_key(Li, Lj, Lk, Lr);
           if ((int)(key / KEY_CLASS_DIV) != LL || (int)((key / 625) % 18) != LK * 2 + XB) continue;
           if (cnt[LL * 625 + t] == 0) continue;
+          P->cls_tup[k].push_back(TupleRange{t, sp + sc, sp + sc + cnt[LL * 625 + t]});
           sc += cnt[LL * 625 + t];
           // the outer side is the ket when LK is the bra's
           nout = std::max(nout, XB ? maxg[Lk] * maxg[Lr] : maxg[Li] * maxg[Lj]);
@@ -820,6 +837,7 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
   a.cls = 0;
   a.gs_pair = gs_pair(P);
   a.gs_esoa = gs_esoa(P);
+  a.shells_canonical = P->shells_canonical;
   a.gs_rec = gs_rec(P);
   a.xoff = 0;
   a.xstride = 0;
@@ -829,7 +847,8 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
 
 static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
-                      const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom) {
+                      const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom,
+                      const std::vector<TupleRange> *tups) {
   // stage events (not while a graph is being captured)
   cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
   auto mark = [&](int i) -> cudaError_t { return P->capturing ? cudaSuccess : cudaEventRecord(E[i], P->st); };
@@ -845,7 +864,17 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
     a.p0count = (unsigned long long *)(P->d_p0count + c);
     a.s2key = (order && P->kind != KIND_ALIGNED) ? P->d_s2key : nullptr;
     a.cls = c;
-    if (stage1_xk(cL[c], (ce[c] - cb[c]) * ngeom, P->nsm)) {
+    if (tups && stage1_tpl(P->kind, cL[c], P->shells_canonical)) {
+      // shell-templated kernels, one launch per shell tuple of the class
+      for (const TupleRange &u : tups[c]) {
+        Stage1Args b = a;
+        b.qbegin = u.begin;
+        b.qend = u.end;
+        b.recbase = recoff[c] + (u.begin - cb[c]) * (int64_t)rs[c];
+        TB_CK(launch_stage1_tpl(P->kind, u.tuple, b, ngeom, P->st));
+        P->launches += 1;
+      }
+    } else if (stage1_xk(cL[c], (ce[c] - cb[c]) * ngeom, P->nsm)) {
       for (const SubRange &u : subs[c]) {
         Stage1Args b = a;
         b.qbegin = u.begin;
@@ -932,7 +961,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       const int64_t nblk = (items + STAGE2_WARPS - 1) / STAGE2_WARPS;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
       TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->st));
-      P->launches += 1;
+      P->launches += 2;  // lean points, then checked prefixes
     }
   }
   TB_CK(mark(3));
@@ -944,7 +973,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
 
 static int plan_exec(thistle_plan *P, double *d_out) {
   int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                      P->cls_rs, P->cls_sub, d_out, true, P->ngeom);
+                      P->cls_rs, P->cls_sub, d_out, true, P->ngeom, P->cls_tup);
   P->fwd_valid = rc == THISTLE_OK;
   return rc;
 }
@@ -1056,7 +1085,7 @@ static int forward_batch(thistle_plan *P) {
     TB_CK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
     P->capturing = true;
     int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
-                        P->cls_rs, P->cls_sub, P->d_result, true, P->ngeom);
+                        P->cls_rs, P->cls_sub, P->d_result, true, P->ngeom, P->cls_tup);
     P->capturing = false;
     cudaError_t e = cudaStreamEndCapture(P->st, &g);
     if (rc != THISTLE_OK) {
@@ -1994,7 +2023,7 @@ int thistle_plan_execute_quartets(thistle_plan *P, const int32_t *quartets, int6
   if (nquart == 0) {
     TB_TRYC(cudaMemsetAsync(P->d_result, 0, sizeof(double) * P->nq, P->st));
   } else {
-    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, sub, P->d_result, false, 1));
+    TB_TRY(run_stages(P, dq, cb, ce, cL, ncls, drec, ro, rs, sub, P->d_result, false, 1, nullptr));
   }
   TB_TRYC(cudaMemcpyAsync(result_host, P->d_result, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
   TB_TRYC(cudaStreamSynchronize(P->st));

@@ -483,6 +483,147 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L))
 }
 
 // ---------------------------------------------------------------------------
+// shell-templated kernel (total j0, LLmax <= 3), thread per quartet
+// ---------------------------------------------------------------------------
+// The register kernel's arithmetic for one shell tuple (Li, Lj, Lk, Lr) of a
+// class, on plans whose s-f groups hold their Cartesian components in the
+// cart_component order: every function's exponents, and with them every E
+// index, are compile-time constants, so all of a quartet's density and E
+// loads are independent (issued ahead of the arithmetic) and repeated E
+// values and convolutions are shared between function quartets.  The values
+// and the order of the operations are those of stage1_reg_kernel, so the
+// density D_TUV is bit-identical to it.
+#ifndef TB_S1_TPL_MAXL
+#define TB_S1_TPL_MAXL 3
+#endif
+
+template <int Li, int Lj, int Lk, int Lr, int KIND>
+__global__ void __launch_bounds__(128) stage1_tpl_kernel(Stage1Args A) {
+  constexpr int L = Li + Lj + Lk + Lr;
+  constexpr int ni = (Li + 1) * (Li + 2) / 2, nj = (Lj + 1) * (Lj + 2) / 2;
+  constexpr int nk = (Lk + 1) * (Lk + 2) / 2, nr = (Lr + 1) * (Lr + 2) / 2;
+  constexpr int TMAX = L < 2 * MAXA ? L : 2 * MAXA;
+  stage1_geometry(A);
+  extern __shared__ double sD[];  // ntuv(L) x 128
+  const int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= A.qend) return;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const int si = A.gstart[Q.gi], sj = A.gstart[Q.gj], sk = A.gstart[Q.gk], sr = A.gstart[Q.gr];
+  const double *tb = A.pairtab + (size_t)pair_index(Q.gi, Q.gj, A.ng) * PAIR_STRIDE + 8;
+  const double *tk = A.pairtab + (size_t)pair_index(Q.gk, Q.gr, A.ng) * PAIR_STRIDE + 8;
+  // E^{l1 l2}_t of one axis of a pair, with this quartet's |E| < 1e-30 skip
+  auto ecoef = [&](const double *tab, int ax, int l1, int l2, int t, bool skip) -> double {
+    const double v = tab[ax * ESZ + (l1 * (MAXA + 1) + l2) * E_T + t];
+    return (skip && fabs(v) < TB_SKIP30) ? 0.0 : v;
+  };
+  double D[ntuv(L)];
+#pragma unroll
+  for (int e = 0; e < ntuv(L); ++e) D[e] = 0.0;
+#pragma unroll
+  for (int a = 0; a < ni; ++a)
+#pragma unroll
+    for (int b = 0; b < nj; ++b) {
+      const int fa = si + a, fb = sj + b;
+      const int64_t rowp = fpair(min(fa, fb), max(fa, fb)) * A.np;
+      // bra coefficients with the (-1)^t sign of src/Integrals.f90:5181
+      double bx[L + 1], by[L + 1], bz[L + 1];
+#pragma unroll
+      for (int t = 0; t <= L; ++t) {
+        const int x1 = cart_component(Li, a, 0), x2 = cart_component(Lj, b, 0);
+        const int y1 = cart_component(Li, a, 1), y2 = cart_component(Lj, b, 1);
+        const int z1 = cart_component(Li, a, 2), z2 = cart_component(Lj, b, 2);
+        const double vx = (t <= TMAX && t <= x1 + x2) ? ecoef(tb, 0, x1, x2, t, Q.skip & 1) : 0.0;
+        const double vy = (t <= TMAX && t <= y1 + y2) ? ecoef(tb, 1, y1, y2, t, Q.skip & 2) : 0.0;
+        const double vz = (t <= TMAX && t <= z1 + z2) ? ecoef(tb, 2, z1, z2, t, Q.skip & 4) : 0.0;
+        bx[t] = (t & 1) ? -vx : vx;
+        by[t] = (t & 1) ? -vy : vy;
+        bz[t] = (t & 1) ? -vz : vz;
+      }
+#pragma unroll
+      for (int c = 0; c < nk; ++c)
+#pragma unroll
+        for (int d = 0; d < nr; ++d) {
+          const int fc = sk + c, fd = sr + d;
+          double z = A.rho[rowp + fpair(min(fc, fd), max(fc, fd))];
+          const int x1 = cart_component(Lk, c, 0), x2 = cart_component(Lr, d, 0);
+          const int y1 = cart_component(Lk, c, 1), y2 = cart_component(Lr, d, 1);
+          const int z1 = cart_component(Lk, c, 2), z2 = cart_component(Lr, d, 2);
+          double kx[TMAX + 1], ky[TMAX + 1], kz[TMAX + 1];
+#pragma unroll
+          for (int t = 0; t <= TMAX; ++t) {
+            kx[t] = t <= x1 + x2 ? ecoef(tk, 0, x1, x2, t, Q.skip & 8) : 0.0;
+            ky[t] = t <= y1 + y2 ? ecoef(tk, 1, y1, y2, t, Q.skip & 16) : 0.0;
+            kz[t] = t <= z1 + z2 ? ecoef(tk, 2, z1, z2, t, false) : 0.0;
+          }
+          // the reference skips primitive quartets with |ztot| < cutoffz
+          z = fabs(z) < A.cutoffz ? 0.0 : z;
+          double Cx[L + 1], Cy[L + 1], Cz[L + 1];
+#pragma unroll
+          for (int T = 0; T <= L; ++T) {
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+            for (int t = 0; t <= T; ++t) {
+              if (T - t > TMAX) continue;
+              sx = fma(bx[t], kx[T - t], sx);
+              sy = fma(by[t], ky[T - t], sy);
+              sz = fma(bz[t], kz[T - t], sz);
+            }
+            Cx[T] = sx * z;
+            Cy[T] = sy;
+            Cz[T] = sz;
+          }
+          int e = 0;
+#pragma unroll
+          for (int T = 0; T <= L; ++T)
+#pragma unroll
+            for (int U = 0; U <= L - T; ++U) {
+              const double w = Cx[T] * Cy[U];
+#pragma unroll
+              for (int V = 0; V <= L - T - U; ++V, ++e) D[e] = fma(w, Cz[V], D[e]);
+            }
+        }
+    }
+  double *col = sD + threadIdx.x;
+#pragma unroll
+  for (int e = 0; e < ntuv(L); ++e) col[e * 128] = D[e];
+  stage1_finish<L, KIND, 1>(A, Q, col, 128, qi, 0, 1u << (threadIdx.x & 31));
+}
+
+// One launch per shell tuple of a class's sub-range (s = Li..Lr, packed as
+// ((Li 5 + Lj) 5 + Lk) 5 + Lr).
+template <int K>
+cudaError_t launch_stage1_tpl_k(int tuple, const Stage1Args &a, int ngeom, cudaStream_t st) {
+  const int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+#define TB_TPL(i, j, k, r)                                                                             \
+  case ((i * 5 + j) * 5 + k) * 5 + r: {                                                              \
+    const size_t smem = (size_t)ntuv(i + j + k + r) * sizeof(double) * 128;                          \
+    cudaError_t e = cudaFuncSetAttribute(stage1_tpl_kernel<i, j, k, r, K>,                           \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
+    if (e != cudaSuccess) return e;                                                                  \
+    stage1_tpl_kernel<i, j, k, r, K><<<dim3((unsigned)((n + 127) / 128), ngeom), 128, smem, st>>>(a); \
+    return cudaGetLastError();                                                                       \
+  }
+  switch (tuple) {
+    TB_TPL(0, 0, 0, 0)
+    TB_TPL(1, 0, 0, 0) TB_TPL(0, 1, 0, 0) TB_TPL(0, 0, 1, 0) TB_TPL(0, 0, 0, 1)
+#if TB_S1_TPL_MAXL >= 2
+    TB_TPL(2, 0, 0, 0) TB_TPL(0, 2, 0, 0) TB_TPL(0, 0, 2, 0) TB_TPL(0, 0, 0, 2)
+    TB_TPL(1, 1, 0, 0) TB_TPL(1, 0, 1, 0) TB_TPL(1, 0, 0, 1) TB_TPL(0, 1, 1, 0) TB_TPL(0, 1, 0, 1) TB_TPL(0, 0, 1, 1)
+#endif
+#if TB_S1_TPL_MAXL >= 3
+    TB_TPL(3, 0, 0, 0) TB_TPL(0, 3, 0, 0) TB_TPL(0, 0, 3, 0) TB_TPL(0, 0, 0, 3)
+    TB_TPL(2, 1, 0, 0) TB_TPL(2, 0, 1, 0) TB_TPL(2, 0, 0, 1) TB_TPL(1, 2, 0, 0) TB_TPL(0, 2, 1, 0) TB_TPL(0, 2, 0, 1)
+    TB_TPL(1, 0, 2, 0) TB_TPL(0, 1, 2, 0) TB_TPL(0, 0, 2, 1) TB_TPL(1, 0, 0, 2) TB_TPL(0, 1, 0, 2) TB_TPL(0, 0, 1, 2)
+    TB_TPL(1, 1, 1, 0) TB_TPL(1, 1, 0, 1) TB_TPL(1, 0, 1, 1) TB_TPL(0, 1, 1, 1)
+#endif
+    default: break;
+  }
+#undef TB_TPL
+  return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
 // shared-memory kernel (LLmax 9..16)
 // ---------------------------------------------------------------------------
 template <int L, int KIND>

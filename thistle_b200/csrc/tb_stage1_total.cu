@@ -4,6 +4,7 @@
 
 namespace tb {
 template cudaError_t launch_stage1_k<KIND_TOTAL>(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
+template cudaError_t launch_stage1_tpl_k<KIND_TOTAL>(int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
 template cudaError_t launch_stage1_xk_k<KIND_TOTAL>(int L, int LK, bool XB, const Stage1Args &a, int ngeom,
                                                       cudaStream_t st);
 template cudaError_t launch_stage1_xsplit_k<KIND_TOTAL>(int L, int LK, bool XB, const Stage1Args &a, double *xbuf,
