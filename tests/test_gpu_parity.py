@@ -202,4 +202,12 @@ def test_split_contraction_matches_fused(oracle, type_):
     with MC.ScatteringPlan.from_problem(p, type_) as pl:
         split = pl.execute()
         fused = pl.execute_quartets(qs[:, :4])
-    assert np.max(rel_err(split, fused)) < 1e-12
+    # the two runs also visit stage 2 in different orders (H-sorted or not);
+    # j2, a small residual of the j0 terms, is held to 1e-12 of itself plus
+    # 1e-14 of the j0 scale (the oracle criterion of j2, 100 times tighter)
+    if type_ == 7:
+        with MC.ScatteringPlan.from_problem(p, 1) as pl:
+            scale = np.max(np.abs(pl.execute()))
+        assert np.all(np.abs(split - fused) <= 1e-12 * np.abs(fused) + 1e-14 * scale)
+    else:
+        assert np.max(rel_err(split, fused)) < 1e-12

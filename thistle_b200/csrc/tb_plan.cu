@@ -961,7 +961,7 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
       const int64_t nblk = (items + STAGE2_WARPS - 1) / STAGE2_WARPS;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
       TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->st));
-      P->launches += 2;  // lean points, then checked prefixes
+      P->launches += 1;
     }
   }
   TB_CK(mark(3));

@@ -43,14 +43,9 @@ constexpr int RESEED = TB_S2_RESEED;
 // with room for the [H, s, kind, order] head in front of it.
 __device__ const double kZeroRecord[4 + LMAXB + 4] = {0};
 
-// The rare-branch helpers (small-x series, P = Q polynomial) are called, not
-// inlined, unless TB_S2_PATCH_INLINE is set: inlined they multiply the code of
-// the checked point loop by K x QB.
-#ifdef TB_S2_PATCH_INLINE
+// The rare-branch helpers (small-x series, P = Q polynomial) are inlined into
+// the checked point loop, which is not unrolled (K copies of each).
 #define TB_S2_PATCH_ATTR __forceinline__
-#else
-#define TB_S2_PATCH_ATTR __noinline__
-#endif
 
 // Series coefficients c_{n,k} and the downward-recurrence factors in constant
 // memory: FP64 instructions read them as constant-bank operands, where
@@ -79,10 +74,31 @@ __device__ __forceinline__ double series_u(double y) {
   return p;
 }
 
+// Crossover of the polynomial form (defined below) and the series terms it
+// needs: the polynomial-form classes (LB <= 8) switch to the series only
+// below poly_crossover(LB), where fewer terms of u_LB, u_LB+1 than
+// series_terms (sized for the recurrence crossover 0.75 LB) reach 1e-17:
+// the smallest NK with |c_{n,NK+1}| x_c^{2 (NK+1)} <= 1e-17 for both orders
+// (6, 8, 10, 11 terms for LB 2-5 against 12-16).
+TB_HD constexpr double poly_crossover(int LB);
+TB_HD constexpr int poly_series_terms(int LB) {
+  const double y = poly_crossover(LB) * poly_crossover(LB);
+  for (int nk = 1; nk < SER_K; ++nk) {
+    bool ok = true;
+    for (int n = LB; n <= LB + 1; ++n) {
+      double t = series_coef(n, nk + 1);
+      for (int j = 0; j <= nk; ++j) t *= y;
+      if ((t < 0 ? -t : t) > 1e-17) ok = false;
+    }
+    if (ok) return nk;
+  }
+  return SER_K;
+}
+
 // x below the crossover: coefficients read from the record (h[0..LB]).
 template <int LB>
 __device__ TB_S2_PATCH_ATTR double bessel_small(const double *__restrict__ h, double y) {
-  constexpr int NK = series_terms(LB);
+  constexpr int NK = LB <= 8 ? poly_series_terms(LB) : series_terms(LB);
   double uhi = series_u<LB + 1, NK>(y);
   double umid = series_u<LB, NK>(y);
   double acc = h[LB] * umid;
@@ -307,7 +323,10 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
     }
     // last point (exclusive) at which any lane of the warp may need a patch:
     // on an ascending uniform tile the series region of a quartet is a
-    // prefix of its points (q < x_c / H), P = Q lanes need every point
+    // prefix of its points (q < x_c / H), P = Q lanes need every point.
+    // Point 0 (below every crossover, often the drivers' 1e-10 off the grid)
+    // is taken apart by the block that starts the tile, so it alone makes no
+    // prefix.
     int mse = 0;
     {
       int lane_end = 0;
@@ -318,33 +337,20 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
           int e = nqb;
           if (A.uniform && nq > 1) {
             const double q1 = qs[1].x, qc = __longlong_as_double(qcb[k]);
-            e = qc <= q1 ? 2 : (int)min((double)nqb, ceil((qc - q1) / dq) + 3.0);
+            e = qc <= q1 ? 0 : (int)min((double)nqb, ceil((qc - q1) / dq) + 3.0);
           }
           lane_end = max(lane_end, e);
         }
       }
       mse = (int)__reduce_max_sync(0xffffffffu, (unsigned)lane_end);
     }
-    // One point of the tile for the warp's 32 K quartets, all K as
+    // One lean point of the tile for the warp's 32 K quartets, all K as
     // straight-line code.  Polynomial form: sum_k (A_k S_k + q B_k C_k) is
     // F q summed over the lanes' quartets (J2: F q^3), the common 1/q (1/q^3)
-    // applied once.  CHECKED points (the prefix before mse) first find the
-    // lanes below the crossover or on the P = Q branch and replace their
-    // terms by the series / polynomial value times the Gaussian g.
-    auto point = [&](const int m, auto checked) -> double {
-      constexpr bool CHECKED = decltype(checked)::value;
+    // applied once.
+    auto point = [&](const int m) -> double {
       const double2 qq = qs[m];
       const double q = qq.x, iq = qq.y;
-      bool sp[K];
-      bool any = false;
-      if constexpr (CHECKED) {
-        const long long qb = __double_as_longlong(q);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          sp[k] = (qb < qcb[k]) | (p0n[k] >= 0);
-          any |= sp[k];
-        }
-      }
       double FA = 0.0, FB = 0.0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -355,35 +361,13 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
           for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
 #pragma unroll
           for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
-          if (CHECKED && sp[k]) ae = bo = 0.0;
           FA = fma(ae, S[k], FA);
           FB = fma(bo, C[k], FB);
         } else {
           // the recurrence is linear in (sin, cos): fed z it gives F g
           double f = bessel_up<LB>(hh[k], q * H[k], S[k], C[k], iq * invH[k]);
           if (J2) f *= iq * iq;
-          if (CHECKED && sp[k]) f = 0.0;
           FA += f;
-        }
-      }
-      double X = 0.0;
-      if constexpr (CHECKED) {
-        if (any) {
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            if (!sp[k]) continue;
-            double v;
-            if (p0n[k] >= 0) {
-              v = p0_poly(hm[k], p0n[k], q * q);
-              if (POLY) v *= J2 ? q * q * q : q;
-            } else {
-              const double x = q * H[k];
-              v = bessel_small<LB>(hm[k], x * x);
-              if (POLY) v *= q;            // total: F q; j2: (F / q^2) q^3
-              else if (J2) v *= iq * iq;
-            }
-            X = fma(v, g[k], X);
-          }
         }
       }
 #pragma unroll
@@ -393,13 +377,54 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
         S[k] = s2;
         wr[k] *= kk[k];
         wi[k] *= kk[k];
-        if constexpr (CHECKED) {
-          g[k] *= rg[k];
-          rg[k] *= kk[k];
-        }
       }
-      if constexpr (POLY) return (fma(q, FB, FA) + X) * (J2 ? iq * iq * iq : iq);
-      else return FA + X;
+      if constexpr (POLY) return fma(q, FB, FA) * (J2 ? iq * iq * iq : iq);
+      else return FA;
+    };
+    // One checked point: each lane evaluates, per quartet, only the branch its
+    // point falls in -- the P = Q polynomial, the small-x series (both times
+    // the Gaussian g), or the lean form -- and advances the rotation and g.
+    auto cpoint = [&](const int m) -> double {
+      const double2 qq = qs[m];
+      const double q = qq.x, iq = qq.y;
+      const long long qb = __double_as_longlong(q);
+      double tot = 0.0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        double v;
+        if (p0n[k] >= 0) {
+          v = p0_poly(hm[k], p0n[k], q * q) * g[k];
+        } else if (qb < qcb[k]) {
+          const double x = q * H[k];
+          v = bessel_small<LB>(hm[k], x * x) * g[k];
+          if (J2) v *= iq * iq;
+        } else {
+          if constexpr (POLY) {
+            const double y = q * q;
+            double ae = pa[k][NA - 1], bo = pb[k][NB - 1];
+#pragma unroll
+            for (int t = NA - 2; t >= 0; --t) ae = fma(ae, y, pa[k][t]);
+#pragma unroll
+            for (int t = NB - 2; t >= 0; --t) bo = fma(bo, y, pb[k][t]);
+            v = fma(q, bo * C[k], ae * S[k]) * (J2 ? iq * iq * iq : iq);
+          } else {
+            v = bessel_up<LB>(hh[k], q * H[k], S[k], C[k], iq * invH[k]);
+            if (J2) v *= iq * iq;
+          }
+        }
+        tot += v;
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double s2 = fma(S[k], wr[k], C[k] * wi[k]);
+        C[k] = fma(C[k], wr[k], -S[k] * wi[k]);
+        S[k] = s2;
+        wr[k] *= kk[k];
+        wi[k] *= kk[k];
+        g[k] *= rg[k];
+        rg[k] *= kk[k];
+      }
+      return tot;
     };
     auto seed = [&](const int m, auto checked) {
       const double q = qs[m].x;
@@ -437,27 +462,37 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
     // Seeds (direct sincos / exp) at the chunk start and every RESEED points
     // after it, all on block boundaries; on a non-uniform tile at every
     // point, and when q[0] lies off the grid (the drivers' 1e-10) again at
-    // point 1.  The checked blocks come first (mse bounds a prefix); the rest
-    // take the lean path, without the Gaussian g.
+    // point 1.  The checked points come first, one at a time with a butterfly
+    // sum each (mse bounds a prefix; the whole chunk on a non-uniform tile),
+    // rounded up to a block boundary; the rest take the lean path in blocks
+    // of QB points, without the Gaussian g, point 0 with the checked branches.
     const bool every = !A.uniform;
     const bool off0 = m0 == 0 && !A.first_on_grid;
-    int mb = m0;
-    for (; mb < m1 && (mb < mse || every || (off0 && mb == 0)); mb += QB) {
-      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb, BoolTag<true>());
-      double Fv[QB];
+    int mce = every ? m1 : max(mse, m0);
+    mce = min(m1, m0 + (max(mce - m0, 0) + QB - 1) / QB * QB);
+#pragma unroll 1
+    for (int m = m0; m < mce; ++m) {
+      if (every || ((m - m0) & (RESEED - 1)) == 0 || (off0 && m == 1)) seed(m, BoolTag<true>());
+      double t = cpoint(m);
 #pragma unroll
-      for (int j = 0; j < QB; ++j) {
-        const int m = mb + j;
-        if (every ? (j > 0 || ((mb - m0) & (RESEED - 1)) != 0) : (off0 && m == 1)) seed(m, BoolTag<true>());
-        Fv[j] = point(m, BoolTag<true>());
-      }
-      reduce(Fv, mb);
+      for (int bit = 16; bit >= 1; bit >>= 1) t += __shfl_xor_sync(0xffffffffu, t, bit);
+      if (lane == 0) acc[m] += t;
     }
-    for (; mb < m1; mb += QB) {
-      if (((mb - m0) & (RESEED - 1)) == 0) seed(mb, BoolTag<false>());
+    for (int mb = mce; mb < m1; mb += QB) {
       double Fv[QB];
+      if (mb == 0) {
+        // point 0 with the checked points' branches, then the lean
+        // recurrence (reseeded at point 1 when point 0 lies off the grid)
+        seed(0, BoolTag<true>());
+        Fv[0] = cpoint(0);
+        if (off0) seed(1, BoolTag<false>());
 #pragma unroll
-      for (int j = 0; j < QB; ++j) Fv[j] = point(mb + j, BoolTag<false>());
+        for (int j = 1; j < QB; ++j) Fv[j] = point(j);
+      } else {
+        if (((mb - m0) & (RESEED - 1)) == 0) seed(mb, BoolTag<false>());
+#pragma unroll
+        for (int j = 0; j < QB; ++j) Fv[j] = point(mb + j);
+      }
       reduce(Fv, mb);
     }
   }
