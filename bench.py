@@ -337,6 +337,7 @@ def fit6_section(ngeom_total, nplain_max, gmax):
             gbuf[b * G:(b + 1) * G] = pl.vjp_batch(2 * (Ib - iref))
         torch.cuda.synchronize()
         t_batch = (time.perf_counter() - t0) / ng
+        stages = fit6_stage_table(pl, xyz, iref, pad, G, min(nplain, 8))
         # spot check: the batched answer of the last geometry against the plain path
         pl.set_batch(1)
         pl.set_centres(*xyz[ng - 1].T)
@@ -356,8 +357,60 @@ def fit6_section(ngeom_total, nplain_max, gmax):
         "quartet_q_per_s_forward_and_adjoint": nquart * p.nq / t_batch,
         "check_vs_plain": {"I_rel": err_i, "grad_rel": err_g},
         "path": "host arrays in and out per batch (set_centres_batch, execute_batch, vjp_batch)",
+        "per_stage_ms_per_geometry": stages,
     }
     return line
+
+
+def fit6_stage_table(pl, xyz, iref, pad, G, nplain):
+    """Per-geometry device time by stage, plain (one geometry per call) and
+    batched (G per call, without CUDA graphs so that the stage events are
+    recorded): the forward stages from the plan's stage events, and the
+    forward and the adjoint call each timed with a synchronize on both sides
+    (host copies included)."""
+    import torch
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    pl.use_graph(False)
+    pl.set_batch(1)
+    pl.stage_totals()
+    tf = tv = 0.0
+    for k in range(nplain):
+        pl.set_centres(*xyz[k].T)
+        Ik, dt = timed(pl.execute)
+        tf += dt
+        _, dt = timed(lambda: pl.vjp(2 * (Ik - iref)))
+        tv += dt
+    st = pl.stage_totals()
+    plain = {k: st[k] / max(st["executions"], 1) for k in ("pair_tables", "stage1", "stage2", "reduce")}
+    plain.update(forward_call=1e3 * tf / nplain, adjoint_call=1e3 * tv / nplain)
+    pl.set_batch(G)
+    pl.set_centres_batch(pad[:G])
+    Ib = pl.execute_batch()
+    pl.vjp_batch(2 * (Ib - iref))
+    pl.stage_totals()
+    tf = tv = 0.0
+    nb = min(2, len(pad) // G)
+    for b in range(nb):
+        pl.set_centres_batch(pad[b * G:(b + 1) * G])
+        Ib, dt = timed(pl.execute_batch)
+        tf += dt
+        _, dt = timed(lambda: pl.vjp_batch(2 * (Ib - iref)))
+        tv += dt
+    st = pl.stage_totals()
+    ng = nb * G
+    batched = {k: st[k] / max(st["executions"], 1) / G for k in ("pair_tables", "stage1", "stage2", "reduce")}
+    batched.update(forward_call=1e3 * tf / ng, adjoint_call=1e3 * tv / ng)
+    pl.use_graph(True)
+    return {"plain": plain, "batched_no_graph": batched,
+            "what": "ms per geometry; pair_tables / stage1 / stage2 / reduce from the plan's stage events "
+                    "(device), forward_call / adjoint_call wall time of one call with host copies"}
 
 
 def run_batch4(args):

@@ -27,7 +27,6 @@ extern "C" {
 #define THISTLE_ERR_NOMEM -6      /* device allocation failed */
 #define THISTLE_ERR_TYPE -7       /* calculation type not provided */
 #define THISTLE_ERR_Q -8          /* q <= 0 (the reference divides by q; drivers use 1e-10 for 0) */
-#define THISTLE_ERR_TIMEOUT -10   /* a bounded device wait gave up */
 
 /* Measured FP64 FMA throughput of the current device in TFLOP/s (a
  * register-resident chain kernel, best of `reps`); the roofline denominator. */

@@ -17,7 +17,6 @@ LIB_PATH = os.environ.get("THISTLE_B200_LIB") or os.path.join(_HERE, "libthistle
 ERRORS = {
     -1: "THISTLE_ERR_ARG", -2: "THISTLE_ERR_SHAPE", -3: "THISTLE_ERR_ANGMOM", -4: "THISTLE_ERR_NONFINITE",
     -5: "THISTLE_ERR_CUDA", -6: "THISTLE_ERR_NOMEM", -7: "THISTLE_ERR_TYPE", -8: "THISTLE_ERR_Q",
-    -10: "THISTLE_ERR_TIMEOUT",
 }
 
 # every symbol include/thistle_b200.h declares
