@@ -309,7 +309,7 @@ __global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, i
 // ---------------------------------------------------------------------------
 
 // Ghat[x][y][z][w] = sum of Gamma_t/8 over the eight index placements of
-// every row (both orders inside each pair, both pair orders); see tb_plan.cu.
+// every row (both orders inside each pair, both pair orders); see tb_density.cu.
 // Deterministic in two steps: every (row, placement) emits (flat index,
 // value); after a stable sort by index each run of equal indices is summed
 // in its sorted (row, placement) order by the run's first element.

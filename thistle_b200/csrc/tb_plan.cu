@@ -9,169 +9,26 @@
 //   pair centres, E12, MD tables  src/Variables.f90:1113-1148
 //   the five quartet loops        src/Integrals.f90:79-468 (bra pair i<=j, ket pair k<=r)
 //   per-quartet kernels           src/Integrals.f90:4955-5226 and variants
-#include <cuda_runtime.h>
-#include <cub/device/device_radix_sort.cuh>
-
-#include <algorithm>
-#include <array>
-#include <chrono>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <string>
-#include <vector>
-
-#include "tb_kernels.h"
-#include "tb_math.cuh"
-#include "thistle_b200.h"
+#include "tb_plan_internal.h"
 
 using namespace tb;
 
-static thread_local std::string g_err;
-
-// THISTLE_B200_TRACE=1 prints the host-side duration of the set-up phases to stderr.
-struct PhaseTrace {
-  bool on = std::getenv("THISTLE_B200_TRACE") != nullptr;
-  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
-  void mark(const char *what) {
-    if (!on) return;
-    auto t1 = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "[thistle_b200] %-28s %9.3f ms\n", what,
-                 std::chrono::duration<double, std::milli>(t1 - t0).count());
-    t0 = t1;
-  }
-};
-
-static int fail(int code, const std::string &msg) {
-  g_err = msg;
-  return code;
-}
+thread_local std::string g_err;
 
 namespace tb {
 int set_error(int code, const std::string &msg) { return fail(code, msg); }
 }  // namespace tb
 
-#define TB_CK(x)                                                                            \
-  do {                                                                                      \
-    cudaError_t e_ = (x);                                                                   \
-    if (e_ != cudaSuccess) return fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-// Device buffers come from the process-wide cache (tb_pool.cu).
-template <class T>
-static int dalloc(T **p, size_t n, const char *what) {
-  *p = nullptr;
-  if (n == 0) n = 1;
-  void *v = nullptr;
-  cudaError_t e = pool_malloc(&v, n * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(e == cudaErrorMemoryAllocation ? THISTLE_ERR_NOMEM : THISTLE_ERR_CUDA,
-                std::string("cudaMalloc of ") + what + " (" + std::to_string(n * sizeof(T)) + " bytes): " +
-                    cudaGetErrorString(e));
-  }
-  *p = (T *)v;
-  return THISTLE_OK;
-}
-template <class T>
-static void dfree(T *&p) {
-  if (p) pool_free((void *)p);
-  p = nullptr;
-}
-
-// Quartets of one LLmax class with equal (LK, XB) (see quartet_key).
-struct SubRange {
-  int LK, XB;
-  int64_t begin, end;
-  int nout = 0;  // most function pairs of an outer (convolved) side; 0: unknown
-};
-
-// quartets of one shell tuple ((Li 5 + Lj) 5 + Lk) 5 + Lr within a class
-struct TupleRange {
-  int tuple;
-  int64_t begin, end;
-};
-
-struct thistle_plan {
-  int type = 0, kind = 0;
-  int ngto = 0, ng = 0, nmo = 0, nmo1 = 0, nzao = 1, nq = 0, maxa = 0, nmat = 0;
-  int shells_canonical = 1;  // s, p, d, f groups: complete shells in cart_component order
-  double cutoffz = 0, cutoffmd = 0, cutoffcentre = 0;
-  std::vector<int> gstart, gcount, gL, flmn;
-  std::vector<double> hq;            // host copy of the q grid (aligned: interleaved q vectors)
-  int qdim = 1;                      // 3 for aligned plans (q vectors)
-  int64_t nquart = 0, np = 0;
-  int ncls = 0;
-  int cls_L[MAXCLS];
-  int64_t cls_begin[MAXCLS], cls_end[MAXCLS], cls_recoff[MAXCLS];
-  int cls_rs[MAXCLS];
-  std::vector<SubRange> cls_sub[MAXCLS];
-  std::vector<TupleRange> cls_tup[MAXCLS];
-  double *d_xbuf = nullptr;  // contraction output of the split contracted-side stage 1
-  int64_t xbuf_len = 0;
-  int64_t rec_total = 0;
-  int *d_gstart = nullptr, *d_gcount = nullptr, *d_flmn = nullptr;
-  double *d_ga = nullptr, *d_xyz = nullptr, *d_q = nullptr, *d_pairtab = nullptr, *d_esoa = nullptr;
-  double *d_rho = nullptr, *d_zao = nullptr, *d_rec = nullptr, *d_partial = nullptr, *d_result = nullptr;
-  uint64_t *d_quart = nullptr;
-  // device-resident density inputs and transform workspaces
-  int *d_mat = nullptr;
-  double *d_C = nullptr, *d_tot = nullptr, *d_D = nullptr, *d_Ds = nullptr, *d_Y = nullptr;
-  double *d_G = nullptr, *d_T1 = nullptr, *d_V = nullptr, *d_T3 = nullptr, *d_Ct = nullptr;
-  // Ghat build: (index, value) per row placement, sorted by index
-  int *d_gk0 = nullptr, *d_gk1 = nullptr;
-  double *d_gv0 = nullptr, *d_gv1 = nullptr;
-  void *d_gsort_tmp = nullptr;
-  size_t gsort_bytes = 0;
-  int gbits = 0;
-  // grouped GEMM of the transform's last pass (one group per b)
-  // quartet enumeration workspaces
-  int64_t *d_braoff = nullptr;
-  int *d_gL = nullptr;
-  uint32_t *d_k0 = nullptr, *d_k1 = nullptr;
-  uint64_t *d_v0 = nullptr;
-  void *d_sort_tmp = nullptr;
-  size_t sort_tmp_bytes = 0;
-  int64_t *d_p0count = nullptr;      // P=Q quartets per class in the last execution
-  // stage-2 visiting order: keys written by stage 1, sorted with the quartet index
-  uint32_t *d_s2key = nullptr, *d_s2key_sorted = nullptr, *d_iota = nullptr, *d_perm = nullptr;
-  void *d_s2sort_tmp = nullptr;
-  size_t s2sort_bytes = 0;
-  int nsm = 0, s2_rows = 0, s2_qtile = 0;
-  int s2_bps[LMAXB + 1];             // resident stage-2 blocks per SM, per Bessel order
-  cudaStream_t st = nullptr;
-  bool own_stream = true;
-  cudaEvent_t ev[10];
-  // per-execution stage events: slot = execution index mod NRING
-  static const int NRING = 64;
-  cudaEvent_t rev[64][5];
-  int64_t ring_next = 0, ring_base = 0;
-  bool have_ev = false;
-  float ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int64_t launches = 0;              // own kernels launched by the last call
-  // geometry batches: ngeom copies of the centres, tables, records and results
-  int ngeom = 1;
-  bool capturing = false;            // inside a CUDA-graph capture (no event records)
-  bool use_graph = false;
-  cudaGraphExec_t gx_fwd = nullptr, gx_vjp = nullptr;
-  std::vector<double> hxyz;          // host copy of the centres (interleaved, ngeom x ngto x 3)
-  bool fwd_valid = false;            // records and visiting order match the current centres
-  // adjoint workspaces (allocated by the first vector-Jacobian product)
-  double *d_dsoa = nullptr, *d_adj = nullptr, *d_gpart = nullptr, *d_v = nullptr, *d_grad = nullptr;
-  int adj_rows = 0;
-};
-
 // ---------------------------------------------------------------------------
 // validation
 // ---------------------------------------------------------------------------
-static bool finite_all(const double *a, int64_t n) {
+bool finite_all(const double *a, int64_t n) {
   for (int64_t i = 0; i < n; ++i)
     if (!std::isfinite(a[i])) return false;
   return true;
 }
 
-static int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const int32_t *l, const int32_t *m,
+int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const int32_t *l, const int32_t *m,
                        const int32_t *n, const double *xx, const double *yy, const double *zz,
                        const int32_t *group) {
   if (ngto <= 0) return fail(THISTLE_ERR_ARG, "ngto must be positive");
@@ -227,7 +84,7 @@ static int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const in
   return THISTLE_OK;
 }
 
-static int check_q(const double *q, int32_t nq) {
+int check_q(const double *q, int32_t nq) {
   if (!q || nq <= 0) return fail(THISTLE_ERR_ARG, "empty q grid");
   for (int i = 0; i < nq; ++i) {
     if (!std::isfinite(q[i])) return fail(THISTLE_ERR_NONFINITE, "non-finite q");
@@ -240,7 +97,7 @@ static int check_q(const double *q, int32_t nq) {
 // ---------------------------------------------------------------------------
 // quartet classes
 // ---------------------------------------------------------------------------
-static int64_t bra_count(int i, int j, int ng, bool all_pairs) {
+int64_t bra_count(int i, int j, int ng, bool all_pairs) {
   if (all_pairs) return npairs(ng);  // resolved CMS: every ket pair
   if (i < j) return (int64_t)(ng - i) * (ng - i - 1) / 2;
   return (int64_t)ng * (ng - 1) / 2 + (ng - i);
@@ -251,7 +108,7 @@ static inline int class_key(int Li, int Lj, int Lk, int Lr) {
 }
 
 // Quartet counts per class key, without enumerating quartets.
-static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt, bool all_pairs) {
+void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt, bool all_pairs) {
   int ng = (int)gL.size();
   cnt.assign(17 * 625, 0);
   if (all_pairs) {
@@ -288,7 +145,7 @@ static void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt, 
 }
 
 // Sorted-by-key layout -> contiguous LLmax classes and record offsets.
-static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
+int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
   int64_t pos = 0, recoff = 0;
   P->ncls = 0;
   int maxg[5] = {0, 0, 0, 0, 0};  // most functions of a group, per shell L
@@ -338,161 +195,11 @@ static int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int k
 }
 
 // ---------------------------------------------------------------------------
-// density transform on the device
-// ---------------------------------------------------------------------------
-// rho(ab,cd) = 1/8 sum_t G_t [S12_t(ab) S34_t(cd) + S34_t(ab) S12_t(cd)],
-// S12_t(ab) = C_{m1 a} C_{m2 b} + C_{m1 b} C_{m2 a}: the ztot of
-// src/Integrals.f90:5163 for every pair of primitive pairs.  With
-// Ghat[x][y][z][w] = G_t/8 summed over the eight placements of each row this
-// is the 4-index transform rho = sum Ghat C_x,a C_y,b C_z,c C_w,d, run as
-// four DGEMM passes: m4 -> d, m3 -> c (pack c<=d), m2 -> b, m1 -> a (a<=b).
-
-#define TB_TRY(x)                    \
-  do {                               \
-    rc = (x);                        \
-    if (rc != THISTLE_OK) goto done; \
-  } while (0)
-#define TB_TRYC(x)                                                                                        \
-  do {                                                                                                    \
-    cudaError_t e_ = (x);                                                                                 \
-    if (e_ != cudaSuccess) {                                                                              \
-      rc = fail(THISTLE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                       \
-      goto done;                                                                                          \
-    }                                                                                                     \
-  } while (0)
-
-static int density_alloc(thistle_plan *P) {
-  int rc = THISTLE_OK;
-  const int n = P->nmo, ngto = P->ngto;
-  const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
-  TB_TRY(dalloc(&P->d_C, (size_t)n * ngto, "MO coefficients"));
-  if (kind_elastic(P->kind)) {
-    const size_t nz = (size_t)P->nzao;
-    TB_TRY(dalloc(&P->d_zao, nz * ngto * ngto, "AO density"));
-    TB_TRY(dalloc(&P->d_D, nz * P->nmo1 * P->nmo1, "1-RDM"));
-    TB_TRY(dalloc(&P->d_Ds, nz * P->nmo1 * P->nmo1, "1-RDM"));
-    TB_TRY(dalloc(&P->d_Y, nz * P->nmo1 * ngto, "1-RDM x C"));
-    TB_TRY(dalloc(&P->d_Ct, (size_t)n * transform_ct_width(ngto), "transform C^T"));
-  } else {
-    TB_TRY(dalloc(&P->d_rho, (size_t)(np * np), "pair density"));
-    TB_TRY(dalloc(&P->d_mat, (size_t)P->nmat * 4, "2-RDM indices"));
-    TB_TRY(dalloc(&P->d_tot, (size_t)P->nmat, "2-RDM values"));
-    TB_TRY(dalloc(&P->d_G, (size_t)n4, "Ghat"));
-    TB_TRY(dalloc(&P->d_T1, (size_t)(n3 * ngto), "transform T1"));
-    TB_TRY(dalloc(&P->d_V, (size_t)(n2 * np), "transform V"));
-    TB_TRY(dalloc(&P->d_T3, (size_t)((int64_t)n * ngto * np), "transform T3"));
-    TB_TRY(dalloc(&P->d_Ct, (size_t)n * transform_ct_width(ngto), "transform C^T"));
-    const int64_t m = std::max<int64_t>(8 * (int64_t)P->nmat, 1);
-    TB_TRY(dalloc(&P->d_gk0, (size_t)m, "Ghat keys"));
-    TB_TRY(dalloc(&P->d_gk1, (size_t)m, "Ghat keys"));
-    TB_TRY(dalloc(&P->d_gv0, (size_t)m, "Ghat values"));
-    TB_TRY(dalloc(&P->d_gv1, (size_t)m, "Ghat values"));
-    P->gbits = 1;
-    while (P->gbits < 31 && ((int64_t)1 << P->gbits) < n4) ++P->gbits;
-    TB_TRYC(cub::DeviceRadixSort::SortPairs(nullptr, P->gsort_bytes, P->d_gk0, P->d_gk1, P->d_gv0, P->d_gv1,
-                                            (int)m, 0, P->gbits, P->st));
-    TB_TRY(dalloc((char **)&P->d_gsort_tmp, P->gsort_bytes, "Ghat sort scratch"));
-  }
-done:
-  return rc;
-}
-
-static int density_upload(thistle_plan *P, const double *mmod, const int32_t *mat, const double *total,
-                          const double *onerdm) {
-  TB_CK(cudaMemcpyAsync(P->d_C, mmod, sizeof(double) * (size_t)P->nmo * P->ngto, cudaMemcpyHostToDevice, P->st));
-  if (kind_elastic(P->kind)) {
-    TB_CK(cudaMemcpyAsync(P->d_D, onerdm, sizeof(double) * (size_t)P->nzao * P->nmo1 * P->nmo1,
-                          cudaMemcpyHostToDevice, P->st));
-  } else if (P->nmat > 0) {
-    TB_CK(cudaMemcpyAsync(P->d_mat, mat, sizeof(int) * (size_t)P->nmat * 4, cudaMemcpyHostToDevice, P->st));
-    TB_CK(cudaMemcpyAsync(P->d_tot, total, sizeof(double) * (size_t)P->nmat, cudaMemcpyHostToDevice, P->st));
-  }
-  return THISTLE_OK;
-}
-
-// Pair density (total, j2) or AO density (elastic) from the device-resident
-// inputs, every GEMM pass on the FP64 tensor cores (tb_transform.cu).
-static int density_run(thistle_plan *P) {
-  int rc = THISTLE_OK;
-  const int n = P->nmo, ngto = P->ngto, cw = transform_ct_width(ngto);
-  const int64_t np = P->np, n2 = (int64_t)n * n, n3 = n2 * n, n4 = n3 * n;
-  TB_TRYC(launch_transform_ct(P->d_C, n, ngto, P->d_Ct, P->st));
-  P->launches += 1;
-  if (kind_elastic(P->kind)) {
-    // Z = C1^T sym(D) C1 (variables_elastic, src/Variables.f90:1199-1217),
-    // C1 the first nmo1 MOs: Y(i, a) = sum_j Ds(i, j) C(j, a), then
-    // Z(a, b) = sum_i C(i, a) Y(i, b)
-    // (the resolved CMS: the same for each of its two 1-RDMs)
-    const int k = P->nmo1;
-    for (int z = 0; z < P->nzao; ++z) {
-      const int64_t dk = (int64_t)z * k * k;
-      TB_TRYC(launch_sym_small(P->d_D + dk, k, P->d_Ds + dk, P->st));
-      DmmaGemmArgs g{};
-      g.A = P->d_Ds + dk; g.sak = k; g.a_batch = 0;
-      g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
-      g.M = k; g.N = ngto; g.K = k;
-      g.D = P->d_Y + (int64_t)z * k * ngto; g.sdm = 1; g.sdj = k; g.d_batch = 0;
-      TB_TRYC(launch_dmma_gemm(g, 0, true, 1, P->st));
-      g.A = P->d_Ct; g.sak = cw;
-      g.B = P->d_Y + (int64_t)z * k * ngto; g.sbk = 1; g.sbj = k;
-      g.M = ngto; g.N = ngto; g.K = k;
-      g.D = P->d_zao + (int64_t)z * ngto * ngto; g.sdm = 1; g.sdj = ngto;
-      TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
-      P->launches += 3;
-    }
-    goto done;
-  }
-  if (P->nmat == 0) {
-    // otherwise the last pass writes every element
-    TB_TRYC(cudaMemsetAsync(P->d_rho, 0, sizeof(double) * (size_t)(np * np), P->st));
-    goto done;
-  }
-  TB_TRYC(cudaMemsetAsync(P->d_G, 0, sizeof(double) * (size_t)n4, P->st));
-  {
-    const int64_t m = 8 * (int64_t)P->nmat;
-    size_t bytes = P->gsort_bytes;
-    TB_TRYC(launch_ghat_emit(P->d_mat, P->d_tot, P->nmat, n, P->d_gk0, P->d_gv0, P->st));
-    TB_TRYC(cub::DeviceRadixSort::SortPairs(P->d_gsort_tmp, bytes, P->d_gk0, P->d_gk1, P->d_gv0, P->d_gv1, (int)m,
-                                            0, P->gbits, P->st));
-    TB_TRYC(launch_ghat_runs(P->d_gk1, P->d_gv1, m, P->d_G, P->st));
-    P->launches += 3;
-  }
-  {
-    DmmaGemmArgs g{};
-    // T1[xyz](a) = sum_w C(w, a) Ghat[x][y][z][w]: (ngto x n^3), leading dimension ngto
-    g.A = P->d_Ct; g.sak = cw; g.a_batch = 0;
-    g.B = P->d_G; g.sbk = 1; g.sbj = n;
-    g.M = ngto; g.N = (int)n3; g.K = n;
-    g.D = P->d_T1; g.sdm = 1; g.sdj = ngto; g.d_batch = 0;
-    TB_TRYC(launch_dmma_gemm(g, 0, false, 1, P->st));
-    // V[xy](fpair(c, d)) = sum_z T1[xyz](d) C(z, c) for c <= d, one batch per xy
-    g.A = P->d_T1; g.sak = ngto; g.a_batch = (int64_t)n * ngto;
-    g.B = P->d_Ct; g.sbk = cw; g.sbj = 1;
-    g.M = ngto; g.N = ngto; g.K = n;
-    g.D = P->d_V; g.sdm = 0; g.sdj = 0; g.d_batch = np;
-    TB_TRYC(launch_dmma_gemm(g, 1, true, (int)n2, P->st));
-    // T3[x](p, b) = sum_y V[xy](p) C(y, b), one batch per x
-    g.A = P->d_V; g.sak = np; g.a_batch = (int64_t)n * np;
-    g.M = (int)np; g.N = ngto; g.K = n;
-    g.D = P->d_T3; g.sdm = 1; g.sdj = np; g.d_batch = (int64_t)ngto * np;
-    TB_TRYC(launch_dmma_gemm(g, 0, true, n, P->st));
-    // rho(p, fpair(a, b)) = sum_x T3[x](p, b) C(x, a) for a <= b, one batch per b
-    g.A = P->d_T3; g.sak = (int64_t)ngto * np; g.a_batch = np;
-    g.M = (int)np; g.N = ngto; g.K = n;
-    g.D = P->d_rho; g.sdm = 1; g.sdj = np; g.d_batch = 0;
-    TB_TRYC(launch_dmma_gemm(g, 2, true, ngto, P->st));
-    P->launches += 4;
-  }
-done:
-  return rc;
-}
-
-// ---------------------------------------------------------------------------
 // quartets on the device: enumerate in bra-pair order, then a stable radix
 // sort on the class key so that each LLmax class is contiguous and each warp
 // of stage 1 sees quartets with identical loop bounds.
 // ---------------------------------------------------------------------------
-static int quartets_alloc(thistle_plan *P) {
+int quartets_alloc(thistle_plan *P) {
   const int ng = P->ng, nb = npairs(ng);
   std::vector<int64_t> off(nb + 1);
   int64_t acc = 0;
@@ -520,7 +227,7 @@ done:
   return rc;
 }
 
-static int quartets_run(thistle_plan *P) {
+int quartets_run(thistle_plan *P) {
   int rc = THISTLE_OK;
   TB_TRYC(launch_quartet_fill(P->ng, P->d_braoff, P->nquart, P->d_gL, P->d_v0, P->d_k0, P->kind == KIND_CMS,
                               P->st));
@@ -534,7 +241,7 @@ done:
 // ---------------------------------------------------------------------------
 // plan lifecycle
 // ---------------------------------------------------------------------------
-static void plan_free(thistle_plan *P) {
+void plan_free(thistle_plan *P) {
   if (!P) return;
   dfree(P->d_gstart); dfree(P->d_gcount); dfree(P->d_flmn); dfree(P->d_ga); dfree(P->d_xyz);
   dfree(P->d_q); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rho); dfree(P->d_zao); dfree(P->d_rec);
@@ -559,11 +266,11 @@ static void plan_free(thistle_plan *P) {
   delete P;
 }
 
-static int64_t gs_pair(const thistle_plan *P) { return (int64_t)npairs(P->ng) * PAIR_STRIDE; }
-static int64_t gs_esoa(const thistle_plan *P) { return esoa_doubles(P->ng, P->maxa); }
-static int64_t gs_rec(const thistle_plan *P) { return std::max<int64_t>(P->rec_total, 1); }
+int64_t gs_pair(const thistle_plan *P) { return (int64_t)npairs(P->ng) * PAIR_STRIDE; }
+int64_t gs_esoa(const thistle_plan *P) { return esoa_doubles(P->ng, P->maxa); }
+int64_t gs_rec(const thistle_plan *P) { return std::max<int64_t>(P->rec_total, 1); }
 
-static void drop_graphs(thistle_plan *P) {
+void drop_graphs(thistle_plan *P) {
   if (P->gx_fwd) cudaGraphExecDestroy(P->gx_fwd);
   if (P->gx_vjp) cudaGraphExecDestroy(P->gx_vjp);
   P->gx_fwd = P->gx_vjp = nullptr;
@@ -571,7 +278,7 @@ static void drop_graphs(thistle_plan *P) {
 
 // (Re)allocates the per-geometry buffers for G geometries (the adjoint's on
 // its next use); the partial-row count s2_rows must be set.
-static int geo_alloc(thistle_plan *P, int G) {
+int geo_alloc(thistle_plan *P, int G) {
   int rc = THISTLE_OK;
   drop_graphs(P);
   dfree(P->d_xyz); dfree(P->d_pairtab); dfree(P->d_esoa); dfree(P->d_rec); dfree(P->d_partial);
@@ -590,7 +297,7 @@ done:
   return rc;
 }
 
-static int upload_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
+int upload_centres(thistle_plan *P, const double *xx, const double *yy, const double *zz) {
   std::vector<double> xyz((size_t)P->ngto * 3);
   for (int i = 0; i < P->ngto; ++i) {
     xyz[3 * i] = xx[i];
@@ -609,7 +316,7 @@ static int upload_centres(thistle_plan *P, const double *xx, const double *yy, c
 }
 
 // All geometries of a batch from one host array (ngeom x ngto x 3, interleaved).
-static int upload_centres_batch(thistle_plan *P, const double *xyz) {
+int upload_centres_batch(thistle_plan *P, const double *xyz) {
   const size_t n = (size_t)P->ngeom * 3 * P->ngto;
   if (P->hxyz.size() == n && std::equal(xyz, xyz + n, P->hxyz.begin())) return THISTLE_OK;
   TB_CK(cudaMemcpyAsync(P->d_xyz, xyz, sizeof(double) * n, cudaMemcpyHostToDevice, P->st));
@@ -619,7 +326,7 @@ static int upload_centres_batch(thistle_plan *P, const double *xyz) {
   return THISTLE_OK;
 }
 
-static int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga, const int32_t *l,
+int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga, const int32_t *l,
                        const int32_t *m, const int32_t *n, const double *xx, const double *yy, const double *zz,
                        const int32_t *group, const double *mmod, int32_t norbs, const int32_t *mat,
                        const double *total, int32_t nmat, const double *onerdm, int32_t nmo1, const double *q,
@@ -789,7 +496,7 @@ done:
 // A tile q[0..n) is "uniform" when q[1..n) is an arithmetic progression to
 // within 2e-14 of its largest value; q[0] may sit off it (the drivers put
 // 1e-10 where the grid starts at 0).
-static void grid_info(const double *q, int n, int &uniform, int &first_on_grid, double &dq) {
+void grid_info(const double *q, int n, int &uniform, int &first_on_grid, double &dq) {
   uniform = 0;
   first_on_grid = 0;
   dq = 0.0;
@@ -806,7 +513,7 @@ static void grid_info(const double *q, int n, int &uniform, int &first_on_grid, 
 // Pair tables, stage 1 per class, the stage-2 visiting order (when `order`),
 // stage 2 per class and q tile, and the fixed-order reduction into d_out.
 // Stage-1 arguments of one class of a quartet list.
-static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t qbegin, int64_t qend,
+Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t qbegin, int64_t qend,
                               double *d_rec, int64_t recbase, int rs) {
   Stage1Args a;
   a.quartets = d_quart;
@@ -845,7 +552,7 @@ static Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, in
   return a;
 }
 
-static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
+int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
                       const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom,
                       const std::vector<TupleRange> *tups) {
@@ -971,14 +678,14 @@ static int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *c
   return THISTLE_OK;
 }
 
-static int plan_exec(thistle_plan *P, double *d_out) {
+int plan_exec(thistle_plan *P, double *d_out) {
   int rc = run_stages(P, P->d_quart, P->cls_begin, P->cls_end, P->cls_L, P->ncls, P->d_rec, P->cls_recoff,
                       P->cls_rs, P->cls_sub, d_out, true, P->ngeom, P->cls_tup);
   P->fwd_valid = rc == THISTLE_OK;
   return rc;
 }
 
-static void read_timings(thistle_plan *P) {
+void read_timings(thistle_plan *P) {
   if (P->ring_next == 0) return;
   cudaEvent_t *E = P->rev[(P->ring_next - 1) % thistle_plan::NRING];
   for (int i = 0; i < 4; ++i) {
@@ -991,14 +698,14 @@ static void read_timings(thistle_plan *P) {
 // grad[g][3 c + axis] = sum_q v[g](q) dI_g(q)/dA_c for every geometry g of the
 // batch (tb_adjoint.cu).  The forward records must be those of the current
 // centres (adjoint_ready runs the forward stages otherwise).
-static int adjoint_check(thistle_plan *P) {
+int adjoint_check(thistle_plan *P) {
   if (P->kind != KIND_TOTAL) return fail(THISTLE_ERR_TYPE, "the adjoint is provided for total j0 (type 1)");
   for (int c = 0; c < P->ncls; ++c)
     if (P->cls_L[c] > 8) return fail(THISTLE_ERR_ANGMOM, "the adjoint covers LLmax <= 8 (s, p, d shells)");
   return THISTLE_OK;
 }
 
-static int adjoint_alloc(thistle_plan *P) {
+int adjoint_alloc(thistle_plan *P) {
   int rc = THISTLE_OK;
   const int G = P->ngeom;
   if (!P->d_dsoa) {
@@ -1018,7 +725,7 @@ done:
 }
 
 // The adjoint stages proper (no allocation, no synchronisation: capturable).
-static int adjoint_stages(thistle_plan *P, const double *d_v, double *d_grad) {
+int adjoint_stages(thistle_plan *P, const double *d_v, double *d_grad) {
   int rc = THISTLE_OK;
   const int G = P->ngeom;
   const int64_t gs_dsoa = dsoa_doubles(P->ng, P->maxa), gs_gpart = (int64_t)P->adj_rows * 3 * P->ng;
@@ -1077,7 +784,7 @@ done:
 }
 
 // Forward stages of the batch into d_result, through the captured graph when enabled.
-static int forward_batch(thistle_plan *P) {
+int forward_batch(thistle_plan *P) {
   if (!P->use_graph) return plan_exec(P, P->d_result);
   if (!P->gx_fwd) {
     // capture once (all buffers exist); replays use the same pointers
@@ -1102,7 +809,7 @@ static int forward_batch(thistle_plan *P) {
   return THISTLE_OK;
 }
 
-static int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
+int plan_vjp(thistle_plan *P, const double *d_v, double *d_grad) {
   int rc = adjoint_check(P);
   if (rc != THISTLE_OK) return rc;
   TB_TRY(adjoint_alloc(P));
@@ -1133,564 +840,9 @@ done:
 }
 
 // ---------------------------------------------------------------------------
-// nuclear-electron term of electron scattering (types 5, 6): elastic plans
-// ---------------------------------------------------------------------------
-// Ine(q) = sum_a sum_(i,k) Zn_a F_ik(q) e12(q, i, k) over the nuclei and the
-// ordered group pairs (nuclei_electron_integration, src/Integrals.f90:2493-2596),
-// for the plan's current centres; geom is (natoms, 3) column-major.
-static int nuclear_term(thistle_plan *P, const double *Zn, const double *geom, int natoms, double *host_out) {
-  if (P->kind != KIND_ELASTIC) return fail(THISTLE_ERR_TYPE, "the nuclear term needs an elastic plan (the 1-RDM)");
-  if (!Zn || !geom || natoms < 1) return fail(THISTLE_ERR_ARG, "nuclear charges and positions are required");
-  if (natoms >= (1 << 16)) return fail(THISTLE_ERR_SHAPE, "at most 65535 nuclei");
-  if (!finite_all(Zn, natoms) || !finite_all(geom, 3 * (int64_t)natoms))
-    return fail(THISTLE_ERR_NONFINITE, "non-finite nuclear charge or position");
-  if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "the nuclear term is computed for single-geometry plans");
-  int rc = THISTLE_OK;
-  uint64_t *d_items = nullptr;
-  double *d_nuc = nullptr, *d_rec = nullptr, *d_out = nullptr;
-  // pair tables of the current centres
-  TB_TRYC(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa, 1,
-                             3 * (int64_t)P->ngto, gs_pair(P), gs_esoa(P), P->st));
-  {
-    const int ng = P->ng;
-    std::vector<std::vector<uint64_t>> byL(2 * 4 + 1);
-    for (int a = 0; a < natoms; ++a)
-      for (int gi = 0; gi < ng; ++gi)
-        for (int gk = 0; gk < ng; ++gk) {
-          const int L = P->gL[gi] + P->gL[gk];
-          if (L < 0 || L > 8) {
-            rc = fail(THISTLE_ERR_ANGMOM, "pair order above 8");
-            goto done;
-          }
-          byL[L].push_back((uint64_t)a | ((uint64_t)gi << 16) | ((uint64_t)gk << 40));
-        }
-    std::vector<uint64_t> items;
-    std::vector<int64_t> beg(10, 0), rec0(10, 0);
-    std::vector<int> rsL(10, 0);
-    int64_t recn = 0;
-    for (int L = 0; L <= 8; ++L) {
-      beg[L] = (int64_t)items.size();
-      items.insert(items.end(), byL[L].begin(), byL[L].end());
-      rsL[L] = L + 7 + ((L + 7) & 1);
-      rec0[L] = recn;
-      recn += (int64_t)byL[L].size() * rsL[L];
-    }
-    beg[9] = (int64_t)items.size();
-    std::vector<double> nuc((size_t)natoms * 8, 0.0);
-    for (int a = 0; a < natoms; ++a) {
-      for (int d = 0; d < 3; ++d) nuc[(size_t)a * 8 + d] = geom[a + (size_t)natoms * d];
-      nuc[(size_t)a * 8 + 4] = Zn[a];
-    }
-    TB_TRY(dalloc(&d_items, items.size(), "nuclear items"));
-    TB_TRY(dalloc(&d_nuc, nuc.size(), "nuclei"));
-    TB_TRY(dalloc(&d_rec, (size_t)std::max<int64_t>(recn, 1), "nuclear records"));
-    TB_TRY(dalloc(&d_out, (size_t)P->nq, "nuclear term"));
-    TB_TRYC(cudaMemcpyAsync(d_items, items.data(), sizeof(uint64_t) * items.size(), cudaMemcpyHostToDevice, P->st));
-    TB_TRYC(cudaMemcpyAsync(d_nuc, nuc.data(), sizeof(double) * nuc.size(), cudaMemcpyHostToDevice, P->st));
-    for (int L = 0; L <= 8; ++L) {
-      if (beg[L + 1] == beg[L]) continue;
-      Stage1Args a = stage1_args(P, nullptr, beg[L], beg[L + 1], d_rec, rec0[L], rsL[L]);
-      TB_TRYC(launch_nuclear(L, a, d_items, d_nuc, P->st));
-    }
-    TB_TRYC(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
-    for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
-      const int tn = std::min(P->s2_qtile, P->nq - q0);
-      int uniform = 0, first_on_grid = 0;
-      double dq = 0.0;
-      grid_info(P->hq.data() + q0, tn, uniform, first_on_grid, dq);
-      for (int L = 0; L <= 8; ++L) {
-        const int64_t nL = beg[L + 1] - beg[L];
-        if (nL == 0) continue;
-        Stage2ClassArgs s;
-        s.rec = d_rec + rec0[L];
-        s.rs = rsL[L];
-        s.nquart = nL;
-        s.perm = nullptr;
-        s.pbase = 0;
-        s.gs_rec = 0;
-        s.gs_partial = 0;
-        s.q = P->d_q + q0;
-        s.nq = tn;
-        s.uniform = uniform;
-        s.first_on_grid = first_on_grid;
-        s.dq = dq;
-        s.chunk = 0;
-        s.j2 = false;
-        s.partial = P->d_partial + q0;
-        s.pstride = P->nq;
-        const int64_t per_block = (int64_t)stage2_quartets_per_warp(L) * STAGE2_WARPS;
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nL + per_block - 1) / per_block, P->s2_rows));
-        TB_TRYC(launch_stage2_class(L, s, grid, 1, P->st));
-      }
-    }
-    TB_TRYC(launch_reduce_batch(P->d_partial, P->s2_rows, P->nq, (int64_t)P->s2_rows * P->nq, d_out, 1, P->st));
-    TB_TRYC(cudaMemcpyAsync(host_out, d_out, sizeof(double) * P->nq, cudaMemcpyDeviceToHost, P->st));
-  }
-done:
-  cudaStreamSynchronize(P->st);
-  dfree(d_items);
-  dfree(d_nuc);
-  dfree(d_rec);
-  dfree(d_out);
-  return rc;
-}
-
-// Inn(q) = sum_ij Zn_i Zn_j sinc(q R_ij), sinc(x) = 1 for |x| < 1e-10
-// (src/main_calculation.f90:302-311, 853-861)
-// ---------------------------------------------------------------------------
-// elastic aligned intensity (type 4): F(q) on q vectors from the AO density
-// ---------------------------------------------------------------------------
-// F(q) of elastic_integration_alig (src/Integrals.f90:2366-2490) for the
-// plan's current centres on nq q vectors (3 interleaved doubles each, host);
-// re / im / abs2 (host, any may be NULL) get F and |F|^2 (tb_formfactor.cu).
-static int form_factor(thistle_plan *P, const double *qvec, int nq, double *re, double *im, double *abs2) {
-  if (!kind_elastic(P->kind)) return fail(THISTLE_ERR_TYPE, "the form factor needs an elastic plan (the 1-RDM)");
-  if (!qvec || nq <= 0) return fail(THISTLE_ERR_ARG, "empty q-vector list");
-  if (!finite_all(qvec, 3 * (int64_t)nq)) return fail(THISTLE_ERR_NONFINITE, "non-finite q vector");
-  if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "the form factor is computed for single-geometry plans");
-  int rc = THISTLE_OK;
-  double *d_rec = nullptr, *d_qv = nullptr, *d_out = nullptr;
-  std::vector<double> h((size_t)3 * nq);
-  TB_TRY(dalloc(&d_rec, (size_t)form_factor_record_doubles(npairs(P->ng)), "form-factor records"));
-  TB_TRY(dalloc(&d_qv, (size_t)3 * nq, "q vectors"));
-  TB_TRY(dalloc(&d_out, (size_t)3 * nq, "form factor"));
-  TB_TRYC(cudaMemcpyAsync(d_qv, qvec, sizeof(double) * 3 * (size_t)nq, cudaMemcpyHostToDevice, P->st));
-  TB_TRYC(launch_pair_tables(P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa, 1,
-                             3 * (int64_t)P->ngto, gs_pair(P), gs_esoa(P), P->st));
-  {
-    const Stage1Args a = stage1_args(P, P->d_quart, 0, 0, nullptr, 0, 0);
-    TB_TRYC(launch_form_factor(a, d_rec, d_qv, nq, d_out, d_out + nq, d_out + 2 * (size_t)nq, P->st));
-  }
-  P->launches = 3;
-  TB_TRYC(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * 3 * (size_t)nq, cudaMemcpyDeviceToHost, P->st));
-  TB_TRYC(cudaStreamSynchronize(P->st));
-  P->fwd_valid = false;  // the pair tables were rebuilt
-  if (re) std::copy(h.begin(), h.begin() + nq, re);
-  if (im) std::copy(h.begin() + nq, h.begin() + 2 * (size_t)nq, im);
-  if (abs2) std::copy(h.begin() + 2 * (size_t)nq, h.end(), abs2);
-done:
-  dfree(d_rec);
-  dfree(d_qv);
-  dfree(d_out);
-  return rc;
-}
-
-// The q vectors of CASE(4) (src/main_calculation.f90:227-241) for nq points:
-// ss = (linspace(0, pi/2, nq) - pi) / 2, k0 = 3.00 * 1.889726125 * 0.529,
-// q = 2 k0 cos(ss) (sin ss, 0, cos ss), written (3, nq) column-major.
-static void elastic_aligned_grid(int nq, double *qal) {
-  const double pi = std::acos(-1.0), k0 = 3.00 * 1.889726125 * 0.529;
-  for (int mm = 0; mm < nq; ++mm) {
-    double ss = nq > 1 ? (pi / 2.0) * (double)mm / (double)(nq - 1) : 0.0;
-    ss = (ss - pi) / 2.0;
-    const double rr = 2.0 * k0 * std::cos(ss);
-    qal[3 * mm] = rr * std::sin(ss) * std::cos(0.0);
-    qal[3 * mm + 1] = rr * std::sin(ss) * std::sin(0.0);
-    qal[3 * mm + 2] = rr * std::cos(ss);
-  }
-}
-
-static void nuclear_nuclear(const double *Zn, const double *geom, int natoms, const double *q, int nq, double *out) {
-  for (int k = 0; k < nq; ++k) out[k] = 0.0;
-  for (int i = 0; i < natoms; ++i)
-    for (int j = 0; j < natoms; ++j) {
-      double r2 = 0.0;
-      for (int d = 0; d < 3; ++d) {
-        const double x = geom[i + (size_t)natoms * d] - geom[j + (size_t)natoms * d];
-        r2 += x * x;
-      }
-      const double R = std::sqrt(r2);
-      for (int k = 0; k < nq; ++k) {
-        const double a = q[k] * R;
-        out[k] += Zn[i] * Zn[j] * (std::fabs(a) < 1e-10 ? 1.0 : std::sin(a) / a);
-      }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// molecule batches: several plans (any bases), one launch per stage and class
-// ---------------------------------------------------------------------------
-struct thistle_batch {
-  std::vector<thistle_plan *> plans;
-  cudaStream_t st = nullptr;
-  int kind = 0, nqmax = 0, rows = 64;  // partial rows per plan: a class's blocks in one launch
-  int64_t nq_total = 0;
-  std::vector<int64_t> out_off;
-  PairDesc *d_pair = nullptr;
-  int64_t *d_pair_pre = nullptr, pair_blocks = 0;
-  struct S1 {
-    int L, LK, XB, n;
-    Stage1Args *d;
-    int64_t *pre, blocks;
-    bool split;            // contraction kernel + convolution kernel through d_xbuf
-    int64_t *prexc, blocksxc;
-  };
-  struct S2 {
-    int LB, n;
-    Stage2ClassArgs *d;
-    int64_t *pre, blocks;
-  };
-  std::vector<S1> s1;
-  std::vector<S2> s2;
-  ReduceDesc *d_red = nullptr;
-  double *d_partial = nullptr, *d_out = nullptr, *d_xbuf = nullptr;
-  int64_t partial_len = 0;
-  bool use_graph = false;
-  cudaGraphExec_t gx = nullptr;
-  int64_t launches = 0;
-};
-
-static void batch_free(thistle_batch *B) {
-  if (!B) return;
-  dfree(B->d_pair); dfree(B->d_pair_pre); dfree(B->d_red); dfree(B->d_partial); dfree(B->d_out);
-  for (auto &x : B->s1) { dfree(x.d); dfree(x.pre); dfree(x.prexc); }
-  dfree(B->d_xbuf);
-  for (auto &x : B->s2) { dfree(x.d); dfree(x.pre); }
-  if (B->gx) cudaGraphExecDestroy(B->gx);
-  delete B;
-}
-
-template <class T>
-static int upload_vec(T **dst, const std::vector<T> &v, cudaStream_t st, const char *what) {
-  int rc = dalloc(dst, v.size(), what);
-  if (rc != THISTLE_OK) return rc;
-  TB_CK(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
-  return THISTLE_OK;
-}
-
-static int batch_run(thistle_batch *B) {
-  cudaStream_t st = B->st;
-  B->launches = 0;
-  TB_CK(launch_pair_tables_batch(B->d_pair, B->d_pair_pre, (int)B->plans.size(), B->pair_blocks, st));
-  B->launches += 1;
-  for (auto &x : B->s1) {
-    if (x.split) {
-      TB_CK(launch_stage1_xsplit_batch(B->kind, x.L, x.LK, x.XB, x.d, x.prexc, x.blocksxc, x.pre, x.blocks, x.n,
-                                       B->d_xbuf, st));
-      B->launches += 2;
-    } else {
-      TB_CK(launch_stage1_batch(B->kind, x.L, x.LK, x.XB, x.d, x.pre, x.n, x.blocks, st));
-      B->launches += 1;
-    }
-  }
-  TB_CK(cudaMemsetAsync(B->d_partial, 0, sizeof(double) * B->partial_len, st));
-  for (auto &x : B->s2) {
-    TB_CK(launch_stage2_class_batch(x.LB, kind_j2(B->kind), x.d, x.pre, x.n, x.blocks, B->nqmax, st));
-    B->launches += 1;
-  }
-  TB_CK(launch_reduce_desc(B->d_red, (int)B->plans.size(), B->nqmax, st));
-  B->launches += 1;
-  return THISTLE_OK;
-}
-
-static int batch_exec(thistle_batch *B) {
-  int rc = THISTLE_OK;
-  // work a plan queued on its own stream (centres, an execution) comes first
-  for (thistle_plan *P : B->plans)
-    if (P->st != B->st) TB_CK(cudaStreamSynchronize(P->st));
-  if (!B->use_graph) {
-    rc = batch_run(B);
-  } else {
-    if (!B->gx) {
-      cudaGraph_t g = nullptr;
-      TB_CK(cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal));
-      rc = batch_run(B);
-      cudaError_t e = cudaStreamEndCapture(B->st, &g);
-      if (rc != THISTLE_OK) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-      }
-      TB_CK(e);
-      e = cudaGraphInstantiate(&B->gx, g, 0);
-      cudaGraphDestroy(g);
-      TB_CK(e);
-    }
-    TB_CK(cudaGraphLaunch(B->gx, B->st));
-  }
-  // the batch rewrote every plan's pair tables and records for its current centres
-  for (thistle_plan *P : B->plans) P->fwd_valid = rc == THISTLE_OK;
-  return rc;
-}
-
-static int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
-  if (!out || !plans || n < 1) return fail(THISTLE_ERR_ARG, "need at least one plan");
-  *out = nullptr;
-  for (int i = 0; i < n; ++i) {
-    const thistle_plan *P = plans[i];
-    if (!P) return fail(THISTLE_ERR_ARG, "null plan in the batch");
-    if (P->kind != plans[0]->kind) return fail(THISTLE_ERR_TYPE, "plans of one batch must share the calculation type");
-    if (P->kind == KIND_ALIGNED) return fail(THISTLE_ERR_TYPE, "aligned plans cannot be batched");
-    if (P->kind == KIND_CMS) return fail(THISTLE_ERR_TYPE, "resolved CMS plans cannot be batched");
-    if (P->ngeom != 1) return fail(THISTLE_ERR_SHAPE, "batched plans hold one geometry each");
-    if (P->nq > STAGE2_QTILE) return fail(THISTLE_ERR_SHAPE, "batched plans need nq <= 1024");
-  }
-  thistle_batch *B = new thistle_batch();
-  int rc = THISTLE_OK;
-  B->plans.assign(plans, plans + n);
-  B->st = plans[0]->st;
-  B->kind = plans[0]->kind;
-  {
-    // every plan once on its own: records, and the stage-2 visiting order
-    for (thistle_plan *P : B->plans) {
-      TB_TRY(plan_exec(P, P->d_result));
-      TB_TRYC(cudaStreamSynchronize(P->st));
-    }
-    std::vector<PairDesc> pd;
-    std::vector<int64_t> ppre(1, 0);
-    std::vector<ReduceDesc> rd;
-    int64_t poff = 0, ooff = 0;
-    for (thistle_plan *P : B->plans) {
-      pd.push_back(PairDesc{P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa});
-      ppre.push_back(ppre.back() + (npairs(P->ng) + 127) / 128);
-      B->nqmax = std::max(B->nqmax, P->nq);
-      B->out_off.push_back(ooff);
-      rd.push_back(ReduceDesc{nullptr, B->rows, P->nq, nullptr});  // pointers below
-      poff += (int64_t)B->rows * P->nq;
-      ooff += P->nq;
-    }
-    B->partial_len = poff;
-    B->nq_total = ooff;
-    TB_TRY(dalloc(&B->d_partial, (size_t)std::max<int64_t>(poff, 1), "batch partial sums"));
-    TB_TRY(dalloc(&B->d_out, (size_t)std::max<int64_t>(ooff, 1), "batch results"));
-    std::vector<double *> part(n);
-    poff = 0;
-    for (int i = 0; i < n; ++i) {
-      part[i] = B->d_partial + poff;
-      rd[i].partial = part[i];
-      rd[i].out = B->d_out + B->out_off[i];
-      poff += (int64_t)B->rows * plans[i]->nq;
-    }
-    B->pair_blocks = ppre.back();
-    TB_TRY(upload_vec(&B->d_pair, pd, B->st, "batch pair descriptors"));
-    TB_TRY(upload_vec(&B->d_pair_pre, ppre, B->st, "batch pair prefix"));
-    TB_TRY(upload_vec(&B->d_red, rd, B->st, "batch reduce descriptors"));
-    // stage 1: items grouped by (L, LK, XB); the kernel choice per L counts
-    // the quartets of every plan
-    int64_t ltot[LMAXQ + 1] = {0};
-    for (thistle_plan *P : B->plans)
-      for (int c = 0; c < P->ncls; ++c) ltot[P->cls_L[c]] += P->cls_end[c] - P->cls_begin[c];
-    std::vector<std::pair<std::array<int, 4>, Stage1Args>> items;  // (L, LK, XB, nout)
-    for (thistle_plan *P : B->plans)
-      for (int c = 0; c < P->ncls; ++c) {
-        Stage1Args a = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c],
-                                   P->cls_rs[c]);
-        const int L = P->cls_L[c];
-        if (stage1_xk(L, ltot[L], P->nsm)) {
-          for (const SubRange &u : P->cls_sub[c]) {
-            Stage1Args b = a;
-            b.qbegin = u.begin;
-            b.qend = u.end;
-            b.recbase = P->cls_recoff[c] + (u.begin - P->cls_begin[c]) * (int64_t)P->cls_rs[c];
-            items.push_back({{L, u.LK, u.XB, u.nout}, b});
-          }
-        } else {
-          items.push_back({{L, -1, 0, 0}, a});
-        }
-      }
-    auto same = [](const std::array<int, 4> &x, const std::array<int, 4> &y) {
-      return x[0] == y[0] && x[1] == y[1] && x[2] == y[2];
-    };
-    std::stable_sort(items.begin(), items.end(), [](const auto &x, const auto &y) {
-      return std::array<int, 3>{x.first[0], x.first[1], x.first[2]} <
-             std::array<int, 3>{y.first[0], y.first[1], y.first[2]};
-    });
-    int64_t xneed = 0;
-    for (size_t i = 0; i < items.size();) {
-      size_t j = i;
-      std::vector<Stage1Args> d;
-      std::vector<int64_t> pre(1, 0), prexc(1, 0);
-      const int L = items[i].first[0], LK = items[i].first[1];
-      // contracted side: split through the batch's contraction buffer when
-      // every item knows its outer-pair count and the group fits in 2 GB
-      bool split = LK >= 0;
-      int64_t xoff = 0;
-      while (j < items.size() && same(items[j].first, items[i].first)) {
-        Stage1Args a = items[j].second;
-        const int64_t nq = a.qend - a.qbegin;
-        const int nout = items[j].first[3];
-        if (LK >= 0 && nout > 0) {
-          int G = 1;
-          while (G < nout) G *= 2;
-          a.xg = G;
-          a.xstride = nout * ntuv(LK);
-          a.xoff = xoff;
-          xoff += nq * a.xstride;
-          prexc.push_back(prexc.back() + (nq * G + 127) / 128);
-        } else {
-          split = false;
-        }
-        d.push_back(a);
-        pre.push_back(pre.back() + stage1_item_blocks(L, LK >= 0, nq));
-        ++j;
-      }
-      if (xoff > (int64_t(1) << 28)) split = false;
-      if (split) xneed = std::max(xneed, xoff);
-      thistle_batch::S1 x{L, LK, items[i].first[2], (int)d.size(), nullptr, nullptr, pre.back(), split, nullptr,
-                          split ? prexc.back() : 0};
-      TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-1 descriptors"));
-      TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-1 prefix"));
-      if (split) TB_TRY(upload_vec(&x.prexc, prexc, B->st, "batch contraction prefix"));
-      B->s1.push_back(x);
-      i = j;
-    }
-    if (xneed > 0) TB_TRY(dalloc(&B->d_xbuf, (size_t)xneed, "batch contraction buffer"));
-    // stage 2: items grouped by Bessel order
-    std::vector<std::pair<int, std::pair<Stage2ClassArgs, int64_t>>> s2items;
-    for (int i = 0; i < n; ++i) {
-      thistle_plan *P = plans[i];
-      int uniform = 0, first_on_grid = 0;
-      double dq = 0.0;
-      grid_info(P->hq.data(), P->nq, uniform, first_on_grid, dq);
-      for (int c = 0; c < P->ncls; ++c) {
-        const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
-        Stage2ClassArgs s;
-        s.rec = P->d_rec + P->cls_recoff[c];
-        s.rs = P->cls_rs[c];
-        s.nquart = P->cls_end[c] - P->cls_begin[c];
-        s.perm = P->d_perm;
-        s.pbase = P->cls_begin[c];
-        s.q = P->d_q;
-        s.nq = P->nq;
-        s.uniform = uniform;
-        s.first_on_grid = first_on_grid;
-        s.dq = dq;
-        s.chunk = 0;
-        s.j2 = kind_j2(P->kind);
-        s.partial = part[i];
-        s.pstride = P->nq;
-        s.gs_rec = 0;
-        s.gs_partial = 0;
-        // one block per STAGE2_WARPS batches of quartets, at most `rows`
-        // (the other plans of the launch fill the GPU)
-        const int64_t per = (int64_t)stage2_quartets_per_warp(LB) * STAGE2_WARPS;
-        const int64_t vg = std::min<int64_t>(B->rows, (s.nquart + per - 1) / per);
-        if (vg <= 0) continue;
-        s2items.push_back({LB, {s, vg}});
-      }
-    }
-    std::stable_sort(s2items.begin(), s2items.end(),
-                     [](const auto &x, const auto &y) { return x.first < y.first; });
-    for (size_t i = 0; i < s2items.size();) {
-      size_t j = i;
-      std::vector<Stage2ClassArgs> d;
-      std::vector<int64_t> pre(1, 0);
-      while (j < s2items.size() && s2items[j].first == s2items[i].first) {
-        d.push_back(s2items[j].second.first);
-        pre.push_back(pre.back() + s2items[j].second.second);
-        ++j;
-      }
-      thistle_batch::S2 x{s2items[i].first, (int)d.size(), nullptr, nullptr, pre.back()};
-      TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-2 descriptors"));
-      TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-2 prefix"));
-      B->s2.push_back(x);
-      i = j;
-    }
-    TB_TRYC(cudaStreamSynchronize(B->st));
-  }
-done:
-  if (rc != THISTLE_OK) {
-    batch_free(B);
-    return rc;
-  }
-  *out = B;
-  return THISTLE_OK;
-}
-
-// The reference's aligned q grid (QCOORD3, src/main_calculation.f90:864-929):
-// the origin, one point on the +y axis, a hexagon of radius dk, then rings of
-// radius i dk (i = 2..31) with ceil(pi / asin(1/(2i))) points each starting on
-// +y, every point lifted onto the Ewald sphere of radius k0; dk =
-// sqrt(3)/2 k0/31.  Unused slots and zero components are 1e-10, as there.
-static void qcoord3_grid(double k0, double *qal /* (3, 3131) column-major */) {
-  const int nring = 30, npts = 3131;
-  const double pi = std::acos(-1.0);
-  const double dk = std::sqrt(3.0) / 2.0 * k0 / (nring + 1.0);
-  double *qx = qal, *qy = qal + 1, *qz = qal + 2;  // stride 3
-  for (int t = 0; t < npts; ++t) qx[3 * t] = qy[3 * t] = qz[3 * t] = 1.0e-10;
-  auto lift = [&](double x, double y) { return k0 * (1.0 - std::sqrt(std::fabs(1.0 - (x * x + y * y) / (k0 * k0)))); };
-  int pos = 1;  // 0-based slot of the +y point
-  qy[3 * pos] = dk;
-  qz[3 * pos] = k0 * (1.0 - std::sqrt(1.0 - 1.0 / ((nring + 1.0) * (nring + 1.0))));
-  for (int i = 1; i <= 5; ++i) {
-    ++pos;
-    const double x = std::sin(i * pi / 3.0) * dk, y = std::cos(i * pi / 3.0) * dk;
-    qx[3 * pos] = x;
-    qy[3 * pos] = y;
-    qz[3 * pos] = k0 * (1.0 - std::sqrt(1.0 - (x * x + y * y) / (k0 * k0)));
-  }
-  for (int i = 2; i <= nring + 1; ++i) {
-    const int np = (int)std::ceil(pi / std::asin(1.0 / (2.0 * i)));
-    const double rc = i * dk, ang = 2.0 * pi / np;
-    ++pos;
-    qy[3 * pos] = rc;
-    qz[3 * pos] = k0 * (1.0 - std::sqrt(std::fabs(1.0 - std::pow((double)i, 2.0) / ((nring + 1.0) * (nring + 1.0)))));
-    for (int j = 1; j <= np - 1; ++j) {
-      ++pos;
-      const double x = std::sin(j * ang) * rc, y = std::cos(j * ang) * rc;
-      qx[3 * pos] = x;
-      qy[3 * pos] = y;
-      qz[3 * pos] = lift(x, y);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
 extern "C" {
-
-int thistle_qcoord3(double k0, double *q_al) {
-  if (!q_al) return fail(THISTLE_ERR_ARG, "null argument");
-  if (!std::isfinite(k0) || !(k0 > 0.0)) return fail(THISTLE_ERR_ARG, "k0 must be finite and positive");
-  qcoord3_grid(k0, q_al);
-  return THISTLE_OK;
-}
-
-int thistle_batch_create(thistle_batch **batch, thistle_plan *const *plans, int32_t nplans) {
-  return batch_create(batch, plans, nplans);
-}
-
-int thistle_batch_use_graph(thistle_batch *B, int32_t enable) {
-  if (!B) return fail(THISTLE_ERR_ARG, "null batch");
-  TB_CK(cudaStreamSynchronize(B->st));
-  if (B->gx) cudaGraphExecDestroy(B->gx);
-  B->gx = nullptr;
-  B->use_graph = enable != 0;
-  return THISTLE_OK;
-}
-
-int thistle_batch_execute_device(thistle_batch *B, double *result_dev) {
-  if (!B || !result_dev) return fail(THISTLE_ERR_ARG, "null argument");
-  int rc = batch_exec(B);
-  if (rc != THISTLE_OK) return rc;
-  TB_CK(cudaMemcpyAsync(result_dev, B->d_out, sizeof(double) * B->nq_total, cudaMemcpyDeviceToDevice, B->st));
-  return THISTLE_OK;
-}
-
-int thistle_batch_execute(thistle_batch *B, double *result_host) {
-  if (!B || !result_host) return fail(THISTLE_ERR_ARG, "null argument");
-  int rc = batch_exec(B);
-  if (rc != THISTLE_OK) return rc;
-  TB_CK(cudaMemcpyAsync(result_host, B->d_out, sizeof(double) * B->nq_total, cudaMemcpyDeviceToHost, B->st));
-  TB_CK(cudaStreamSynchronize(B->st));
-  return THISTLE_OK;
-}
-
-int thistle_batch_info(const thistle_batch *B, int64_t *info) {
-  if (!B || !info) return fail(THISTLE_ERR_ARG, "null argument");
-  info[0] = (int64_t)B->plans.size();
-  info[1] = B->nq_total;
-  info[2] = B->launches;
-  return THISTLE_OK;
-}
-
-int thistle_batch_destroy(thistle_batch *B) {
-  if (B) {
-    if (B->st) cudaStreamSynchronize(B->st);
-    batch_free(B);
-  }
-  return THISTLE_OK;
-}
 
 int thistle_plan_vjp(thistle_plan *P, const double *v_host, double *grad_host) {
   if (!P || !v_host || !grad_host) return fail(THISTLE_ERR_ARG, "null argument");
@@ -2123,110 +1275,6 @@ int thistle_plan_destroy(thistle_plan *P) {
     tr.mark("plan destroy");
   }
   return THISTLE_OK;
-}
-
-int thistle_plan_form_factor(thistle_plan *P, const double *qvec, int32_t nq, double *re_host, double *im_host,
-                             double *abs2_host) {
-  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
-  return form_factor(P, qvec, nq, re_host, im_host, abs2_host);
-}
-
-int thistle_elastic_aligned_grid(int32_t nq, double *q_al) {
-  if (nq <= 0 || !q_al) return fail(THISTLE_ERR_ARG, "nq must be positive and q_al non-null");
-  elastic_aligned_grid(nq, q_al);
-  return THISTLE_OK;
-}
-
-int thistle_plan_nuclear(thistle_plan *P, const double *Zn, const double *geom, int32_t natoms, double *ine_host) {
-  if (!P || !ine_host) return fail(THISTLE_ERR_ARG, "null argument");
-  return nuclear_term(P, Zn, geom, natoms, ine_host);
-}
-
-int thistle_total_scattering(int32_t type, const double *Zn, const double *geom, int32_t natoms, int32_t maxl,
-                             int32_t ngto, int32_t ng, const double *ga, const int32_t *l, const int32_t *m,
-                             const int32_t *n, const double *xx, const double *yy, const double *zz,
-                             const double *mmod, int32_t norbs, const double *q, int32_t nq, const int32_t *group,
-                             double cutoffz, double cutoffmd, double cutoffcentre, const int32_t *mat,
-                             const double *total, int32_t nmat, const double *onerdm, int32_t nmo1,
-                             double *q_abs_out, double *result_out) {
-  if (!result_out) return fail(THISTLE_ERR_ARG, "null result");
-  if (maxl < 0) return fail(THISTLE_ERR_ARG, "maxl must be >= 0");
-  if (type == THISTLE_TOTAL_ELECTRON || type == THISTLE_ELASTIC_ELECTRON) {
-    // I_e - 2 Ine + Inn (src/main_calculation.f90:277-329, 330-...), I_e the
-    // total (type 5) or elastic (type 6) j0 intensity
-    if (!Zn || !geom || natoms < 1) return fail(THISTLE_ERR_ARG, "electron scattering needs Zn and geom");
-    if (!onerdm || nmo1 <= 0) return fail(THISTLE_ERR_ARG, "electron scattering needs the 1-RDM");
-    if (!q || nq <= 0) return fail(THISTLE_ERR_ARG, "empty q grid");
-    thistle_plan *E = nullptr, *T = nullptr;
-    int rc = plan_create(&E, THISTLE_ELASTIC_J0, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, nullptr, nullptr,
-                         0, onerdm, nmo1, q, nq, cutoffz, cutoffmd, cutoffcentre);
-    if (rc != THISTLE_OK) return rc;
-    std::vector<double> ie((size_t)nq), ine((size_t)nq), inn((size_t)nq);
-    if (ng != E->ng) rc = fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
-    if (rc == THISTLE_OK && type == THISTLE_TOTAL_ELECTRON) {
-      rc = plan_create(&T, THISTLE_TOTAL_J0, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, mat, total, nmat,
-                       nullptr, 0, q, nq, cutoffz, cutoffmd, cutoffcentre);
-      if (rc == THISTLE_OK) rc = thistle_plan_execute(T, ie.data());
-    }
-    if (rc == THISTLE_OK && type == THISTLE_ELASTIC_ELECTRON) rc = thistle_plan_execute(E, ie.data());
-    if (rc == THISTLE_OK) rc = nuclear_term(E, Zn, geom, natoms, ine.data());
-    if (rc == THISTLE_OK) {
-      nuclear_nuclear(Zn, geom, natoms, q, nq, inn.data());
-      for (int k = 0; k < nq; ++k) result_out[k] = ie[k] - 2.0 * ine[k] + inn[k];
-      if (q_abs_out)
-        for (int k = 0; k < nq; ++k) q_abs_out[k] = q[k];
-    }
-    if (T) thistle_plan_destroy(T);
-    thistle_plan_destroy(E);
-    return rc;
-  }
-  if (type == THISTLE_ELASTIC_ALIGNED) {
-    // CASE(4): |F(q)|^2 on the reference's own grid of nq vectors, whatever q
-    // holds; q_abs_out gets |q| (src/main_calculation.f90:218-265)
-    if (!onerdm || nmo1 <= 0) return fail(THISTLE_ERR_ARG, "the elastic aligned intensity needs the 1-RDM");
-    if (nq <= 0) return fail(THISTLE_ERR_ARG, "nq must be positive");
-    std::vector<double> qal((size_t)3 * nq), qabs((size_t)nq);
-    elastic_aligned_grid(nq, qal.data());
-    for (int i = 0; i < nq; ++i)
-      qabs[i] = std::sqrt(qal[3 * i] * qal[3 * i] + qal[3 * i + 1] * qal[3 * i + 1] + qal[3 * i + 2] * qal[3 * i + 2]);
-    thistle_plan *E = nullptr;
-    int rc = plan_create(&E, THISTLE_ELASTIC_J0, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, nullptr, nullptr,
-                         0, onerdm, nmo1, qabs.data(), nq, cutoffz, cutoffmd, cutoffcentre);
-    if (rc != THISTLE_OK) return rc;
-    if (ng != E->ng) rc = fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
-    if (rc == THISTLE_OK) rc = form_factor(E, qal.data(), nq, nullptr, nullptr, result_out);
-    if (rc == THISTLE_OK && q_abs_out) std::copy(qabs.begin(), qabs.end(), q_abs_out);
-    thistle_plan_destroy(E);
-    return rc;
-  }
-  // type 3 evaluates on the reference's own aligned grid (QCOORD3 with
-  // k0 = 10.583544175, 3131 vectors), whatever q holds; q_abs_out gets |q|
-  std::vector<double> qal;
-  if (type == THISTLE_TOTAL_ALIGNED) {
-    if (nq != 3131) return fail(THISTLE_ERR_SHAPE, "type 3 runs on the 3131-vector QCOORD3 grid: nq must be 3131");
-    qal.resize(3 * 3131);
-    qcoord3_grid(10.583544175, qal.data());
-    q = qal.data();
-  }
-  thistle_plan *P = nullptr;
-  int rc = plan_create(&P, type, ngto, ga, l, m, n, xx, yy, zz, group, mmod, norbs, mat, total, nmat, onerdm, nmo1,
-                       q, nq, cutoffz, cutoffmd, cutoffcentre);
-  if (rc != THISTLE_OK) return rc;
-  if (ng != P->ng) {
-    plan_free(P);
-    return fail(THISTLE_ERR_SHAPE, "ng differs from maxval(group)");
-  }
-  PhaseTrace tr;
-  rc = thistle_plan_execute(P, result_out);
-  tr.mark("execute");
-  if (rc == THISTLE_OK && q_abs_out) {
-    for (int i = 0; i < nq; ++i)
-      q_abs_out[i] = type == THISTLE_TOTAL_ALIGNED
-                         ? std::sqrt(q[3 * i] * q[3 * i] + q[3 * i + 1] * q[3 * i + 1] + q[3 * i + 2] * q[3 * i + 2])
-                         : q[i];
-  }
-  thistle_plan_destroy(P);
-  return rc;
 }
 
 }  // extern "C"

@@ -6,7 +6,7 @@
 // accumulate).  The chain replaces the reference's z11/z22 build and its
 // per-quartet dgemm pair (src/Variables.f90:1045-1065, src/Integrals.f90:
 // 109-127): rho(ab,cd) = sum Ghat[x][y][z][w] C(x,a) C(y,b) C(z,c) C(w,d),
-// with Ghat the rows' eight index placements (tb_plan.cu), as
+// with Ghat the rows' eight index placements (tb_density.cu), as
 //   T1[x y z](a) = sum_w C(w,a) Ghat[x][y][z][w]
 //   V[x y](c<=d) = sum_z T1[x y z](d) C(z,c)        (packed pair c <= d)
 //   T3[x](p, b)  = sum_y V[x y](p) C(y,b)
