@@ -440,13 +440,23 @@ cudaError_t launch_stage1_xk(int kind, int L, int LK, bool XB, const Stage1Args 
 }
 
 cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
-                                 cudaStream_t st) {
-  if (kind == KIND_TOTAL) return launch_stage1_xsplit_k<KIND_TOTAL>(L, LK, XB, a, xbuf, nout, st);
-  if (kind == KIND_ELASTIC) return launch_stage1_xsplit_k<KIND_ELASTIC>(L, LK, XB, a, xbuf, nout, st);
-  if (kind == KIND_ALIGNED) return launch_stage1_xsplit_k<KIND_ALIGNED>(L, LK, XB, a, xbuf, nout, st);
-  if (kind == KIND_ELASTIC_J2) return launch_stage1_xsplit_k<KIND_ELASTIC_J2>(L, LK, XB, a, xbuf, nout, st);
-  if (kind == KIND_CMS) return launch_stage1_xsplit_k<KIND_CMS>(L, LK, XB, a, xbuf, nout, st);
-  return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, st);
+                                 cudaStream_t st, bool with_xc) {
+  if (kind == KIND_TOTAL) return launch_stage1_xsplit_k<KIND_TOTAL>(L, LK, XB, a, xbuf, nout, with_xc, st);
+  if (kind == KIND_ELASTIC) return launch_stage1_xsplit_k<KIND_ELASTIC>(L, LK, XB, a, xbuf, nout, with_xc, st);
+  if (kind == KIND_ALIGNED) return launch_stage1_xsplit_k<KIND_ALIGNED>(L, LK, XB, a, xbuf, nout, with_xc, st);
+  if (kind == KIND_ELASTIC_J2) return launch_stage1_xsplit_k<KIND_ELASTIC_J2>(L, LK, XB, a, xbuf, nout, with_xc, st);
+  if (kind == KIND_CMS) return launch_stage1_xsplit_k<KIND_CMS>(L, LK, XB, a, xbuf, nout, with_xc, st);
+  return launch_stage1_xsplit_k<KIND_J2>(L, LK, XB, a, xbuf, nout, with_xc, st);
+}
+
+bool stage1_xct(int kind, int LK, int shells_canonical) {
+  return kind == KIND_TOTAL && shells_canonical && LK <= 3;
+}
+
+cudaError_t launch_stage1_xct(int kind, int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride,
+                              int64_t xbase, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_xct_k<KIND_TOTAL>(tuple, XB, a, xbuf, xstride, xbase, st);
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,

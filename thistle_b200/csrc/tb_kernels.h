@@ -176,11 +176,22 @@ cudaError_t launch_nuclear(int L, const Stage1Args &a, const uint64_t *items, co
                            cudaStream_t st);
 // the same sub-range of one geometry as two kernels through xbuf (at least
 // (qend - qbegin) * nout * ntuv(LK) doubles; nout = most outer function pairs)
+// (with_xc false: the convolution alone, X already written by the
+// shell-templated contraction launch_stage1_xct, one launch per shell tuple)
 template <int K>
-cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout, bool with_xc,
                                    cudaStream_t st);
 cudaError_t launch_stage1_xsplit(int kind, int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
-                                 cudaStream_t st);
+                                 cudaStream_t st, bool with_xc = true);
+template <int K>
+cudaError_t launch_stage1_xct_k(int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride, int64_t xbase,
+                                cudaStream_t st);
+// whether a contracted-side sub-range (kind, LK) takes the shell-templated
+// contraction, and its launcher (a: the tuple's quartets; xbase: the first
+// quartet of the sub-range, the buffer's row 0)
+bool stage1_xct(int kind, int LK, int shells_canonical);
+cudaError_t launch_stage1_xct(int kind, int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride,
+                              int64_t xbase, cudaStream_t st);
 // molecule batches: the contraction (blocks from prexc) then the convolution
 // (blocks from pre, as the fused kernel) over every item of one (L, LK, XB)
 template <int K>

@@ -589,8 +589,24 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
         b.recbase = recoff[c] + (u.begin - cb[c]) * (int64_t)rs[c];
         const int64_t need = (u.end - u.begin) * (int64_t)u.nout * ntuv(u.LK);
         if (ngeom == 1 && u.nout > 0 && P->d_xbuf && need <= P->xbuf_len) {
-          TB_CK(launch_stage1_xsplit(P->kind, cL[c], u.LK, u.XB != 0, b, P->d_xbuf, u.nout, P->st));
-          P->launches += 2;
+          if (tups && stage1_xct(P->kind, u.LK, P->shells_canonical)) {
+            // the contraction per shell tuple (templated), then the
+            // convolution of the whole sub-range from the same buffer
+            for (const TupleRange &w : tups[c]) {
+              if (w.begin < u.begin || w.end > u.end) continue;
+              Stage1Args bt = b;
+              bt.qbegin = w.begin;
+              bt.qend = w.end;
+              TB_CK(launch_stage1_xct(P->kind, w.tuple, u.XB != 0, bt, P->d_xbuf, u.nout * ntuv(u.LK), u.begin,
+                                      P->st));
+              P->launches += 1;
+            }
+            TB_CK(launch_stage1_xsplit(P->kind, cL[c], u.LK, u.XB != 0, b, P->d_xbuf, u.nout, P->st, false));
+            P->launches += 1;
+          } else {
+            TB_CK(launch_stage1_xsplit(P->kind, cL[c], u.LK, u.XB != 0, b, P->d_xbuf, u.nout, P->st));
+            P->launches += 2;
+          }
         } else {
           TB_CK(launch_stage1_xk(P->kind, cL[c], u.LK, u.XB != 0, b, ngeom, P->st));
           P->launches += 1;

@@ -959,6 +959,117 @@ __global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__
   stage1_xc_body<L, KIND, LK, XB>(A, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, xbuf, G, xstride);
 }
 
+// Shell-templated contraction (total j0, contracted side LK <= 3, plans with
+// canonical shells): stage1_xc_body's arithmetic for one pair of inner shells
+// (L1, L2) -- the inner function pairs and their Cartesian exponents are
+// compile-time, so the density and E loads of a thread are independent of
+// each other and issued ahead of the products.  X_o goes to
+// xbuf[(qi - xbase) xstride + o NX + e] like stage1_xc_body's.
+template <int L1, int L2, bool XB, int KIND>
+__global__ void __launch_bounds__(128) stage1_xct_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride,
+                                                         int64_t xbase) {
+  constexpr int LK = L1 + L2, NX = ntuv(LK);
+  constexpr int n1 = (L1 + 1) * (L1 + 2) / 2, n2 = (L2 + 1) * (L2 + 2) / 2;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t qi = A.qbegin + t / G;
+  const int o = (int)(t % G);
+  if (qi >= A.qend) return;
+  const QuartetHead Q = quartet_head<KIND>(A, qi);
+  const XkSides S = xk_sides<XB>(A, Q);
+  if (o >= S.nout) return;
+  int fa, fb, fc, fd;
+  xk_outer<0, XB>(A, Q, S, o, fa, fb, fc, fd, nullptr, nullptr, nullptr);
+  const int s1 = XB ? S.si : S.sk, s2 = XB ? S.sj : S.sr;
+  const double *tab = A.pairtab + (size_t)(XB ? S.pb : S.pk) * PAIR_STRIDE + 8;
+  const bool skx = XB ? (Q.skip & 1) : (Q.skip & 8), sky = XB ? (Q.skip & 2) : (Q.skip & 16);
+  const bool skz = XB ? (Q.skip & 4) : false;
+  auto ecoef = [&](int ax, int l1, int l2, int tt, bool skip) -> double {
+    const double v = tab[ax * ESZ + (l1 * (MAXA + 1) + l2) * E_T + tt];
+    return (skip && fabs(v) < TB_SKIP30) ? 0.0 : v;
+  };
+  int64_t rowp = 0;
+  double zo = 0.0;
+  if (!XB) {
+    rowp = kind_elastic(KIND) ? 0 : fpair(min(fa, fb), max(fa, fb)) * A.np;
+    zo = kind_elastic(KIND) ? A.zao[(size_t)fa * A.ngto + fb] : 0.0;
+  } else {
+    zo = kind_elastic(KIND) ? A.zket[(size_t)fc * A.ngto + fd] : 0.0;
+  }
+  double X[NX];
+#pragma unroll
+  for (int e = 0; e < NX; ++e) X[e] = 0.0;
+#pragma unroll
+  for (int c1 = 0; c1 < n1; ++c1)
+#pragma unroll
+    for (int c2 = 0; c2 < n2; ++c2) {
+      const int g1 = s1 + c1, g2 = s2 + c2;  // (ga, gb2) on the bra side, (gc, gd) on the ket side
+      double z;
+      if (kind_elastic(KIND)) {
+        z = (XB ? A.zao : A.zket)[(size_t)g1 * A.ngto + g2] * zo;
+      } else {
+        const int64_t rp = XB ? fpair(min(g1, g2), max(g1, g2)) * A.np : rowp;
+        z = XB ? A.rho[rp + fpair(min(fc, fd), max(fc, fd))] : A.rho[rp + fpair(min(g1, g2), max(g1, g2))];
+      }
+      // the reference skips primitive quartets with |ztot| < cutoffz
+      z = fabs(z) < A.cutoffz ? 0.0 : z;
+      const int x1 = cart_component(L1, c1, 0), x2 = cart_component(L2, c2, 0);
+      const int y1 = cart_component(L1, c1, 1), y2 = cart_component(L2, c2, 1);
+      const int z1 = cart_component(L1, c1, 2), z2 = cart_component(L2, c2, 2);
+      double cx[LK + 1], cy[LK + 1], cz[LK + 1];
+#pragma unroll
+      for (int tt = 0; tt <= LK; ++tt) {
+        const double sg = (XB && (tt & 1)) ? -1.0 : 1.0;
+        cx[tt] = sg * (tt <= x1 + x2 ? ecoef(0, x1, x2, tt, skx) : 0.0);
+        cy[tt] = sg * (tt <= y1 + y2 ? ecoef(1, y1, y2, tt, sky) : 0.0);
+        cz[tt] = sg * (tt <= z1 + z2 ? ecoef(2, z1, z2, tt, skz) : 0.0);
+      }
+      int e = 0;
+#pragma unroll
+      for (int tt = 0; tt <= LK; ++tt) {
+        const double w1 = z * cx[tt];
+#pragma unroll
+        for (int u = 0; u <= LK - tt; ++u) {
+          const double w2 = w1 * cy[u];
+#pragma unroll
+          for (int v = 0; v <= LK - tt - u; ++v, ++e) X[e] = fma(w2, cz[v], X[e]);
+        }
+      }
+    }
+  double *xo = xbuf + (qi - xbase) * (int64_t)xstride + o * NX;
+#pragma unroll
+  for (int e = 0; e < NX; ++e) xo[e] = X[e];
+}
+
+// One launch per shell tuple ((Li 5 + Lj) 5 + Lk) 5 + Lr: its inner shells
+// are (Li, Lj) when the bra is the contracted side (XB), else (Lk, Lr).
+template <int K>
+cudaError_t launch_stage1_xct_k(int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride, int64_t xbase,
+                                cudaStream_t st) {
+  const int64_t n = a.qend - a.qbegin;
+  if (n <= 0) return cudaSuccess;
+  const int Li = tuple / 125, Lj = (tuple / 25) % 5, Lk = (tuple / 5) % 5, Lr = tuple % 5;
+  const int L1 = XB ? Li : Lk, L2 = XB ? Lj : Lr;
+  const int Lo1 = XB ? Lk : Li, Lo2 = XB ? Lr : Lj;
+  const int nout = (Lo1 + 1) * (Lo1 + 2) / 2 * ((Lo2 + 1) * (Lo2 + 2) / 2);
+  int G = 1;
+  while (G < nout) G *= 2;
+  const int64_t nthr = n * G;
+  const unsigned grid = (unsigned)((nthr + 127) / 128);
+#define TB_XCT(l1, l2)                                                                          \
+  if (L1 == l1 && L2 == l2) {                                                                  \
+    if (XB) stage1_xct_kernel<l1, l2, true, K><<<grid, 128, 0, st>>>(a, xbuf, G, xstride, xbase);  \
+    else stage1_xct_kernel<l1, l2, false, K><<<grid, 128, 0, st>>>(a, xbuf, G, xstride, xbase);    \
+    return cudaGetLastError();                                                                 \
+  }
+  TB_XCT(0, 0)
+  TB_XCT(1, 0) TB_XCT(0, 1)
+  TB_XCT(2, 0) TB_XCT(1, 1) TB_XCT(0, 2)
+  TB_XCT(3, 0) TB_XCT(2, 1) TB_XCT(1, 2) TB_XCT(0, 3)
+#undef TB_XCT
+  return cudaErrorInvalidValue;
+}
+
+
 // Molecule batches: item i's contraction threads in blocks prexc[i] ..
 template <int L, int KIND, int LK, bool XB>
 __global__ void __launch_bounds__(128)
@@ -1069,14 +1180,18 @@ cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int 
 // Contracted-side classes of a single geometry in two kernels: the
 // contraction into xbuf (G threads per quartet), then convolution + epilogue.
 template <int L, int K, int LK, bool XB>
-static cudaError_t launch_stage1_xsplit_l(const Stage1Args &a, int64_t n, double *xbuf, int nout, cudaStream_t st) {
+static cudaError_t launch_stage1_xsplit_l(const Stage1Args &a, int64_t n, double *xbuf, int nout, bool with_xc,
+                                          cudaStream_t st) {
   int G = 1;
   while (G < nout) G *= 2;
   const int xstride = nout * ntuv(LK);
   const int64_t nthr = n * G;
-  stage1_xc_kernel<L, K, LK, XB><<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(a, xbuf, G, xstride);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (with_xc) {  // otherwise X was written by the shell-templated contraction
+    stage1_xc_kernel<L, K, LK, XB><<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(a, xbuf, G, xstride);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   const int thr = 128;
   const size_t smem = (size_t)ntuv(L) * sizeof(double) * thr;
   e = cudaFuncSetAttribute(stage1_xb_kernel<L, K, LK, XB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1086,14 +1201,14 @@ static cudaError_t launch_stage1_xsplit_l(const Stage1Args &a, int64_t n, double
 }
 
 template <int K>
-cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout,
+cudaError_t launch_stage1_xsplit_k(int L, int LK, bool XB, const Stage1Args &a, double *xbuf, int nout, bool with_xc,
                                    cudaStream_t st) {
   const int64_t n = a.qend - a.qbegin;
   if (n <= 0) return cudaSuccess;
 #define TB_XS(l, lk)                                                                         \
   if (L == l && LK == lk)                                                                   \
-    return XB ? launch_stage1_xsplit_l<l, K, lk, true>(a, n, xbuf, nout, st)                 \
-              : launch_stage1_xsplit_l<l, K, lk, false>(a, n, xbuf, nout, st);
+    return XB ? launch_stage1_xsplit_l<l, K, lk, true>(a, n, xbuf, nout, with_xc, st)        \
+              : launch_stage1_xsplit_l<l, K, lk, false>(a, n, xbuf, nout, with_xc, st);
   TB_XS(4, 0) TB_XS(4, 1) TB_XS(4, 2)
   TB_XS(5, 0) TB_XS(5, 1) TB_XS(5, 2)
   TB_XS(6, 0) TB_XS(6, 1) TB_XS(6, 2) TB_XS(6, 3)

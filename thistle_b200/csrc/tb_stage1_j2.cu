@@ -7,7 +7,7 @@ template cudaError_t launch_stage1_k<KIND_J2>(int L, const Stage1Args &a, int ng
 template cudaError_t launch_stage1_xk_k<KIND_J2>(int L, int LK, bool XB, const Stage1Args &a, int ngeom,
                                                       cudaStream_t st);
 template cudaError_t launch_stage1_xsplit_k<KIND_J2>(int L, int LK, bool XB, const Stage1Args &a, double *xbuf,
-                                                     int nout, cudaStream_t st);
+                                                     int nout, bool with_xc, cudaStream_t st);
 template cudaError_t launch_stage1_xsplit_batch_k<KIND_J2>(int L, int LK, int XB, const Stage1Args *d,
                                                            const int64_t *prexc, int64_t blocksxc, const int64_t *pre,
                                                            int64_t blocks, int n, double *xbuf, cudaStream_t st);
