@@ -23,9 +23,10 @@ int set_error(int code, const std::string &msg) { return fail(code, msg); }
 // validation
 // ---------------------------------------------------------------------------
 bool finite_all(const double *a, int64_t n) {
-  for (int64_t i = 0; i < n; ++i)
-    if (!std::isfinite(a[i])) return false;
-  return true;
+  // x - x is 0 for finite x and NaN for NaN or Inf: one branch-free pass
+  double acc = 0.0;
+  for (int64_t i = 0; i < n; ++i) acc += a[i] - a[i];
+  return acc == 0.0;
 }
 
 int check_basis(thistle_plan *P, int32_t ngto, const double *ga, const int32_t *l, const int32_t *m,
@@ -145,15 +146,37 @@ void class_counts(const std::vector<int> &gL, std::vector<int64_t> &cnt, bool al
 }
 
 // Sorted-by-key layout -> contiguous LLmax classes and record offsets.
+// The 625 shell tuples ((Li 5 + Lj) 5 + Lk) 5 + Lr in class-sort order:
+// LLmax, then the sub-range (LK, XB), then the tuple (the order of quartet_key).
+static const std::vector<int> &tuple_sort_order() {
+  static const std::vector<int> order = [] {
+    std::vector<int> o(625);
+    for (int t = 0; t < 625; ++t) o[t] = t;
+    std::stable_sort(o.begin(), o.end(), [](int a, int b) {
+      const uint32_t ka = quartet_key(a / 125, (a / 25) % 5, (a / 5) % 5, a % 5);
+      const uint32_t kb = quartet_key(b / 125, (b / 25) % 5, (b / 5) % 5, b % 5);
+      return ka / 625 < kb / 625;
+    });
+    return o;
+  }();
+  return order;
+}
+
 int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
   int64_t pos = 0, recoff = 0;
   P->ncls = 0;
   int maxg[5] = {0, 0, 0, 0, 0};  // most functions of a group, per shell L
   for (int g = 0; g < P->ng; ++g)
     if (P->gL[g] >= 0 && P->gL[g] <= 4) maxg[P->gL[g]] = std::max(maxg[P->gL[g]], P->gcount[g]);
+  const std::vector<int> &order = tuple_sort_order();
+  size_t oi = 0;  // order is sorted by LLmax: each class's tuples are a contiguous run
   for (int LL = 0; LL <= LMAXQ; ++LL) {
+    const size_t o0 = oi;
+    while (oi < order.size() && quartet_key(order[oi] / 125, (order[oi] / 25) % 5, (order[oi] / 5) % 5,
+                                            order[oi] % 5) / KEY_CLASS_DIV == (uint32_t)LL)
+      ++oi;
     int64_t c = 0;
-    for (int t = 0; t < 625; ++t) c += cnt[LL * 625 + t];
+    for (size_t j = o0; j < oi; ++j) c += cnt[LL * 625 + order[j]];
     if (c == 0) continue;
     if (P->ncls >= MAXCLS) return fail(THISTLE_ERR_ARG, "too many quartet classes");
     int k = P->ncls++;
@@ -165,27 +188,30 @@ int setup_classes(thistle_plan *P, const std::vector<int64_t> &cnt, int kind) {
     rs += rs & 1;
     P->cls_rs[k] = rs;
     P->cls_recoff[k] = recoff;
-    // sub-ranges in key order: (LK, XB) ascending
+    // sub-ranges in key order: (LK, XB) ascending, tuples ascending within
     P->cls_sub[k].clear();
     P->cls_tup[k].clear();
     int64_t sp = pos;
-    for (int LK = 0; LK <= 8; ++LK)
-      for (int XB = 0; XB <= 1; ++XB) {
-        int64_t sc = 0;
-        int nout = 0;
-        for (int t = 0; t < 625; ++t) {
-          const int Li = t / 125, Lj = (t / 25) % 5, Lk = (t / 5) % 5, Lr = t % 5;
-          const uint32_t key = quartet_key(Li, Lj, Lk, Lr);
-          if ((int)(key / KEY_CLASS_DIV) != LL || (int)((key / 625) % 18) != LK * 2 + XB) continue;
-          if (cnt[LL * 625 + t] == 0) continue;
-          P->cls_tup[k].push_back(TupleRange{t, sp + sc, sp + sc + cnt[LL * 625 + t]});
-          sc += cnt[LL * 625 + t];
-          // the outer side is the ket when LK is the bra's
-          nout = std::max(nout, XB ? maxg[Lk] * maxg[Lr] : maxg[Li] * maxg[Lj]);
-        }
-        if (sc > 0) P->cls_sub[k].push_back(SubRange{LK, XB, sp, sp + sc, nout});
-        sp += sc;
+    size_t j = o0;
+    while (j < oi) {
+      const int sub = (int)((quartet_key(order[j] / 125, (order[j] / 25) % 5, (order[j] / 5) % 5, order[j] % 5) /
+                             625) % 18);
+      int64_t sc = 0;
+      int nout = 0;
+      const int LK = sub / 2, XB = sub % 2;
+      for (; j < oi; ++j) {
+        const int t = order[j];
+        const int Li = t / 125, Lj = (t / 25) % 5, Lk = (t / 5) % 5, Lr = t % 5;
+        if ((int)((quartet_key(Li, Lj, Lk, Lr) / 625) % 18) != sub) break;
+        if (cnt[LL * 625 + t] == 0) continue;
+        P->cls_tup[k].push_back(TupleRange{t, sp + sc, sp + sc + cnt[LL * 625 + t]});
+        sc += cnt[LL * 625 + t];
+        // the outer side is the ket when LK is the bra's
+        nout = std::max(nout, XB ? maxg[Lk] * maxg[Lr] : maxg[Li] * maxg[Lj]);
       }
+      if (sc > 0) P->cls_sub[k].push_back(SubRange{LK, XB, sp, sp + sc, nout});
+      sp += sc;
+    }
     recoff += c * rs;
     pos += c;
   }
@@ -259,7 +285,7 @@ void plan_free(thistle_plan *P) {
   dfree(P->d_sort_tmp);
   if (P->have_ev) {
     for (int i = 0; i < 10; ++i) cudaEventDestroy(P->ev[i]);
-    for (int r = 0; r < thistle_plan::NRING; ++r)
+    for (int r = 0; r < P->rev_made; ++r)
       for (int i = 0; i < 5; ++i) cudaEventDestroy(P->rev[r][i]);
   }
   if (P->st && P->own_stream) cudaStreamDestroy(P->st);
@@ -345,6 +371,7 @@ int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga
   std::vector<int64_t> cnt;
   PhaseTrace tr;
   TB_TRY(check_basis(P, ngto, ga, l, m, n, xx, yy, zz, group));
+  tr.mark("basis checks");
   if (type == THISTLE_TOTAL_ALIGNED) {
     // q holds nq vectors, (3, nq) column-major like the reference's q_al
     if (!q || nq <= 0) { rc = fail(THISTLE_ERR_ARG, "empty q-vector list"); goto done; }
@@ -387,22 +414,31 @@ int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga
       rc = fail(THISTLE_ERR_ARG, "at most 215 MOs for the 2-RDM transform (norbs^4 must index in 32 bits)");
       goto done;
     }
-    for (int64_t i = 0; i < (int64_t)nmat * 4; ++i)
-      if (mat[i] < 1 || mat[i] > norbs) {
-        rc = fail(THISTLE_ERR_SHAPE, "2-RDM index out of range 1..norbs at row " + std::to_string(i % nmat + 1));
-        goto done;
+    {
+      // branch-free range pass; the offending row is looked up only on failure
+      int32_t lo = 1, hi = 1;
+      for (int64_t i = 0; i < (int64_t)nmat * 4; ++i) {
+        lo = std::min(lo, mat[i]);
+        hi = std::max(hi, mat[i]);
       }
+      if (lo < 1 || hi > norbs)
+        for (int64_t i = 0; i < (int64_t)nmat * 4; ++i)
+          if (mat[i] < 1 || mat[i] > norbs) {
+            rc = fail(THISTLE_ERR_SHAPE, "2-RDM index out of range 1..norbs at row " + std::to_string(i % nmat + 1));
+            goto done;
+          }
+    }
     if (nmat > 0 && !finite_all(total, nmat)) { rc = fail(THISTLE_ERR_NONFINITE, "non-finite 2-RDM value"); goto done; }
     P->nmat = nmat;
   }
+  tr.mark("density input checks");
   class_counts(P->gL, cnt, P->kind == KIND_CMS);
+  tr.mark("class counts");
   TB_TRY(setup_classes(P, cnt, P->kind));
-  tr.mark("validation, classes");
+  tr.mark("classes");
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
   for (int i = 0; i < 10; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
-  for (int r = 0; r < thistle_plan::NRING; ++r)
-    for (int i = 0; i < 5; ++i) TB_TRYC(cudaEventCreate(&P->rev[r][i]));
-  P->have_ev = true;
+  P->have_ev = true;  // the ring's stage events are made as executions reach their slots
   tr.mark("stream, events");
   TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
@@ -556,8 +592,14 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
                       const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom,
                       const std::vector<TupleRange> *tups) {
-  // stage events (not while a graph is being captured)
-  cudaEvent_t *E = P->rev[P->ring_next % thistle_plan::NRING];
+  // stage events (not while a graph is being captured); a ring slot's events
+  // are made the first time an execution reaches it
+  const int slot = (int)(P->ring_next % thistle_plan::NRING);
+  if (!P->capturing && slot >= P->rev_made) {
+    for (int i = 0; i < 5; ++i) TB_CK(cudaEventCreate(&P->rev[slot][i]));
+    P->rev_made = slot + 1;
+  }
+  cudaEvent_t *E = P->rev[slot];
   auto mark = [&](int i) -> cudaError_t { return P->capturing ? cudaSuccess : cudaEventRecord(E[i], P->st); };
   if (!P->capturing) P->ring_next += 1;
   TB_CK(mark(0));

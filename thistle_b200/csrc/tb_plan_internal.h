@@ -138,6 +138,7 @@ struct thistle_plan {
   // per-execution stage events: slot = execution index mod NRING
   static const int NRING = 64;
   cudaEvent_t rev[64][5];
+  int rev_made = 0;  // slots 0 .. rev_made-1 hold events (made as executions first reach them)
   int64_t ring_next = 0, ring_base = 0;
   bool have_ev = false;
   float ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
