@@ -425,9 +425,12 @@ def batch4_section(nmol, chunk, gb, reps_arg):
     fit the device; per chunk every molecule gets its plan (density transform,
     quartet list), then the chunk's I(q) is computed twice: once plan by plan
     (the plain GPU path, one integrator call per molecule) and once as a
-    molecule batch (one launch per stage and class, replayed from a CUDA
-    graph).  Both integrator paths start from the same plans and copy I(q) to
-    host memory; set-up time is reported separately."""
+    molecule batch (stage 2 one persistent launch over every (molecule,
+    class, block) item, the other stages one launch per kernel shape,
+    replayed from a CUDA graph) at the stage-2 pair tile the batch tuner
+    picks for the chunk.  Both integrator paths start from the same plans and
+    copy I(q) to host memory; set-up and tuning time are reported
+    separately."""
     import torch
     from thistle_b200 import _abi
     from thistle_b200 import inputs as I
@@ -440,7 +443,7 @@ def batch4_section(nmol, chunk, gb, reps_arg):
     budget = gb * 1e9
     t_setup = t_plain = t_batch = 0.0
     qq = 0
-    nchunks, launches, err = 0, [], 0.0
+    nchunks, launches, tiles, err, t_tune = 0, [], [], 0.0, 0.0
     i = 0
     while i < len(mols):
         plans = []
@@ -463,9 +466,13 @@ def batch4_section(nmol, chunk, gb, reps_arg):
         t0 = time.perf_counter()
         singles = [pl.execute() for pl in plans]
         t_plain += time.perf_counter() - t0
-        # batched: every molecule of the chunk in one launch per stage and class
+        # batched: stage 2 of every molecule of the chunk in one persistent launch
         with MC.MoleculeBatch(plans) as b:
             b.use_graph(True)
+            t0 = time.perf_counter()
+            k, nw, _ = b.autotune()
+            t_tune += time.perf_counter() - t0
+            tiles.append([k, nw])
             for _ in range(2):
                 b.execute()
             torch.cuda.synchronize()
@@ -490,7 +497,8 @@ def batch4_section(nmol, chunk, gb, reps_arg):
         "plain_molecules_per_s": n / t_plain, "batched_over_plain": t_plain / t_batch,
         "quartet_q_per_s_batched": qq / t_batch, "quartet_q_per_s_plain": qq / t_plain,
         "setup_s_per_molecule": t_setup / n, "input_generation_s": t_gen,
-        "kernel_launches_per_chunk": launches[:4], "check_vs_plain_max_rel": err,
+        "kernel_launches_per_chunk": launches[:4], "stage2_tile_per_chunk": tiles[:4],
+        "tune_s_per_chunk": t_tune / max(1, nchunks), "check_vs_plain_max_rel": err,
         "path": "integrator only, from plans already built; host I(q) out (MoleculeBatch.execute vs "
                 "ScatteringPlan.execute per molecule)",
     }

@@ -23,7 +23,7 @@ extern "C" {
 #define THISTLE_ERR_SHAPE -2      /* inconsistent group / index layout */
 #define THISTLE_ERR_ANGMOM -3     /* l, m or n above 4 (g), or LLmax beyond the Bessel tables */
 #define THISTLE_ERR_NONFINITE -4  /* NaN or Inf in an input array */
-#define THISTLE_ERR_CUDA -5       /* CUDA runtime, cuBLAS or kernel failure */
+#define THISTLE_ERR_CUDA -5       /* CUDA runtime or kernel failure */
 #define THISTLE_ERR_NOMEM -6      /* device allocation failed */
 #define THISTLE_ERR_TYPE -7       /* calculation type not provided */
 #define THISTLE_ERR_Q -8          /* q <= 0 (the reference divides by q; drivers use 1e-10 for 0) */
@@ -167,8 +167,11 @@ int thistle_plan_vjp_device(thistle_plan *plan, const double *v_dev, double *gra
  * CUDA graph (forward, and the adjoint stages) and replay it; the graph is
  * dropped when the batch size changes.
  * autotune_batch times forward + adjoint per geometry for ngeom = 1, 2, 4, ..
- * <= gmax and two stage-2 q tiles, keeps the fastest (ngeom, q tile) in the
- * plan and reports it with its geometries per second.
+ * <= gmax and two stage-2 q tiles, then the four stage-2 pair tiles at the
+ * best of those, keeps the fastest (ngeom, q tile, pair tile) in the plan
+ * and reports it with its geometries per second (stage2_tile reads the pair
+ * tile).  set_stage2_tile sets the pair tile: quartets per lane 1 or 2,
+ * warps per block 4 or 8 (default 2 x 4); aligned plans have none.
  */
 int thistle_plan_set_batch(thistle_plan *plan, int32_t ngeom);
 int thistle_plan_set_centres_batch(thistle_plan *plan, const double *xyz);
@@ -184,6 +187,8 @@ int thistle_plan_vjp_batch_device(thistle_plan *plan, const double *v_dev, doubl
 int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);
 int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom_best, int32_t *qtile_best,
                                 double *geoms_per_s);
+int thistle_plan_set_stage2_tile(thistle_plan *plan, int32_t quartets_per_lane, int32_t warps_per_block);
+int thistle_plan_stage2_tile(const thistle_plan *plan, int32_t *quartets_per_lane, int32_t *warps_per_block);
 /*
  * Nuclear-electron term of an elastic plan (type 2) for its current centres:
  * ine_host[q] = sum_a Zn_a sum over ordered group pairs (i,k) of the pair's
@@ -212,14 +217,22 @@ int thistle_elastic_aligned_grid(int32_t nq, double *q_al);
 /*
  * Molecule batches (no reference counterpart).  Several plans -- any bases,
  * one geometry each, the same calculation type, nq <= 1024 -- executed
- * together: pair tables, stage 1 per class, stage 2 per class and the
- * reductions each run as one launch over every plan, its blocks spread over
- * the plans in proportion to their work.  batch_create runs every plan once
- * (records and stage-2 visiting order) and builds the launch tables; the
- * plans must outlive the batch and keep their stream.  execute writes the
- * plans' I(q) one after the other (sum of their nq doubles).  use_graph
- * captures the launches once in a CUDA graph and replays it.  info: [0]
- * plans, [1] total q points, [2] kernels launched by the last execution.
+ * together: the pair tables and the reductions run as one launch over every
+ * plan, stage 1 as one launch per kernel shape, and stage 2 as ONE
+ * persistent launch whose resident blocks take (plan, class, block) work
+ * items from an atomic counter, heaviest Bessel order first; each item
+ * writes its own partial rows, so results do not depend on the schedule.
+ * batch_create runs every plan once (records and stage-2 visiting order)
+ * and builds the launch tables; the plans must outlive the batch and keep
+ * their stream.  execute writes the plans' I(q) one after the other (sum of
+ * their nq doubles).  use_graph captures the launches once in a CUDA graph
+ * and replays it.  info: [0] plans, [1] total q points, [2] kernels
+ * launched by the last execution.
+ * set_stage2_tile picks the stage-2 pair tile (quartets per lane 1 or 2,
+ * warps per block 4 or 8; default 2 x 4) and stage2_tile reads it; autotune
+ * times the batch at the four tiles, keeps the fastest and reports it with
+ * its molecules per second.  The plan functions of the same names do this
+ * for one plan (thistle_plan_autotune_batch tunes the tile too).
  */
 typedef struct thistle_batch thistle_batch;
 int thistle_batch_create(thistle_batch **batch, thistle_plan *const *plans, int32_t nplans);
@@ -227,6 +240,10 @@ int thistle_batch_use_graph(thistle_batch *batch, int32_t enable);
 int thistle_batch_execute(thistle_batch *batch, double *result_host);
 int thistle_batch_execute_device(thistle_batch *batch, double *result_dev);
 int thistle_batch_info(const thistle_batch *batch, int64_t *info);
+int thistle_batch_set_stage2_tile(thistle_batch *batch, int32_t quartets_per_lane, int32_t warps_per_block);
+int thistle_batch_stage2_tile(const thistle_batch *batch, int32_t *quartets_per_lane, int32_t *warps_per_block);
+int thistle_batch_autotune(thistle_batch *batch, int32_t *quartets_per_lane, int32_t *warps_per_block,
+                           double *molecules_per_s);
 int thistle_batch_destroy(thistle_batch *batch);
 /* The 3131 aligned q vectors of the reference (QCOORD3,
  * src/main_calculation.f90:864-929) for beam wavevector k0, written as a

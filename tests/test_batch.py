@@ -67,8 +67,31 @@ def test_autotune_picks_a_batch():
         pl.use_graph(True)
         g, qt, gps = pl.autotune_batch(8)
         assert g in (1, 2, 4, 8) and gps > 0 and 64 <= qt <= p.nq
+        assert pl.stage2_tile() in ((2, 4), (2, 8), (1, 4), (1, 8))
         probs = _geometries(p, g, seed=9)
         pl.set_centres_batch(_xyz(probs))
         out = pl.execute_batch()
     ref = MC.scattering(probs[-1], 1)
     assert _rel(out[-1], ref) < 1e-12
+
+
+@pytest.mark.parametrize("kind", [MC.TOTAL_J0, MC.TOTAL_J2])
+def test_stage2_pair_tiles_agree(kind):
+    """Every stage-2 pair tile (quartets per lane x warps per block) sums the
+    same quartets at the same points: results agree to rounding, and each
+    tile is reproducible run to run.  The 3-atom s/p/d case has polynomial
+    orders (LB <= 8) and, for j2, recurrence orders (9, 10)."""
+    p = I.config3_ab6(nq=200, natoms=3)
+    with MC.ScatteringPlan.from_problem(p, kind) as pl:
+        assert pl.stage2_tile() == (2, 4)
+        ref = pl.execute()
+        for k, nw in ((2, 8), (1, 4), (1, 8), (2, 4)):
+            pl.set_stage2_tile(k, nw)
+            assert pl.stage2_tile() == (k, nw)
+            a = pl.execute()
+            assert _rel(a, ref) < 1e-13
+            assert np.array_equal(a, pl.execute())
+        with pytest.raises(MC.ThistleError):
+            pl.set_stage2_tile(3, 4)
+        with pytest.raises(MC.ThistleError):
+            pl.set_stage2_tile(2, 6)

@@ -1,6 +1,8 @@
 """Molecule batches: plans of different molecules and basis sizes executed
-together, one launch per stage and class over all of them (optionally
-replayed from a CUDA graph), against each plan executed on its own."""
+together -- stage 2 as one persistent launch over every (plan, class, block)
+item, the other stages one launch per kernel shape (optionally replayed from
+a CUDA graph) -- against each plan executed on its own, at every stage-2
+pair tile, and the batch tuner."""
 import numpy as np
 import pytest
 
@@ -73,3 +75,41 @@ def test_batch_rejects_mixed_types(molecules):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("tile", [(2, 8), (1, 4), (1, 8)])
+def test_batch_pair_tiles(molecules, tile):
+    plans = [MC.ScatteringPlan.from_problem(m, MC.TOTAL_J2) for m in molecules]
+    try:
+        singles = [p.execute() for p in plans]
+        with MC.MoleculeBatch(plans) as b:
+            b.use_graph(True)
+            b.set_stage2_tile(*tile)
+            assert b.stage2_tile() == tile
+            out = b.execute()
+            again = b.execute()
+        for o, s, a in zip(out, singles, again):
+            assert _rel(o, s) < 1e-12
+            assert np.array_equal(o, a)
+    finally:
+        for p in plans:
+            p.close()
+
+
+def test_batch_autotune(molecules):
+    plans = [MC.ScatteringPlan.from_problem(m, MC.TOTAL_J0) for m in molecules]
+    try:
+        singles = [p.execute() for p in plans]
+        with MC.MoleculeBatch(plans) as b:
+            b.use_graph(True)
+            k, nw, mps = b.autotune()
+            assert (k, nw) in ((2, 4), (2, 8), (1, 4), (1, 8)) and mps > 0
+            assert b.stage2_tile() == (k, nw)
+            out = b.execute()
+            with pytest.raises(MC.ThistleError):
+                b.set_stage2_tile(1, 5)
+        for o, s in zip(out, singles):
+            assert _rel(o, s) < 1e-12
+    finally:
+        for p in plans:
+            p.close()

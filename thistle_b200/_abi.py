@@ -33,7 +33,8 @@ EXPORTS = sorted([
     "thistle_plan_autotune_batch", "thistle_batch_create", "thistle_batch_use_graph", "thistle_batch_execute",
     "thistle_batch_execute_device", "thistle_batch_info", "thistle_batch_destroy", "thistle_plan_nuclear",
     "thistle_plan_density", "thistle_plan_form_factor", "thistle_elastic_aligned_grid",
-    "thistle_plan_set_centres_batch_device",
+    "thistle_plan_set_centres_batch_device", "thistle_plan_set_stage2_tile", "thistle_plan_stage2_tile",
+    "thistle_batch_set_stage2_tile", "thistle_batch_stage2_tile", "thistle_batch_autotune",
 ])
 
 
@@ -111,7 +112,12 @@ def lib():
                        ("thistle_batch_create", [C.POINTER(VP), C.POINTER(VP), C.c_int32]),
                        ("thistle_batch_use_graph", [VP, C.c_int32]), ("thistle_batch_execute", [VP, D]),
                        ("thistle_batch_execute_device", [VP, VP]), ("thistle_batch_info", [VP, I64]),
-                       ("thistle_batch_destroy", [VP]), ("thistle_plan_nuclear", [VP, D, D, C.c_int32, D])):
+                       ("thistle_batch_destroy", [VP]), ("thistle_plan_nuclear", [VP, D, D, C.c_int32, D]),
+                       ("thistle_plan_set_stage2_tile", [VP, C.c_int32, C.c_int32]),
+                       ("thistle_plan_stage2_tile", [VP, I32, I32]),
+                       ("thistle_batch_set_stage2_tile", [VP, C.c_int32, C.c_int32]),
+                       ("thistle_batch_stage2_tile", [VP, I32, I32]),
+                       ("thistle_batch_autotune", [VP, I32, I32, D])):
         getattr(L, name).restype = C.c_int
         getattr(L, name).argtypes = args
     L.thistle_qcoord3.restype = C.c_int

@@ -90,11 +90,12 @@ int nuclear_term(thistle_plan *P, const double *Zn, const double *geom, int nato
         s.dq = dq;
         s.chunk = 0;
         s.j2 = false;
+        s.lb = L;
         s.partial = P->d_partial + q0;
         s.pstride = P->nq;
-        const int64_t per_block = (int64_t)stage2_quartets_per_warp(L) * STAGE2_WARPS;
+        const int64_t per_block = (int64_t)stage2_quartets_per_warp(L, P->s2_tile) * P->s2_tile.nw;
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nL + per_block - 1) / per_block, P->s2_rows));
-        TB_TRYC(launch_stage2_class(L, s, grid, 1, P->st));
+        TB_TRYC(launch_stage2_class(L, s, grid, 1, P->s2_tile, P->st));
       }
     }
     TB_TRYC(launch_reduce_batch(P->d_partial, P->s2_rows, P->nq, (int64_t)P->s2_rows * P->nq, d_out, 1, P->st));

@@ -77,22 +77,35 @@ struct Stage2ClassArgs {
   double dq;
   int chunk;                  // q points per work item (multiple of 64), 0 = the whole tile
   int j2;                     // Bessel records are j2 (F / q^2)
+  int lb;                     // Bessel order (read by the persistent molecule-batch kernel)
   double *partial;            // gridDim.x rows of pstride doubles, accumulated (+=)
   int64_t pstride;
   int64_t gs_rec, gs_partial; // per-geometry strides (blockIdx.y is the geometry)
 };
-#ifndef TB_S2_WARPS
-#define TB_S2_WARPS 4
-#endif
-constexpr int STAGE2_WARPS = TB_S2_WARPS;
+// Stage-2 pair tile: quartets per lane k (1 or 2; orders above 8 always use
+// 1) and warps per block nw (4 or 8).  Every shape sums the same quartets at
+// the same points; only the order of the floating-point additions differs.
+struct Stage2Tile {
+  int k = 2;
+  int nw = 4;
+};
+constexpr int STAGE2_MAXWARPS = 8;
 // q points a stage-2 block holds in shared memory at once
 constexpr int STAGE2_QTILE = 1024;
-int stage2_quartets_per_warp(int LB);
-int stage2_class_blocks_per_sm(int LB, bool j2, int nq);
-cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st);
-// molecule batches: n items (device descriptors d), item i's blocks pre[i] .. pre[i+1]-1
-cudaError_t launch_stage2_class_batch(int LB, bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n,
-                                      int64_t blocks, int nqmax, cudaStream_t st);
+bool stage2_tile_valid(Stage2Tile t);
+int stage2_quartets_per_warp(int LB, Stage2Tile t);
+int stage2_class_blocks_per_sm(int LB, bool j2, int nq, Stage2Tile t);
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, Stage2Tile t,
+                                cudaStream_t st);
+// Molecule batches: ONE persistent launch over every (plan, class, block)
+// item.  Item i (descriptor d[i], Bessel order d[i].lb) owns the virtual
+// blocks pre[i] .. pre[i+1]-1; resident blocks take virtual blocks from the
+// atomic counter *next (zero before the launch) until all `blocks` are done,
+// so no block waits on another.  Each virtual block writes its own partial
+// row, which keeps the result independent of the schedule.
+int stage2_persistent_blocks_per_sm(bool j2, int nqmax, Stage2Tile t);
+cudaError_t launch_stage2_persistent(bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n, int64_t blocks,
+                                     int nqmax, int grid, Stage2Tile t, unsigned long long *next, cudaStream_t st);
 
 // Aligned intensity of one LLmax class on q vectors (tb_aligned.cu).
 struct AlignedArgs {

@@ -1,16 +1,15 @@
-// Molecule batches: several plans (any bases) run as one launch per stage and
-// class over descriptor tables, optionally replayed from a CUDA graph.
+// Molecule batches: several plans (any bases) run over descriptor tables,
+// optionally replayed from a CUDA graph.  Stage 1 is one launch per kernel
+// shape (L, LK, XB); stage 2, the dominant stage, is ONE persistent launch
+// over every (plan, class, block) item of the batch.
 #include "tb_plan_internal.h"
 
 using namespace tb;
 
-// ---------------------------------------------------------------------------
-// molecule batches: several plans (any bases), one launch per stage and class
-// ---------------------------------------------------------------------------
 struct thistle_batch {
   std::vector<thistle_plan *> plans;
   cudaStream_t st = nullptr;
-  int kind = 0, nqmax = 0, rows = 64;  // partial rows per plan: a class's blocks in one launch
+  int kind = 0, nqmax = 0;
   int64_t nq_total = 0;
   std::vector<int64_t> out_off;
   PairDesc *d_pair = nullptr;
@@ -22,13 +21,14 @@ struct thistle_batch {
     bool split;            // contraction kernel + convolution kernel through d_xbuf
     int64_t *prexc, blocksxc;
   };
-  struct S2 {
-    int LB, n;
-    Stage2ClassArgs *d;
-    int64_t *pre, blocks;
-  };
   std::vector<S1> s1;
-  std::vector<S2> s2;
+  // stage 2: items (plan, class) heaviest Bessel order first, item i owning
+  // virtual blocks s2_pre[i] .. s2_pre[i+1]-1, each with its own partial row
+  Stage2Tile tile;
+  Stage2ClassArgs *d_s2 = nullptr;
+  int64_t *d_s2pre = nullptr, s2_blocks = 0;
+  int n_s2 = 0, s2_grid = 0;
+  unsigned long long *d_next = nullptr;  // the persistent launch's work counter
   ReduceDesc *d_red = nullptr;
   double *d_partial = nullptr, *d_out = nullptr, *d_xbuf = nullptr;
   int64_t partial_len = 0;
@@ -42,7 +42,7 @@ void batch_free(thistle_batch *B) {
   dfree(B->d_pair); dfree(B->d_pair_pre); dfree(B->d_red); dfree(B->d_partial); dfree(B->d_out);
   for (auto &x : B->s1) { dfree(x.d); dfree(x.pre); dfree(x.prexc); }
   dfree(B->d_xbuf);
-  for (auto &x : B->s2) { dfree(x.d); dfree(x.pre); }
+  dfree(B->d_s2); dfree(B->d_s2pre); dfree(B->d_next);
   if (B->gx) cudaGraphExecDestroy(B->gx);
   delete B;
 }
@@ -71,10 +71,10 @@ int batch_run(thistle_batch *B) {
     }
   }
   TB_CK(cudaMemsetAsync(B->d_partial, 0, sizeof(double) * B->partial_len, st));
-  for (auto &x : B->s2) {
-    TB_CK(launch_stage2_class_batch(x.LB, kind_j2(B->kind), x.d, x.pre, x.n, x.blocks, B->nqmax, st));
-    B->launches += 1;
-  }
+  TB_CK(cudaMemsetAsync(B->d_next, 0, sizeof(unsigned long long), st));
+  TB_CK(launch_stage2_persistent(kind_j2(B->kind), B->d_s2, B->d_s2pre, B->n_s2, B->s2_blocks, B->nqmax, B->s2_grid,
+                                 B->tile, B->d_next, st));
+  B->launches += 1;
   TB_CK(launch_reduce_desc(B->d_red, (int)B->plans.size(), B->nqmax, st));
   B->launches += 1;
   return THISTLE_OK;
@@ -109,6 +109,95 @@ int batch_exec(thistle_batch *B) {
   return rc;
 }
 
+// Stage-2 items of the batch for its pair tile: every (plan, class) with
+// quartets, heaviest Bessel order first (the persistent launch's tail is then
+// light work), each with up to one GPU's worth of virtual blocks.  A virtual
+// block adds into its own partial row of its plan, so the partial rows of a
+// plan are the sum of its items' virtual blocks, and the reduction over them
+// does not depend on which resident block ran which virtual block.
+static int batch_stage2_setup(thistle_batch *B) {
+  int rc = THISTLE_OK;
+  const int n = (int)B->plans.size();
+  const bool j2 = kind_j2(B->kind);
+  dfree(B->d_s2); dfree(B->d_s2pre); dfree(B->d_red); dfree(B->d_partial);
+  B->d_s2 = nullptr;
+  B->d_s2pre = nullptr;
+  B->d_red = nullptr;
+  B->d_partial = nullptr;
+  const int nsm = B->plans[0]->nsm;
+  const int bps = stage2_persistent_blocks_per_sm(j2, B->nqmax, B->tile);
+  const int64_t cap = (int64_t)nsm * bps;
+  struct Item {
+    int LB, plan;
+    int64_t row, vg;
+    Stage2ClassArgs s;
+  };
+  std::vector<Item> items;
+  std::vector<int64_t> prow(n, 0);
+  for (int i = 0; i < n; ++i) {
+    thistle_plan *P = B->plans[i];
+    int uniform = 0, first_on_grid = 0;
+    double dq = 0.0;
+    grid_info(P->hq.data(), P->nq, uniform, first_on_grid, dq);
+    for (int c = 0; c < P->ncls; ++c) {
+      const int LB = P->cls_L[c] + (j2 ? 2 : 0);
+      Stage2ClassArgs s;
+      s.rec = P->d_rec + P->cls_recoff[c];
+      s.rs = P->cls_rs[c];
+      s.nquart = P->cls_end[c] - P->cls_begin[c];
+      s.perm = P->d_perm;
+      s.pbase = P->cls_begin[c];
+      s.q = P->d_q;
+      s.nq = P->nq;
+      s.uniform = uniform;
+      s.first_on_grid = first_on_grid;
+      s.dq = dq;
+      s.chunk = 0;
+      s.j2 = j2;
+      s.lb = LB;
+      s.pstride = P->nq;
+      s.gs_rec = 0;
+      s.gs_partial = 0;
+      const int64_t per = (int64_t)stage2_quartets_per_warp(LB, B->tile) * B->tile.nw;
+      const int64_t vg = std::min<int64_t>(cap, (s.nquart + per - 1) / per);
+      if (vg <= 0) continue;
+      items.push_back(Item{LB, i, prow[i], vg, s});
+      prow[i] += vg;
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.LB > y.LB; });
+  std::vector<int64_t> poff(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    prow[i] = std::max<int64_t>(prow[i], 1);  // a plan without quartets still reduces one zero row
+    poff[i + 1] = poff[i] + prow[i] * B->plans[i]->nq;
+  }
+  B->partial_len = poff[n];
+  TB_TRY(dalloc(&B->d_partial, (size_t)std::max<int64_t>(B->partial_len, 1), "batch partial sums"));
+  {
+    std::vector<ReduceDesc> rd;
+    for (int i = 0; i < n; ++i)
+      rd.push_back(ReduceDesc{B->d_partial + poff[i], (int)prow[i], B->plans[i]->nq, B->d_out + B->out_off[i]});
+    std::vector<Stage2ClassArgs> d;
+    std::vector<int64_t> pre(1, 0);
+    for (Item &it : items) {
+      it.s.partial = B->d_partial + poff[it.plan] + it.row * B->plans[it.plan]->nq;
+      d.push_back(it.s);
+      pre.push_back(pre.back() + it.vg);
+    }
+    B->n_s2 = (int)d.size();
+    B->s2_blocks = pre.back();
+    B->s2_grid = (int)std::max<int64_t>(1, std::min<int64_t>(cap, B->s2_blocks));
+    TB_TRY(upload_vec(&B->d_red, rd, B->st, "batch reduce descriptors"));
+    if (!d.empty()) {
+      TB_TRY(upload_vec(&B->d_s2, d, B->st, "batch stage-2 descriptors"));
+      TB_TRY(upload_vec(&B->d_s2pre, pre, B->st, "batch stage-2 prefix"));
+    }
+    TB_TRYC(cudaStreamSynchronize(B->st));
+  }
+done:
+  return rc;
+}
+
 int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
   if (!out || !plans || n < 1) return fail(THISTLE_ERR_ARG, "need at least one plan");
   *out = nullptr;
@@ -134,33 +223,20 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
     }
     std::vector<PairDesc> pd;
     std::vector<int64_t> ppre(1, 0);
-    std::vector<ReduceDesc> rd;
-    int64_t poff = 0, ooff = 0;
+    int64_t ooff = 0;
     for (thistle_plan *P : B->plans) {
       pd.push_back(PairDesc{P->ng, P->maxa, P->d_gstart, P->d_flmn, P->d_ga, P->d_xyz, P->d_pairtab, P->d_esoa});
       ppre.push_back(ppre.back() + (npairs(P->ng) + 127) / 128);
       B->nqmax = std::max(B->nqmax, P->nq);
       B->out_off.push_back(ooff);
-      rd.push_back(ReduceDesc{nullptr, B->rows, P->nq, nullptr});  // pointers below
-      poff += (int64_t)B->rows * P->nq;
       ooff += P->nq;
     }
-    B->partial_len = poff;
     B->nq_total = ooff;
-    TB_TRY(dalloc(&B->d_partial, (size_t)std::max<int64_t>(poff, 1), "batch partial sums"));
     TB_TRY(dalloc(&B->d_out, (size_t)std::max<int64_t>(ooff, 1), "batch results"));
-    std::vector<double *> part(n);
-    poff = 0;
-    for (int i = 0; i < n; ++i) {
-      part[i] = B->d_partial + poff;
-      rd[i].partial = part[i];
-      rd[i].out = B->d_out + B->out_off[i];
-      poff += (int64_t)B->rows * plans[i]->nq;
-    }
+    TB_TRY(dalloc(&B->d_next, 1, "batch work counter"));
     B->pair_blocks = ppre.back();
     TB_TRY(upload_vec(&B->d_pair, pd, B->st, "batch pair descriptors"));
     TB_TRY(upload_vec(&B->d_pair_pre, ppre, B->st, "batch pair prefix"));
-    TB_TRY(upload_vec(&B->d_red, rd, B->st, "batch reduce descriptors"));
     // stage 1: items grouped by (L, LK, XB); the kernel choice per L counts
     // the quartets of every plan
     int64_t ltot[LMAXQ + 1] = {0};
@@ -231,57 +307,7 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
       i = j;
     }
     if (xneed > 0) TB_TRY(dalloc(&B->d_xbuf, (size_t)xneed, "batch contraction buffer"));
-    // stage 2: items grouped by Bessel order
-    std::vector<std::pair<int, std::pair<Stage2ClassArgs, int64_t>>> s2items;
-    for (int i = 0; i < n; ++i) {
-      thistle_plan *P = plans[i];
-      int uniform = 0, first_on_grid = 0;
-      double dq = 0.0;
-      grid_info(P->hq.data(), P->nq, uniform, first_on_grid, dq);
-      for (int c = 0; c < P->ncls; ++c) {
-        const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
-        Stage2ClassArgs s;
-        s.rec = P->d_rec + P->cls_recoff[c];
-        s.rs = P->cls_rs[c];
-        s.nquart = P->cls_end[c] - P->cls_begin[c];
-        s.perm = P->d_perm;
-        s.pbase = P->cls_begin[c];
-        s.q = P->d_q;
-        s.nq = P->nq;
-        s.uniform = uniform;
-        s.first_on_grid = first_on_grid;
-        s.dq = dq;
-        s.chunk = 0;
-        s.j2 = kind_j2(P->kind);
-        s.partial = part[i];
-        s.pstride = P->nq;
-        s.gs_rec = 0;
-        s.gs_partial = 0;
-        // one block per STAGE2_WARPS batches of quartets, at most `rows`
-        // (the other plans of the launch fill the GPU)
-        const int64_t per = (int64_t)stage2_quartets_per_warp(LB) * STAGE2_WARPS;
-        const int64_t vg = std::min<int64_t>(B->rows, (s.nquart + per - 1) / per);
-        if (vg <= 0) continue;
-        s2items.push_back({LB, {s, vg}});
-      }
-    }
-    std::stable_sort(s2items.begin(), s2items.end(),
-                     [](const auto &x, const auto &y) { return x.first < y.first; });
-    for (size_t i = 0; i < s2items.size();) {
-      size_t j = i;
-      std::vector<Stage2ClassArgs> d;
-      std::vector<int64_t> pre(1, 0);
-      while (j < s2items.size() && s2items[j].first == s2items[i].first) {
-        d.push_back(s2items[j].second.first);
-        pre.push_back(pre.back() + s2items[j].second.second);
-        ++j;
-      }
-      thistle_batch::S2 x{s2items[i].first, (int)d.size(), nullptr, nullptr, pre.back()};
-      TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-2 descriptors"));
-      TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-2 prefix"));
-      B->s2.push_back(x);
-      i = j;
-    }
+    TB_TRY(batch_stage2_setup(B));
     TB_TRYC(cudaStreamSynchronize(B->st));
   }
 done:
@@ -325,6 +351,63 @@ int thistle_batch_execute(thistle_batch *B, double *result_host) {
   if (rc != THISTLE_OK) return rc;
   TB_CK(cudaMemcpyAsync(result_host, B->d_out, sizeof(double) * B->nq_total, cudaMemcpyDeviceToHost, B->st));
   TB_CK(cudaStreamSynchronize(B->st));
+  return THISTLE_OK;
+}
+
+int thistle_batch_set_stage2_tile(thistle_batch *B, int32_t quartets_per_lane, int32_t warps_per_block) {
+  if (!B) return fail(THISTLE_ERR_ARG, "null batch");
+  const Stage2Tile t{quartets_per_lane, warps_per_block};
+  if (!stage2_tile_valid(t)) return fail(THISTLE_ERR_ARG, "stage-2 tile: quartets per lane 1 or 2, warps 4 or 8");
+  if (t.k == B->tile.k && t.nw == B->tile.nw) return THISTLE_OK;
+  TB_CK(cudaStreamSynchronize(B->st));
+  if (B->gx) cudaGraphExecDestroy(B->gx);
+  B->gx = nullptr;
+  B->tile = t;
+  return batch_stage2_setup(B);
+}
+
+int thistle_batch_stage2_tile(const thistle_batch *B, int32_t *quartets_per_lane, int32_t *warps_per_block) {
+  if (!B || !quartets_per_lane || !warps_per_block) return fail(THISTLE_ERR_ARG, "null argument");
+  *quartets_per_lane = B->tile.k;
+  *warps_per_block = B->tile.nw;
+  return THISTLE_OK;
+}
+
+int thistle_batch_autotune(thistle_batch *B, int32_t *quartets_per_lane, int32_t *warps_per_block,
+                           double *molecules_per_s) {
+  if (!B || !quartets_per_lane || !warps_per_block || !molecules_per_s) return fail(THISTLE_ERR_ARG, "null argument");
+  const Stage2Tile tiles[4] = {{2, 4}, {2, 8}, {1, 4}, {1, 8}};
+  const int reps = 3;
+  double best = -1.0;
+  Stage2Tile bestT = B->tile;
+  cudaEvent_t e0, e1;
+  TB_CK(cudaEventCreate(&e0));
+  TB_CK(cudaEventCreate(&e1));
+  int rc = THISTLE_OK;
+  for (int t = 0; t < 4 && rc == THISTLE_OK; ++t) {
+    rc = thistle_batch_set_stage2_tile(B, tiles[t].k, tiles[t].nw);
+    for (int w = 0; w < 2 + reps && rc == THISTLE_OK; ++w) {
+      if (w == 2 && cudaEventRecord(e0, B->st) != cudaSuccess) rc = fail(THISTLE_ERR_CUDA, "event record");
+      if (rc == THISTLE_OK) rc = batch_exec(B);
+    }
+    float ms = 0;
+    if (rc == THISTLE_OK && (cudaEventRecord(e1, B->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                             cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      rc = fail(THISTLE_ERR_CUDA, "batch autotune timing");
+    const double mps = ms > 0 ? B->plans.size() * reps / (ms * 1e-3) : 0.0;
+    if (rc == THISTLE_OK && mps > best) {
+      best = mps;
+      bestT = tiles[t];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != THISTLE_OK) return rc;
+  rc = thistle_batch_set_stage2_tile(B, bestT.k, bestT.nw);
+  if (rc != THISTLE_OK) return rc;
+  *quartets_per_lane = bestT.k;
+  *warps_per_block = bestT.nw;
+  *molecules_per_s = best;
   return THISTLE_OK;
 }
 

@@ -352,6 +352,23 @@ int upload_centres_batch(thistle_plan *P, const double *xyz) {
   return THISTLE_OK;
 }
 
+// Resident stage-2 blocks per SM of every class for the plan's q tile and
+// pair tile, and the partial-row count (one row per resident block).  The
+// aligned kernel instead takes quartet slices, one partial row each.
+void stage2_layout(thistle_plan *P) {
+  int maxbps = 1;
+  for (int b = 0; b <= LMAXB; ++b) P->s2_bps[b] = 0;
+  for (int c = 0; c < P->ncls && P->kind != KIND_ALIGNED; ++c) {
+    const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
+    P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, kind_j2(P->kind), P->s2_qtile, P->s2_tile);
+    maxbps = std::max(maxbps, P->s2_bps[LB]);
+  }
+  if (P->kind == KIND_ALIGNED)
+    P->s2_rows = std::min(std::max(1, 4 * P->nsm / std::max(1, (P->nq + 127) / 128)), 4 * P->nsm);
+  else
+    P->s2_rows = P->nsm * maxbps;
+}
+
 int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga, const int32_t *l,
                        const int32_t *m, const int32_t *n, const double *xx, const double *yy, const double *zz,
                        const int32_t *group, const double *mmod, int32_t norbs, const int32_t *mat,
@@ -466,16 +483,7 @@ int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga
     TB_TRYC(cudaGetDevice(&dev));
     TB_TRYC(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
     P->s2_qtile = std::min(nq, STAGE2_QTILE);
-    int maxbps = 1;
-    for (int b = 0; b <= LMAXB; ++b) P->s2_bps[b] = 0;
-    for (int c = 0; c < P->ncls && P->kind != KIND_ALIGNED; ++c) {
-      int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
-      P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, kind_j2(P->kind), P->s2_qtile);
-      maxbps = std::max(maxbps, P->s2_bps[LB]);
-    }
-    // aligned: quartet slices of the q-vector kernel (one partial row each)
-    P->s2_rows = P->kind == KIND_ALIGNED ? std::max(1, 4 * P->nsm / std::max(1, (nq + 127) / 128)) : P->nsm * maxbps;
-    if (P->kind == KIND_ALIGNED) P->s2_rows = std::min(P->s2_rows, 4 * P->nsm);
+    stage2_layout(P);
     // contraction buffer of the split contracted-side stage 1: the largest
     // sub-range's quartets x outer pairs x ntuv(LK), up to 2 GB (larger
     // sub-ranges keep the fused kernel)
@@ -710,22 +718,24 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       s.first_on_grid = first_on_grid;
       s.dq = dq;
       s.j2 = kind_j2(P->kind);
+      s.lb = LB;
       s.partial = P->d_partial + q0;
       s.pstride = P->nq;
       // a class too small to fill the GPU several times over is also split
       // over q, in chunks of 64 points (the reseed interval)
-      const int64_t per_warp = stage2_quartets_per_warp(LB);
+      const int64_t per_warp = stage2_quartets_per_warp(LB, P->s2_tile);
+      const int NW = P->s2_tile.nw;
       const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
-      const int64_t resident = (int64_t)P->nsm * bps * STAGE2_WARPS;
+      const int64_t resident = (int64_t)P->nsm * bps * NW;
       const int64_t nbatch = (s.nquart + per_warp - 1) / per_warp * ngeom;
       const int nseg = (tn + 63) / 64;
       int nch = (int)std::min<int64_t>(nseg, std::max<int64_t>(1, (8 * resident + nbatch - 1) / nbatch));
       s.chunk = nch <= 1 ? 0 : 64 * ((nseg + nch - 1) / nch);
       if (s.chunk > 0) nch = (tn + s.chunk - 1) / s.chunk;
       const int64_t items = nbatch / ngeom * nch;
-      const int64_t nblk = (items + STAGE2_WARPS - 1) / STAGE2_WARPS;
+      const int64_t nblk = (items + NW - 1) / NW;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
-      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->st));
+      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->s2_tile, P->st));
       P->launches += 1;
     }
   }
@@ -1009,23 +1019,50 @@ done:
   return rc;
 }
 
-// Stage-2 q tile (points per shared-memory tile): recomputes the resident
-// blocks per class and the partial-row count; buffers are reallocated.
+// Stage-2 q tile (points per shared-memory tile) or pair tile changed:
+// recompute the resident blocks per class and the partial-row count, and
+// reallocate the partial sums (the only buffer sized by it).  Centres,
+// records and captured graphs of other shapes are dropped or kept as they
+// stay valid: the records do, the graphs do not.
+static int stage2_relayout(thistle_plan *P) {
+  TB_CK(cudaStreamSynchronize(P->st));
+  drop_graphs(P);
+  stage2_layout(P);
+  dfree(P->d_partial);
+  P->d_partial = nullptr;
+  return dalloc(&P->d_partial, (size_t)P->ngeom * P->s2_rows * P->nq, "partial sums");
+}
+
 static int set_qtile(thistle_plan *P, int qt) {
   P->s2_qtile = std::max(1, std::min(qt, std::min(P->nq, STAGE2_QTILE)));
-  int maxbps = 1;
-  for (int c = 0; c < P->ncls; ++c) {
-    const int LB = P->cls_L[c] + (kind_j2(P->kind) ? 2 : 0);
-    P->s2_bps[LB] = stage2_class_blocks_per_sm(LB, kind_j2(P->kind), P->s2_qtile);
-    maxbps = std::max(maxbps, P->s2_bps[LB]);
-  }
-  P->s2_rows = P->nsm * maxbps;
-  std::vector<double> keep = P->hxyz;
-  const int G = P->ngeom;
-  int rc = geo_alloc(P, G);
+  return stage2_relayout(P);
+}
+
+static int set_tile(thistle_plan *P, Stage2Tile t) {
+  P->s2_tile = t;
+  return stage2_relayout(P);
+}
+
+// Geometries per second of forward + adjoint at the plan's current shape
+// (3 timed runs after 2 untimed ones), or a negative status.
+static int time_batch(thistle_plan *P, cudaEvent_t e0, cudaEvent_t e1, double *gps) {
+  const int reps = 3;
+  int rc = adjoint_alloc(P);
   if (rc != THISTLE_OK) return rc;
-  P->hxyz.clear();
-  return upload_centres_batch(P, keep.data());
+  TB_CK(cudaMemsetAsync(P->d_v, 0, sizeof(double) * P->ngeom * P->nq, P->st));
+  for (int w = 0; w < 2 + reps && rc == THISTLE_OK; ++w) {
+    if (w == 2) TB_CK(cudaEventRecord(e0, P->st));
+    P->fwd_valid = false;
+    rc = forward_batch(P);
+    if (rc == THISTLE_OK) rc = plan_vjp(P, P->d_v, P->d_grad);
+  }
+  if (rc != THISTLE_OK) return rc;
+  TB_CK(cudaEventRecord(e1, P->st));
+  TB_CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  TB_CK(cudaEventElapsedTime(&ms, e0, e1));
+  *gps = ms > 0 ? P->ngeom * reps / (ms * 1e-3) : 0.0;
+  return THISTLE_OK;
 }
 
 int thistle_plan_autotune_batch(thistle_plan *P, int32_t gmax, int32_t *g_best, int32_t *qtile_best,
@@ -1037,38 +1074,29 @@ int thistle_plan_autotune_batch(thistle_plan *P, int32_t gmax, int32_t *g_best, 
   const int qfull = std::min(P->nq, STAGE2_QTILE);
   int qts[2] = {qfull, std::max(64, (qfull / 2 + 63) / 64 * 64)};
   const int nqt = qts[1] < qfull ? 2 : 1;
+  const Stage2Tile tiles[4] = {{2, 4}, {2, 8}, {1, 4}, {1, 8}};
   double best = -1.0;
   int bestG = 1, bestQ = qfull;
+  Stage2Tile bestT = tiles[0];
   cudaEvent_t e0, e1;
   TB_CK(cudaEventCreate(&e0));
   TB_CK(cudaEventCreate(&e1));
-  for (int G = 1; G <= gmax; G *= 2) {
+  // batch size and q tile at the default pair tile, then the pair tiles at
+  // the best of those
+  rc = set_tile(P, tiles[0]);
+  for (int G = 1; G <= gmax && rc == THISTLE_OK; G *= 2) {
     bool fits = true;
     for (int t = 0; t < nqt && fits; ++t) {
       rc = thistle_plan_set_batch(P, G);
       if (rc == THISTLE_OK) rc = set_qtile(P, qts[t]);
-      if (rc == THISTLE_OK) rc = adjoint_alloc(P);
-      if (rc != THISTLE_OK) {
+      double gps = 0.0;
+      if (rc == THISTLE_OK) rc = time_batch(P, e0, e1, &gps);
+      if (rc == THISTLE_ERR_NOMEM) {
         fits = false;  // no room for this batch: keep the best so far
+        rc = THISTLE_OK;
         break;
       }
-      cudaMemsetAsync(P->d_v, 0, sizeof(double) * G * P->nq, P->st);
-      const int reps = 3;
-      for (int w = 0; w < 2 + reps && rc == THISTLE_OK; ++w) {
-        if (w == 2) cudaEventRecord(e0, P->st);
-        P->fwd_valid = false;
-        rc = forward_batch(P);
-        if (rc == THISTLE_OK) rc = plan_vjp(P, P->d_v, P->d_grad);
-      }
-      cudaEventRecord(e1, P->st);
-      if (cudaEventSynchronize(e1) != cudaSuccess || rc != THISTLE_OK) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return rc != THISTLE_OK ? rc : fail(THISTLE_ERR_CUDA, "autotune run failed");
-      }
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      const double gps = ms > 0 ? G * reps / (ms * 1e-3) : 0.0;
+      if (rc != THISTLE_OK) break;
       if (gps > best) {
         best = gps;
         bestG = G;
@@ -1077,15 +1105,41 @@ int thistle_plan_autotune_batch(thistle_plan *P, int32_t gmax, int32_t *g_best, 
     }
     if (!fits) break;
   }
+  if (rc == THISTLE_OK) rc = thistle_plan_set_batch(P, bestG);
+  if (rc == THISTLE_OK) rc = set_qtile(P, bestQ);
+  for (int t = 1; t < 4 && rc == THISTLE_OK; ++t) {
+    rc = set_tile(P, tiles[t]);
+    double gps = 0.0;
+    if (rc == THISTLE_OK) rc = time_batch(P, e0, e1, &gps);
+    if (rc == THISTLE_OK && gps > best) {
+      best = gps;
+      bestT = tiles[t];
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaGetLastError();
-  rc = thistle_plan_set_batch(P, bestG);
-  if (rc == THISTLE_OK) rc = set_qtile(P, bestQ);
   if (rc != THISTLE_OK) return rc;
+  TB_TRY(set_tile(P, bestT));
   *g_best = bestG;
   *qtile_best = bestQ;
   *geoms_per_s = best;
+done:
+  return rc;
+}
+
+int thistle_plan_set_stage2_tile(thistle_plan *P, int32_t quartets_per_lane, int32_t warps_per_block) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  const Stage2Tile t{quartets_per_lane, warps_per_block};
+  if (!stage2_tile_valid(t)) return fail(THISTLE_ERR_ARG, "stage-2 tile: quartets per lane 1 or 2, warps 4 or 8");
+  if (P->kind == KIND_ALIGNED) return fail(THISTLE_ERR_TYPE, "aligned plans have no stage-2 pair tile");
+  if (t.k == P->s2_tile.k && t.nw == P->s2_tile.nw) return THISTLE_OK;
+  return set_tile(P, t);
+}
+
+int thistle_plan_stage2_tile(const thistle_plan *P, int32_t *quartets_per_lane, int32_t *warps_per_block) {
+  if (!P || !quartets_per_lane || !warps_per_block) return fail(THISTLE_ERR_ARG, "null argument");
+  *quartets_per_lane = P->s2_tile.k;
+  *warps_per_block = P->s2_tile.nw;
   return THISTLE_OK;
 }
 

@@ -132,6 +132,7 @@ struct thistle_plan {
   size_t s2sort_bytes = 0;
   int nsm = 0, s2_rows = 0, s2_qtile = 0;
   int s2_bps[LMAXB + 1];             // resident stage-2 blocks per SM, per Bessel order
+  Stage2Tile s2_tile;                // stage-2 pair tile (quartets per lane, warps per block)
   cudaStream_t st = nullptr;
   bool own_stream = true;
   cudaEvent_t ev[10];
@@ -194,6 +195,7 @@ TB_INTERNAL int plan_create(thistle_plan **out, int32_t type, int32_t ngto, cons
                        const int32_t *group, const double *mmod, int32_t norbs, const int32_t *mat,
                        const double *total, int32_t nmat, const double *onerdm, int32_t nmo1, const double *q,
                        int32_t nq, double cutoffz, double cutoffmd, double cutoffcentre);
+TB_INTERNAL void stage2_layout(thistle_plan *P);
 TB_INTERNAL void grid_info(const double *q, int n, int &uniform, int &first_on_grid, double &dq);
 TB_INTERNAL Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t qbegin, int64_t qend,
                               double *d_rec, int64_t recbase, int rs);

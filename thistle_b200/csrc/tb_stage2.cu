@@ -161,24 +161,18 @@ struct BoolTag {
   static constexpr bool value = B;
 };
 
-// quartets per lane, and the resident blocks per SM the register allocation
-// aims at (4 blocks of 4 warps: 128 registers a thread).  Measured on the
-// AB6 step, two quartets per lane at 4 blocks per SM beat 1 (6 blocks), 3
-// (3 blocks) and 2 at 3 or 5 blocks by 1-8 %.
-#ifndef TB_S2_MINB
-#define TB_S2_MINB 4
-#endif
-#ifndef TB_S2_K03
-#define TB_S2_K03 2
-#endif
-#ifndef TB_S2_K45
-#define TB_S2_K45 2
-#endif
-#ifndef TB_S2_K68
-#define TB_S2_K68 2
-#endif
-TB_HD constexpr int stage2_k(int LB) {
-  return LB <= 3 ? TB_S2_K03 : (LB <= 5 ? TB_S2_K45 : (LB <= 8 ? TB_S2_K68 : 1));
+// Quartets per lane K and the register budget.  The polynomial-form orders
+// (LB <= 8) take K = 2 (the default pair tile) or 1, the recurrence orders
+// always 1.  K = 2 and every recurrence order get 128 registers a thread (4
+// blocks of 4 warps or 2 of 8 per SM), K = 1 of a polynomial order 85 (6
+// blocks of 4 warps, 3 of 8).  Measured on the AB6 step, two quartets per
+// lane at 4 blocks of 4 warps beat 1 (6 blocks), 3 (3 blocks) and 2 at 3 or
+// 5 blocks by 1-8 %; smaller molecules may prefer another shape, which the
+// plan and batch tuners measure.
+TB_HD constexpr int stage2_keff(int LB, int k) { return LB <= 8 ? k : 1; }
+template <int LB, int K>
+constexpr int stage2_minb() {
+  return (K == 1 && LB <= 8) ? 3 : 2;
 }
 
 // Crossover of the polynomial form: the smallest x at which its float64 error
@@ -205,7 +199,7 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
   const int nq = A.nq, nqb = padded_nq(nq);
   double2 *qs = reinterpret_cast<double2 *>(sm);  // (q, 1/q), padded with the last point
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = STAGE2_WARPS;
+  const int NW = blockDim.x >> 5;
   double *acc = sm + 2 * nqb + warp * nqb;
   for (int i = threadIdx.x; i < nqb; i += blockDim.x) {
     const double q = A.q[i < nq ? i : nq - 1];
@@ -500,21 +494,20 @@ __device__ __forceinline__ void stage2_class_body(Stage2ClassArgs &A, int64_t vb
   // fixed-order sum of the warp rows, added to this block's partial row
   for (int i = threadIdx.x; i < nq; i += blockDim.x) {
     double t = 0.0;
-#pragma unroll
     for (int w = 0; w < NW; ++w) t += sm[2 * nqb + w * nqb + i];
     A.partial[(size_t)vb * A.pstride + i] += t;
   }
 }
 
 template <int LB, int K, bool J2>
-__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB) stage2_class_kernel(Stage2ClassArgs A) {
+__global__ void __launch_bounds__(STAGE2_MAXWARPS * 32, (stage2_minb<LB, K>())) stage2_class_kernel(Stage2ClassArgs A) {
   // geometry blockIdx.y of a batch
   A.rec += blockIdx.y * A.gs_rec;
   A.partial += blockIdx.y * A.gs_partial;
   stage2_class_body<LB, K, J2>(A, blockIdx.x, gridDim.x);
 }
 
-// Molecule batches: item i's blocks are pre[i] .. pre[i+1]-1 (its vgrid).
+// Molecule batches: item i's virtual blocks are pre[i] .. pre[i+1]-1.
 __device__ __forceinline__ int s2_batch_item(const int64_t *__restrict__ pre, int n, int64_t b) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
@@ -525,91 +518,126 @@ __device__ __forceinline__ int s2_batch_item(const int64_t *__restrict__ pre, in
   return lo;
 }
 
+// One virtual block of a batch item, as a separately allocated function: the
+// persistent kernel calls the body of every order through one switch.
 template <int LB, int K, bool J2>
-__global__ void __launch_bounds__(STAGE2_WARPS * 32, TB_S2_MINB)
-    stage2_class_batch(const Stage2ClassArgs *__restrict__ d, const int64_t *__restrict__ pre, int n) {
-  const int it = s2_batch_item(pre, n, blockIdx.x);
+__device__ __noinline__ void stage2_item(const Stage2ClassArgs *__restrict__ d, int it, int64_t vb, int64_t vgrid) {
   Stage2ClassArgs A = d[it];
-  stage2_class_body<LB, K, J2>(A, blockIdx.x - pre[it], pre[it + 1] - pre[it]);
+  stage2_class_body<LB, K, J2>(A, vb, vgrid);
 }
 
-size_t class_smem(int nq) { return sizeof(double) * (size_t)padded_nq(nq) * (2 + STAGE2_WARPS); }
+// The persistent molecule-batch kernel: a block takes the next virtual block
+// from the counter, runs it, and repeats until none is left.  Items are
+// ordered heaviest order first by the host, so the tail is short work.
+template <int KS, bool J2>
+__global__ void __launch_bounds__(STAGE2_MAXWARPS * 32, 2)
+    stage2_persistent(const Stage2ClassArgs *__restrict__ d, const int64_t *__restrict__ pre, int n, int64_t blocks,
+                      unsigned long long *__restrict__ next) {
+  __shared__ long long take;
+  for (;;) {
+    __syncthreads();  // the previous virtual block's shared-memory reads are done
+    if (threadIdx.x == 0) take = (long long)atomicAdd(next, 1ull);
+    __syncthreads();
+    const int64_t b = take;
+    if (b >= blocks) return;
+    const int it = s2_batch_item(pre, n, b);
+    const int64_t vb = b - pre[it], vgrid = pre[it + 1] - pre[it];
+    const int lb = d[it].lb;
+    if constexpr (J2) {
+      switch (lb) {
+#define TB_C(n_) case n_: stage2_item<n_, stage2_keff(n_, KS), true>(d, it, vb, vgrid); break;
+        TB_C(2) TB_C(3) TB_C(4) TB_C(5) TB_C(6) TB_C(7) TB_C(8) TB_C(9) TB_C(10)
+        TB_C(11) TB_C(12) TB_C(13) TB_C(14) TB_C(15) TB_C(16) TB_C(17) TB_C(18)
+#undef TB_C
+        default: break;
+      }
+    } else {
+      switch (lb) {
+#define TB_C(n_) case n_: stage2_item<n_, stage2_keff(n_, KS), false>(d, it, vb, vgrid); break;
+        TB_C(0) TB_C(1) TB_C(2) TB_C(3) TB_C(4) TB_C(5) TB_C(6) TB_C(7) TB_C(8)
+        TB_C(9) TB_C(10) TB_C(11) TB_C(12) TB_C(13) TB_C(14) TB_C(15) TB_C(16)
+#undef TB_C
+        default: break;
+      }
+    }
+  }
+}
 
-template <int LB, bool J2>
-cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st) {
-  constexpr int K = stage2_k(LB);
-  size_t smem = class_smem(a.nq);
+size_t class_smem(int nq, int nw) { return sizeof(double) * (size_t)padded_nq(nq) * (2 + nw); }
+
+template <int LB, int K, bool J2>
+cudaError_t launch_class_lk(const Stage2ClassArgs &a, int grid, int ngeom, int nw, cudaStream_t st) {
+  size_t smem = class_smem(a.nq, nw);
   cudaError_t e =
       cudaFuncSetAttribute(stage2_class_kernel<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  stage2_class_kernel<LB, K, J2><<<dim3(grid, ngeom), STAGE2_WARPS * 32, smem, st>>>(a);
+  stage2_class_kernel<LB, K, J2><<<dim3(grid, ngeom), nw * 32, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int LB, bool J2>
-int blocks_per_sm_l(int nq) {
-  constexpr int K = stage2_k(LB);
-  size_t smem = class_smem(nq);
-  if (cudaFuncSetAttribute(stage2_class_kernel<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return 1;
+cudaError_t launch_class_l(const Stage2ClassArgs &a, int grid, int ngeom, Stage2Tile t, cudaStream_t st) {
+  if constexpr (LB <= 8)
+    if (t.k == 2) return launch_class_lk<LB, 2, J2>(a, grid, ngeom, t.nw, st);
+  return launch_class_lk<LB, 1, J2>(a, grid, ngeom, t.nw, st);
+}
+
+template <class F>
+int occupancy(F *kernel, int nw, size_t smem) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage2_class_kernel<LB, K, J2>, STAGE2_WARPS * 32, smem) !=
-      cudaSuccess)
-    return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nw * 32, smem) != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
 
 template <int LB, bool J2>
-cudaError_t launch_class_batch_l(const Stage2ClassArgs *d, const int64_t *pre, int n, int64_t blocks, int nqmax,
-                                 cudaStream_t st) {
-  constexpr int K = stage2_k(LB);
-  size_t smem = class_smem(nqmax);
+int blocks_per_sm_l(int nq, Stage2Tile t) {
+  const size_t smem = class_smem(nq, t.nw);
+  if constexpr (LB <= 8)
+    if (t.k == 2) return occupancy(stage2_class_kernel<LB, 2, J2>, t.nw, smem);
+  return occupancy(stage2_class_kernel<LB, 1, J2>, t.nw, smem);
+}
+
+template <int KS, bool J2>
+cudaError_t launch_persistent_k(const Stage2ClassArgs *d, const int64_t *pre, int n, int64_t blocks, int nqmax,
+                                int grid, int nw, unsigned long long *next, cudaStream_t st) {
+  const size_t smem = class_smem(nqmax, nw);
   cudaError_t e =
-      cudaFuncSetAttribute(stage2_class_batch<LB, K, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(stage2_persistent<KS, J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  stage2_class_batch<LB, K, J2><<<(unsigned)blocks, STAGE2_WARPS * 32, smem, st>>>(d, pre, n);
+  stage2_persistent<KS, J2><<<grid, nw * 32, smem, st>>>(d, pre, n, blocks, next);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_stage2_class_batch(int LB, bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n,
-                                      int64_t blocks, int nqmax, cudaStream_t st) {
-  if (n <= 0 || blocks <= 0) return cudaSuccess;
-  if (j2) {
-    switch (LB) {
-#define TB_L(n_) case n_: return launch_class_batch_l<n_, true>(d, pre, n, blocks, nqmax, st);
-      TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8) TB_L(9) TB_L(10)
-      TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16) TB_L(17) TB_L(18)
-#undef TB_L
-      default: return cudaErrorInvalidValue;
-    }
-  }
-  switch (LB) {
-#define TB_L(n_) case n_: return launch_class_batch_l<n_, false>(d, pre, n, blocks, nqmax, st);
-    TB_L(0) TB_L(1) TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8)
-    TB_L(9) TB_L(10) TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16)
-#undef TB_L
-    default: return cudaErrorInvalidValue;
-  }
+bool stage2_tile_valid(Stage2Tile t) { return (t.k == 1 || t.k == 2) && (t.nw == 4 || t.nw == 8); }
+
+int stage2_persistent_blocks_per_sm(bool j2, int nqmax, Stage2Tile t) {
+  const size_t smem = class_smem(nqmax, t.nw);
+  if (j2) return t.k == 2 ? occupancy(stage2_persistent<2, true>, t.nw, smem)
+                          : occupancy(stage2_persistent<1, true>, t.nw, smem);
+  return t.k == 2 ? occupancy(stage2_persistent<2, false>, t.nw, smem)
+                  : occupancy(stage2_persistent<1, false>, t.nw, smem);
 }
 
-int stage2_quartets_per_warp(int LB) {
-  switch (LB) {
-#define TB_K(n) case n: return 32 * stage2_k(n);
-    TB_K(0) TB_K(1) TB_K(2) TB_K(3) TB_K(4) TB_K(5) TB_K(6) TB_K(7) TB_K(8) TB_K(9)
-    TB_K(10) TB_K(11) TB_K(12) TB_K(13) TB_K(14) TB_K(15) TB_K(16) TB_K(17) TB_K(18)
-#undef TB_K
-    default: return 32;
-  }
+cudaError_t launch_stage2_persistent(bool j2, const Stage2ClassArgs *d, const int64_t *pre, int n, int64_t blocks,
+                                     int nqmax, int grid, Stage2Tile t, unsigned long long *next, cudaStream_t st) {
+  if (n <= 0 || blocks <= 0 || grid <= 0) return cudaSuccess;
+  if (!stage2_tile_valid(t)) return cudaErrorInvalidValue;
+  if (j2) return t.k == 2 ? launch_persistent_k<2, true>(d, pre, n, blocks, nqmax, grid, t.nw, next, st)
+                          : launch_persistent_k<1, true>(d, pre, n, blocks, nqmax, grid, t.nw, next, st);
+  return t.k == 2 ? launch_persistent_k<2, false>(d, pre, n, blocks, nqmax, grid, t.nw, next, st)
+                  : launch_persistent_k<1, false>(d, pre, n, blocks, nqmax, grid, t.nw, next, st);
 }
+
+int stage2_quartets_per_warp(int LB, Stage2Tile t) { return 32 * stage2_keff(LB, t.k); }
 
 // total / elastic classes have LB = LLmax (0..16), j2 classes LLmax + 2 (2..18)
-int stage2_class_blocks_per_sm(int LB, bool j2, int nq) {
+int stage2_class_blocks_per_sm(int LB, bool j2, int nq, Stage2Tile t) {
   if (j2) {
     switch (LB) {
-#define TB_B(n) case n: return blocks_per_sm_l<n, true>(nq);
+#define TB_B(n) case n: return blocks_per_sm_l<n, true>(nq, t);
       TB_B(2) TB_B(3) TB_B(4) TB_B(5) TB_B(6) TB_B(7) TB_B(8) TB_B(9) TB_B(10)
       TB_B(11) TB_B(12) TB_B(13) TB_B(14) TB_B(15) TB_B(16) TB_B(17) TB_B(18)
 #undef TB_B
@@ -617,7 +645,7 @@ int stage2_class_blocks_per_sm(int LB, bool j2, int nq) {
     }
   }
   switch (LB) {
-#define TB_B(n) case n: return blocks_per_sm_l<n, false>(nq);
+#define TB_B(n) case n: return blocks_per_sm_l<n, false>(nq, t);
     TB_B(0) TB_B(1) TB_B(2) TB_B(3) TB_B(4) TB_B(5) TB_B(6) TB_B(7) TB_B(8)
     TB_B(9) TB_B(10) TB_B(11) TB_B(12) TB_B(13) TB_B(14) TB_B(15) TB_B(16)
 #undef TB_B
@@ -625,11 +653,13 @@ int stage2_class_blocks_per_sm(int LB, bool j2, int nq) {
   }
 }
 
-cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, cudaStream_t st) {
+cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int ngeom, Stage2Tile t,
+                                cudaStream_t st) {
   if (a.nquart <= 0 || grid <= 0) return cudaSuccess;
+  if (!stage2_tile_valid(t)) return cudaErrorInvalidValue;
   if (a.j2) {
     switch (LB) {
-#define TB_L(n) case n: return launch_class_l<n, true>(a, grid, ngeom, st);
+#define TB_L(n) case n: return launch_class_l<n, true>(a, grid, ngeom, t, st);
       TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8) TB_L(9) TB_L(10)
       TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16) TB_L(17) TB_L(18)
 #undef TB_L
@@ -637,7 +667,7 @@ cudaError_t launch_stage2_class(int LB, const Stage2ClassArgs &a, int grid, int 
     }
   }
   switch (LB) {
-#define TB_L(n) case n: return launch_class_l<n, false>(a, grid, ngeom, st);
+#define TB_L(n) case n: return launch_class_l<n, false>(a, grid, ngeom, t, st);
     TB_L(0) TB_L(1) TB_L(2) TB_L(3) TB_L(4) TB_L(5) TB_L(6) TB_L(7) TB_L(8)
     TB_L(9) TB_L(10) TB_L(11) TB_L(12) TB_L(13) TB_L(14) TB_L(15) TB_L(16)
 #undef TB_L

@@ -288,11 +288,22 @@ class ScatteringPlan:
         check(_abi.lib().thistle_plan_use_graph(self._p, int(bool(enable))))
 
     def autotune_batch(self, gmax: int):
-        """Pick the batch size and stage-2 q tile by timing forward + adjoint; returns (ngeom, qtile, geoms/s)."""
+        """Pick the batch size, the stage-2 q tile and the stage-2 pair tile by
+        timing forward + adjoint; returns (ngeom, qtile, geoms/s) and leaves
+        the pair tile in the plan (``stage2_tile``)."""
         g, qt, gps = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
         check(_abi.lib().thistle_plan_autotune_batch(self._p, int(gmax), C.byref(g), C.byref(qt), C.byref(gps)))
         self.ngeom = g.value
         return g.value, qt.value, gps.value
+
+    def set_stage2_tile(self, quartets_per_lane: int, warps_per_block: int):
+        """Stage-2 pair tile: quartets per lane (1, 2) and warps per block (4, 8)."""
+        check(_abi.lib().thistle_plan_set_stage2_tile(self._p, int(quartets_per_lane), int(warps_per_block)))
+
+    def stage2_tile(self):
+        k, nw = C.c_int32(0), C.c_int32(0)
+        check(_abi.lib().thistle_plan_stage2_tile(self._p, C.byref(k), C.byref(nw)))
+        return k.value, nw.value
 
     def set_centres_batch_device(self, ptr: int):
         """Centres of every geometry from device memory ((ngeom, ngto, 3)
@@ -399,7 +410,8 @@ class ScatteringPlan:
 class MoleculeBatch:
     """Several plans (different molecules and bases, one geometry each, the
     same calculation type, at most 1024 q points each) executed together:
-    each stage and class runs as one launch over all of them.  The plans must
+    stage 2 is one persistent launch over every (plan, class, block) item,
+    the other stages one launch per kernel shape.  The plans must
     stay open while the batch is used; ``execute`` returns one I(q) array per
     plan, for each plan's current centres."""
 
@@ -419,23 +431,27 @@ class MoleculeBatch:
         check(_abi.lib().thistle_batch_execute(self._b, dptr(out)))
         return np.split(out, self._split)
 
-    def set_centres_batch_device(self, ptr: int):
-        """Centres of every geometry from device memory ((ngeom, ngto, 3)
-        doubles at ``ptr``), stream-ordered on the plan's stream."""
-        check(_abi.lib().thistle_plan_set_centres_batch_device(self._p, C.c_void_p(ptr)))
-
-    def execute_batch_device(self, ptr: int):
-        """I(q) of every geometry, (ngeom, nq) doubles to the device address ``ptr``."""
-        check(_abi.lib().thistle_plan_execute_batch_device(self._p, C.c_void_p(ptr)))
-
-    def vjp_batch_device(self, v_ptr: int, grad_ptr: int):
-        """Device cotangents (ngeom, nq) -> group-centre gradients (ngeom, ng, 3)."""
-        check(_abi.lib().thistle_plan_vjp_batch_device(self._p, C.c_void_p(v_ptr), C.c_void_p(grad_ptr)))
-
     def execute_device(self, ptr: int):
         """All plans' I(q), one after the other, to the device address ``ptr``
         (stream-ordered on the first plan's stream)."""
         check(_abi.lib().thistle_batch_execute_device(self._b, C.c_void_p(ptr)))
+
+    def set_stage2_tile(self, quartets_per_lane: int, warps_per_block: int):
+        """Stage-2 pair tile of the persistent launch: quartets per lane (1, 2)
+        and warps per block (4, 8)."""
+        check(_abi.lib().thistle_batch_set_stage2_tile(self._b, int(quartets_per_lane), int(warps_per_block)))
+
+    def stage2_tile(self):
+        k, nw = C.c_int32(0), C.c_int32(0)
+        check(_abi.lib().thistle_batch_stage2_tile(self._b, C.byref(k), C.byref(nw)))
+        return k.value, nw.value
+
+    def autotune(self):
+        """Time the batch at the four stage-2 pair tiles and keep the fastest;
+        returns (quartets per lane, warps per block, molecules/s)."""
+        k, nw, mps = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
+        check(_abi.lib().thistle_batch_autotune(self._b, C.byref(k), C.byref(nw), C.byref(mps)))
+        return k.value, nw.value, mps.value
 
     def info(self):
         a = np.zeros(3, dtype=np.int64)
