@@ -424,6 +424,12 @@ cudaError_t launch_stage1_tpl(int kind, int tuple, const Stage1Args &a, int ngeo
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_stage1_tpl_batch(int kind, int tuple, const Stage1Args *d, const int64_t *pre, int n,
+                                    int64_t blocks, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_tpl_batch_k<KIND_TOTAL>(tuple, d, pre, n, blocks, st);
+  return cudaErrorInvalidValue;
+}
+
 bool stage1_xk(int L, int64_t nquart, int nsm) {
   if (L < TB_S1_XK_MIN) return false;
   if (L <= 6) return true;

@@ -169,6 +169,13 @@ bool stage1_tpl(int kind, int L, int shells_canonical);
 template <int K>
 cudaError_t launch_stage1_tpl_k(int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
 cudaError_t launch_stage1_tpl(int kind, int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
+// molecule batches: n items of one shell tuple (descriptors d), item i's
+// blocks pre[i] .. pre[i+1]-1 (128 quartets each)
+template <int K>
+cudaError_t launch_stage1_tpl_batch_k(int tuple, const Stage1Args *d, const int64_t *pre, int n, int64_t blocks,
+                                      cudaStream_t st);
+cudaError_t launch_stage1_tpl_batch(int kind, int tuple, const Stage1Args *d, const int64_t *pre, int n,
+                                    int64_t blocks, cudaStream_t st);
 cudaError_t launch_stage1(int kind, int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 template <int K>
 cudaError_t launch_stage1_xk_k(int L, int LK, bool XB, const Stage1Args &a, int ngeom, cudaStream_t st);

@@ -20,6 +20,7 @@ struct thistle_batch {
     int64_t *pre, blocks;
     bool split;            // contraction kernel + convolution kernel through d_xbuf
     int64_t *prexc, blocksxc;
+    bool tpl = false;      // shell-templated kernel of shell tuple XB (LK = -2)
   };
   std::vector<S1> s1;
   // stage 2: items (plan, class) heaviest Bessel order first, item i owning
@@ -61,7 +62,10 @@ int batch_run(thistle_batch *B) {
   TB_CK(launch_pair_tables_batch(B->d_pair, B->d_pair_pre, (int)B->plans.size(), B->pair_blocks, st));
   B->launches += 1;
   for (auto &x : B->s1) {
-    if (x.split) {
+    if (x.tpl) {
+      TB_CK(launch_stage1_tpl_batch(B->kind, x.XB, x.d, x.pre, x.n, x.blocks, st));
+      B->launches += 1;
+    } else if (x.split) {
       TB_CK(launch_stage1_xsplit_batch(B->kind, x.L, x.LK, x.XB, x.d, x.prexc, x.blocksxc, x.pre, x.blocks, x.n,
                                        B->d_xbuf, st));
       B->launches += 2;
@@ -248,7 +252,16 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
         Stage1Args a = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c],
                                    P->cls_rs[c]);
         const int L = P->cls_L[c];
-        if (stage1_xk(L, ltot[L], P->nsm)) {
+        if (stage1_tpl(P->kind, L, P->shells_canonical) && !P->cls_tup[c].empty()) {
+          // shell-templated kernels: items keyed (L, -2, shell tuple)
+          for (const TupleRange &u : P->cls_tup[c]) {
+            Stage1Args b = a;
+            b.qbegin = u.begin;
+            b.qend = u.end;
+            b.recbase = P->cls_recoff[c] + (u.begin - P->cls_begin[c]) * (int64_t)P->cls_rs[c];
+            items.push_back({{L, -2, u.tuple, 0}, b});
+          }
+        } else if (stage1_xk(L, ltot[L], P->nsm)) {
           for (const SubRange &u : P->cls_sub[c]) {
             Stage1Args b = a;
             b.qbegin = u.begin;
@@ -293,13 +306,14 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
           split = false;
         }
         d.push_back(a);
-        pre.push_back(pre.back() + stage1_item_blocks(L, LK >= 0, nq));
+        pre.push_back(pre.back() + (LK == -2 ? (nq + 127) / 128 : stage1_item_blocks(L, LK >= 0, nq)));
         ++j;
       }
       if (xoff > (int64_t(1) << 28)) split = false;
       if (split) xneed = std::max(xneed, xoff);
       thistle_batch::S1 x{L, LK, items[i].first[2], (int)d.size(), nullptr, nullptr, pre.back(), split, nullptr,
                           split ? prexc.back() : 0};
+      x.tpl = LK == -2;
       TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-1 descriptors"));
       TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-1 prefix"));
       if (split) TB_TRY(upload_vec(&x.prexc, prexc, B->st, "batch contraction prefix"));

@@ -498,14 +498,13 @@ __global__ void __launch_bounds__(128, stage1_reg_minblocks(L))
 #endif
 
 template <int Li, int Lj, int Lk, int Lr, int KIND>
-__global__ void __launch_bounds__(128) stage1_tpl_kernel(Stage1Args A) {
+__device__ __forceinline__ void stage1_tpl_body(const Stage1Args &A, int64_t vb) {
   constexpr int L = Li + Lj + Lk + Lr;
   constexpr int ni = (Li + 1) * (Li + 2) / 2, nj = (Lj + 1) * (Lj + 2) / 2;
   constexpr int nk = (Lk + 1) * (Lk + 2) / 2, nr = (Lr + 1) * (Lr + 2) / 2;
   constexpr int TMAX = L < 2 * MAXA ? L : 2 * MAXA;
-  stage1_geometry(A);
   extern __shared__ double sD[];  // ntuv(L) x 128
-  const int64_t qi = A.qbegin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t qi = A.qbegin + vb * blockDim.x + threadIdx.x;
   if (qi >= A.qend) return;
   const QuartetHead Q = quartet_head<KIND>(A, qi);
   const int si = A.gstart[Q.gi], sj = A.gstart[Q.gj], sk = A.gstart[Q.gk], sr = A.gstart[Q.gr];
@@ -589,6 +588,22 @@ __global__ void __launch_bounds__(128) stage1_tpl_kernel(Stage1Args A) {
   stage1_finish<L, KIND, 1>(A, Q, col, 128, qi, 0, 1u << (threadIdx.x & 31));
 }
 
+template <int Li, int Lj, int Lk, int Lr, int KIND>
+__global__ void __launch_bounds__(128) stage1_tpl_kernel(Stage1Args A) {
+  stage1_geometry(A);
+  stage1_tpl_body<Li, Lj, Lk, Lr, KIND>(A, blockIdx.x);
+}
+
+// Molecule batches: item i (one plan's quartets of this shell tuple) owns
+// blocks pre[i] .. pre[i+1]-1.
+template <int Li, int Lj, int Lk, int Lr, int KIND>
+__global__ void __launch_bounds__(128)
+    stage1_tpl_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  const Stage1Args A = d[it];
+  stage1_tpl_body<Li, Lj, Lk, Lr, KIND>(A, blockIdx.x - pre[it]);
+}
+
 // One launch per shell tuple of a class's sub-range (s = Li..Lr, packed as
 // ((Li 5 + Lj) 5 + Lk) 5 + Lr).
 template <int K>
@@ -603,6 +618,38 @@ cudaError_t launch_stage1_tpl_k(int tuple, const Stage1Args &a, int ngeom, cudaS
     if (e != cudaSuccess) return e;                                                                  \
     stage1_tpl_kernel<i, j, k, r, K><<<dim3((unsigned)((n + 127) / 128), ngeom), 128, smem, st>>>(a); \
     return cudaGetLastError();                                                                       \
+  }
+  switch (tuple) {
+    TB_TPL(0, 0, 0, 0)
+    TB_TPL(1, 0, 0, 0) TB_TPL(0, 1, 0, 0) TB_TPL(0, 0, 1, 0) TB_TPL(0, 0, 0, 1)
+#if TB_S1_TPL_MAXL >= 2
+    TB_TPL(2, 0, 0, 0) TB_TPL(0, 2, 0, 0) TB_TPL(0, 0, 2, 0) TB_TPL(0, 0, 0, 2)
+    TB_TPL(1, 1, 0, 0) TB_TPL(1, 0, 1, 0) TB_TPL(1, 0, 0, 1) TB_TPL(0, 1, 1, 0) TB_TPL(0, 1, 0, 1) TB_TPL(0, 0, 1, 1)
+#endif
+#if TB_S1_TPL_MAXL >= 3
+    TB_TPL(3, 0, 0, 0) TB_TPL(0, 3, 0, 0) TB_TPL(0, 0, 3, 0) TB_TPL(0, 0, 0, 3)
+    TB_TPL(2, 1, 0, 0) TB_TPL(2, 0, 1, 0) TB_TPL(2, 0, 0, 1) TB_TPL(1, 2, 0, 0) TB_TPL(0, 2, 1, 0) TB_TPL(0, 2, 0, 1)
+    TB_TPL(1, 0, 2, 0) TB_TPL(0, 1, 2, 0) TB_TPL(0, 0, 2, 1) TB_TPL(1, 0, 0, 2) TB_TPL(0, 1, 0, 2) TB_TPL(0, 0, 1, 2)
+    TB_TPL(1, 1, 1, 0) TB_TPL(1, 1, 0, 1) TB_TPL(1, 0, 1, 1) TB_TPL(0, 1, 1, 1)
+#endif
+    default: break;
+  }
+#undef TB_TPL
+  return cudaErrorInvalidValue;
+}
+
+template <int K>
+cudaError_t launch_stage1_tpl_batch_k(int tuple, const Stage1Args *d, const int64_t *pre, int n, int64_t blocks,
+                                      cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+#define TB_TPL(i, j, k, r)                                                                           \
+  case ((i * 5 + j) * 5 + k) * 5 + r: {                                                            \
+    const size_t smem = (size_t)ntuv(i + j + k + r) * sizeof(double) * 128;                        \
+    cudaError_t e = cudaFuncSetAttribute(stage1_tpl_batch<i, j, k, r, K>,                          \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    if (e != cudaSuccess) return e;                                                                \
+    stage1_tpl_batch<i, j, k, r, K><<<(unsigned)blocks, 128, smem, st>>>(d, pre, n);               \
+    return cudaGetLastError();                                                                     \
   }
   switch (tuple) {
     TB_TPL(0, 0, 0, 0)
