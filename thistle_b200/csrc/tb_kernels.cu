@@ -465,6 +465,12 @@ cudaError_t launch_stage1_xct(int kind, int tuple, bool XB, const Stage1Args &a,
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_stage1_xct_batch(int kind, int tuple, bool XB, const Stage1Args *d, const int64_t *pre, int n,
+                                    int64_t blocks, double *xbuf, cudaStream_t st) {
+  if (kind == KIND_TOTAL) return launch_stage1_xct_batch_k<KIND_TOTAL>(tuple, XB, d, pre, n, blocks, xbuf, st);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stage1_xsplit_batch(int kind, int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
                                        int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,
                                        cudaStream_t st) {

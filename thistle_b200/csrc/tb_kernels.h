@@ -212,8 +212,17 @@ cudaError_t launch_stage1_xct_k(int tuple, bool XB, const Stage1Args &a, double 
 bool stage1_xct(int kind, int LK, int shells_canonical);
 cudaError_t launch_stage1_xct(int kind, int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride,
                               int64_t xbase, cudaStream_t st);
-// molecule batches: the contraction (blocks from prexc) then the convolution
-// (blocks from pre, as the fused kernel) over every item of one (L, LK, XB)
+// molecule batches: the shell-templated contraction over n items of one
+// shell tuple (item i: blocks pre[i] .. pre[i+1]-1, X at xbuf + d[i].xoff
+// from its first quartet, d[i].xg threads per quartet)
+template <int K>
+cudaError_t launch_stage1_xct_batch_k(int tuple, bool XB, const Stage1Args *d, const int64_t *pre, int n,
+                                      int64_t blocks, double *xbuf, cudaStream_t st);
+cudaError_t launch_stage1_xct_batch(int kind, int tuple, bool XB, const Stage1Args *d, const int64_t *pre, int n,
+                                    int64_t blocks, double *xbuf, cudaStream_t st);
+// molecule batches: the contraction (blocks from prexc; none when blocksxc is
+// 0, X then written by launch_stage1_xct_batch) then the convolution (blocks
+// from pre, as the fused kernel) over every item of one (L, LK, XB)
 template <int K>
 cudaError_t launch_stage1_xsplit_batch_k(int L, int LK, int XB, const Stage1Args *d, const int64_t *prexc,
                                          int64_t blocksxc, const int64_t *pre, int64_t blocks, int n, double *xbuf,

@@ -2,6 +2,8 @@
 // optionally replayed from a CUDA graph.  Stage 1 is one launch per kernel
 // shape (L, LK, XB); stage 2, the dominant stage, is ONE persistent launch
 // over every (plan, class, block) item of the batch.
+#include <map>
+
 #include "tb_plan_internal.h"
 
 using namespace tb;
@@ -21,6 +23,14 @@ struct thistle_batch {
     bool split;            // contraction kernel + convolution kernel through d_xbuf
     int64_t *prexc, blocksxc;
     bool tpl = false;      // shell-templated kernel of shell tuple XB (LK = -2)
+    // split groups of canonical total-j0 plans: the shell-templated
+    // contraction, one launch per shell tuple, replaces the generic one
+    struct Xct {
+      int tuple, n;
+      Stage1Args *d;
+      int64_t *pre, blocks;
+    };
+    std::vector<Xct> xct;
   };
   std::vector<S1> s1;
   // stage 2: items (plan, class) heaviest Bessel order first, item i owning
@@ -41,7 +51,10 @@ struct thistle_batch {
 void batch_free(thistle_batch *B) {
   if (!B) return;
   dfree(B->d_pair); dfree(B->d_pair_pre); dfree(B->d_red); dfree(B->d_partial); dfree(B->d_out);
-  for (auto &x : B->s1) { dfree(x.d); dfree(x.pre); dfree(x.prexc); }
+  for (auto &x : B->s1) {
+    dfree(x.d); dfree(x.pre); dfree(x.prexc);
+    for (auto &y : x.xct) { dfree(y.d); dfree(y.pre); }
+  }
   dfree(B->d_xbuf);
   dfree(B->d_s2); dfree(B->d_s2pre); dfree(B->d_next);
   if (B->gx) cudaGraphExecDestroy(B->gx);
@@ -66,9 +79,13 @@ int batch_run(thistle_batch *B) {
       TB_CK(launch_stage1_tpl_batch(B->kind, x.XB, x.d, x.pre, x.n, x.blocks, st));
       B->launches += 1;
     } else if (x.split) {
-      TB_CK(launch_stage1_xsplit_batch(B->kind, x.L, x.LK, x.XB, x.d, x.prexc, x.blocksxc, x.pre, x.blocks, x.n,
-                                       B->d_xbuf, st));
-      B->launches += 2;
+      for (auto &y : x.xct) {
+        TB_CK(launch_stage1_xct_batch(B->kind, y.tuple, x.XB != 0, y.d, y.pre, y.n, y.blocks, B->d_xbuf, st));
+        B->launches += 1;
+      }
+      TB_CK(launch_stage1_xsplit_batch(B->kind, x.L, x.LK, x.XB, x.d, x.prexc, x.xct.empty() ? x.blocksxc : 0,
+                                       x.pre, x.blocks, x.n, B->d_xbuf, st));
+      B->launches += x.xct.empty() ? 2 : 1;
     } else {
       TB_CK(launch_stage1_batch(B->kind, x.L, x.LK, x.XB, x.d, x.pre, x.n, x.blocks, st));
       B->launches += 1;
@@ -246,9 +263,10 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
     int64_t ltot[LMAXQ + 1] = {0};
     for (thistle_plan *P : B->plans)
       for (int c = 0; c < P->ncls; ++c) ltot[P->cls_L[c]] += P->cls_end[c] - P->cls_begin[c];
-    std::vector<std::pair<std::array<int, 4>, Stage1Args>> items;  // (L, LK, XB, nout)
-    for (thistle_plan *P : B->plans)
-      for (int c = 0; c < P->ncls; ++c) {
+    std::vector<std::pair<std::array<int, 6>, Stage1Args>> items;  // (L, LK, XB, nout, plan, class)
+    for (int pi = 0; pi < n; ++pi)
+      for (int c = 0; c < plans[pi]->ncls; ++c) {
+        thistle_plan *P = plans[pi];
         Stage1Args a = stage1_args(P, P->d_quart, P->cls_begin[c], P->cls_end[c], P->d_rec, P->cls_recoff[c],
                                    P->cls_rs[c]);
         const int L = P->cls_L[c];
@@ -259,7 +277,7 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
             b.qbegin = u.begin;
             b.qend = u.end;
             b.recbase = P->cls_recoff[c] + (u.begin - P->cls_begin[c]) * (int64_t)P->cls_rs[c];
-            items.push_back({{L, -2, u.tuple, 0}, b});
+            items.push_back({{L, -2, u.tuple, 0, pi, c}, b});
           }
         } else if (stage1_xk(L, ltot[L], P->nsm)) {
           for (const SubRange &u : P->cls_sub[c]) {
@@ -267,13 +285,13 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
             b.qbegin = u.begin;
             b.qend = u.end;
             b.recbase = P->cls_recoff[c] + (u.begin - P->cls_begin[c]) * (int64_t)P->cls_rs[c];
-            items.push_back({{L, u.LK, u.XB, u.nout}, b});
+            items.push_back({{L, u.LK, u.XB, u.nout, pi, c}, b});
           }
         } else {
-          items.push_back({{L, -1, 0, 0}, a});
+          items.push_back({{L, -1, 0, 0, pi, c}, a});
         }
       }
-    auto same = [](const std::array<int, 4> &x, const std::array<int, 4> &y) {
+    auto same = [](const std::array<int, 6> &x, const std::array<int, 6> &y) {
       return x[0] == y[0] && x[1] == y[1] && x[2] == y[2];
     };
     std::stable_sort(items.begin(), items.end(), [](const auto &x, const auto &y) {
@@ -314,6 +332,37 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
       thistle_batch::S1 x{L, LK, items[i].first[2], (int)d.size(), nullptr, nullptr, pre.back(), split, nullptr,
                           split ? prexc.back() : 0};
       x.tpl = LK == -2;
+      // the shell-templated contraction when every plan of the group takes
+      // it and its shell tuples tile each sub-range
+      bool xct = split && stage1_xct(B->kind, LK, 1);
+      std::map<int, std::vector<Stage1Args>> bytup;
+      for (size_t t = i; t < j && xct; ++t) {
+        const thistle_plan *P = plans[items[t].first[4]];
+        const int c = items[t].first[5];
+        const Stage1Args &a = d[t - i];
+        xct = stage1_xct(P->kind, LK, P->shells_canonical);
+        int64_t covered = 0;
+        for (const TupleRange &w : P->cls_tup[c]) {
+          if (!xct || w.begin < a.qbegin || w.end > a.qend) continue;
+          Stage1Args bt = a;
+          bt.qbegin = w.begin;
+          bt.qend = w.end;
+          bt.xoff = a.xoff + (w.begin - a.qbegin) * (int64_t)a.xstride;
+          bytup[w.tuple].push_back(bt);
+          covered += w.end - w.begin;
+        }
+        if (covered != a.qend - a.qbegin) xct = false;
+      }
+      if (xct) {
+        for (auto &kv : bytup) {
+          std::vector<int64_t> tp(1, 0);
+          for (const Stage1Args &bt : kv.second) tp.push_back(tp.back() + ((bt.qend - bt.qbegin) * bt.xg + 127) / 128);
+          thistle_batch::S1::Xct y{kv.first, (int)kv.second.size(), nullptr, nullptr, tp.back()};
+          TB_TRY(upload_vec(&y.d, kv.second, B->st, "batch contraction descriptors"));
+          TB_TRY(upload_vec(&y.pre, tp, B->st, "batch contraction prefix"));
+          x.xct.push_back(y);
+        }
+      }
       TB_TRY(upload_vec(&x.d, d, B->st, "batch stage-1 descriptors"));
       TB_TRY(upload_vec(&x.pre, pre, B->st, "batch stage-1 prefix"));
       if (split) TB_TRY(upload_vec(&x.prexc, prexc, B->st, "batch contraction prefix"));

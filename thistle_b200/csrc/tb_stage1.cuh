@@ -1013,11 +1013,10 @@ __global__ void __launch_bounds__(128) stage1_xc_kernel(Stage1Args A, double *__
 // each other and issued ahead of the products.  X_o goes to
 // xbuf[(qi - xbase) xstride + o NX + e] like stage1_xc_body's.
 template <int L1, int L2, bool XB, int KIND>
-__global__ void __launch_bounds__(128) stage1_xct_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride,
-                                                         int64_t xbase) {
+__device__ __forceinline__ void stage1_xct_body(const Stage1Args &A, int64_t t, double *__restrict__ xbuf, int G,
+                                                int xstride, int64_t xbase) {
   constexpr int LK = L1 + L2, NX = ntuv(LK);
   constexpr int n1 = (L1 + 1) * (L1 + 2) / 2, n2 = (L2 + 1) * (L2 + 2) / 2;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t qi = A.qbegin + t / G;
   const int o = (int)(t % G);
   if (qi >= A.qend) return;
@@ -1087,6 +1086,25 @@ __global__ void __launch_bounds__(128) stage1_xct_kernel(Stage1Args A, double *_
   for (int e = 0; e < NX; ++e) xo[e] = X[e];
 }
 
+template <int L1, int L2, bool XB, int KIND>
+__global__ void __launch_bounds__(128) stage1_xct_kernel(Stage1Args A, double *__restrict__ xbuf, int G, int xstride,
+                                                         int64_t xbase) {
+  stage1_xct_body<L1, L2, XB, KIND>(A, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, xbuf, G, xstride, xbase);
+}
+
+// Molecule batches: item i (one plan's quartets of one shell tuple inside a
+// split sub-range) owns blocks pre[i] .. pre[i+1]-1; its X rows start A.xoff
+// doubles into the batch's buffer at its first quartet.
+template <int L1, int L2, bool XB, int KIND>
+__global__ void __launch_bounds__(128)
+    stage1_xct_batch(const Stage1Args *__restrict__ d, const int64_t *__restrict__ pre, int n,
+                     double *__restrict__ xbuf) {
+  const int it = batch_item(pre, n, blockIdx.x);
+  const Stage1Args A = d[it];
+  stage1_xct_body<L1, L2, XB, KIND>(A, (blockIdx.x - pre[it]) * blockDim.x + threadIdx.x, xbuf + A.xoff, A.xg,
+                                    A.xstride, A.qbegin);
+}
+
 // One launch per shell tuple ((Li 5 + Lj) 5 + Lk) 5 + Lr: its inner shells
 // are (Li, Lj) when the bra is the contracted side (XB), else (Lk, Lr).
 template <int K>
@@ -1107,6 +1125,26 @@ cudaError_t launch_stage1_xct_k(int tuple, bool XB, const Stage1Args &a, double 
     if (XB) stage1_xct_kernel<l1, l2, true, K><<<grid, 128, 0, st>>>(a, xbuf, G, xstride, xbase);  \
     else stage1_xct_kernel<l1, l2, false, K><<<grid, 128, 0, st>>>(a, xbuf, G, xstride, xbase);    \
     return cudaGetLastError();                                                                 \
+  }
+  TB_XCT(0, 0)
+  TB_XCT(1, 0) TB_XCT(0, 1)
+  TB_XCT(2, 0) TB_XCT(1, 1) TB_XCT(0, 2)
+  TB_XCT(3, 0) TB_XCT(2, 1) TB_XCT(1, 2) TB_XCT(0, 3)
+#undef TB_XCT
+  return cudaErrorInvalidValue;
+}
+
+template <int K>
+cudaError_t launch_stage1_xct_batch_k(int tuple, bool XB, const Stage1Args *d, const int64_t *pre, int n,
+                                      int64_t blocks, double *xbuf, cudaStream_t st) {
+  if (n <= 0 || blocks <= 0) return cudaSuccess;
+  const int Li = tuple / 125, Lj = (tuple / 25) % 5, Lk = (tuple / 5) % 5, Lr = tuple % 5;
+  const int L1 = XB ? Li : Lk, L2 = XB ? Lj : Lr;
+#define TB_XCT(l1, l2)                                                                             \
+  if (L1 == l1 && L2 == l2) {                                                                     \
+    if (XB) stage1_xct_batch<l1, l2, true, K><<<(unsigned)blocks, 128, 0, st>>>(d, pre, n, xbuf);  \
+    else stage1_xct_batch<l1, l2, false, K><<<(unsigned)blocks, 128, 0, st>>>(d, pre, n, xbuf);    \
+    return cudaGetLastError();                                                                    \
   }
   TB_XCT(0, 0)
   TB_XCT(1, 0) TB_XCT(0, 1)
@@ -1271,9 +1309,12 @@ template <int L, int K, int LK, bool XB>
 static cudaError_t launch_stage1_xsplit_batch_l(const Stage1Args *d, const int64_t *prexc, int64_t blocksxc,
                                                 const int64_t *pre, int64_t blocks, int n, double *xbuf,
                                                 cudaStream_t st) {
-  stage1_xc_batch<L, K, LK, XB><<<(unsigned)blocksxc, 128, 0, st>>>(d, prexc, n, xbuf);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (blocksxc > 0) {  // otherwise X was written by the shell-templated contraction
+    stage1_xc_batch<L, K, LK, XB><<<(unsigned)blocksxc, 128, 0, st>>>(d, prexc, n, xbuf);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   const size_t smem = (size_t)ntuv(L) * sizeof(double) * 128;
   e = cudaFuncSetAttribute(stage1_xb_batch<L, K, LK, XB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -5,6 +5,8 @@
 namespace tb {
 template cudaError_t launch_stage1_k<KIND_TOTAL>(int L, const Stage1Args &a, int ngeom, cudaStream_t st);
 template cudaError_t launch_stage1_tpl_k<KIND_TOTAL>(int tuple, const Stage1Args &a, int ngeom, cudaStream_t st);
+template cudaError_t launch_stage1_xct_batch_k<KIND_TOTAL>(int tuple, bool XB, const Stage1Args *d, const int64_t *pre,
+                                                           int n, int64_t blocks, double *xbuf, cudaStream_t st);
 template cudaError_t launch_stage1_tpl_batch_k<KIND_TOTAL>(int tuple, const Stage1Args *d, const int64_t *pre, int n,
                                                            int64_t blocks, cudaStream_t st);
 template cudaError_t launch_stage1_xct_k<KIND_TOTAL>(int tuple, bool XB, const Stage1Args &a, double *xbuf, int xstride,
