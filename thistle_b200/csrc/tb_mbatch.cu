@@ -305,13 +305,17 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
       std::vector<int64_t> pre(1, 0), prexc(1, 0);
       const int L = items[i].first[0], LK = items[i].first[1];
       // contracted side: split through the batch's contraction buffer when
-      // every item knows its outer-pair count and the group fits in 2 GB
+      // every item knows its outer-pair count and the group fits in 2 GB; a
+      // larger set of items of one key becomes several groups, which run one
+      // after another through the same buffer
+      constexpr int64_t XLIMIT = int64_t(1) << 28;
       bool split = LK >= 0;
       int64_t xoff = 0;
       while (j < items.size() && same(items[j].first, items[i].first)) {
         Stage1Args a = items[j].second;
         const int64_t nq = a.qend - a.qbegin;
         const int nout = items[j].first[3];
+        if (LK >= 0 && nout > 0 && !d.empty() && xoff + nq * nout * ntuv(LK) > XLIMIT) break;
         if (LK >= 0 && nout > 0) {
           int G = 1;
           while (G < nout) G *= 2;
@@ -327,7 +331,7 @@ int batch_create(thistle_batch **out, thistle_plan *const *plans, int32_t n) {
         pre.push_back(pre.back() + (LK == -2 ? (nq + 127) / 128 : stage1_item_blocks(L, LK >= 0, nq)));
         ++j;
       }
-      if (xoff > (int64_t(1) << 28)) split = false;
+      if (xoff > XLIMIT) split = false;
       if (split) xneed = std::max(xneed, xoff);
       thistle_batch::S1 x{L, LK, items[i].first[2], (int)d.size(), nullptr, nullptr, pre.back(), split, nullptr,
                           split ? prexc.back() : 0};
