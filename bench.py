@@ -201,13 +201,14 @@ def run_reference(args, rank, world):
     L = llmax_of_quartets(p, qs)
     rng = np.random.default_rng(17)
     # each step a sample stratified by LLmax class (in proportion to the class
-    # sizes) of about two seconds of work on all host threads, sized from a
-    # first untimed call
+    # sizes) of 0.25-2 s of work on all host threads (about a minute for the
+    # whole run), sized from a first untimed call
     frac = 2e-5
     idx = stratified_indices(L, frac, rng)
     t0 = time.perf_counter()
     O.scattering(p, 1, quartets=qs[idx], nthreads=ncores)
-    frac = min(1.0, frac * 2.0 / max(time.perf_counter() - t0, 1e-3))
+    step_s = min(2.0, max(0.25, 60.0 / max(1, args.warmup + args.steps)))
+    frac = min(1.0, frac * step_s / max(time.perf_counter() - t0, 1e-3))
     times, counts = [], []
     for s in range(args.warmup + args.steps):
         idx = stratified_indices(L, frac, rng)
@@ -414,7 +415,7 @@ def fit6_stage_table(pl, xyz, iref, pad, G, nplain):
 
 
 def run_batch4(args):
-    print(json.dumps(batch4_section(args.batch_molecules, args.batch_chunk, args.batch_gb, args.steps)),
+    print(json.dumps(batch4_section(args.batch_molecules, args.batch_chunk, args.batch_gb, min(args.steps, 10))),
           flush=True)
     return 0
 
@@ -567,7 +568,8 @@ def bench_extras(args, p, plan, stream, stage1_ms, peak_tf, fwd_ms):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=120,
+                    help="timed steps (AB6: 120 steps are about 2.2 s, so the clock record has samples under load)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="thistle", choices=["thistle", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
