@@ -293,15 +293,28 @@ __global__ void __launch_bounds__(256) stage2_kernel(Stage2Args A) {
   }
 }
 
-__global__ void reduce_kernel(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out,
-                              int64_t gs_in) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nq) return;
+// Sum of nblocks partial rows (row stride nq) at every q point of geometry
+// blockIdx.y: a block takes 32 points, lane = point; warp w adds rows w,
+// w + 8, w + 16, .. in order, then the 8 warp sums are added in warp order
+// (a fixed order whatever the launch).
+constexpr int REDUCE_WARPS = 8;
+__global__ void __launch_bounds__(REDUCE_WARPS * 32)
+    reduce_kernel(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out, int64_t gs_in) {
+  __shared__ double sm[REDUCE_WARPS][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
   partial += blockIdx.y * gs_in;
-  out += (int64_t)blockIdx.y * nq;
   double t = 0.0;
-  for (int b = 0; b < nblocks; ++b) t += partial[(size_t)b * nq + i];
-  out[i] = t;
+  if (i < nq)
+    for (int b = w; b < nblocks; b += REDUCE_WARPS) t += partial[(size_t)b * nq + i];
+  sm[w][lane] = t;
+  __syncthreads();
+  if (w == 0 && i < nq) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < REDUCE_WARPS; ++k) s += sm[k][lane];
+    out[(int64_t)blockIdx.y * nq + i] = s;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -527,13 +540,13 @@ cudaError_t launch_stage2(const Stage2Args &a, int grid, int nwarps, cudaStream_
 }
 
 cudaError_t launch_reduce(const double *partial, int nblocks, int nq, double *out, cudaStream_t st) {
-  reduce_kernel<<<(nq + 127) / 128, 128, 0, st>>>(partial, nblocks, nq, out, 0);
+  reduce_kernel<<<(nq + 31) / 32, REDUCE_WARPS * 32, 0, st>>>(partial, nblocks, nq, out, 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_batch(const double *partial, int nblocks, int nq, int64_t gs_in, double *out, int ngeom,
                                 cudaStream_t st) {
-  reduce_kernel<<<dim3((nq + 127) / 128, ngeom), 128, 0, st>>>(partial, nblocks, nq, out, gs_in);
+  reduce_kernel<<<dim3((nq + 31) / 32, ngeom), REDUCE_WARPS * 32, 0, st>>>(partial, nblocks, nq, out, gs_in);
   return cudaGetLastError();
 }
 

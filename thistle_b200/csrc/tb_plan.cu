@@ -288,6 +288,9 @@ void plan_free(thistle_plan *P) {
     for (int r = 0; r < P->rev_made; ++r)
       for (int i = 0; i < 5; ++i) cudaEventDestroy(P->rev[r][i]);
   }
+  if (P->ev_fork) cudaEventDestroy(P->ev_fork);
+  if (P->ev_join) cudaEventDestroy(P->ev_join);
+  if (P->st2) cudaStreamDestroy(P->st2);
   if (P->st && P->own_stream) cudaStreamDestroy(P->st);
   delete P;
 }
@@ -315,7 +318,7 @@ int geo_alloc(thistle_plan *P, int G) {
   TB_TRY(dalloc(&P->d_pairtab, (size_t)G * gs_pair(P), "pair tables"));
   TB_TRY(dalloc(&P->d_esoa, (size_t)G * gs_esoa(P), "transposed E tables"));
   TB_TRY(dalloc(&P->d_rec, (size_t)G * gs_rec(P), "quartet records"));
-  TB_TRY(dalloc(&P->d_partial, (size_t)G * P->s2_rows * P->nq, "partial sums"));
+  TB_TRY(dalloc(&P->d_partial, (size_t)G * 2 * P->s2_rows * P->nq, "partial sums"));
   TB_TRY(dalloc(&P->d_p0count, (size_t)G * MAXCLS, "P0 counters"));
   TB_TRY(dalloc(&P->d_result, (size_t)G * P->nq, "result"));
   P->fwd_valid = false;
@@ -456,6 +459,11 @@ int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
   for (int i = 0; i < 10; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
   P->have_ev = true;  // the ring's stage events are made as executions reach their slots
+  // the side stream of the small stage-2 classes and its fork / join events
+  // (made here: executions may be captured into a graph)
+  TB_TRYC(cudaStreamCreateWithFlags(&P->st2, cudaStreamNonBlocking));
+  TB_TRYC(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+  TB_TRYC(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
   tr.mark("stream, events");
   TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
@@ -696,7 +704,23 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
                                           P->d_perm, (int)nall, 0, 11, P->st));
     P->launches += 1;
   }
-  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq * ngeom, P->st));
+  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)2 * P->s2_rows * P->nq * ngeom, P->st));
+  // classes with fewer warp batches than one wave of resident warps run on
+  // the side stream, overlapping the large classes instead of leaving most of
+  // the GPU idle; they add into the second block of partial rows
+  const int64_t prow = (int64_t)P->s2_rows * P->nq;
+  auto small_class = [&](int c) {
+    const int LB = cL[c] + (kind_j2(P->kind) ? 2 : 0);
+    const int64_t per_warp = stage2_quartets_per_warp(LB, P->s2_tile);
+    const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
+    return (ce[c] - cb[c] + per_warp - 1) / per_warp * ngeom < (int64_t)P->nsm * bps * P->s2_tile.nw;
+  };
+  bool fork = false;
+  for (int c = 0; c < ncls; ++c) fork = fork || (ce[c] > cb[c] && small_class(c));
+  if (fork) {
+    TB_CK(cudaEventRecord(P->ev_fork, P->st));
+    TB_CK(cudaStreamWaitEvent(P->st2, P->ev_fork, 0));
+  }
   for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
     const int tn = std::min(P->s2_qtile, P->nq - q0);
     int uniform = 0, first_on_grid = 0;
@@ -710,7 +734,7 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       s.nquart = ce[c] - cb[c];
       s.perm = order ? P->d_perm : nullptr;
       s.gs_rec = gs_rec(P);
-      s.gs_partial = (int64_t)P->s2_rows * P->nq;
+      s.gs_partial = 2 * prow;
       s.pbase = cb[c];
       s.q = P->d_q + q0;
       s.nq = tn;
@@ -719,7 +743,8 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       s.dq = dq;
       s.j2 = kind_j2(P->kind);
       s.lb = LB;
-      s.partial = P->d_partial + q0;
+      const bool side = fork && small_class(c);
+      s.partial = P->d_partial + (side ? prow : 0) + q0;
       s.pstride = P->nq;
       // a class too small to fill the GPU several times over is also split
       // over q, in chunks of 64 points (the reseed interval)
@@ -735,12 +760,16 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       const int64_t items = nbatch / ngeom * nch;
       const int64_t nblk = (items + NW - 1) / NW;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
-      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->s2_tile, P->st));
+      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->s2_tile, side ? P->st2 : P->st));
       P->launches += 1;
     }
   }
+  if (fork) {
+    TB_CK(cudaEventRecord(P->ev_join, P->st2));
+    TB_CK(cudaStreamWaitEvent(P->st, P->ev_join, 0));
+  }
   TB_CK(mark(3));
-  TB_CK(launch_reduce_batch(P->d_partial, P->s2_rows, P->nq, (int64_t)P->s2_rows * P->nq, d_out, ngeom, P->st));
+  TB_CK(launch_reduce_batch(P->d_partial, 2 * P->s2_rows, P->nq, 2 * prow, d_out, ngeom, P->st));
   P->launches += 1;
   TB_CK(mark(4));
   return THISTLE_OK;
@@ -1030,7 +1059,7 @@ static int stage2_relayout(thistle_plan *P) {
   stage2_layout(P);
   dfree(P->d_partial);
   P->d_partial = nullptr;
-  return dalloc(&P->d_partial, (size_t)P->ngeom * P->s2_rows * P->nq, "partial sums");
+  return dalloc(&P->d_partial, (size_t)P->ngeom * 2 * P->s2_rows * P->nq, "partial sums");
 }
 
 static int set_qtile(thistle_plan *P, int qt) {

@@ -135,6 +135,12 @@ struct thistle_plan {
   Stage2Tile s2_tile;                // stage-2 pair tile (quartets per lane, warps per block)
   cudaStream_t st = nullptr;
   bool own_stream = true;
+  // stage-2 classes too small to fill the GPU run on st2, forked from st
+  // after stage 1 and joined before the reduction, into partial rows
+  // s2_rows .. 2 s2_rows - 1 of each geometry (the others use rows 0 ..
+  // s2_rows - 1)
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev[10];
   // per-execution stage events: slot = execution index mod NRING
   static const int NRING = 64;
