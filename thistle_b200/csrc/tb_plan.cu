@@ -604,6 +604,10 @@ Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t q
   return a;
 }
 
+#ifndef TB_S2_SIDE_WAVES
+#define TB_S2_SIDE_WAVES 8
+#endif
+
 int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
                       const int *cL, int ncls, double *d_rec, const int64_t *recoff, const int *rs,
                       const std::vector<SubRange> *subs, double *d_out, bool order, int ngeom,
@@ -705,15 +709,16 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
     P->launches += 1;
   }
   TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)2 * P->s2_rows * P->nq * ngeom, P->st));
-  // classes with fewer warp batches than one wave of resident warps run on
-  // the side stream, overlapping the large classes instead of leaving most of
-  // the GPU idle; they add into the second block of partial rows
+  // classes with fewer warp batches than TB_S2_SIDE_WAVES waves of resident
+  // warps run on the side stream, overlapping the large classes instead of
+  // leaving most of the GPU idle; they add into the second block of partial
+  // rows
   const int64_t prow = (int64_t)P->s2_rows * P->nq;
   auto small_class = [&](int c) {
     const int LB = cL[c] + (kind_j2(P->kind) ? 2 : 0);
     const int64_t per_warp = stage2_quartets_per_warp(LB, P->s2_tile);
     const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
-    return (ce[c] - cb[c] + per_warp - 1) / per_warp * ngeom < (int64_t)P->nsm * bps * P->s2_tile.nw;
+    return (ce[c] - cb[c] + per_warp - 1) / per_warp * ngeom < (int64_t)TB_S2_SIDE_WAVES * P->nsm * bps * P->s2_tile.nw;
   };
   bool fork = false;
   for (int c = 0; c < ncls; ++c) fork = fork || (ce[c] > cb[c] && small_class(c));
