@@ -188,6 +188,11 @@ int thistle_plan_use_graph(thistle_plan *plan, int32_t enable);
 int thistle_plan_autotune_batch(thistle_plan *plan, int32_t gmax, int32_t *ngeom_best, int32_t *qtile_best,
                                 double *geoms_per_s);
 int thistle_plan_set_stage2_tile(thistle_plan *plan, int32_t quartets_per_lane, int32_t warps_per_block);
+/* Stage overlap (default on): each LLmax class's stage-2 visiting order is
+ * sorted right after its stage 1, and its stage 2 starts on the plan's
+ * internal streams while the later classes' stage 1 runs.  Off: stage 2
+ * starts after the whole of stage 1.  The result is the same either way. */
+int thistle_plan_set_pipeline(thistle_plan *plan, int32_t enable);
 int thistle_plan_stage2_tile(const thistle_plan *plan, int32_t *quartets_per_lane, int32_t *warps_per_block);
 /*
  * Nuclear-electron term of an elastic plan (type 2) for its current centres:

@@ -95,3 +95,17 @@ def test_stage2_pair_tiles_agree(kind):
             pl.set_stage2_tile(3, 4)
         with pytest.raises(MC.ThistleError):
             pl.set_stage2_tile(2, 6)
+
+
+@pytest.mark.parametrize("kind", [MC.TOTAL_J0, MC.ELASTIC_J0, MC.TOTAL_J2])
+def test_stage_overlap_is_exact(kind):
+    """Stage 2 of a class overlapping the later classes' stage 1 (per-class
+    visiting-order sorts) gives bit for bit the result of the serial order."""
+    p = I.config3_ab6(nq=200, natoms=3)
+    with MC.ScatteringPlan.from_problem(p, kind) as pl:
+        on = pl.execute()
+        pl.set_pipeline(False)
+        off = pl.execute()
+        pl.set_pipeline(True)
+        again = pl.execute()
+    assert np.array_equal(on, off) and np.array_equal(on, again)

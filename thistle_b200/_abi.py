@@ -35,6 +35,7 @@ EXPORTS = sorted([
     "thistle_plan_density", "thistle_plan_form_factor", "thistle_elastic_aligned_grid",
     "thistle_plan_set_centres_batch_device", "thistle_plan_set_stage2_tile", "thistle_plan_stage2_tile",
     "thistle_batch_set_stage2_tile", "thistle_batch_stage2_tile", "thistle_batch_autotune",
+    "thistle_plan_set_pipeline",
 ])
 
 
@@ -114,6 +115,7 @@ def lib():
                        ("thistle_batch_execute_device", [VP, VP]), ("thistle_batch_info", [VP, I64]),
                        ("thistle_batch_destroy", [VP]), ("thistle_plan_nuclear", [VP, D, D, C.c_int32, D]),
                        ("thistle_plan_set_stage2_tile", [VP, C.c_int32, C.c_int32]),
+                       ("thistle_plan_set_pipeline", [VP, C.c_int32]),
                        ("thistle_plan_stage2_tile", [VP, I32, I32]),
                        ("thistle_batch_set_stage2_tile", [VP, C.c_int32, C.c_int32]),
                        ("thistle_batch_stage2_tile", [VP, I32, I32]),

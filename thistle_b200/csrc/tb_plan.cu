@@ -286,11 +286,14 @@ void plan_free(thistle_plan *P) {
   if (P->have_ev) {
     for (int i = 0; i < 10; ++i) cudaEventDestroy(P->ev[i]);
     for (int r = 0; r < P->rev_made; ++r)
-      for (int i = 0; i < 5; ++i) cudaEventDestroy(P->rev[r][i]);
+      for (int i = 0; i < 6; ++i) cudaEventDestroy(P->rev[r][i]);
   }
-  if (P->ev_fork) cudaEventDestroy(P->ev_fork);
   if (P->ev_join) cudaEventDestroy(P->ev_join);
+  if (P->ev_join3) cudaEventDestroy(P->ev_join3);
+  for (int c = 0; c < MAXCLS; ++c)
+    if (P->ev_cls[c]) cudaEventDestroy(P->ev_cls[c]);
   if (P->st2) cudaStreamDestroy(P->st2);
+  if (P->st3) cudaStreamDestroy(P->st3);
   if (P->st && P->own_stream) cudaStreamDestroy(P->st);
   delete P;
 }
@@ -459,11 +462,13 @@ int plan_create(thistle_plan **out, int32_t type, int32_t ngto, const double *ga
   TB_TRYC(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
   for (int i = 0; i < 10; ++i) TB_TRYC(cudaEventCreate(&P->ev[i]));
   P->have_ev = true;  // the ring's stage events are made as executions reach their slots
-  // the side stream of the small stage-2 classes and its fork / join events
-  // (made here: executions may be captured into a graph)
+  // the stage-2 streams and their events (made here: executions may be
+  // captured into a graph)
   TB_TRYC(cudaStreamCreateWithFlags(&P->st2, cudaStreamNonBlocking));
-  TB_TRYC(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
   TB_TRYC(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
+  TB_TRYC(cudaStreamCreateWithFlags(&P->st3, cudaStreamNonBlocking));
+  TB_TRYC(cudaEventCreateWithFlags(&P->ev_join3, cudaEventDisableTiming));
+  for (int c = 0; c < MAXCLS; ++c) TB_TRYC(cudaEventCreateWithFlags(&P->ev_cls[c], cudaEventDisableTiming));
   tr.mark("stream, events");
   TB_TRY(dalloc(&P->d_gstart, (size_t)P->ng, "groups"));
   TB_TRY(dalloc(&P->d_gcount, (size_t)P->ng, "groups"));
@@ -616,7 +621,7 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
   // are made the first time an execution reaches it
   const int slot = (int)(P->ring_next % thistle_plan::NRING);
   if (!P->capturing && slot >= P->rev_made) {
-    for (int i = 0; i < 5; ++i) TB_CK(cudaEventCreate(&P->rev[slot][i]));
+    for (int i = 0; i < 6; ++i) TB_CK(cudaEventCreate(&P->rev[slot][i]));
     P->rev_made = slot + 1;
   }
   cudaEvent_t *E = P->rev[slot];
@@ -627,6 +632,24 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
                            ngeom, 3 * (int64_t)P->ngto, gs_pair(P), gs_esoa(P), P->st));
   P->launches += 1;
   TB_CK(cudaMemsetAsync(P->d_p0count, 0, sizeof(int64_t) * MAXCLS * ngeom, P->st));
+  const bool aligned = P->kind == KIND_ALIGNED;
+  if (!aligned)
+    TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)2 * P->s2_rows * P->nq * ngeom, P->st));
+  // Pipelined stages: each class's visiting order is sorted right after its
+  // stage 1 (its keys, bits 0-5: the H bucket; the stable radix sort gives the
+  // order the sort over all quartets by (class, bucket) gives), so its stage 2
+  // may start while the later classes' stage 1 runs.  Needs each class's sort
+  // to fit the scratch sized for the whole sort.
+  bool pipe = P->pipeline && order && !aligned;
+  for (int c = 0; c < ncls && pipe; ++c) {
+    size_t need = 0;
+    if (ce[c] > cb[c])
+      TB_CK(cub::DeviceRadixSort::SortPairs(nullptr, need, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)(ce[c] - cb[c]), 0,
+                                            6, P->st));
+    pipe = need <= P->s2sort_bytes;
+  }
+  bool m5 = false;  // E5: the first class's stage 2 may start
   TB_CK(mark(1));
   for (int c = 0; c < ncls; ++c) {
     Stage1Args a = stage1_args(P, d_quart, cb[c], ce[c], d_rec, recoff[c], rs[c]);
@@ -678,8 +701,19 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       TB_CK(launch_stage1(P->kind, cL[c], a, ngeom, P->st));
       P->launches += 1;
     }
+    if (pipe && ce[c] > cb[c]) {
+      size_t bytes = P->s2sort_bytes;
+      TB_CK(cub::DeviceRadixSort::SortPairs(P->d_s2sort_tmp, bytes, P->d_s2key + cb[c], P->d_s2key_sorted + cb[c],
+                                            P->d_iota + cb[c], P->d_perm + cb[c], (int)(ce[c] - cb[c]), 0, 6,
+                                            P->st));
+      P->launches += 1;
+      TB_CK(cudaEventRecord(P->ev_cls[c], P->st));
+      if (!m5) TB_CK(mark(5));
+      m5 = true;
+    }
   }
   TB_CK(mark(2));
+  if (aligned) TB_CK(mark(5));
   int64_t nall = ncls > 0 ? ce[ncls - 1] : 0;
   if (P->kind == KIND_ALIGNED) {
     TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)P->s2_rows * P->nq, P->st));
@@ -702,17 +736,21 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
     TB_CK(mark(4));
     return THISTLE_OK;
   }
-  if (order && nall > 0) {
-    size_t bytes = P->s2sort_bytes;
-    TB_CK(cub::DeviceRadixSort::SortPairs(P->d_s2sort_tmp, bytes, P->d_s2key, P->d_s2key_sorted, P->d_iota,
-                                          P->d_perm, (int)nall, 0, 11, P->st));
-    P->launches += 1;
+  if (!pipe) {
+    if (order && nall > 0) {
+      size_t bytes = P->s2sort_bytes;
+      TB_CK(cub::DeviceRadixSort::SortPairs(P->d_s2sort_tmp, bytes, P->d_s2key, P->d_s2key_sorted, P->d_iota,
+                                            P->d_perm, (int)nall, 0, 11, P->st));
+      P->launches += 1;
+    }
+    // every class's stage 2 waits for the whole of stage 1 (and the sort)
+    for (int c = 0; c < ncls; ++c) TB_CK(cudaEventRecord(P->ev_cls[c], P->st));
   }
-  TB_CK(cudaMemsetAsync(P->d_partial, 0, sizeof(double) * (size_t)2 * P->s2_rows * P->nq * ngeom, P->st));
+  if (!m5) TB_CK(mark(5));
   // classes with fewer warp batches than TB_S2_SIDE_WAVES waves of resident
-  // warps run on the side stream, overlapping the large classes instead of
-  // leaving most of the GPU idle; they add into the second block of partial
-  // rows
+  // warps run on the side stream st2, the others on st3, so the small classes
+  // overlap the large ones instead of leaving most of the GPU idle; the
+  // side-stream classes add into the second block of partial rows
   const int64_t prow = (int64_t)P->s2_rows * P->nq;
   auto small_class = [&](int c) {
     const int LB = cL[c] + (kind_j2(P->kind) ? 2 : 0);
@@ -720,18 +758,14 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
     const int bps = P->s2_bps[LB] > 0 ? P->s2_bps[LB] : 1;
     return (ce[c] - cb[c] + per_warp - 1) / per_warp * ngeom < (int64_t)TB_S2_SIDE_WAVES * P->nsm * bps * P->s2_tile.nw;
   };
-  bool fork = false;
-  for (int c = 0; c < ncls; ++c) fork = fork || (ce[c] > cb[c] && small_class(c));
-  if (fork) {
-    TB_CK(cudaEventRecord(P->ev_fork, P->st));
-    TB_CK(cudaStreamWaitEvent(P->st2, P->ev_fork, 0));
-  }
+  bool used2 = false, used3 = false;
   for (int q0 = 0; q0 < P->nq; q0 += P->s2_qtile) {
     const int tn = std::min(P->s2_qtile, P->nq - q0);
     int uniform = 0, first_on_grid = 0;
     double dq = 0.0;
     grid_info(P->hq.data() + q0, tn, uniform, first_on_grid, dq);
     for (int c = 0; c < ncls; ++c) {
+      if (ce[c] <= cb[c]) continue;
       const int LB = cL[c] + (kind_j2(P->kind) ? 2 : 0);
       Stage2ClassArgs s;
       s.rec = d_rec + recoff[c];
@@ -748,7 +782,7 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       s.dq = dq;
       s.j2 = kind_j2(P->kind);
       s.lb = LB;
-      const bool side = fork && small_class(c);
+      const bool side = small_class(c);
       s.partial = P->d_partial + (side ? prow : 0) + q0;
       s.pstride = P->nq;
       // a class too small to fill the GPU several times over is also split
@@ -765,13 +799,21 @@ int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, cons
       const int64_t items = nbatch / ngeom * nch;
       const int64_t nblk = (items + NW - 1) / NW;
       const int grid = (int)std::min<int64_t>(nblk, std::min(P->s2_rows, P->nsm * bps));
-      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->s2_tile, side ? P->st2 : P->st));
+      if (grid <= 0) continue;
+      cudaStream_t sc = side ? P->st2 : P->st3;
+      TB_CK(cudaStreamWaitEvent(sc, P->ev_cls[c], 0));
+      (side ? used2 : used3) = true;
+      TB_CK(launch_stage2_class(LB, s, grid, ngeom, P->s2_tile, sc));
       P->launches += 1;
     }
   }
-  if (fork) {
+  if (used2) {
     TB_CK(cudaEventRecord(P->ev_join, P->st2));
     TB_CK(cudaStreamWaitEvent(P->st, P->ev_join, 0));
+  }
+  if (used3) {
+    TB_CK(cudaEventRecord(P->ev_join3, P->st3));
+    TB_CK(cudaStreamWaitEvent(P->st, P->ev_join3, 0));
   }
   TB_CK(mark(3));
   TB_CK(launch_reduce_batch(P->d_partial, 2 * P->s2_rows, P->nq, 2 * prow, d_out, ngeom, P->st));
@@ -787,12 +829,17 @@ int plan_exec(thistle_plan *P, double *d_out) {
   return rc;
 }
 
+// Stage intervals of one execution's ring events: pair tables E0-E1, stage 1
+// E1-E2, stage 2 E5-E3 (from the moment the first class's stage 2 may start:
+// it overlaps the later classes' stage 1), reduction E3-E4.
+static const int kStageFrom[4] = {0, 1, 5, 3}, kStageTo[4] = {1, 2, 3, 4};
+
 void read_timings(thistle_plan *P) {
   if (P->ring_next == 0) return;
   cudaEvent_t *E = P->rev[(P->ring_next - 1) % thistle_plan::NRING];
   for (int i = 0; i < 4; ++i) {
     float t = 0;
-    if (cudaEventElapsedTime(&t, E[i], E[i + 1]) == cudaSuccess) P->ms[i] = t;
+    if (cudaEventElapsedTime(&t, E[kStageFrom[i]], E[kStageTo[i]]) == cudaSuccess) P->ms[i] = t;
   }
 }
 
@@ -1177,6 +1224,14 @@ int thistle_plan_stage2_tile(const thistle_plan *P, int32_t *quartets_per_lane, 
   return THISTLE_OK;
 }
 
+int thistle_plan_set_pipeline(thistle_plan *P, int32_t enable) {
+  if (!P) return fail(THISTLE_ERR_ARG, "null plan");
+  TB_CK(cudaStreamSynchronize(P->st));
+  drop_graphs(P);
+  P->pipeline = enable != 0;
+  return THISTLE_OK;
+}
+
 int thistle_plan_use_graph(thistle_plan *P, int32_t enable) {
   if (!P) return fail(THISTLE_ERR_ARG, "null plan");
   TB_CK(cudaStreamSynchronize(P->st));
@@ -1397,7 +1452,7 @@ int thistle_plan_stage_totals(thistle_plan *P, double *ms4, int64_t *nexec) {
     cudaEvent_t *E = P->rev[k % thistle_plan::NRING];
     for (int i = 0; i < 4; ++i) {
       float t = 0;
-      TB_CK(cudaEventElapsedTime(&t, E[i], E[i + 1]));
+      TB_CK(cudaEventElapsedTime(&t, E[kStageFrom[i]], E[kStageTo[i]]));
       ms4[i] += t;
     }
   }

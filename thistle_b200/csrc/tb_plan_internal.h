@@ -135,16 +135,21 @@ struct thistle_plan {
   Stage2Tile s2_tile;                // stage-2 pair tile (quartets per lane, warps per block)
   cudaStream_t st = nullptr;
   bool own_stream = true;
-  // stage-2 classes too small to fill the GPU run on st2, forked from st
-  // after stage 1 and joined before the reduction, into partial rows
-  // s2_rows .. 2 s2_rows - 1 of each geometry (the others use rows 0 ..
-  // s2_rows - 1)
+  // stage-2 classes too small to fill the GPU run on st2, joined into st
+  // before the reduction, into partial rows s2_rows .. 2 s2_rows - 1 of each
+  // geometry (the others use rows 0 .. s2_rows - 1)
   cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_join = nullptr;
+  // the other stage-2 classes run on st3; class c's stage 2 waits for
+  // ev_cls[c], recorded on st once its stage 1 and its visiting-order sort
+  // are done, so stage 2 of the first classes overlaps stage 1 of the later
+  cudaStream_t st3 = nullptr;
+  cudaEvent_t ev_join3 = nullptr;
+  cudaEvent_t ev_cls[MAXCLS] = {};
   cudaEvent_t ev[10];
   // per-execution stage events: slot = execution index mod NRING
   static const int NRING = 64;
-  cudaEvent_t rev[64][5];
+  cudaEvent_t rev[64][6];
   int rev_made = 0;  // slots 0 .. rev_made-1 hold events (made as executions first reach them)
   int64_t ring_next = 0, ring_base = 0;
   bool have_ev = false;
@@ -154,6 +159,7 @@ struct thistle_plan {
   int ngeom = 1;
   bool capturing = false;            // inside a CUDA-graph capture (no event records)
   bool use_graph = false;
+  bool pipeline = true;  // stage 2 of a class may start before the later classes' stage 1
   cudaGraphExec_t gx_fwd = nullptr, gx_vjp = nullptr;
   std::vector<double> hxyz;          // host copy of the centres (interleaved, ngeom x ngto x 3)
   bool fwd_valid = false;            // records and visiting order match the current centres

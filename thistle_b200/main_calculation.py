@@ -300,6 +300,11 @@ class ScatteringPlan:
         """Stage-2 pair tile: quartets per lane (1, 2) and warps per block (4, 8)."""
         check(_abi.lib().thistle_plan_set_stage2_tile(self._p, int(quartets_per_lane), int(warps_per_block)))
 
+    def set_pipeline(self, enable: bool = True):
+        """Overlap each class's stage 2 with the later classes' stage 1 (the
+        default); the result is the same either way."""
+        check(_abi.lib().thistle_plan_set_pipeline(self._p, int(bool(enable))))
+
     def stage2_tile(self):
         k, nw = C.c_int32(0), C.c_int32(0)
         check(_abi.lib().thistle_plan_stage2_tile(self._p, C.byref(k), C.byref(nw)))
