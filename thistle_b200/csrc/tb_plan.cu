@@ -610,7 +610,7 @@ Stage1Args stage1_args(const thistle_plan *P, const uint64_t *d_quart, int64_t q
 }
 
 #ifndef TB_S2_SIDE_WAVES
-#define TB_S2_SIDE_WAVES 8
+#define TB_S2_SIDE_WAVES 16
 #endif
 
 int run_stages(thistle_plan *P, const uint64_t *d_quart, const int64_t *cb, const int64_t *ce,
